@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark: Kohn-Sham H|psi> state-applications per second on a B200.
+
+Workload (one "step" = one H application to every orbital of the set):
+  C2 -- cubic a = 20.52 bohr, 96^3 grid, 256 orbitals, 64 atoms (2x2x2 diamond
+  supercell, jittered), Gaussian V_loc, l = 0,1 KB projectors (sphere 2 bohr),
+  seeded synthetic orbitals orthonormalised in FP64.  Every orbital set is
+  1.8 GB (FP32) / 3.6 GB (FP64), far larger than the 126 MB L2, so no flush is
+  needed between steps.
+
+The headline ``value`` is the mixed form (FP32 FFTs / potential / projector
+contraction, FP64 reductions); the plain FP64 form is timed beside it under
+``fp64`` with the mixed form's error against it.  ``e2e`` is the same metric
+through the C ABI with host buffers: every step copies the orbitals in from
+pinned host memory and H|psi> back out.
+
+``--impl reference`` times the reference algorithm's CPU restatement (the FP64
+oracle: pocketFFT over all host threads + numpy/OpenBLAS) on a bounded sample
+of the same workload.
+
+Multi-GPU (torchrun): every rank applies H to its own full orbital set (the
+operator has no exchange between states), timing is the max over ranks and
+``value`` the total over ranks (weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "H·psi applications/s (96^3, 256 states) mixed vs FP64; serving p50/p99 latency"
+UNIT = "state-applications/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(kernel_key):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/ncu_traffic.txt: 'key bytes' lines)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel_key:
+                    return float(parts[1])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU restatement timing
+
+
+def cpu_sample(sysm, nsample, min_seconds=10.0, max_steps=50):
+    """Time the FP64 oracle (reference algorithm restated on the CPU) on nsample states of the workload."""
+    import numpy as np
+    import oracle as O
+    O.set_fft_workers(os.cpu_count() or 1)
+    cell = O.Cell(sysm.lattice)
+    rs = O.RealSpace(cell, sysm.sizes)
+    pa = O.ProjectorAll.pack([O.build_projector(rs, R, sysm.radius, sysm.rc, sysm.kb[a])
+                              for a, R in enumerate(sysm.positions)])
+    oh = O.Hamiltonian(rs, sysm.local_potential(), pa)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(sysm.sizes + (nsample,)) + 1j * rng.standard_normal(sysm.sizes + (nsample,))
+    oh.apply_real(x)  # warm
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        oh.apply_real(x)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or steps >= max_steps:
+            break
+    return nsample * steps / el, el, steps
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from inq_b200 import synthetic
+    sysm = synthetic.config("c2")
+    import numpy as np
+    import oracle as O
+    nsample = 8
+    O.set_fft_workers(os.cpu_count() or 1)
+    cell = O.Cell(sysm.lattice)
+    rs = O.RealSpace(cell, sysm.sizes)
+    pa = O.ProjectorAll.pack([O.build_projector(rs, R, sysm.radius, sysm.rc, sysm.kb[a])
+                              for a, R in enumerate(sysm.positions)])
+    oh = O.Hamiltonian(rs, sysm.local_potential(), pa)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(sysm.sizes + (nsample,)) + 1j * rng.standard_normal(sysm.sizes + (nsample,))
+    for _ in range(args.warmup):
+        oh.apply_real(x)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oh.apply_real(x)
+    el = time.perf_counter() - t0
+    v = nsample * args.steps / el
+    cores = os.cpu_count() or 1
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "c2: H|psi> on 96^3, 64 atoms; sample of 8 of the 256 orbitals per step",
+                       "grid": 96, "states_per_step": nsample, "atoms": 64},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{nsample} orbitals of the 96^3 / 64-atom workload per step, FP64"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    import inq_b200 as ib
+    from inq_b200 import synthetic
+
+    ctx = ib.Context(local)
+    sysm = synthetic.config("c2", seed=20240601 + rank)
+    basis, ham, phi64 = synthetic.build(sysm, ctx=ctx)
+    phi32 = phi64.converted(ib.F32)
+    out64 = phi64.skeleton()
+    out32 = phi32.skeleton()
+    S, N = sysm.nst, sysm.npoints
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+
+    def barrier():
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def time_loop(fn, steps):
+        barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        barrier()
+        return ms
+
+    # warm up both forms
+    for _ in range(args.warmup):
+        ham.apply(phi32, out32)
+        ham.apply(phi64, out64)
+    ctx.synchronize()
+
+    # timed: mixed form (headline) with clock sampling, then FP64
+    launches0 = ctx.launch_count()
+    with ClockSampler(local) as clk:
+        ms32 = time_loop(lambda: ham.apply(phi32, out32), args.steps)
+    launches = ctx.launch_count() - launches0
+    ms64 = time_loop(lambda: ham.apply(phi64, out64), args.steps)
+
+    v32 = world * S * args.steps / (ms32 / 1000.0)
+    v64 = world * S * args.steps / (ms64 / 1000.0)
+
+    # accuracy of the mixed form against the FP64 form on the full workload
+    ham.apply(phi64, out64)
+    ham.apply(phi32, out32)
+    ctx.synchronize()
+    h64 = torch.from_numpy(out64.matrix())
+    h32 = torch.from_numpy(out32.matrix()).to(torch.complex128)
+    rel_err = float(torch.linalg.vector_norm(h32 - h64) / torch.linalg.vector_norm(h64))
+    del h64, h32
+    e64, _ = ham.eigenvalues(phi64)
+    e32, _ = ham.eigenvalues(phi32)
+    eig_err = float(np.max(np.abs(e32 - e64)))
+
+    # dominant kernel: the batched FFT pass (3 launches in to_fourier, each reads and writes the set once)
+    f32 = phi32.skeleton(ib.FOURIER_SPACE)
+    reps = max(3, args.steps)
+    for _ in range(2):
+        ctx.check(ctx.lib.inqb_to_fourier(phi32.handle, f32.handle))
+    ms_fft = time_loop(lambda: ctx.check(ctx.lib.inqb_to_fourier(phi32.handle, f32.handle)), reps)
+    per_launch_s = ms_fft / 1000.0 / (3 * reps)
+    alg_bytes = 2.0 * N * S * 8
+    achieved = alg_bytes / per_launch_s / 1e9
+    peak, peak_kind = measured_hbm_gbs()
+    traffic = profile_traffic("fft_pass_kernel_f32_c2")
+    # whole-operator algorithmic bytes s_c (5N + 3P) per state
+    _, _, P = ham.projectors_info()
+    b_alg = 8.0 * (5 * N + 3 * P) * S
+    h_achieved = b_alg / (ms32 / 1000.0 / args.steps) / 1e9
+
+    # e2e through the C ABI with pinned host buffers (mixed form)
+    host_in = torch.empty((N, S), dtype=torch.complex64, pin_memory=True)
+    host_in.copy_(torch.from_numpy(phi32.matrix()))
+    host_out = torch.empty((N, S), dtype=torch.complex64, pin_memory=True)
+    e2e_in = phi32.skeleton()
+    lib = ctx.lib
+
+    def e2e_step():
+        ctx.check(lib.inqb_orbitals_upload(e2e_in.handle, host_in.data_ptr()))
+        ctx.check(lib.inqb_apply(ham.handle, e2e_in.handle, out32.handle))
+        ctx.check(lib.inqb_orbitals_download(out32.handle, host_out.data_ptr()))
+
+    e2e_step()
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_v = world * S * e2e_steps / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nsample = 8
+        v, el, st = cpu_sample(sysm, nsample)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"FP64 oracle on {nsample} of the 256 orbitals of the same workload, {st} applications "
+                         f"in {el:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded C2 construction)",
+            "config": {"workload": "c2: H|psi> 96^3 grid, 256 states, 64 atoms, mixed form (FP32, FP64 reductions)",
+                       "grid": [96, 96, 96], "states": S, "atoms": sysm.natoms, "sphere_points": P,
+                       "l2": "inputs larger than L2 (1.8 GB orbital set), no flush",
+                       "parallelism": f"each of {world} rank(s) holds its own 256-state set"},
+            "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "dtype": "f64"},
+            "mixed_over_fp64": v32 / v64,
+            "accuracy": {"rel_err_hpsi_mixed_vs_fp64": rel_err, "max_eigenvalue_err_ha": eig_err},
+            "roofline": {"bound": "hbm", "kernel": "fft_pass_kernel<float> (one 1-D FFT pass over the set)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes, "launch_ms": per_launch_s * 1000.0},
+            "operator_roofline": {"alg_bytes_per_step": b_alg, "achieved_gbs": h_achieved,
+                                  "frac": h_achieved / peak, "formula": "8 B * (5N + 3P) * S"},
+            "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": N * S * 8, "d2h_bytes_per_step": N * S * 8},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

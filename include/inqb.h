@@ -1,0 +1,190 @@
+/*
+ * inqb.h -- C ABI of libinqb200.so, the B200 (sm_100a) implementation of the
+ * Kohn-Sham Hamiltonian application H|psi> and the real-time ETRS step.
+ *
+ * Every entry point returns an int status (INQB_OK = 0); the message of the
+ * last failure on a context is returned by inqb_last_error().  No C++
+ * exception crosses this boundary.  Handles own their device memory.  A
+ * context owns one CUDA stream; calls on one context are not thread-safe,
+ * calls on distinct contexts are.
+ *
+ * Data layouts are the reference's:
+ *   orbitals  [npoint][nst] complex (state index fastest; npoint = nx*ny*nz
+ *             with z fastest), i.e. field_set::matrix() of
+ *             src/basis/field_set.hpp:41,62, hypercubic [nx][ny][nz][nst];
+ *   potential [npoint][nspin] float64 (scalar_potential(), field_set of
+ *             src/hamiltonian/ks_hamiltonian.hpp:45);
+ *   vectors   covariant components for k-points and the vector potential,
+ *             lattice vectors as rows in cartesian bohr.
+ * Complex numbers are interleaved (re, im) pairs of the orbital precision:
+ * float64 pairs for INQB_F64, float32 pairs for INQB_F32.
+ */
+#ifndef INQB_H
+#define INQB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { INQB_OK = 0, INQB_ERR_ARG = 1, INQB_ERR_CUDA = 2, INQB_ERR_STATE = 3, INQB_ERR_MEMORY = 4,
+       INQB_ERR_UNSUPPORTED = 5, INQB_ERR_NUMERIC = 6, INQB_ERR_TIMEOUT = 7 };
+
+enum { INQB_REAL_SPACE = 0, INQB_FOURIER_SPACE = 1 };   /* orbital_set<real_space|fourier_space> */
+enum { INQB_F64 = 0, INQB_F32 = 1 };                    /* plain FP64 form, mixed (FP32) form */
+
+typedef struct inqb_ctx inqb_ctx;
+typedef struct inqb_basis inqb_basis;
+typedef struct inqb_orbitals inqb_orbitals;
+typedef struct inqb_hamiltonian inqb_hamiltonian;
+
+/* ---- context ------------------------------------------------------------- */
+/* Replaces the process-wide runtime of the reference (input/environment.hpp:27-92,
+ * gpurun host.hpp:40-145): one device, one stream, explicit device memory. */
+int inqb_ctx_create(int device, inqb_ctx **out);
+int inqb_ctx_destroy(inqb_ctx *ctx);
+const char *inqb_last_error(const inqb_ctx *ctx);
+int inqb_ctx_synchronize(inqb_ctx *ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own work. */
+int inqb_ctx_stream(inqb_ctx *ctx, void **stream);
+/* Number of kernels this library launched on the context so far. */
+int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
+/* Free and total device memory in bytes (admission control for serving). */
+int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
+
+/* ---- basis ---------------------------------------------------------------- */
+/* basis::real_space(cell, sizes) (src/basis/real_space.hpp:40-49) with its
+ * reciprocal basis::fourier_space (src/basis/fourier_space.hpp:33-38, serial order). */
+int inqb_basis_create(inqb_ctx *ctx, const double lattice[9], int nx, int ny, int nz, inqb_basis **out);
+int inqb_basis_destroy(inqb_basis *basis);
+/* real_space::volume_element (real_space.hpp:216-218). */
+int inqb_basis_volume_element(const inqb_basis *basis, double *dv);
+
+/* ---- orbital sets --------------------------------------------------------- */
+/* states::orbital_set(basis, nst, spinor_dim, kpoint, spin_index, comm)
+ * (src/states/orbital_set.hpp:40-48); spinor_dim must be 1. */
+int inqb_orbitals_create(inqb_ctx *ctx, const inqb_basis *basis, int nst, int spinor_dim,
+                         const double kpoint_cov[3], int spin_index, int space, int precision,
+                         inqb_orbitals **out);
+int inqb_orbitals_destroy(inqb_orbitals *orb);
+/* Host <-> device copies of the whole set, layout [npoint][nst] in the set's precision. */
+int inqb_orbitals_upload(inqb_orbitals *orb, const void *host);
+int inqb_orbitals_download(const inqb_orbitals *orb, void *host);
+/* Device pointer of the set's storage (npoint*nst complex of the set's precision). */
+int inqb_orbitals_device_ptr(const inqb_orbitals *orb, void **ptr);
+/* Device-to-device copy src -> dst (same shape and precision); field_set copy-assign. */
+int inqb_orbitals_copy(const inqb_orbitals *src, inqb_orbitals *dst);
+/* Fill every coefficient with (re, im) (field_set::fill, src/basis/field_set.hpp). */
+int inqb_orbitals_fill(inqb_orbitals *orb, double re, double im);
+/* Re-tag the basis space of a set without touching its data. */
+int inqb_orbitals_set_space(inqb_orbitals *orb, int space);
+int inqb_orbitals_info(const inqb_orbitals *orb, int *nst, int *space, int *precision, long long *npoint);
+/* Seeded synthetic orbitals (the generator of the benchmark configurations; the
+ * reference's operations::randomize, src/operations/randomize.hpp:66, uses PCG32
+ * instead): Fourier coefficients N(0,1) + i N(0,1) for |G|^2/2 < ecut, zero outside,
+ * from SplitMix64 counters (seed, state*npoint + point) and Box-Muller. The set is
+ * tagged Fourier-space. */
+int inqb_orbitals_randomize_gsphere(inqb_orbitals *orb, uint64_t seed, double ecut);
+/* Element-wise precision conversion src -> dst (F64 <-> F32, same shape otherwise). */
+int inqb_orbitals_convert(const inqb_orbitals *src, inqb_orbitals *dst);
+
+/* ---- transforms ----------------------------------------------------------- */
+/* operations::transform::to_fourier (src/operations/transform.hpp:186-216): unnormalised forward DFT. */
+int inqb_to_fourier(const inqb_orbitals *in, inqb_orbitals *out);
+/* operations::transform::to_real (src/operations/transform.hpp:220-249): backward DFT, times 1/N if normalize. */
+int inqb_to_real(const inqb_orbitals *in, inqb_orbitals *out, int normalize);
+/* operations::laplacian (src/operations/laplacian.hpp:59-81) on a Fourier-space set:
+ * out = factor*(-|G|^2 + gradcoeff.G) * in, gradcoeff contravariant. in may equal out. */
+int inqb_laplacian(const inqb_orbitals *in, inqb_orbitals *out, double factor, const double gradcoeff_contra[3]);
+
+/* ---- Hamiltonian ---------------------------------------------------------- */
+/* hamiltonian::ks_hamiltonian<PotentialType>(basis, ...) (ks_hamiltonian.hpp:92-102):
+ * scalar potential zero, no projectors, exchange disabled. */
+int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, inqb_hamiltonian **out);
+int inqb_hamiltonian_destroy(inqb_hamiltonian *ham);
+/* ks_hamiltonian::scalar_potential() assignment; V is host [npoint][nspin] float64. */
+int inqb_potential_set(inqb_hamiltonian *ham, const double *V);
+/* ks_hamiltonian::uniform_vector_potential() assignment (covariant, ks_hamiltonian.hpp:259-264). */
+int inqb_vector_potential_set(inqb_hamiltonian *ham, const double A_cov[3]);
+/* projector_all packing (projector_all.hpp:40-109): padded host tables
+ *   points   [nproj][maxsph][3] int32 grid indices (-1 for padding)
+ *   pos      [nproj][maxsph][3] float32 contravariant offsets from the atom
+ *   matrices [nproj][maxnlm][maxsph] float64 projector values
+ *   coeff    [nproj][maxnlm][maxnlm] float64 KB coefficients
+ *   npts     [nproj], nlm [nproj] (nlm <= 4). */
+int inqb_projectors_set(inqb_hamiltonian *ham, int nproj, int maxsph, int maxnlm, const int32_t *points,
+                        const float *pos, const double *matrices, const double *coeff, const int32_t *npts,
+                        const int32_t *nlm);
+/* ks_hamiltonian::update_projectors for the synthetic Gaussian projectors
+ * (projector.hpp:38-113 + spherical_grid.hpp:59-160): one projector per atom,
+ * l = 0 and l = 1 (nlm = 4), radial exp(-r^2/rc^2) on the sphere |r-R| <= radius,
+ * KB coefficients kb [natoms][4][4]. positions are cartesian [natoms][3]. */
+int inqb_projectors_build_gaussian(inqb_hamiltonian *ham, int natoms, const double *positions, double radius,
+                                   double rc, const double *kb);
+int inqb_projectors_info(const inqb_hamiltonian *ham, int *nproj, int *maxsph, long long *total_points);
+/* Host-only (no device, no context): basis::spherical_grid(basis, center, radius)
+ * (src/basis/spherical_grid.hpp:59-160).  Writes up to `capacity` points: grid indices
+ * [n][3] int32, float32 distances [n] and float32 contravariant offsets [n][3] (any
+ * output may be NULL); *npoints receives the full count.  Returns INQB_ERR_ARG with the
+ * count set when capacity is too small. */
+int inqb_spherical_grid(const double lattice[9], int nx, int ny, int nz, const double center[3], double radius,
+                        long long capacity, int32_t *points, float *distance, float *relpos, long long *npoints);
+/* Host copy of the packed projector tables (any pointer may be NULL). */
+int inqb_projectors_get(const inqb_hamiltonian *ham, int32_t *points, float *pos, double *matrices,
+                        int32_t *npts);
+
+/* ks_hamiltonian::operator() (ks_hamiltonian.hpp:137-180): out = H in.  Real- or
+ * Fourier-space form from in's space tag; out must be a distinct set of the same shape. */
+int inqb_apply(const inqb_hamiltonian *ham, const inqb_orbitals *in, inqb_orbitals *out);
+/* ks_hamiltonian::non_local (ks_hamiltonian.hpp:106-120). */
+int inqb_non_local(const inqb_hamiltonian *ham, const inqb_orbitals *in, inqb_orbitals *out);
+/* ks_hamiltonian::non_local_energy (ks_hamiltonian.hpp:124-133, projector_all.hpp:306-327);
+ * occupations host [nst]. */
+int inqb_non_local_energy(const inqb_hamiltonian *ham, const inqb_orbitals *phi, const double *occupations,
+                          double *energy);
+/* ks_hamiltonian::kinetic_expectation_value (ks_hamiltonian.hpp:184-197): host out [nst]. */
+int inqb_kinetic_expectation_value(const inqb_hamiltonian *ham, const inqb_orbitals *phi, double *out);
+
+/* ---- orbital-set linear algebra ------------------------------------------- */
+/* operations::overlap (overlap.hpp:26-95): S[i][j] = dV sum_r conj(a[r][i]) b[r][j]; host out
+ * [nst_a][nst_b] complex128. */
+int inqb_overlap(const inqb_orbitals *a, const inqb_orbitals *b, double *out);
+/* operations::overlap_diagonal (overlap_diagonal.hpp:25-55): host out [nst] complex128. */
+int inqb_overlap_diagonal(const inqb_orbitals *a, const inqb_orbitals *b, double *out);
+/* operations::orthogonalize (orthogonalize.hpp:25-31): FP64 overlap, FP64 Cholesky
+ * (matrix/cholesky.hpp:28-99), phi <- phi U^-1 (rotate.hpp:147-156). */
+int inqb_orthogonalize(inqb_orbitals *phi);
+/* operations::shift (shift.hpp:33-43): phi += (re + i im) * chi. */
+int inqb_shift(double re, double im, const inqb_orbitals *chi, inqb_orbitals *phi);
+/* operations::rotate (rotate.hpp:27-62): phi <- phi R, R host [nst][nst] complex128 row-major. */
+int inqb_rotate(inqb_orbitals *phi, const double *R);
+/* energy::calculate eigenvalue part (energy.hpp:83-89): eig[s] = Re<phi|H phi>/<phi|phi>,
+ * normres[s] = <r|r> with r = H phi - eig phi.  Host outputs [nst]. */
+int inqb_eigenvalues(const inqb_hamiltonian *ham, const inqb_orbitals *phi, double *eig, double *normres);
+
+/* ---- real time ------------------------------------------------------------ */
+/* operations::exponential_in_place (exponential.hpp:21-34): phi <- sum_n (f H)^n/n! phi, f = re + i im. */
+int inqb_exponential_in_place(const inqb_hamiltonian *ham, double re, double im, inqb_orbitals *phi, int order);
+/* operations::exponential_2_for_1 (exponential.hpp:50-69): exp1 <- exp(f1 H) phi, phi <- exp(f2 H) phi. */
+int inqb_exponential_2_for_1(const inqb_hamiltonian *ham, double f1_re, double f1_im, double f2_re,
+                             double f2_im, inqb_orbitals *phi, inqb_orbitals *exp1, int order);
+/* observables::density::calculate (density.hpp:78-101), non-spinor: out host or device
+ * [npoint] float64 = sum over sets and states of occ |phi|^2; occupations host, per set [nst]. */
+int inqb_density(inqb_orbitals *const *phis, int nsets, const double *const *occupations, double *density_host);
+/* kick::zero_step (kick.hpp:58-70): phi *= exp(i E_cov . r_contra), E cartesian. */
+int inqb_kick(inqb_orbitals *phi, const double efield_cart[3]);
+/* observables::dipole(density) (dipole.hpp:24-40) of a host density [npoint]: dV sum r n(r). */
+int inqb_dipole(const inqb_basis *basis, const double *density_host, double dipole[3]);
+/* One ETRS step (real_time/etrs.hpp:22-79) with a fixed Hamiltonian (no self-consistent
+ * potential update): all sets advanced by dt; returns the density [npoint] (host, may be
+ * NULL), the electronic dipole (may be NULL) and the number of SCF iterations taken. */
+int inqb_etrs_step(const inqb_hamiltonian *ham, inqb_orbitals *const *phis, int nsets,
+                   const double *const *occupations, double dt, int nscf_max, double scf_threshold,
+                   double *density_host, double dipole[3], int *iterations);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INQB_H */

@@ -1,0 +1,574 @@
+"""Python host interface of the B200 H|psi> path, named after the reference's C++ API.
+
+The classes mirror the reference types a caller of ``ks_hamiltonian`` handles:
+
+* :class:`Cell`          -- systems::cell (src/systems/cell.hpp:26-215)
+* :class:`RealSpace`     -- basis::real_space (src/basis/real_space.hpp:25-230)
+* :class:`FourierSpace`  -- basis::fourier_space (src/basis/fourier_space.hpp:24-140)
+* :class:`OrbitalSet`    -- states::orbital_set (src/states/orbital_set.hpp:18-192)
+* :class:`KSHamiltonian` -- hamiltonian::ks_hamiltonian (src/hamiltonian/ks_hamiltonian.hpp:35-275)
+
+and the free functions of operations::transform, operations::overlap,
+operations::orthogonalize, operations::exponential, observables::density /
+dipole, perturbations::kick and real_time::etrs.  Every call goes through the
+C ABI of libinqb200.so; arrays cross it as [npoint][nst] complex, the
+reference's field_set::matrix() layout.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import heapq
+import math
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import F32, F64, FOURIER_SPACE, REAL_SPACE, check, dptr
+
+# ---------------------------------------------------------------- context
+
+
+class Context:
+    """One device, one stream (the C ABI's inqb_ctx)."""
+
+    _default: dict = {}
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        code = self.lib.inqb_ctx_create(device, C.byref(h))
+        if code != 0:
+            msg = self.lib.inqb_last_error(None)
+            raise _lib.InqbError(code, msg.decode() if msg else "")
+        self.handle = h
+        self.device = device
+
+    @classmethod
+    def default(cls, device: int = 0) -> "Context":
+        if device not in cls._default:
+            cls._default[device] = Context(device)
+        return cls._default[device]
+
+    def check(self, code):
+        check(code, self.handle)
+
+    def synchronize(self):
+        self.check(self.lib.inqb_ctx_synchronize(self.handle))
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self.check(self.lib.inqb_ctx_stream(self.handle, C.byref(p)))
+        return p.value or 0
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        self.check(self.lib.inqb_ctx_launch_count(self.handle, C.byref(n)))
+        return n.value
+
+    def mem_info(self):
+        f, t = C.c_size_t(), C.c_size_t()
+        self.check(self.lib.inqb_ctx_mem_info(self.handle, C.byref(f), C.byref(t)))
+        return f.value, t.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.inqb_ctx_destroy(self.handle)
+            self.handle = None
+
+
+# ---------------------------------------------------------------- cell and bases
+
+
+def nextprod(factors, n):
+    """Smallest product of powers of ``factors`` that is >= n (math/nextprod.hpp)."""
+    if n <= 1:
+        return 1
+    heap = list(factors)
+    heapq.heapify(heap)
+    seen = set(heap)
+    while heap:
+        cur = heapq.heappop(heap)
+        if cur >= n:
+            return cur
+        for f in factors:
+            if cur * f not in seen:
+                seen.add(cur * f)
+                heapq.heappush(heap, cur * f)
+    raise ValueError(n)
+
+
+class Cell:
+    """Lattice vectors as rows (cartesian bohr), systems::cell."""
+
+    def __init__(self, lattice, periodicity: int = 3):
+        self.lattice = np.ascontiguousarray(np.asarray(lattice, dtype=np.float64).reshape(3, 3))
+        self.periodicity = periodicity
+        a0, a1, a2 = self.lattice
+        self.volume = float(np.dot(a0, np.cross(a1, a2)))
+        if self.volume < 1e-10:
+            raise ValueError("the lattice volume is not positive")
+        self.reciprocal = 2.0 * math.pi / self.volume * np.array([np.cross(a1, a2), np.cross(a2, a0), np.cross(a0, a1)])
+
+    @classmethod
+    def cubic(cls, a):
+        return cls(np.diag([a, a, a]))
+
+    @classmethod
+    def orthorhombic(cls, a, b, c):
+        return cls(np.diag([a, b, c]))
+
+    def lengths(self):
+        return np.sqrt(np.sum(self.lattice ** 2, axis=1))
+
+    # metric helpers (cell.hpp:146-215)
+    def cov_to_cart(self, v):
+        return (self.reciprocal / (2.0 * math.pi)).T @ np.asarray(v, dtype=np.float64)
+
+    def cart_to_cov(self, v):
+        return self.lattice @ np.asarray(v, dtype=np.float64)
+
+    def cart_to_contra(self, v):
+        return (self.reciprocal / (2.0 * math.pi)) @ np.asarray(v, dtype=np.float64)
+
+    def contra_to_cart(self, v):
+        return self.lattice.T @ np.asarray(v, dtype=np.float64)
+
+
+class RealSpace:
+    """basis::real_space on one device."""
+
+    def __init__(self, cell: Cell, spacing: float | None = None, sizes: Sequence[int] | None = None,
+                 ctx: Context | None = None):
+        self.cell = cell
+        if sizes is None:
+            if spacing is None:
+                raise ValueError("give a spacing or the grid sizes")
+            sizes = [nextprod([2, 3, 5, 7], int(math.floor(l / spacing + 0.5))) for l in cell.lengths()]
+        self.sizes = tuple(int(s) for s in sizes)
+        self.ctx = ctx or Context.default()
+        lib = self.ctx.lib
+        h = C.c_void_p()
+        self.ctx.check(lib.inqb_basis_create(self.ctx.handle, dptr(cell.lattice.reshape(-1).copy()), *self.sizes,
+                                             C.byref(h)))
+        self.handle = h
+
+    def size(self) -> int:
+        return self.sizes[0] * self.sizes[1] * self.sizes[2]
+
+    def volume_element(self) -> float:
+        return self.cell.volume / self.size()
+
+    def rspacing(self):
+        return self.cell.lengths() / np.array(self.sizes)
+
+    def reciprocal(self) -> "FourierSpace":
+        return FourierSpace(self)
+
+    def rvector_contra(self):
+        """[nx,ny,nz,3] contravariant point positions in the symmetric range (real_space.hpp:127-135)."""
+        idx = [np.where(np.arange(n) >= (n + 1) // 2, np.arange(n) - n, np.arange(n)) * (1.0 / n) for n in self.sizes]
+        X, Y, Z = np.meshgrid(*idx, indexing="ij")
+        return np.stack([X, Y, Z], axis=-1)
+
+    def rvector_cartesian(self):
+        return self.rvector_contra() @ self.cell.lattice
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) and self.ctx.handle:
+                self.ctx.lib.inqb_basis_destroy(self.handle)
+        except Exception:
+            pass
+
+
+class FourierSpace:
+    """basis::fourier_space(real_space): same grid, serial (non-reversed) order."""
+
+    def __init__(self, rs: RealSpace):
+        self.real_space = rs
+        self.sizes = rs.sizes
+        self.cell = rs.cell
+
+    def size(self):
+        return self.real_space.size()
+
+    def volume_element(self):
+        return self.cell.volume / (self.size() * self.size())  # fourier_space.hpp:48-50
+
+
+def spherical_grid(cell: Cell, sizes, center, radius):
+    """basis::spherical_grid on the host: (points [n,3] int32, distance [n] float32, relpos [n,3] float32)."""
+    lib = _lib.load()
+    lat = np.ascontiguousarray(cell.lattice.reshape(-1))
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    n = C.c_longlong()
+    code = lib.inqb_spherical_grid(dptr(lat), *[int(x) for x in sizes], dptr(c), float(radius), 0, None, None, None,
+                                   C.byref(n))
+    if code not in (0, _lib.INQB_OK) and n.value == 0:
+        check(code)
+    npts = n.value
+    pts = np.zeros((npts, 3), np.int32)
+    dist = np.zeros(npts, np.float32)
+    rel = np.zeros((npts, 3), np.float32)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    check(lib.inqb_spherical_grid(dptr(lat), *[int(x) for x in sizes], dptr(c), float(radius), npts, vp(pts), vp(dist),
+                                  vp(rel), C.byref(n)))
+    return pts, dist, rel
+
+
+# ---------------------------------------------------------------- orbital sets
+
+
+class OrbitalSet:
+    """states::orbital_set<real_space|fourier_space, complex> with device storage [npoint][nst]."""
+
+    def __init__(self, basis: RealSpace, nst: int, spinor_dim: int = 1, kpoint=(0.0, 0.0, 0.0), spin_index: int = 0,
+                 space: int = REAL_SPACE, precision: int = F64):
+        self.basis = basis
+        self.ctx = basis.ctx
+        self.nst = int(nst)
+        self._kpoint = np.asarray(kpoint, dtype=np.float64).copy()
+        self._spin = int(spin_index)
+        self.precision = precision
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.inqb_orbitals_create(self.ctx.handle, basis.handle, self.nst, spinor_dim,
+                                                         dptr(self._kpoint), self._spin, space, precision, C.byref(h)))
+        self.handle = h
+
+    # --- reference-style accessors
+    def set_size(self):
+        return self.nst
+
+    local_set_size = set_size
+
+    def kpoint(self):
+        return self._kpoint.copy()
+
+    def spin_index(self):
+        return self._spin
+
+    @property
+    def space(self) -> int:
+        sp = C.c_int()
+        self.ctx.check(self.ctx.lib.inqb_orbitals_info(self.handle, None, C.byref(sp), None, None))
+        return sp.value
+
+    @property
+    def dtype(self):
+        return np.complex128 if self.precision == F64 else np.complex64
+
+    def skeleton(self, space: int | None = None) -> "OrbitalSet":
+        """A new, uninitialised set with the same basis, size, k-point and spin (orbital_set::skeleton)."""
+        return OrbitalSet(self.basis, self.nst, 1, self._kpoint, self._spin, self.space if space is None else space,
+                          self.precision)
+
+    def copy(self) -> "OrbitalSet":
+        out = self.skeleton()
+        self.ctx.check(self.ctx.lib.inqb_orbitals_copy(self.handle, out.handle))
+        return out
+
+    def assign(self, other: "OrbitalSet"):
+        self.ctx.check(self.ctx.lib.inqb_orbitals_copy(other.handle, self.handle))
+
+    def fill(self, value):
+        v = complex(value)
+        self.ctx.check(self.ctx.lib.inqb_orbitals_fill(self.handle, v.real, v.imag))
+
+    def randomize_gsphere(self, seed: int, ecut: float):
+        """Seeded N(0,1) Fourier coefficients inside |G|^2/2 < ecut (tags the set Fourier-space)."""
+        self.ctx.check(self.ctx.lib.inqb_orbitals_randomize_gsphere(self.handle, int(seed) & (2**64 - 1), float(ecut)))
+        return self
+
+    def converted(self, precision: int) -> "OrbitalSet":
+        """A copy of this set in another precision (F64 <-> F32)."""
+        out = OrbitalSet(self.basis, self.nst, 1, self._kpoint, self._spin, self.space, precision)
+        if precision == self.precision:
+            out.assign(self)
+        else:
+            self.ctx.check(self.ctx.lib.inqb_orbitals_convert(self.handle, out.handle))
+        return out
+
+    def set_space(self, space: int):
+        self.ctx.check(self.ctx.lib.inqb_orbitals_set_space(self.handle, space))
+
+    def upload(self, arr):
+        a = np.ascontiguousarray(np.asarray(arr).reshape(self.basis.size(), self.nst), dtype=self.dtype)
+        self.ctx.check(self.ctx.lib.inqb_orbitals_upload(self.handle, a.ctypes.data_as(C.c_void_p)))
+        return self
+
+    def matrix(self) -> np.ndarray:
+        """Host copy [npoint][nst] (field_set::matrix())."""
+        out = np.empty((self.basis.size(), self.nst), dtype=self.dtype)
+        self.ctx.check(self.ctx.lib.inqb_orbitals_download(self.handle, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def hypercubic(self) -> np.ndarray:
+        """Host copy [nx][ny][nz][nst] (field_set::hypercubic())."""
+        return self.matrix().reshape(self.basis.sizes + (self.nst,))
+
+    def device_ptr(self) -> int:
+        p = C.c_void_p()
+        self.ctx.check(self.ctx.lib.inqb_orbitals_device_ptr(self.handle, C.byref(p)))
+        return p.value
+
+    def nbytes(self) -> int:
+        return self.basis.size() * self.nst * (16 if self.precision == F64 else 8)
+
+    @classmethod
+    def from_array(cls, basis, arr, kpoint=(0.0, 0.0, 0.0), spin_index=0, space=REAL_SPACE, precision=F64):
+        a = np.asarray(arr)
+        nst = a.shape[-1]
+        return cls(basis, nst, 1, kpoint, spin_index, space, precision).upload(a)
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) and self.ctx.handle:
+                self.ctx.lib.inqb_orbitals_destroy(self.handle)
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- Hamiltonian
+
+
+class KSHamiltonian:
+    """hamiltonian::ks_hamiltonian with the exchange operator disabled and no relativistic projectors."""
+
+    def __init__(self, basis: RealSpace, nspin: int = 1):
+        self.basis = basis
+        self.ctx = basis.ctx
+        self.nspin = nspin
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.inqb_hamiltonian_create(self.ctx.handle, basis.handle, nspin, C.byref(h)))
+        self.handle = h
+        self._A = np.zeros(3)
+
+    # scalar_potential() (ks_hamiltonian.hpp:252-254): [npoint][nspin] float64
+    def set_scalar_potential(self, V):
+        v = np.ascontiguousarray(np.asarray(V, dtype=np.float64).reshape(self.basis.size(), self.nspin))
+        self.ctx.check(self.ctx.lib.inqb_potential_set(self.handle, dptr(v)))
+
+    @property
+    def uniform_vector_potential(self):
+        return self._A.copy()
+
+    @uniform_vector_potential.setter
+    def uniform_vector_potential(self, A_cov):
+        self._A = np.asarray(A_cov, dtype=np.float64).copy()
+        self.ctx.check(self.ctx.lib.inqb_vector_potential_set(self.handle, dptr(self._A)))
+
+    def set_projectors(self, points, positions, matrices, coeff, npts, nlm):
+        """Packed projector_all tables (see include/inqb.h inqb_projectors_set)."""
+        points = np.ascontiguousarray(points, dtype=np.int32)
+        positions = np.ascontiguousarray(positions, dtype=np.float32)
+        matrices = np.ascontiguousarray(matrices, dtype=np.float64)
+        coeff = np.ascontiguousarray(coeff, dtype=np.float64)
+        npts = np.ascontiguousarray(npts, dtype=np.int32)
+        nlm = np.ascontiguousarray(nlm, dtype=np.int32)
+        nproj, maxsph = points.shape[0], points.shape[1]
+        maxnlm = matrices.shape[1]
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        self.ctx.check(self.ctx.lib.inqb_projectors_set(self.handle, nproj, maxsph, maxnlm, vp(points), vp(positions),
+                                                        vp(matrices), vp(coeff), vp(npts), vp(nlm)))
+
+    def update_projectors_gaussian(self, positions, radius, rc, kb):
+        """Synthetic KB projectors (l = 0, 1; radial exp(-r^2/rc^2)) at cartesian atom positions."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        kbv = np.ascontiguousarray(kb, dtype=np.float64).reshape(len(pos), 4, 4)
+        self.ctx.check(self.ctx.lib.inqb_projectors_build_gaussian(self.handle, len(pos), dptr(pos), float(radius),
+                                                                   float(rc), dptr(kbv)))
+
+    def projectors_info(self):
+        n, m, t = C.c_int(), C.c_int(), C.c_longlong()
+        self.ctx.check(self.ctx.lib.inqb_projectors_info(self.handle, C.byref(n), C.byref(m), C.byref(t)))
+        return n.value, m.value, t.value
+
+    def projector_tables(self):
+        nproj, maxsph, _ = self.projectors_info()
+        points = np.zeros((nproj, maxsph, 3), np.int32)
+        pos = np.zeros((nproj, maxsph, 3), np.float32)
+        mats = np.zeros((nproj, 4, maxsph), np.float64)
+        npts = np.zeros(nproj, np.int32)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        self.ctx.check(self.ctx.lib.inqb_projectors_get(self.handle, vp(points), vp(pos), vp(mats), vp(npts)))
+        return points, pos, mats, npts
+
+    # operator() (ks_hamiltonian.hpp:137-180)
+    def __call__(self, phi: OrbitalSet) -> OrbitalSet:
+        out = phi.skeleton()
+        self.apply(phi, out)
+        return out
+
+    def apply(self, phi: OrbitalSet, out: OrbitalSet):
+        self.ctx.check(self.ctx.lib.inqb_apply(self.handle, phi.handle, out.handle))
+        return out
+
+    def non_local(self, phi: OrbitalSet) -> OrbitalSet:
+        out = phi.skeleton()
+        self.ctx.check(self.ctx.lib.inqb_non_local(self.handle, phi.handle, out.handle))
+        return out
+
+    def non_local_energy(self, phi: OrbitalSet, occupations) -> float:
+        occ = np.ascontiguousarray(occupations, dtype=np.float64)
+        e = C.c_double()
+        self.ctx.check(self.ctx.lib.inqb_non_local_energy(self.handle, phi.handle, dptr(occ), C.byref(e)))
+        return e.value
+
+    def kinetic_expectation_value(self, phi: OrbitalSet):
+        out = np.zeros(phi.nst)
+        self.ctx.check(self.ctx.lib.inqb_kinetic_expectation_value(self.handle, phi.handle, dptr(out)))
+        return out
+
+    def eigenvalues(self, phi: OrbitalSet):
+        eig = np.zeros(phi.nst)
+        res = np.zeros(phi.nst)
+        self.ctx.check(self.ctx.lib.inqb_eigenvalues(self.handle, phi.handle, dptr(eig), dptr(res)))
+        return eig, res
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) and self.ctx.handle:
+                self.ctx.lib.inqb_hamiltonian_destroy(self.handle)
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- operations
+
+
+def to_fourier(phi: OrbitalSet) -> OrbitalSet:
+    out = phi.skeleton(FOURIER_SPACE)
+    phi.ctx.check(phi.ctx.lib.inqb_to_fourier(phi.handle, out.handle))
+    return out
+
+
+def to_real(fphi: OrbitalSet, normalize: bool = True) -> OrbitalSet:
+    out = fphi.skeleton(REAL_SPACE)
+    fphi.ctx.check(fphi.ctx.lib.inqb_to_real(fphi.handle, out.handle, int(bool(normalize))))
+    return out
+
+
+def laplacian(fphi: OrbitalSet, factor: float = 1.0, gradcoeff=(0.0, 0.0, 0.0)) -> OrbitalSet:
+    out = fphi.skeleton(FOURIER_SPACE)
+    g = np.asarray(gradcoeff, dtype=np.float64)
+    fphi.ctx.check(fphi.ctx.lib.inqb_laplacian(fphi.handle, out.handle, float(factor), dptr(g)))
+    return out
+
+
+def overlap(phi1: OrbitalSet, phi2: OrbitalSet | None = None) -> np.ndarray:
+    phi2 = phi1 if phi2 is None else phi2
+    out = np.zeros((phi1.nst, phi2.nst), np.complex128)
+    phi1.ctx.check(phi1.ctx.lib.inqb_overlap(phi1.handle, phi2.handle, out.view(np.float64).reshape(-1).ctypes.data_as(_lib.DP)))
+    return out
+
+
+def overlap_diagonal(phi1: OrbitalSet, phi2: OrbitalSet | None = None) -> np.ndarray:
+    phi2 = phi1 if phi2 is None else phi2
+    out = np.zeros(phi1.nst, np.complex128)
+    phi1.ctx.check(phi1.ctx.lib.inqb_overlap_diagonal(phi1.handle, phi2.handle,
+                                                      out.view(np.float64).ctypes.data_as(_lib.DP)))
+    return out
+
+
+def orthogonalize(phi: OrbitalSet):
+    phi.ctx.check(phi.ctx.lib.inqb_orthogonalize(phi.handle))
+    return phi
+
+
+def rotate(phi: OrbitalSet, R):
+    r = np.ascontiguousarray(R, dtype=np.complex128)
+    phi.ctx.check(phi.ctx.lib.inqb_rotate(phi.handle, r.view(np.float64).reshape(-1).ctypes.data_as(_lib.DP)))
+    return phi
+
+
+def shift(factor, chi: OrbitalSet, phi: OrbitalSet):
+    f = complex(factor)
+    phi.ctx.check(phi.ctx.lib.inqb_shift(f.real, f.imag, chi.handle, phi.handle))
+
+
+def exponential_in_place(ham: KSHamiltonian, factor, phi: OrbitalSet, order: int = 4):
+    f = complex(factor)
+    ham.ctx.check(ham.ctx.lib.inqb_exponential_in_place(ham.handle, f.real, f.imag, phi.handle, order))
+
+
+def exponential(ham: KSHamiltonian, factor, phi: OrbitalSet, order: int = 4) -> OrbitalSet:
+    out = phi.copy()
+    exponential_in_place(ham, factor, out, order)
+    return out
+
+
+def exponential_2_for_1(ham: KSHamiltonian, factor1, factor2, phi: OrbitalSet, order: int = 4) -> OrbitalSet:
+    """Returns exp(factor1 H) phi and replaces phi by exp(factor2 H) phi (exponential.hpp:50-69)."""
+    exp1 = phi.skeleton()
+    f1, f2 = complex(factor1), complex(factor2)
+    ham.ctx.check(ham.ctx.lib.inqb_exponential_2_for_1(ham.handle, f1.real, f1.imag, f2.real, f2.imag, phi.handle,
+                                                       exp1.handle, order))
+    return exp1
+
+
+def _ptr_arrays(phis, occs):
+    hs = (C.c_void_p * len(phis))(*[p.handle.value for p in phis])
+    occ_arrays = [np.ascontiguousarray(o, dtype=np.float64) for o in occs]
+    optrs = (_lib.DP * len(occs))(*[dptr(o) for o in occ_arrays])
+    return hs, optrs, occ_arrays
+
+
+def density(phis: Sequence[OrbitalSet], occupations: Sequence) -> np.ndarray:
+    """observables::density::calculate: n = sum_sets sum_s occ_s |phi_s|^2, [npoint] float64."""
+    hs, optrs, keep = _ptr_arrays(phis, occupations)
+    out = np.zeros(phis[0].basis.size())
+    phis[0].ctx.check(phis[0].ctx.lib.inqb_density(hs, len(phis), optrs, dptr(out)))
+    return out
+
+
+def dipole(basis: RealSpace, dens) -> np.ndarray:
+    d = np.ascontiguousarray(dens, dtype=np.float64).reshape(-1)
+    out = np.zeros(3)
+    basis.ctx.check(basis.ctx.lib.inqb_dipole(basis.handle, dptr(d), dptr(out)))
+    return out
+
+
+class Kick:
+    """perturbations::kick (kick.hpp:22-121).
+
+    gauge 'length' multiplies the orbitals by exp(i E_cov . r) with E = -kick at the
+    zero step; 'velocity' instead sets the uniform vector potential A = -kick
+    (the reference's automatic choice for periodic cells)."""
+
+    def __init__(self, cell: Cell, kick_field, gauge: str = "automatic"):
+        k = np.asarray(kick_field, dtype=np.float64)
+        if gauge == "automatic":
+            gauge = "velocity" if cell.periodicity > 0 else "length"
+        self.gauge = gauge
+        self.efield = -k if gauge == "length" else np.zeros(3)
+        self.vpot = -k if gauge == "velocity" else np.zeros(3)
+        self.cell = cell
+
+    def zero_step(self, phi: OrbitalSet):
+        if np.any(self.efield != 0.0):
+            apply_phase_kick(phi, self.efield)
+
+    def uniform_vector_potential(self, time: float = 0.0):
+        return self.vpot.copy()
+
+
+def apply_phase_kick(phi: OrbitalSet, efield_cart):
+    """phi *= exp(i E_cov . r) (kick::zero_step body, kick.hpp:64-69)."""
+    e = np.asarray(efield_cart, dtype=np.float64)
+    phi.ctx.check(phi.ctx.lib.inqb_kick(phi.handle, dptr(e)))
+
+
+def etrs(ham: KSHamiltonian, phis: Sequence[OrbitalSet], occupations: Sequence, dt: float, nscf: int = 5,
+         scf_threshold: float = 5e-5, want_density: bool = False):
+    """One ETRS step (real_time/etrs.hpp:22-79) with a fixed Hamiltonian.
+
+    Returns (density or None, electronic dipole [3], number of SCF iterations)."""
+    hs, optrs, keep = _ptr_arrays(phis, occupations)
+    dens = np.zeros(phis[0].basis.size()) if want_density else None
+    dip = np.zeros(3)
+    iters = C.c_int()
+    ham.ctx.check(ham.ctx.lib.inqb_etrs_step(ham.handle, hs, len(phis), optrs, float(dt), int(nscf), float(scf_threshold),
+                                             dptr(dens) if dens is not None else None, dptr(dip), C.byref(iters)))
+    return dens, dip, iters.value

@@ -1,0 +1,1267 @@
+// extern "C" entry points of libinqb200 (declared in include/inqb.h).
+//
+// Each entry point validates its arguments, runs the device work on the
+// context's stream and converts exceptions into status codes.  The operator
+// sequences follow the reference's ks_hamiltonian (ks_hamiltonian.hpp:137-180);
+// the kernels they call fuse several of the reference's whole-array passes
+// (fft.cu explains which).
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <memory>
+#include <numeric>
+
+#include "inqb_internal.h"
+#include "sphere.h"
+
+using namespace inqb;
+
+namespace {
+
+thread_local std::string g_err_noctx;
+
+template <typename F> int guarded(Ctx *ctx, F &&f) {
+  try {
+    f();
+    return INQB_OK;
+  } catch (const Error &e) {
+    if (ctx) ctx->err = e.what();
+    else g_err_noctx = e.what();
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    if (ctx) ctx->err = "host allocation failed";
+    return INQB_ERR_MEMORY;
+  } catch (const std::exception &e) {
+    if (ctx) ctx->err = e.what();
+    else g_err_noctx = e.what();
+    return INQB_ERR_STATE;
+  }
+}
+
+void set_device(Ctx &ctx) { INQB_CUDA(cudaSetDevice(ctx.device)); }
+
+size_t csize(int precision) { return precision == INQB_F64 ? 16 : 8; }
+
+// cell_metric conversions for the small vectors of the operator (cell.hpp:176-211)
+void cov_to_cart(const Basis &b, const double v[3], double out[3]) {
+  for (int j = 0; j < 3; j++) out[j] = (b.rlat[0][j] * v[0] + b.rlat[1][j] * v[1]) + b.rlat[2][j] * v[2];
+}
+void cart_to_contra(const Basis &b, const double v[3], double out[3]) {
+  for (int k = 0; k < 3; k++) out[k] = b.rlat[k][0] * v[0] + b.rlat[k][1] * v[1] + b.rlat[k][2] * v[2];
+}
+void cart_to_cov(const Basis &b, const double v[3], double out[3]) {
+  for (int k = 0; k < 3; k++) out[k] = b.lat[k][0] * v[0] + b.lat[k][1] * v[1] + b.lat[k][2] * v[2];
+}
+void contra_to_cart(const Basis &b, const double v[3], double out[3]) {
+  for (int j = 0; j < 3; j++) out[j] = (b.lat[0][j] * v[0] + b.lat[1][j] * v[1]) + b.lat[2][j] * v[2];
+}
+double norm_cov(const Basis &b, const double v[3]) {
+  double c[3];
+  cov_to_cart(b, v, c);
+  return c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+}
+
+void check_same_shape(const Orbitals &a, const Orbitals &b) {
+  INQB_REQUIRE(a.basis == b.basis, INQB_ERR_ARG, "orbital sets live on different bases");
+  INQB_REQUIRE(a.nst == b.nst, INQB_ERR_ARG, "orbital sets have different numbers of states");
+  INQB_REQUIRE(a.precision == b.precision, INQB_ERR_ARG, "orbital sets have different precisions");
+}
+
+// ------------------------------------------------------------------ transforms
+
+template <typename R>
+void fft3d(Ctx &ctx, const Basis &b, const C2<R> *in, C2<R> *out, int S, int dir, R scale) {
+  PassArgs<R> a;
+  a.S = S;
+  a.dir = dir;
+  const int order_f[3] = {2, 1, 0};
+  const int order_b[3] = {0, 1, 2};
+  const int *order = dir > 0 ? order_f : order_b;
+  for (int k = 0; k < 3; k++) {
+    a.axis = order[k];
+    a.in = (k == 0) ? in : out;
+    a.out = out;
+    a.scale = (k == 2) ? scale : R(1);
+    launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
+  }
+}
+
+// ------------------------------------------------------------------ Hamiltonian pieces
+
+template <typename R> C2<R> *proj_buf(Hamiltonian &h, int S, int which) {
+  const size_t need = size_t(std::max(1, h.proj.nproj)) * 4 * S * sizeof(C2<double>);
+  if (need > h.proj_bytes) {
+    if (h.d_projraw) INQB_CUDA(cudaFree(h.d_projraw));
+    if (h.d_projD) INQB_CUDA(cudaFree(h.d_projD));
+    h.d_projraw = h.d_projD = nullptr;
+    h.proj_bytes = 0;
+    INQB_CUDA(cudaMalloc(&h.d_projraw, need));
+    INQB_CUDA(cudaMalloc(&h.d_projD, need));
+    h.proj_bytes = need;
+  }
+  return static_cast<C2<R> *>(which == 0 ? h.d_projraw : h.d_projD);
+}
+
+void ensure_tables(Hamiltonian &h, const double kA[3]) {
+  if (h.proj.nproj == 0) return;
+  if (h.proj.kA[0] == kA[0] && h.proj.kA[1] == kA[1] && h.proj.kA[2] == kA[2]) return;
+  launch_nl_tables(*h.ctx, *h.basis, h, kA);
+}
+
+struct Accum {
+  void *acc1 = nullptr, *acc2 = nullptr;
+  double c1[2] = {0, 0}, c2[2] = {0, 0};
+};
+
+template <typename R>
+void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &acc) {
+  Ctx &ctx = *h.ctx;
+  const Basis &b = *h.basis;
+  const int S = in.nst;
+  const C2<R> *psi = static_cast<const C2<R> *>(in.data);
+  C2<R> *hpsi = static_cast<C2<R> *>(out.data);
+  double kA[3] = {in.kpoint[0] + h.A[0], in.kpoint[1] + h.A[1], in.kpoint[2] + h.A[2]};
+
+  C2<R> *projD = nullptr;
+  if (h.proj.nproj > 0) {
+    ensure_tables(h, kA);
+    C2<R> *praw = proj_buf<R>(h, S, 0);
+    projD = proj_buf<R>(h, S, 1);
+    launch_nl_project<R>(ctx, b, h, psi, S, praw, projD);
+  }
+  double ktmp[3], kc[3];
+  cov_to_cart(b, kA, ktmp);
+  cart_to_contra(b, ktmp, kc);
+
+  PassArgs<R> a;
+  a.S = S;
+  a.dir = +1;
+  // forward z, y
+  a.axis = 2;
+  a.in = psi;
+  a.out = hpsi;
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
+  a.axis = 1;
+  a.in = hpsi;
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
+  // x: forward, kinetic factor -0.5*(-|G|^2 + gc.G), gc = -2 (k+A)^contra, backward
+  a.axis = 0;
+  a.mid_kinetic = 1;
+  a.lap_factor = -0.5;
+  for (int i = 0; i < 3; i++) a.gc[i] = -2.0 * kc[i];
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
+  a.mid_kinetic = 0;
+  // backward y, then z with the real-space epilogue
+  a.dir = -1;
+  a.axis = 1;
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
+  a.axis = 2;
+  a.scale = R(1.0 / double(b.npoints));
+  a.psi = psi;
+  if constexpr (sizeof(R) == 8) a.V = h.d_V;
+  else a.V = h.d_V32;
+  a.nspin = h.nspin;
+  a.spin = in.spin_index;
+  a.vshift = R(0.5 * norm_cov(b, kA));
+  if (h.proj.nproj > 0) {
+    a.nl_offs = h.proj.d_offs;
+    a.nl_hit = h.proj.d_hit;
+    if constexpr (sizeof(R) == 8) a.nl_hcoef = h.proj.d_hcoef;
+    else a.nl_hcoef = h.proj.d_hcoef32;
+    a.projD = projD;
+    a.maxsph = h.proj.maxsph;
+  }
+  a.acc1 = static_cast<C2<R> *>(acc.acc1);
+  a.acc2 = static_cast<C2<R> *>(acc.acc2);
+  a.c1 = mk<C2<R>>(R(acc.c1[0]), R(acc.c1[1]));
+  a.c2 = mk<C2<R>>(R(acc.c2[0]), R(acc.c2[1]));
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_FINAL_REAL);
+}
+
+template <typename R> void apply_fourier(Hamiltonian &h, const Orbitals &in, Orbitals &out) {
+  Ctx &ctx = *h.ctx;
+  const Basis &b = *h.basis;
+  const int S = in.nst;
+  const C2<R> *fpsi = static_cast<const C2<R> *>(in.data);
+  C2<R> *w = static_cast<C2<R> *>(out.data);
+  double kA[3] = {in.kpoint[0] + h.A[0], in.kpoint[1] + h.A[1], in.kpoint[2] + h.A[2]};
+  double ktmp[3], kc[3];
+  cov_to_cart(b, kA, ktmp);
+  cart_to_contra(b, ktmp, kc);
+
+  // psi_rs = to_real(fpsi) in the output buffer
+  fft3d<R>(ctx, b, fpsi, w, S, -1, R(1.0 / double(b.npoints)));
+  C2<R> *projD = nullptr;
+  if (h.proj.nproj > 0) {
+    ensure_tables(h, kA);
+    C2<R> *praw = proj_buf<R>(h, S, 0);
+    projD = proj_buf<R>(h, S, 1);
+    launch_nl_project<R>(ctx, b, h, w, S, praw, projD);
+  }
+  PassArgs<R> a;
+  a.S = S;
+  a.dir = +1;
+  a.axis = 2;
+  a.in = w;
+  a.out = w;
+  if constexpr (sizeof(R) == 8) a.V = h.d_V;
+  else a.V = h.d_V32;
+  a.nspin = h.nspin;
+  a.spin = in.spin_index;
+  a.vshift = R(0.5 * norm_cov(b, kA));
+  if (h.proj.nproj > 0) {
+    a.nl_offs = h.proj.d_offs;
+    a.nl_hit = h.proj.d_hit;
+    if constexpr (sizeof(R) == 8) a.nl_hcoef = h.proj.d_hcoef;
+    else a.nl_hcoef = h.proj.d_hcoef32;
+    a.projD = projD;
+    a.maxsph = h.proj.maxsph;
+  }
+  launch_fft_pass<R>(ctx, b, a, PRO_VPSI, EPI_STORE);
+  PassArgs<R> c;
+  c.S = S;
+  c.dir = +1;
+  c.axis = 1;
+  c.in = w;
+  c.out = w;
+  launch_fft_pass<R>(ctx, b, c, PRO_NONE, EPI_STORE);
+  c.axis = 0;
+  c.psi = fpsi;
+  c.lap_factor = -0.5;
+  for (int i = 0; i < 3; i++) c.gc[i] = -2.0 * kc[i];
+  launch_fft_pass<R>(ctx, b, c, PRO_NONE, EPI_LAPL_ADD);
+}
+
+void apply_any(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &acc = Accum()) {
+  check_same_shape(in, out);
+  INQB_REQUIRE(in.basis == h.basis, INQB_ERR_ARG, "orbitals and Hamiltonian live on different bases");
+  INQB_REQUIRE(in.data != out.data, INQB_ERR_ARG, "H|psi> needs distinct input and output sets");
+  INQB_REQUIRE(in.spin_index >= 0 && in.spin_index < h.nspin, INQB_ERR_ARG, "spin index out of range");
+  if (in.space == INQB_REAL_SPACE) {
+    if (in.precision == INQB_F64) apply_real<double>(h, in, out, acc);
+    else apply_real<float>(h, in, out, acc);
+  } else {
+    INQB_REQUIRE(acc.acc1 == nullptr && acc.acc2 == nullptr, INQB_ERR_UNSUPPORTED,
+                 "Taylor accumulation is implemented for real-space sets");
+    if (in.precision == INQB_F64) apply_fourier<double>(h, in, out);
+    else apply_fourier<float>(h, in, out);
+  }
+  out.space = in.space;
+  for (int i = 0; i < 3; i++) out.kpoint[i] = in.kpoint[i];
+  out.spin_index = in.spin_index;
+}
+
+// scratch orbital set with the shape of `like`
+struct TempSet {
+  Orbitals o;
+  Ctx *ctx;
+  explicit TempSet(const Orbitals &like) : o(like), ctx(like.ctx) { o.data = dev_alloc(*ctx, like.bytes()); }
+  ~TempSet() {
+    if (o.data) cudaFreeAsync(o.data, ctx->stream);
+  }
+  TempSet(const TempSet &) = delete;
+  TempSet &operator=(const TempSet &) = delete;
+};
+
+void copy_set(const Orbitals &src, Orbitals &dst) {
+  check_same_shape(src, dst);
+  INQB_CUDA(cudaMemcpyAsync(dst.data, src.data, src.bytes(), cudaMemcpyDeviceToDevice, src.ctx->stream));
+  dst.space = src.space;
+}
+
+// exponential_2_for_1 / exponential_in_place (exponential.hpp:21-69) with every shift fused into the
+// epilogue of the H application that produces the term.
+void exponential(Hamiltonian &h, std::complex<double> f1, std::complex<double> f2, Orbitals &phi, Orbitals *exp1,
+                 int order) {
+  INQB_REQUIRE(order >= 1, INQB_ERR_ARG, "order must be >= 1");
+  INQB_REQUIRE(phi.space == INQB_REAL_SPACE, INQB_ERR_UNSUPPORTED, "exponential is implemented for real-space sets");
+  if (exp1) copy_set(phi, *exp1);
+  TempSet ta(phi), tb(phi);
+  std::complex<double> c1 = 1.0, c2 = 1.0;
+  const Orbitals *src = &phi;
+  Orbitals *bufs[2] = {&ta.o, &tb.o};
+  for (int it = 1; it <= order; it++) {
+    c1 *= f1 / double(it);
+    c2 *= f2 / double(it);
+    Accum acc;
+    if (exp1) {
+      acc.acc1 = exp1->data;
+      acc.c1[0] = c1.real();
+      acc.c1[1] = c1.imag();
+    }
+    acc.acc2 = phi.data;
+    acc.c2[0] = c2.real();
+    acc.c2[1] = c2.imag();
+    Orbitals *dst = bufs[(it - 1) % 2];
+    apply_any(h, *src, *dst, acc);
+    src = dst;
+  }
+}
+
+template <typename R> double *occ_to_device(Ctx &ctx, const double *occ, int S) {
+  double *d = static_cast<double *>(dev_alloc(ctx, sizeof(double) * S));
+  INQB_CUDA(cudaMemcpyAsync(d, occ, sizeof(double) * S, cudaMemcpyHostToDevice, ctx.stream));
+  return d;
+}
+
+void density_dev(Ctx &ctx, inqb_orbitals *const *phis, int nsets, const double *const *occ, double *dens) {
+  for (int k = 0; k < nsets; k++) {
+    const Orbitals &o = *phis[k];
+    double *docc = static_cast<double *>(dev_alloc(ctx, sizeof(double) * o.nst));
+    INQB_CUDA(cudaMemcpyAsync(docc, occ[k], sizeof(double) * o.nst, cudaMemcpyHostToDevice, ctx.stream));
+    if (o.precision == INQB_F64)
+      launch_density<double>(ctx, static_cast<const double2 *>(o.data), o.nst, o.basis->npoints, docc, dens, k > 0);
+    else
+      launch_density<float>(ctx, static_cast<const float2 *>(o.data), o.nst, o.basis->npoints, docc, dens, k > 0);
+    dev_free(ctx, docc);
+  }
+}
+
+void dipole_host(const Basis &b, const double *dens, double out[3]) {
+  double acc[3] = {0, 0, 0};
+  const int nx = b.n[0], ny = b.n[1], nz = b.n[2];
+  long long pt = 0;
+  for (int ix = 0; ix < nx; ix++)
+    for (int iy = 0; iy < ny; iy++)
+      for (int iz = 0; iz < nz; iz++, pt++) {
+        const int s[3] = {ix >= (nx + 1) / 2 ? ix - nx : ix, iy >= (ny + 1) / 2 ? iy - ny : iy,
+                          iz >= (nz + 1) / 2 ? iz - nz : iz};
+        const double c[3] = {s[0] * (1.0 / nx), s[1] * (1.0 / ny), s[2] * (1.0 / nz)};
+        double r[3];
+        contra_to_cart(b, c, r);
+        for (int j = 0; j < 3; j++) acc[j] += r[j] * dens[pt];
+      }
+  const double dv = b.volume / double(b.npoints);
+  for (int j = 0; j < 3; j++) out[j] = dv * acc[j];
+}
+
+// Cholesky S = U^H U (upper, matrix/cholesky.hpp:28-89) and U^{-1} (invert_triangular.hpp:20-60), host FP64.
+void cholesky_inverse(int n, const std::complex<double> *S, std::complex<double> *X) {
+  std::vector<std::complex<double>> U(size_t(n) * n, 0.0);
+  for (int j = 0; j < n; j++) {
+    double d = S[size_t(j) * n + j].real();
+    for (int k = 0; k < j; k++) d -= std::norm(U[size_t(k) * n + j]);
+    INQB_REQUIRE(d > 0.0, INQB_ERR_NUMERIC, "overlap matrix is not positive definite (orthogonalize)");
+    const double ujj = std::sqrt(d);
+    U[size_t(j) * n + j] = ujj;
+    for (int i = j + 1; i < n; i++) {
+      std::complex<double> v = S[size_t(j) * n + i];
+      for (int k = 0; k < j; k++) v -= std::conj(U[size_t(k) * n + j]) * U[size_t(k) * n + i];
+      U[size_t(j) * n + i] = v / ujj;
+    }
+  }
+  std::fill(X, X + size_t(n) * n, std::complex<double>(0.0));
+  for (int i = 0; i < n; i++) {
+    X[size_t(i) * n + i] = 1.0 / U[size_t(i) * n + i];
+    for (int j = i + 1; j < n; j++) {
+      std::complex<double> s = 0.0;
+      for (int k = i; k < j; k++) s += X[size_t(i) * n + k] * U[size_t(k) * n + j];
+      X[size_t(i) * n + j] = -s / U[size_t(j) * n + j];
+    }
+  }
+}
+
+void overlap_dev(const Orbitals &a, const Orbitals &b, double2 *out_dev) {
+  Ctx &ctx = *a.ctx;
+  INQB_REQUIRE(a.basis == b.basis && a.precision == b.precision, INQB_ERR_ARG, "overlap of incompatible sets");
+  const double dv = a.basis->volume / double(a.basis->npoints);
+  if (a.precision == INQB_F64)
+    launch_overlap<double>(ctx, static_cast<const double2 *>(a.data), a.nst, static_cast<const double2 *>(b.data),
+                           b.nst, a.basis->npoints, dv, out_dev);
+  else
+    launch_overlap<float>(ctx, static_cast<const float2 *>(a.data), a.nst, static_cast<const float2 *>(b.data), b.nst,
+                          a.basis->npoints, dv, out_dev);
+}
+
+void ovdiag_dev(const Orbitals &a, const Orbitals &b, double2 *out_dev) {
+  check_same_shape(a, b);
+  Ctx &ctx = *a.ctx;
+  const double dv = a.basis->volume / double(a.basis->npoints);
+  if (a.precision == INQB_F64)
+    launch_overlap_diag<double>(ctx, static_cast<const double2 *>(a.data), static_cast<const double2 *>(b.data), a.nst,
+                                a.basis->npoints, dv, out_dev);
+  else
+    launch_overlap_diag<float>(ctx, static_cast<const float2 *>(a.data), static_cast<const float2 *>(b.data), a.nst,
+                               a.basis->npoints, dv, out_dev);
+}
+
+void rotate_dev(Orbitals &phi, const double2 *Rdev) {
+  if (phi.precision == INQB_F64)
+    launch_rotate<double>(*phi.ctx, static_cast<double2 *>(phi.data), phi.nst, phi.basis->npoints, Rdev);
+  else
+    launch_rotate<float>(*phi.ctx, static_cast<float2 *>(phi.data), phi.nst, phi.basis->npoints, Rdev);
+}
+
+template <typename T> std::vector<T> download(Ctx &ctx, const void *dev, size_t n) {
+  std::vector<T> h(n);
+  INQB_CUDA(cudaMemcpyAsync(h.data(), dev, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx.stream));
+  INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+  return h;
+}
+
+void free_projectors(Projectors &P) {
+  void *ptrs[] = {P.d_pt, P.d_pos, P.d_mat, P.d_coeff, P.d_coeff32, P.d_npts, P.d_offs, P.d_hit,
+                  P.d_gcoef, P.d_hcoef, P.d_gcoef32, P.d_hcoef32};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  P = Projectors();
+}
+
+template <typename T> T *upload_vec(const std::vector<T> &v) {
+  T *d = nullptr;
+  const size_t bytes = std::max<size_t>(sizeof(T), v.size() * sizeof(T));
+  INQB_CUDA(cudaMalloc(&d, bytes));
+  if (!v.empty()) INQB_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return d;
+}
+
+// projector_all packing (projector_all.hpp:40-109) + per-grid-point hit lists for the owner-computes scatter
+void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int32_t *points, const float *pos,
+                    const double *matrices, const double *coeff, const int32_t *npts, const int32_t *nlm) {
+  const Basis &b = *h.basis;
+  INQB_REQUIRE(nproj >= 0 && maxsph >= 0, INQB_ERR_ARG, "negative projector table size");
+  INQB_REQUIRE(maxnlm >= 0 && maxnlm <= 4, INQB_ERR_UNSUPPORTED, "at most 4 (l <= 1) projector functions per atom");
+  INQB_CUDA(cudaStreamSynchronize(h.ctx->stream));
+  free_projectors(h.proj);
+  Projectors &P = h.proj;
+  P.nproj = nproj;
+  P.maxsph = maxsph;
+  P.maxnlm = maxnlm;
+  if (nproj == 0) return;
+  P.h_points.assign(points, points + size_t(nproj) * maxsph * 3);
+  P.h_pos.assign(pos, pos + size_t(nproj) * maxsph * 3);
+  P.h_mat.assign(matrices, matrices + size_t(nproj) * maxnlm * maxsph);
+  P.h_coeff.assign(coeff, coeff + size_t(nproj) * maxnlm * maxnlm);
+  P.h_npts.assign(npts, npts + nproj);
+  P.h_nlm.assign(nlm, nlm + nproj);
+
+  std::vector<int> flat(size_t(nproj) * maxsph, -1);
+  std::vector<double> mat4(size_t(nproj) * 4 * maxsph, 0.0);
+  std::vector<double> coeff4(size_t(nproj) * 16, 0.0);
+  std::vector<float> coeff4f(size_t(nproj) * 16, 0.0f);
+  std::vector<std::pair<long long, int>> hits;  // (grid point, p*maxsph + i)
+  for (int p = 0; p < nproj; p++) {
+    INQB_REQUIRE(npts[p] >= 0 && npts[p] <= maxsph, INQB_ERR_ARG, "sphere size out of range");
+    INQB_REQUIRE(nlm[p] >= 0 && nlm[p] <= maxnlm, INQB_ERR_ARG, "nlm out of range");
+    for (int i = 0; i < npts[p]; i++) {
+      const int32_t *g = points + (size_t(p) * maxsph + i) * 3;
+      INQB_REQUIRE(g[0] >= 0 && g[0] < b.n[0] && g[1] >= 0 && g[1] < b.n[1] && g[2] >= 0 && g[2] < b.n[2],
+                   INQB_ERR_ARG, "projector point outside the grid");
+      const long long pt = (static_cast<long long>(g[0]) * b.n[1] + g[1]) * b.n[2] + g[2];
+      flat[size_t(p) * maxsph + i] = int(pt);
+      hits.push_back({pt, p * maxsph + i});
+    }
+    for (int l = 0; l < nlm[p]; l++)
+      for (int i = 0; i < npts[p]; i++)
+        mat4[(size_t(p) * 4 + l) * maxsph + i] = matrices[(size_t(p) * maxnlm + l) * maxsph + i];
+    for (int l = 0; l < nlm[p]; l++)
+      for (int j = 0; j < nlm[p]; j++) {
+        coeff4[p * 16 + l * 4 + j] = coeff[(size_t(p) * maxnlm + l) * maxnlm + j];
+        coeff4f[p * 16 + l * 4 + j] = float(coeff4[p * 16 + l * 4 + j]);
+      }
+  }
+  std::stable_sort(hits.begin(), hits.end(),
+                   [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) { return x.first < y.first; });
+  P.total = (long long)hits.size();
+  INQB_REQUIRE(P.total < (1LL << 31), INQB_ERR_UNSUPPORTED, "too many sphere points");
+  std::vector<int> offs(size_t(b.npoints) + 1, 0);
+  std::vector<int> hit(hits.size());
+  for (size_t k = 0; k < hits.size(); k++) {
+    offs[size_t(hits[k].first) + 1]++;
+    hit[k] = hits[k].second;
+  }
+  for (long long i = 0; i < b.npoints; i++) offs[size_t(i) + 1] += offs[size_t(i)];
+
+  P.d_pt = upload_vec(flat);
+  P.d_pos = upload_vec(P.h_pos);
+  P.d_mat = upload_vec(mat4);
+  P.d_coeff = upload_vec(coeff4);
+  P.d_coeff32 = upload_vec(coeff4f);
+  P.d_npts = upload_vec(P.h_npts);
+  P.d_offs = upload_vec(offs);
+  P.d_hit = upload_vec(hit);
+  INQB_CUDA(cudaMalloc(&P.d_gcoef, sizeof(double2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4)));
+  INQB_CUDA(cudaMalloc(&P.d_gcoef32, sizeof(float2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4)));
+  INQB_CUDA(cudaMalloc(&P.d_hcoef, sizeof(double2) * std::max<size_t>(1, size_t(P.total) * 4)));
+  INQB_CUDA(cudaMalloc(&P.d_hcoef32, sizeof(float2) * std::max<size_t>(1, size_t(P.total) * 4)));
+  P.kA[0] = P.kA[1] = P.kA[2] = 1e300;  // tables are built on first use for a given k + A
+}
+
+}  // namespace
+
+// ============================================================================ C ABI
+
+extern "C" {
+
+int inqb_ctx_create(int device, inqb_ctx **out) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(out != nullptr, INQB_ERR_ARG, "null output handle");
+    int ndev = 0;
+    INQB_CUDA(cudaGetDeviceCount(&ndev));
+    INQB_REQUIRE(device >= 0 && device < ndev, INQB_ERR_ARG, "no such CUDA device");
+    INQB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    INQB_CUDA(cudaGetDeviceProperties(&prop, device));
+    INQB_REQUIRE(prop.major >= 10, INQB_ERR_UNSUPPORTED,
+                 "libinqb200 is built for sm_100a (B200); this device is sm_" + std::to_string(prop.major) +
+                     std::to_string(prop.minor));
+    auto *c = new inqb_ctx();
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    c->max_smem_optin = prop.sharedMemPerBlockOptin;
+    INQB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    *out = c;
+  });
+}
+
+int inqb_ctx_destroy(inqb_ctx *ctx) {
+  if (!ctx) return INQB_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return INQB_OK;
+}
+
+const char *inqb_last_error(const inqb_ctx *ctx) { return ctx ? ctx->err.c_str() : g_err_noctx.c_str(); }
+
+int inqb_ctx_synchronize(inqb_ctx *ctx) {
+  return guarded(ctx, [&] {
+    set_device(*ctx);
+    INQB_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int inqb_ctx_stream(inqb_ctx *ctx, void **stream) {
+  return guarded(ctx, [&] { *stream = reinterpret_cast<void *>(ctx->stream); });
+}
+
+int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count) {
+  return guarded(ctx, [&] { *count = ctx->launches; });
+}
+
+int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes) {
+  return guarded(ctx, [&] {
+    set_device(*ctx);
+    INQB_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
+  });
+}
+
+int inqb_basis_create(inqb_ctx *ctx, const double lattice[9], int nx, int ny, int nz, inqb_basis **out) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && lattice && out, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(nx > 0 && ny > 0 && nz > 0, INQB_ERR_ARG, "grid sizes must be positive");
+    set_device(*ctx);
+    auto *b = new inqb_basis();
+    try {
+      b->ctx = ctx;
+      basis_metric(lattice, b->lat, b->rec, b->rlat, b->volume);
+      b->n[0] = nx;
+      b->n[1] = ny;
+      b->n[2] = nz;
+      b->npoints = (long long)nx * ny * nz;
+      for (int ax = 0; ax < 3; ax++) {
+        const int n = b->n[ax];
+        b->radices[ax] = fft_radices(n);
+        std::vector<double2> t64(n);
+        std::vector<float2> t32(n);
+        const long double two_pi = 6.283185307179586476925286766559005768L;
+        for (int t = 0; t < n; t++) {
+          const long double ang = two_pi * (long double)t / (long double)n;
+          t64[t] = make_double2(double(cosl(ang)), double(-sinl(ang)));
+          t32[t] = make_float2(float(cosl(ang)), float(-sinl(ang)));
+        }
+        INQB_CUDA(cudaMalloc(&b->tw64[ax], sizeof(double2) * n));
+        INQB_CUDA(cudaMalloc(&b->tw32[ax], sizeof(float2) * n));
+        INQB_CUDA(cudaMemcpy(b->tw64[ax], t64.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+        INQB_CUDA(cudaMemcpy(b->tw32[ax], t32.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+      }
+    } catch (...) {
+      for (int ax = 0; ax < 3; ax++) {
+        if (b->tw64[ax]) cudaFree(b->tw64[ax]);
+        if (b->tw32[ax]) cudaFree(b->tw32[ax]);
+      }
+      delete b;
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int inqb_basis_destroy(inqb_basis *b) {
+  if (!b) return INQB_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  for (int ax = 0; ax < 3; ax++) {
+    if (b->tw64[ax]) cudaFree(b->tw64[ax]);
+    if (b->tw32[ax]) cudaFree(b->tw32[ax]);
+  }
+  delete b;
+  return INQB_OK;
+}
+
+int inqb_basis_volume_element(const inqb_basis *b, double *dv) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    INQB_REQUIRE(b && dv, INQB_ERR_ARG, "null argument");
+    *dv = b->volume / double(b->npoints);
+  });
+}
+
+int inqb_orbitals_create(inqb_ctx *ctx, const inqb_basis *basis, int nst, int spinor_dim, const double kpoint_cov[3],
+                         int spin_index, int space, int precision, inqb_orbitals **out) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && basis && out, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(nst > 0, INQB_ERR_ARG, "number of states must be positive");
+    INQB_REQUIRE(spinor_dim == 1, INQB_ERR_UNSUPPORTED, "spinor orbital sets are not implemented");
+    INQB_REQUIRE(space == INQB_REAL_SPACE || space == INQB_FOURIER_SPACE, INQB_ERR_ARG, "bad space tag");
+    INQB_REQUIRE(precision == INQB_F64 || precision == INQB_F32, INQB_ERR_ARG, "bad precision tag");
+    INQB_REQUIRE(spin_index >= 0, INQB_ERR_ARG, "bad spin index");
+    set_device(*ctx);
+    auto *o = new inqb_orbitals();
+    o->ctx = ctx;
+    o->basis = basis;
+    o->nst = nst;
+    for (int i = 0; i < 3; i++) o->kpoint[i] = kpoint_cov ? kpoint_cov[i] : 0.0;
+    o->spin_index = spin_index;
+    o->space = space;
+    o->precision = precision;
+    cudaError_t e = cudaMalloc(&o->data, o->bytes());
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      delete o;
+      throw Error(INQB_ERR_MEMORY, "device allocation of an orbital set failed: " + std::string(cudaGetErrorString(e)));
+    }
+    *out = o;
+  });
+}
+
+int inqb_orbitals_destroy(inqb_orbitals *o) {
+  if (!o) return INQB_OK;
+  cudaSetDevice(o->ctx->device);
+  cudaStreamSynchronize(o->ctx->stream);
+  if (o->data) cudaFree(o->data);
+  delete o;
+  return INQB_OK;
+}
+
+int inqb_orbitals_upload(inqb_orbitals *o, const void *host) {
+  return guarded(o ? o->ctx : nullptr, [&] {
+    INQB_REQUIRE(o && host, INQB_ERR_ARG, "null argument");
+    set_device(*o->ctx);
+    INQB_CUDA(cudaMemcpyAsync(o->data, host, o->bytes(), cudaMemcpyHostToDevice, o->ctx->stream));
+    INQB_CUDA(cudaStreamSynchronize(o->ctx->stream));
+  });
+}
+
+int inqb_orbitals_download(const inqb_orbitals *o, void *host) {
+  return guarded(o ? o->ctx : nullptr, [&] {
+    INQB_REQUIRE(o && host, INQB_ERR_ARG, "null argument");
+    set_device(*o->ctx);
+    INQB_CUDA(cudaMemcpyAsync(host, o->data, o->bytes(), cudaMemcpyDeviceToHost, o->ctx->stream));
+    INQB_CUDA(cudaStreamSynchronize(o->ctx->stream));
+  });
+}
+
+int inqb_orbitals_device_ptr(const inqb_orbitals *o, void **ptr) {
+  return guarded(o ? o->ctx : nullptr, [&] {
+    INQB_REQUIRE(o && ptr, INQB_ERR_ARG, "null argument");
+    *ptr = o->data;
+  });
+}
+
+int inqb_orbitals_copy(const inqb_orbitals *src, inqb_orbitals *dst) {
+  return guarded(src ? src->ctx : nullptr, [&] {
+    INQB_REQUIRE(src && dst, INQB_ERR_ARG, "null argument");
+    set_device(*src->ctx);
+    copy_set(*src, *dst);
+    for (int i = 0; i < 3; i++) dst->kpoint[i] = src->kpoint[i];
+    dst->spin_index = src->spin_index;
+  });
+}
+
+int inqb_orbitals_fill(inqb_orbitals *o, double re, double im) {
+  return guarded(o ? o->ctx : nullptr, [&] {
+    INQB_REQUIRE(o, INQB_ERR_ARG, "null argument");
+    set_device(*o->ctx);
+    const long long n = o->basis->npoints * o->nst;
+    if (o->precision == INQB_F64) launch_fill<double>(*o->ctx, static_cast<double2 *>(o->data), n, re, im);
+    else launch_fill<float>(*o->ctx, static_cast<float2 *>(o->data), n, re, im);
+  });
+}
+
+int inqb_orbitals_set_space(inqb_orbitals *o, int space) {
+  return guarded(o ? o->ctx : nullptr, [&] {
+    INQB_REQUIRE(o && (space == INQB_REAL_SPACE || space == INQB_FOURIER_SPACE), INQB_ERR_ARG, "bad argument");
+    o->space = space;
+  });
+}
+
+int inqb_orbitals_info(const inqb_orbitals *o, int *nst, int *space, int *precision, long long *npoint) {
+  return guarded(o ? o->ctx : nullptr, [&] {
+    INQB_REQUIRE(o, INQB_ERR_ARG, "null argument");
+    if (nst) *nst = o->nst;
+    if (space) *space = o->space;
+    if (precision) *precision = o->precision;
+    if (npoint) *npoint = o->basis->npoints;
+  });
+}
+
+int inqb_orbitals_randomize_gsphere(inqb_orbitals *o, uint64_t seed, double ecut) {
+  return guarded(o ? o->ctx : nullptr, [&] {
+    INQB_REQUIRE(o, INQB_ERR_ARG, "null argument");
+    set_device(*o->ctx);
+    if (o->precision == INQB_F64)
+      launch_randomize_gsphere<double>(*o->ctx, *o->basis, static_cast<double2 *>(o->data), o->nst, seed, ecut);
+    else
+      launch_randomize_gsphere<float>(*o->ctx, *o->basis, static_cast<float2 *>(o->data), o->nst, seed, ecut);
+    o->space = INQB_FOURIER_SPACE;
+  });
+}
+
+int inqb_orbitals_convert(const inqb_orbitals *src, inqb_orbitals *dst) {
+  return guarded(src ? src->ctx : nullptr, [&] {
+    INQB_REQUIRE(src && dst, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(src->basis == dst->basis && src->nst == dst->nst, INQB_ERR_ARG, "conversion between different shapes");
+    set_device(*src->ctx);
+    launch_convert(*src->ctx, src->data, src->precision, dst->data, dst->precision, src->basis->npoints * src->nst);
+    dst->space = src->space;
+    for (int i = 0; i < 3; i++) dst->kpoint[i] = src->kpoint[i];
+    dst->spin_index = src->spin_index;
+  });
+}
+
+int inqb_to_fourier(const inqb_orbitals *in, inqb_orbitals *out) {
+  return guarded(in ? in->ctx : nullptr, [&] {
+    INQB_REQUIRE(in && out, INQB_ERR_ARG, "null argument");
+    check_same_shape(*in, *out);
+    INQB_REQUIRE(in->space == INQB_REAL_SPACE, INQB_ERR_ARG, "to_fourier needs a real-space set");
+    set_device(*in->ctx);
+    if (in->precision == INQB_F64)
+      fft3d<double>(*in->ctx, *in->basis, static_cast<const double2 *>(in->data), static_cast<double2 *>(out->data),
+                    in->nst, +1, 1.0);
+    else
+      fft3d<float>(*in->ctx, *in->basis, static_cast<const float2 *>(in->data), static_cast<float2 *>(out->data),
+                   in->nst, +1, 1.0f);
+    out->space = INQB_FOURIER_SPACE;
+    for (int i = 0; i < 3; i++) out->kpoint[i] = in->kpoint[i];
+    out->spin_index = in->spin_index;
+  });
+}
+
+int inqb_to_real(const inqb_orbitals *in, inqb_orbitals *out, int normalize) {
+  return guarded(in ? in->ctx : nullptr, [&] {
+    INQB_REQUIRE(in && out, INQB_ERR_ARG, "null argument");
+    check_same_shape(*in, *out);
+    INQB_REQUIRE(in->space == INQB_FOURIER_SPACE, INQB_ERR_ARG, "to_real needs a Fourier-space set");
+    set_device(*in->ctx);
+    const double sc = normalize ? 1.0 / double(in->basis->npoints) : 1.0;
+    if (in->precision == INQB_F64)
+      fft3d<double>(*in->ctx, *in->basis, static_cast<const double2 *>(in->data), static_cast<double2 *>(out->data),
+                    in->nst, -1, sc);
+    else
+      fft3d<float>(*in->ctx, *in->basis, static_cast<const float2 *>(in->data), static_cast<float2 *>(out->data),
+                   in->nst, -1, float(sc));
+    out->space = INQB_REAL_SPACE;
+    for (int i = 0; i < 3; i++) out->kpoint[i] = in->kpoint[i];
+    out->spin_index = in->spin_index;
+  });
+}
+
+int inqb_laplacian(const inqb_orbitals *in, inqb_orbitals *out, double factor, const double gradcoeff_contra[3]) {
+  return guarded(in ? in->ctx : nullptr, [&] {
+    INQB_REQUIRE(in && out, INQB_ERR_ARG, "null argument");
+    check_same_shape(*in, *out);
+    INQB_REQUIRE(in->space == INQB_FOURIER_SPACE, INQB_ERR_ARG, "laplacian is implemented for Fourier-space sets");
+    set_device(*in->ctx);
+    double gc[3] = {0, 0, 0};
+    if (gradcoeff_contra)
+      for (int i = 0; i < 3; i++) gc[i] = gradcoeff_contra[i];
+    if (in->precision == INQB_F64)
+      launch_laplacian<double>(*in->ctx, *in->basis, static_cast<const double2 *>(in->data),
+                               static_cast<double2 *>(out->data), in->nst, factor, gc);
+    else
+      launch_laplacian<float>(*in->ctx, *in->basis, static_cast<const float2 *>(in->data),
+                              static_cast<float2 *>(out->data), in->nst, factor, gc);
+    out->space = INQB_FOURIER_SPACE;
+  });
+}
+
+int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, inqb_hamiltonian **out) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && basis && out, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(nspin >= 1 && nspin <= 2, INQB_ERR_UNSUPPORTED, "nspin must be 1 or 2");
+    set_device(*ctx);
+    auto *h = new inqb_hamiltonian();
+    h->ctx = ctx;
+    h->basis = basis;
+    h->nspin = nspin;
+    const size_t nv = size_t(basis->npoints) * nspin;
+    INQB_CUDA(cudaMalloc(&h->d_V, sizeof(double) * nv));
+    INQB_CUDA(cudaMalloc(&h->d_V32, sizeof(float) * nv));
+    INQB_CUDA(cudaMemsetAsync(h->d_V, 0, sizeof(double) * nv, ctx->stream));
+    INQB_CUDA(cudaMemsetAsync(h->d_V32, 0, sizeof(float) * nv, ctx->stream));
+    INQB_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = h;
+  });
+}
+
+int inqb_hamiltonian_destroy(inqb_hamiltonian *h) {
+  if (!h) return INQB_OK;
+  cudaSetDevice(h->ctx->device);
+  cudaStreamSynchronize(h->ctx->stream);
+  free_projectors(h->proj);
+  if (h->d_V) cudaFree(h->d_V);
+  if (h->d_V32) cudaFree(h->d_V32);
+  if (h->d_projraw) cudaFree(h->d_projraw);
+  if (h->d_projD) cudaFree(h->d_projD);
+  delete h;
+  return INQB_OK;
+}
+
+int inqb_potential_set(inqb_hamiltonian *h, const double *V) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && V, INQB_ERR_ARG, "null argument");
+    set_device(*h->ctx);
+    const size_t nv = size_t(h->basis->npoints) * h->nspin;
+    std::vector<float> v32(V, V + nv);
+    INQB_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    INQB_CUDA(cudaMemcpy(h->d_V, V, sizeof(double) * nv, cudaMemcpyHostToDevice));
+    INQB_CUDA(cudaMemcpy(h->d_V32, v32.data(), sizeof(float) * nv, cudaMemcpyHostToDevice));
+  });
+}
+
+int inqb_vector_potential_set(inqb_hamiltonian *h, const double A_cov[3]) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && A_cov, INQB_ERR_ARG, "null argument");
+    for (int i = 0; i < 3; i++) h->A[i] = A_cov[i];
+  });
+}
+
+int inqb_projectors_set(inqb_hamiltonian *h, int nproj, int maxsph, int maxnlm, const int32_t *points, const float *pos,
+                        const double *matrices, const double *coeff, const int32_t *npts, const int32_t *nlm) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(nproj == 0 || (points && pos && matrices && coeff && npts && nlm), INQB_ERR_ARG, "null table");
+    set_device(*h->ctx);
+    set_projectors(*h, nproj, maxsph, maxnlm, points, pos, matrices, coeff, npts, nlm);
+  });
+}
+
+int inqb_projectors_build_gaussian(inqb_hamiltonian *h, int natoms, const double *positions, double radius, double rc,
+                                   const double *kb) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && (natoms == 0 || (positions && kb)), INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(radius > 0.0 && rc > 0.0, INQB_ERR_ARG, "radius and rc must be positive");
+    set_device(*h->ctx);
+    std::vector<SphereList> sph(natoms);
+    int maxsph = 0;
+    for (int a = 0; a < natoms; a++) {
+      spherical_grid_build(*h->basis, positions + 3 * a, radius, sph[a]);
+      maxsph = std::max<int>(maxsph, int(sph[a].points.size()));
+    }
+    std::vector<int32_t> points(size_t(natoms) * maxsph * 3, -1), npts(natoms), nlm(natoms, 4);
+    std::vector<float> pos(size_t(natoms) * maxsph * 3, 0.0f);
+    std::vector<double> mats(size_t(natoms) * 4 * maxsph, 0.0);
+    for (int a = 0; a < natoms; a++) {
+      const size_t n = sph[a].points.size();
+      npts[a] = int(n);
+      std::vector<double> m;
+      gaussian_projector_values(*h->basis, sph[a], rc, m);
+      for (size_t i = 0; i < n; i++) {
+        for (int d = 0; d < 3; d++) {
+          points[(size_t(a) * maxsph + i) * 3 + d] = sph[a].points[i][d];
+          pos[(size_t(a) * maxsph + i) * 3 + d] = sph[a].relpos[i][d];
+        }
+        for (int l = 0; l < 4; l++) mats[(size_t(a) * 4 + l) * maxsph + i] = m[l * n + i];
+      }
+    }
+    set_projectors(*h, natoms, maxsph, 4, points.data(), pos.data(), mats.data(), kb, npts.data(), nlm.data());
+  });
+}
+
+int inqb_spherical_grid(const double lattice[9], int nx, int ny, int nz, const double center[3], double radius,
+                        long long capacity, int32_t *points, float *distance, float *relpos, long long *npoints) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(lattice && center && npoints, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(nx > 0 && ny > 0 && nz > 0 && radius >= 0.0, INQB_ERR_ARG, "bad grid or radius");
+    Basis b;
+    basis_metric(lattice, b.lat, b.rec, b.rlat, b.volume);
+    b.n[0] = nx;
+    b.n[1] = ny;
+    b.n[2] = nz;
+    b.npoints = (long long)nx * ny * nz;
+    SphereList sph;
+    spherical_grid_build(b, center, radius, sph);
+    const long long n = (long long)sph.points.size();
+    *npoints = n;
+    INQB_REQUIRE(n <= capacity, INQB_ERR_ARG, "capacity too small for the sphere");
+    for (long long i = 0; i < n; i++) {
+      for (int d = 0; d < 3; d++) {
+        if (points) points[i * 3 + d] = sph.points[size_t(i)][d];
+        if (relpos) relpos[i * 3 + d] = sph.relpos[size_t(i)][d];
+      }
+      if (distance) distance[i] = sph.distance[size_t(i)];
+    }
+  });
+}
+
+int inqb_projectors_info(const inqb_hamiltonian *h, int *nproj, int *maxsph, long long *total_points) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h, INQB_ERR_ARG, "null argument");
+    if (nproj) *nproj = h->proj.nproj;
+    if (maxsph) *maxsph = h->proj.maxsph;
+    if (total_points) *total_points = h->proj.total;
+  });
+}
+
+int inqb_projectors_get(const inqb_hamiltonian *h, int32_t *points, float *pos, double *matrices, int32_t *npts) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h, INQB_ERR_ARG, "null argument");
+    const Projectors &P = h->proj;
+    if (points) std::copy(P.h_points.begin(), P.h_points.end(), points);
+    if (pos) std::copy(P.h_pos.begin(), P.h_pos.end(), pos);
+    if (matrices) std::copy(P.h_mat.begin(), P.h_mat.end(), matrices);
+    if (npts) std::copy(P.h_npts.begin(), P.h_npts.end(), npts);
+  });
+}
+
+int inqb_apply(const inqb_hamiltonian *hc, const inqb_orbitals *in, inqb_orbitals *out) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && in && out, INQB_ERR_ARG, "null argument");
+    set_device(*h->ctx);
+    apply_any(*h, *in, *out);
+  });
+}
+
+int inqb_non_local(const inqb_hamiltonian *hc, const inqb_orbitals *in, inqb_orbitals *out) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && in && out, INQB_ERR_ARG, "null argument");
+    check_same_shape(*in, *out);
+    INQB_REQUIRE(in->space == INQB_REAL_SPACE, INQB_ERR_ARG, "non_local needs a real-space set");
+    set_device(*h->ctx);
+    Ctx &ctx = *h->ctx;
+    const long long n = h->basis->npoints * in->nst;
+    if (h->proj.nproj == 0) {
+      if (in->precision == INQB_F64) launch_fill<double>(ctx, static_cast<double2 *>(out->data), n, 0, 0);
+      else launch_fill<float>(ctx, static_cast<float2 *>(out->data), n, 0, 0);
+      return;
+    }
+    double kA[3] = {in->kpoint[0] + h->A[0], in->kpoint[1] + h->A[1], in->kpoint[2] + h->A[2]};
+    ensure_tables(*h, kA);
+    if (in->precision == INQB_F64) {
+      auto *praw = proj_buf<double>(*h, in->nst, 0);
+      auto *pd = proj_buf<double>(*h, in->nst, 1);
+      launch_nl_project<double>(ctx, *h->basis, *h, static_cast<const double2 *>(in->data), in->nst, praw, pd);
+      launch_nl_scatter<double>(ctx, *h->basis, *h, pd, in->nst, static_cast<double2 *>(out->data));
+    } else {
+      auto *praw = proj_buf<float>(*h, in->nst, 0);
+      auto *pd = proj_buf<float>(*h, in->nst, 1);
+      launch_nl_project<float>(ctx, *h->basis, *h, static_cast<const float2 *>(in->data), in->nst, praw, pd);
+      launch_nl_scatter<float>(ctx, *h->basis, *h, pd, in->nst, static_cast<float2 *>(out->data));
+    }
+    out->space = INQB_REAL_SPACE;
+  });
+}
+
+int inqb_non_local_energy(const inqb_hamiltonian *hc, const inqb_orbitals *phi, const double *occ, double *energy) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && phi && occ && energy, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(phi->space == INQB_REAL_SPACE, INQB_ERR_ARG, "non_local_energy needs a real-space set");
+    set_device(*h->ctx);
+    Ctx &ctx = *h->ctx;
+    *energy = 0.0;
+    if (h->proj.nproj == 0) return;
+    const int S = phi->nst;
+    double kA[3] = {phi->kpoint[0] + h->A[0], phi->kpoint[1] + h->A[1], phi->kpoint[2] + h->A[2]};
+    ensure_tables(*h, kA);
+    const size_t n = size_t(h->proj.nproj) * 4 * S;
+    std::vector<double> pr, pd;
+    if (phi->precision == INQB_F64) {
+      auto *praw = proj_buf<double>(*h, S, 0);
+      auto *pD = proj_buf<double>(*h, S, 1);
+      launch_nl_project<double>(ctx, *h->basis, *h, static_cast<const double2 *>(phi->data), S, praw, pD);
+      pr = download<double>(ctx, praw, 2 * n);
+      pd = download<double>(ctx, pD, 2 * n);
+    } else {
+      auto *praw = proj_buf<float>(*h, S, 0);
+      auto *pD = proj_buf<float>(*h, S, 1);
+      launch_nl_project<float>(ctx, *h->basis, *h, static_cast<const float2 *>(phi->data), S, praw, pD);
+      auto a = download<float>(ctx, praw, 2 * n), b = download<float>(ctx, pD, 2 * n);
+      pr.assign(a.begin(), a.end());
+      pd.assign(b.begin(), b.end());
+    }
+    // projector_all::energy (projector_all.hpp:306-327): sum f_s Re(conj(p) D p)
+    double en = 0.0;
+    for (size_t k = 0; k < n; k++) {
+      const int s = int(k % S);
+      en += occ[s] * (pr[2 * k] * pd[2 * k] + pr[2 * k + 1] * pd[2 * k + 1]);
+    }
+    *energy = en;
+  });
+}
+
+int inqb_kinetic_expectation_value(const inqb_hamiltonian *hc, const inqb_orbitals *phi, double *out) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && phi && out, INQB_ERR_ARG, "null argument");
+    set_device(*h->ctx);
+    Ctx &ctx = *h->ctx;
+    const Basis &b = *h->basis;
+    const int S = phi->nst;
+    double kA[3] = {phi->kpoint[0] + h->A[0], phi->kpoint[1] + h->A[1], phi->kpoint[2] + h->A[2]};
+    double kt[3], kc[3];
+    cov_to_cart(b, kA, kt);
+    cart_to_contra(b, kt, kc);
+    double gc[3] = {-2.0 * kc[0], -2.0 * kc[1], -2.0 * kc[2]};
+    double gcart[3];
+    contra_to_cart(b, gc, gcart);
+    const double k2 = -0.25 * (gcart[0] * gcart[0] + gcart[1] * gcart[1] + gcart[2] * gcart[2]);
+    const double fac = -0.5 * (b.volume / (double(b.npoints) * double(b.npoints)));
+    double *d_out = static_cast<double *>(dev_alloc(ctx, sizeof(double) * S));
+    if (phi->space == INQB_REAL_SPACE) {
+      TempSet f(*phi);
+      if (phi->precision == INQB_F64) {
+        fft3d<double>(ctx, b, static_cast<const double2 *>(phi->data), static_cast<double2 *>(f.o.data), S, +1, 1.0);
+        launch_kinetic_ev<double>(ctx, b, static_cast<const double2 *>(f.o.data), S, fac, gc, k2, d_out);
+      } else {
+        fft3d<float>(ctx, b, static_cast<const float2 *>(phi->data), static_cast<float2 *>(f.o.data), S, +1, 1.0f);
+        launch_kinetic_ev<float>(ctx, b, static_cast<const float2 *>(f.o.data), S, fac, gc, k2, d_out);
+      }
+    } else {
+      if (phi->precision == INQB_F64)
+        launch_kinetic_ev<double>(ctx, b, static_cast<const double2 *>(phi->data), S, fac, gc, k2, d_out);
+      else
+        launch_kinetic_ev<float>(ctx, b, static_cast<const float2 *>(phi->data), S, fac, gc, k2, d_out);
+    }
+    auto v = download<double>(ctx, d_out, S);
+    std::copy(v.begin(), v.end(), out);
+    dev_free(ctx, d_out);
+  });
+}
+
+int inqb_overlap(const inqb_orbitals *a, const inqb_orbitals *b, double *out) {
+  return guarded(a ? a->ctx : nullptr, [&] {
+    INQB_REQUIRE(a && b && out, INQB_ERR_ARG, "null argument");
+    set_device(*a->ctx);
+    Ctx &ctx = *a->ctx;
+    double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * a->nst * b->nst));
+    overlap_dev(*a, *b, d);
+    auto v = download<double>(ctx, d, size_t(2) * a->nst * b->nst);
+    std::copy(v.begin(), v.end(), out);
+    dev_free(ctx, d);
+  });
+}
+
+int inqb_overlap_diagonal(const inqb_orbitals *a, const inqb_orbitals *b, double *out) {
+  return guarded(a ? a->ctx : nullptr, [&] {
+    INQB_REQUIRE(a && b && out, INQB_ERR_ARG, "null argument");
+    set_device(*a->ctx);
+    Ctx &ctx = *a->ctx;
+    double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * a->nst));
+    ovdiag_dev(*a, *b, d);
+    auto v = download<double>(ctx, d, size_t(2) * a->nst);
+    std::copy(v.begin(), v.end(), out);
+    dev_free(ctx, d);
+  });
+}
+
+int inqb_orthogonalize(inqb_orbitals *phi) {
+  return guarded(phi ? phi->ctx : nullptr, [&] {
+    INQB_REQUIRE(phi, INQB_ERR_ARG, "null argument");
+    set_device(*phi->ctx);
+    Ctx &ctx = *phi->ctx;
+    const int S = phi->nst;
+    double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * S * S));
+    overlap_dev(*phi, *phi, d);
+    auto Sh = download<std::complex<double>>(ctx, d, size_t(S) * S);
+    std::vector<std::complex<double>> X(size_t(S) * S);
+    cholesky_inverse(S, Sh.data(), X.data());
+    INQB_CUDA(cudaMemcpyAsync(d, X.data(), sizeof(double2) * S * S, cudaMemcpyHostToDevice, ctx.stream));
+    rotate_dev(*phi, d);
+    dev_free(ctx, d);
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+  });
+}
+
+int inqb_shift(double re, double im, const inqb_orbitals *chi, inqb_orbitals *phi) {
+  return guarded(phi ? phi->ctx : nullptr, [&] {
+    INQB_REQUIRE(chi && phi, INQB_ERR_ARG, "null argument");
+    check_same_shape(*chi, *phi);
+    set_device(*phi->ctx);
+    const long long n = phi->basis->npoints * phi->nst;
+    if (phi->precision == INQB_F64)
+      launch_axpy<double>(*phi->ctx, static_cast<double2 *>(phi->data), static_cast<const double2 *>(chi->data), n, re,
+                          im);
+    else
+      launch_axpy<float>(*phi->ctx, static_cast<float2 *>(phi->data), static_cast<const float2 *>(chi->data), n, re, im);
+  });
+}
+
+int inqb_rotate(inqb_orbitals *phi, const double *R) {
+  return guarded(phi ? phi->ctx : nullptr, [&] {
+    INQB_REQUIRE(phi && R, INQB_ERR_ARG, "null argument");
+    set_device(*phi->ctx);
+    Ctx &ctx = *phi->ctx;
+    const int S = phi->nst;
+    double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * S * S));
+    INQB_CUDA(cudaMemcpyAsync(d, R, sizeof(double2) * S * S, cudaMemcpyHostToDevice, ctx.stream));
+    rotate_dev(*phi, d);
+    dev_free(ctx, d);
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+  });
+}
+
+int inqb_eigenvalues(const inqb_hamiltonian *hc, const inqb_orbitals *phi, double *eig, double *normres) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && phi && eig, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(phi->space == INQB_REAL_SPACE, INQB_ERR_ARG, "eigenvalues need a real-space set");
+    set_device(*h->ctx);
+    Ctx &ctx = *h->ctx;
+    const int S = phi->nst;
+    TempSet hp(*phi);
+    apply_any(*h, *phi, hp.o);
+    double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * 2 * S));
+    ovdiag_dev(*phi, *phi, d);
+    ovdiag_dev(*phi, hp.o, d + S);
+    auto v = download<double2>(ctx, d, size_t(2) * S);
+    std::vector<double> e(S);
+    for (int s = 0; s < S; s++) e[s] = v[S + s].x / v[s].x;  // overlap_diagonal_normalized, real part
+    std::copy(e.begin(), e.end(), eig);
+    if (normres) {
+      double *de = static_cast<double *>(dev_alloc(ctx, sizeof(double) * S));
+      INQB_CUDA(cudaMemcpyAsync(de, e.data(), sizeof(double) * S, cudaMemcpyHostToDevice, ctx.stream));
+      if (phi->precision == INQB_F64)
+        launch_shift_vec<double>(ctx, static_cast<double2 *>(hp.o.data), static_cast<const double2 *>(phi->data), S,
+                                 phi->basis->npoints, de, -1.0);
+      else
+        launch_shift_vec<float>(ctx, static_cast<float2 *>(hp.o.data), static_cast<const float2 *>(phi->data), S,
+                                phi->basis->npoints, de, -1.0);
+      ovdiag_dev(hp.o, hp.o, d);
+      auto r = download<double2>(ctx, d, size_t(S));
+      for (int s = 0; s < S; s++) normres[s] = r[s].x;
+      dev_free(ctx, de);
+    }
+    dev_free(ctx, d);
+  });
+}
+
+int inqb_exponential_in_place(const inqb_hamiltonian *hc, double re, double im, inqb_orbitals *phi, int order) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && phi, INQB_ERR_ARG, "null argument");
+    set_device(*h->ctx);
+    exponential(*h, 0.0, std::complex<double>(re, im), *phi, nullptr, order);
+  });
+}
+
+int inqb_exponential_2_for_1(const inqb_hamiltonian *hc, double f1_re, double f1_im, double f2_re, double f2_im,
+                             inqb_orbitals *phi, inqb_orbitals *exp1, int order) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && phi && exp1, INQB_ERR_ARG, "null argument");
+    check_same_shape(*phi, *exp1);
+    set_device(*h->ctx);
+    exponential(*h, std::complex<double>(f1_re, f1_im), std::complex<double>(f2_re, f2_im), *phi, exp1, order);
+  });
+}
+
+int inqb_density(inqb_orbitals *const *phis, int nsets, const double *const *occ, double *density_host) {
+  Ctx *ctx = (phis && nsets > 0 && phis[0]) ? phis[0]->ctx : nullptr;
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && occ && density_host, INQB_ERR_ARG, "null argument");
+    set_device(*ctx);
+    const Basis &b = *phis[0]->basis;
+    double *d = static_cast<double *>(dev_alloc(*ctx, sizeof(double) * b.npoints));
+    density_dev(*ctx, phis, nsets, occ, d);
+    INQB_CUDA(cudaMemcpyAsync(density_host, d, sizeof(double) * b.npoints, cudaMemcpyDeviceToHost, ctx->stream));
+    dev_free(*ctx, d);
+    INQB_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int inqb_kick(inqb_orbitals *phi, const double efield_cart[3]) {
+  return guarded(phi ? phi->ctx : nullptr, [&] {
+    INQB_REQUIRE(phi && efield_cart, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(phi->space == INQB_REAL_SPACE, INQB_ERR_ARG, "kick needs a real-space set");
+    set_device(*phi->ctx);
+    double ecov[3];
+    cart_to_cov(*phi->basis, efield_cart, ecov);
+    if (phi->precision == INQB_F64)
+      launch_kick<double>(*phi->ctx, *phi->basis, static_cast<double2 *>(phi->data), phi->nst, ecov);
+    else
+      launch_kick<float>(*phi->ctx, *phi->basis, static_cast<float2 *>(phi->data), phi->nst, ecov);
+  });
+}
+
+int inqb_dipole(const inqb_basis *b, const double *density_host, double dipole[3]) {
+  return guarded(b ? b->ctx : nullptr, [&] {
+    INQB_REQUIRE(b && density_host && dipole, INQB_ERR_ARG, "null argument");
+    dipole_host(*b, density_host, dipole);
+  });
+}
+
+int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int nsets, const double *const *occ,
+                   double dt, int nscf_max, double scf_threshold, double *density_host, double dipole[3],
+                   int *iterations) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && phis && nsets > 0 && occ, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(nscf_max >= 1, INQB_ERR_ARG, "nscf_max must be >= 1");
+    set_device(*h->ctx);
+    Ctx &ctx = *h->ctx;
+    const Basis &b = *h->basis;
+    // etrs.hpp:33-40: half step saved, full step predicted, both from one set of H^n phi
+    std::vector<std::unique_ptr<TempSet>> save;
+    for (int k = 0; k < nsets; k++) {
+      save.emplace_back(new TempSet(*phis[k]));
+      exponential(*h, std::complex<double>(0.0, -dt / 2.0), std::complex<double>(0.0, -dt), *phis[k], &save[k]->o, 4);
+    }
+    double *dens = static_cast<double *>(dev_alloc(ctx, sizeof(double) * b.npoints));
+    double *old = static_cast<double *>(dev_alloc(ctx, sizeof(double) * b.npoints));
+    double *delta_dev = static_cast<double *>(dev_alloc(ctx, sizeof(double)));
+    density_dev(ctx, phis, nsets, occ, dens);
+    // (the Hamiltonian is fixed: update_hamiltonian of etrs.hpp:51 has nothing to update)
+    int it = 0;
+    for (int iscf = 0; iscf < nscf_max; iscf++) {
+      for (int k = 0; k < nsets; k++) {
+        copy_set(save[k]->o, *phis[k]);  // restore (etrs.hpp:54-56) and phi = save (etrs.hpp:63)
+        exponential(*h, 0.0, std::complex<double>(0.0, -dt / 2.0), *phis[k], nullptr, 4);
+      }
+      std::swap(old, dens);
+      density_dev(ctx, phis, nsets, occ, dens);
+      launch_absdiff_sum(ctx, old, dens, b.npoints, delta_dev);
+      double delta = 0.0;
+      INQB_CUDA(cudaMemcpyAsync(&delta, delta_dev, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+      INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+      delta *= b.volume / double(b.npoints);
+      it = iscf + 1;
+      if (delta < scf_threshold || iscf == nscf_max - 1) break;
+    }
+    if (iterations) *iterations = it;
+    if (density_host || dipole) {
+      std::vector<double> hd(size_t(b.npoints));
+      INQB_CUDA(cudaMemcpyAsync(hd.data(), dens, sizeof(double) * b.npoints, cudaMemcpyDeviceToHost, ctx.stream));
+      INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+      if (density_host) std::copy(hd.begin(), hd.end(), density_host);
+      if (dipole) dipole_host(b, hd.data(), dipole);
+    }
+    dev_free(ctx, dens);
+    dev_free(ctx, old);
+    dev_free(ctx, delta_dev);
+    save.clear();
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+  });
+}
+
+}  // extern "C"

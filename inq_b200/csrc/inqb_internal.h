@@ -1,0 +1,221 @@
+// Internal declarations of libinqb200: handle structs, device helpers, launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/inqb.h"
+
+namespace inqb {
+
+// ------------------------------------------------------------------ errors
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define INQB_CUDA(call)                                                                         \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      throw ::inqb::Error(INQB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define INQB_REQUIRE(cond, code, msg)                     \
+  do {                                                    \
+    if (!(cond)) throw ::inqb::Error((code), (msg));      \
+  } while (0)
+
+// ------------------------------------------------------------------ complex
+
+template <typename R> struct c2_of;
+template <> struct c2_of<double> { using type = double2; };
+template <> struct c2_of<float> { using type = float2; };
+template <typename R> using C2 = typename c2_of<R>::type;
+
+template <typename T> __host__ __device__ __forceinline__ T mk(decltype(T::x) a, decltype(T::x) b) {
+  T r;
+  r.x = a;
+  r.y = b;
+  return r;
+}
+template <typename T> __host__ __device__ __forceinline__ T cadd(T a, T b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T> __host__ __device__ __forceinline__ T csub(T a, T b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T> __host__ __device__ __forceinline__ T cmul(T a, T b) {
+  return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename T> __host__ __device__ __forceinline__ T cconjmul(T a, T b) {  // conj(a) * b
+  return mk<T>(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+template <typename T> __host__ __device__ __forceinline__ T cscale(T a, decltype(T::x) s) {
+  return mk<T>(a.x * s, a.y * s);
+}
+
+// ------------------------------------------------------------------ handles
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long long launches = 0;
+  int num_sms = 0;
+  size_t max_smem_optin = 0;
+};
+
+struct Basis {
+  Ctx *ctx = nullptr;
+  double lat[3][3];      // lattice vectors a_i (rows, cartesian)
+  double rlat[3][3];     // reciprocal / 2pi (cell_metric::rlat_)
+  double rec[3][3];      // reciprocal vectors (cell::reciprocal)
+  double volume = 0.0;
+  int n[3] = {0, 0, 0};
+  long long npoints = 0;
+  // per-axis twiddle tables exp(-2 pi i t / n), t < n
+  void *tw64[3] = {nullptr, nullptr, nullptr};
+  void *tw32[3] = {nullptr, nullptr, nullptr};
+  std::vector<int> radices[3];
+};
+
+struct Orbitals {
+  Ctx *ctx = nullptr;
+  const Basis *basis = nullptr;
+  int nst = 0;
+  double kpoint[3] = {0, 0, 0};
+  int spin_index = 0;
+  int space = INQB_REAL_SPACE;
+  int precision = INQB_F64;
+  void *data = nullptr;
+  size_t bytes() const { return size_t(basis->npoints) * nst * (precision == INQB_F64 ? 16 : 8); }
+};
+
+// Nonlocal projector tables on the device, for one (k + A).
+struct Projectors {
+  int nproj = 0, maxsph = 0, maxnlm = 0;
+  long long total = 0;                   // sum of sphere sizes
+  // host copies (packed, as given)
+  std::vector<int32_t> h_points;         // [nproj][maxsph][3]
+  std::vector<float> h_pos;              // [nproj][maxsph][3]
+  std::vector<double> h_mat;             // [nproj][maxnlm][maxsph]
+  std::vector<double> h_coeff;           // [nproj][maxnlm][maxnlm]
+  std::vector<int32_t> h_npts, h_nlm;
+  // device
+  int *d_pt = nullptr;                   // [nproj][maxsph] flat grid index, -1 pad
+  float *d_pos = nullptr;                // [nproj][maxsph][3]
+  double *d_mat = nullptr;               // [nproj][4][maxsph] (nlm padded to 4)
+  double *d_coeff = nullptr;             // [nproj][4][4]
+  float *d_coeff32 = nullptr;
+  int *d_npts = nullptr;
+  int *d_offs = nullptr;                 // [npoints + 1] CSR of sphere hits per grid point
+  int *d_hit = nullptr;                  // [total] (p * maxsph + i) for each hit, sorted by point then p
+  // (k+A)-dependent coefficient tables
+  double kA[3] = {1e300, 1e300, 1e300};
+  double2 *d_gcoef = nullptr;            // [nproj][maxsph][4]  dV e^{+ik.r} M
+  double2 *d_hcoef = nullptr;            // [total][4]          e^{-ik.r} M
+  float2 *d_gcoef32 = nullptr;
+  float2 *d_hcoef32 = nullptr;
+};
+
+struct Hamiltonian {
+  Ctx *ctx = nullptr;
+  const Basis *basis = nullptr;
+  int nspin = 1;
+  double *d_V = nullptr;                 // [npoints][nspin]
+  float *d_V32 = nullptr;
+  double A[3] = {0, 0, 0};
+  Projectors proj;
+  // device scratch for the projections of the current apply
+  void *d_projraw = nullptr, *d_projD = nullptr;
+  size_t proj_bytes = 0;
+};
+
+// ------------------------------------------------------------------ launchers (kernels.cu)
+
+// One batched 1-D FFT pass over axis `axis` of a [nx][ny][nz][S] array.
+enum Prologue { PRO_NONE = 0, PRO_VPSI = 1 };
+enum Epilogue { EPI_STORE = 0, EPI_FINAL_REAL = 1, EPI_LAPL_ADD = 2 };
+
+template <typename R> struct PassArgs {
+  const C2<R> *in = nullptr;
+  C2<R> *out = nullptr;
+  int S = 0;
+  int axis = 0;
+  int dir = +1;                 // +1 forward (e^{-i}), -1 backward
+  int mid_kinetic = 0;          // forward, multiply by lapl factor, backward (same axis)
+  R scale = R(1);               // applied at the store
+  // lapl factor data: factor*(-|G|^2 + gc.G)
+  double lap_factor = 0.0, gc[3] = {0, 0, 0};
+  // final-real / prologue data
+  const C2<R> *psi = nullptr;   // orbital input for V psi (real form) or lapl-add source (Fourier form)
+  const R *V = nullptr;
+  int nspin = 1, spin = 0;
+  R vshift = R(0);
+  const int *nl_offs = nullptr;
+  const int *nl_hit = nullptr;
+  const C2<R> *nl_hcoef = nullptr;
+  const C2<R> *projD = nullptr;
+  int maxsph = 0;
+  // Taylor accumulators: acc1 += c1 * out, acc2 += c2 * out
+  C2<R> *acc1 = nullptr, *acc2 = nullptr;
+  C2<R> c1, c2;
+};
+
+template <typename R>
+void launch_fft_pass(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue);
+
+template <typename R>
+void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<R> *psi, int S, C2<R> *projraw,
+                       C2<R> *projD);
+void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[3]);
+template <typename R>
+void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out);
+
+template <typename R> void launch_fill(Ctx &ctx, C2<R> *p, long long n, double re, double im);
+template <typename R>
+void launch_axpy(Ctx &ctx, C2<R> *y, const C2<R> *x, long long n, double re, double im);
+template <typename R>
+void launch_laplacian(Ctx &ctx, const Basis &b, const C2<R> *in, C2<R> *out, int S, double factor,
+                      const double gc[3]);
+template <typename R>
+void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, long long npoints, double dv,
+                    double2 *out_dev /*[Sa][Sb]*/);
+template <typename R>
+void launch_overlap_diag(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long long npoints, double dv,
+                         double2 *out_dev /*[S]*/);
+template <typename R>
+void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev);
+template <typename R>
+void launch_density(Ctx &ctx, const C2<R> *phi, int S, long long npoints, const double *occ_dev, double *dens,
+                    int accumulate);
+template <typename R> void launch_kick(Ctx &ctx, const Basis &b, C2<R> *phi, int S, const double ecov[3]);
+template <typename R>
+void launch_shift_vec(Ctx &ctx, C2<R> *y, const C2<R> *x, int S, long long npoints, const double *coef_dev,
+                      double scale);
+template <typename R>
+void launch_kinetic_ev(Ctx &ctx, const Basis &b, const C2<R> *fphi, int S, double factor, const double gc[3],
+                       double k2, double *out_dev /*[S]*/);
+void launch_absdiff_sum(Ctx &ctx, const double *a, const double *b, long long n, double *out_dev);
+template <typename R>
+void launch_randomize_gsphere(Ctx &ctx, const Basis &b, C2<R> *phi, int S, unsigned long long seed, double ecut);
+void launch_convert(Ctx &ctx, const void *in, int in_prec, void *out, int out_prec, long long n);
+
+// ------------------------------------------------------------------ host helpers (host.cpp)
+
+std::vector<int> fft_radices(int n);
+void basis_metric(const double lattice[9], double lat[3][3], double rec[3][3], double rlat[3][3], double &volume);
+
+// scratch allocation on the context stream (stream-ordered pool)
+void *dev_alloc(Ctx &ctx, size_t bytes);
+void dev_free(Ctx &ctx, void *p);
+
+}  // namespace inqb
+
+struct inqb_ctx : inqb::Ctx {};
+struct inqb_basis : inqb::Basis {};
+struct inqb_orbitals : inqb::Orbitals {};
+struct inqb_hamiltonian : inqb::Hamiltonian {};

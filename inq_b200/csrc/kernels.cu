@@ -1,0 +1,663 @@
+// Nonlocal projector kernels and the orbital-set kernels around the FFT passes.
+//
+// Every reduction here has a fixed order (warp shuffles in a fixed tree, per-block
+// partials summed in index order by a second kernel), so results are bitwise
+// reproducible run to run; no floating-point atomics are used anywhere.
+
+#include "inqb_internal.h"
+
+namespace inqb {
+
+static inline unsigned grid_for(long long n, int threads, long long cap = 148LL * 64) {
+  long long g = (n + threads - 1) / threads;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return unsigned(g);
+}
+
+#define LAUNCHED(ctx)                   \
+  do {                                  \
+    INQB_CUDA(cudaGetLastError());      \
+    (ctx).launches++;                   \
+  } while (0)
+
+// ------------------------------------------------------------------ nonlocal tables
+// gcoef[p][i][l] = dV * e^{+i kA.pos} * M[p][l][i]   (gather side, projector_all.hpp:120-128,156)
+// hcoef[h][l]    = e^{-i kA.pos} * M[p][l][i]        (apply side, projector_all.hpp:281-287)
+__global__ void nl_tables_kernel(int nproj, int maxsph, const int *__restrict__ pt, const float *__restrict__ pos,
+                                 const double *__restrict__ mat, double dv, double k0, double k1, double k2,
+                                 double2 *gcoef, float2 *gcoef32) {
+  const long long total = (long long)nproj * maxsph;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int p = int(idx / maxsph), i = int(idx % maxsph);
+    double2 ph = make_double2(0.0, 0.0);
+    if (pt[idx] >= 0) {
+      // dot(kpoint, pos) of the reference: covariant double times float contravariant
+      double arg = k0 * double(pos[idx * 3 + 0]) + k1 * double(pos[idx * 3 + 1]) + k2 * double(pos[idx * 3 + 2]);
+      double sn, cs;
+      sincos(arg, &sn, &cs);
+      ph = make_double2(cs, sn);
+    }
+    for (int l = 0; l < 4; l++) {
+      double m = mat[((long long)p * 4 + l) * maxsph + i];
+      double2 g = make_double2(dv * m * ph.x, dv * m * ph.y);
+      gcoef[idx * 4 + l] = g;
+      gcoef32[idx * 4 + l] = make_float2(float(g.x), float(g.y));
+    }
+  }
+}
+
+__global__ void nl_hit_kernel(long long total, const int *__restrict__ hit, int maxsph, const float *__restrict__ pos,
+                              const double *__restrict__ mat, double k0, double k1, double k2, double2 *hcoef,
+                              float2 *hcoef32) {
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < total;
+       h += (long long)gridDim.x * blockDim.x) {
+    const long long idx = hit[h];
+    const int p = int(idx / maxsph), i = int(idx % maxsph);
+    double arg = k0 * double(pos[idx * 3 + 0]) + k1 * double(pos[idx * 3 + 1]) + k2 * double(pos[idx * 3 + 2]);
+    double sn, cs;
+    sincos(arg, &sn, &cs);
+    for (int l = 0; l < 4; l++) {
+      double m = mat[((long long)p * 4 + l) * maxsph + i];
+      double2 c = make_double2(m * cs, -m * sn);
+      hcoef[h * 4 + l] = c;
+      hcoef32[h * 4 + l] = make_float2(float(c.x), float(c.y));
+    }
+  }
+}
+
+void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[3]) {
+  Projectors &P = h.proj;
+  if (P.nproj == 0 || P.maxsph == 0) return;
+  const double dv = b.volume / double(b.npoints);
+  const long long total = (long long)P.nproj * P.maxsph;
+  nl_tables_kernel<<<grid_for(total, 256), 256, 0, ctx.stream>>>(P.nproj, P.maxsph, P.d_pt, P.d_pos, P.d_mat, dv,
+                                                                 kA[0], kA[1], kA[2], P.d_gcoef, P.d_gcoef32);
+  LAUNCHED(ctx);
+  if (P.total > 0) {
+    nl_hit_kernel<<<grid_for(P.total, 256), 256, 0, ctx.stream>>>(P.total, P.d_hit, P.maxsph, P.d_pos, P.d_mat, kA[0],
+                                                                  kA[1], kA[2], P.d_hcoef, P.d_hcoef32);
+    LAUNCHED(ctx);
+  }
+  for (int i = 0; i < 3; i++) P.kA[i] = kA[i];
+}
+
+// ------------------------------------------------------------------ nonlocal projection
+// proj[p][l][s] = sum_i gcoef[p][i][l] * psi[pt_i][s]; projD = coeff[p] . proj
+// (projector_all.hpp:113-211).  CTA = (projector p, 32 states); 8 warps stride over
+// the sphere points; lanes are consecutive states so each warp load is one contiguous
+// row segment of the state-fastest layout.  The 8 warp partials are summed in order.
+template <typename R>
+__global__ void __launch_bounds__(256) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
+                                                         const int *__restrict__ pt, const C2<R> *__restrict__ gcoef,
+                                                         const int *__restrict__ npts, const R *__restrict__ coeff,
+                                                         int maxsph, C2<R> *projraw, C2<R> *projD) {
+  using T = C2<R>;
+  __shared__ T part[8][4][32];
+  const int p = blockIdx.x;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const int s = blockIdx.y * 32 + lane;
+  const bool active = s < S;
+  const int np = npts[p];
+  T acc[4];
+#pragma unroll
+  for (int l = 0; l < 4; l++) acc[l] = mk<T>(R(0), R(0));
+  const long long rowbase = (long long)p * maxsph;
+  int i = wp;
+#pragma unroll 1
+  for (; i + 8 * 3 < np; i += 8 * 4) {
+    T v[4];
+    int q[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) q[u] = __ldg(&pt[rowbase + i + 8 * u]);
+#pragma unroll
+    for (int u = 0; u < 4; u++) v[u] = active ? psi[(long long)q[u] * S + s] : mk<T>(R(0), R(0));
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+#pragma unroll
+      for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(gcoef[(rowbase + i + 8 * u) * 4 + l], v[u]));
+    }
+  }
+  for (; i < np; i += 8) {
+    const int q = __ldg(&pt[rowbase + i]);
+    T v = active ? psi[(long long)q * S + s] : mk<T>(R(0), R(0));
+#pragma unroll
+    for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(gcoef[(rowbase + i) * 4 + l], v));
+  }
+#pragma unroll
+  for (int l = 0; l < 4; l++) part[wp][l][lane] = acc[l];
+  __syncthreads();
+  if (wp == 0 && active) {
+    T pr[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      T t = part[0][l][lane];
+      for (int k = 1; k < 8; k++) t = cadd(t, part[k][l][lane]);
+      pr[l] = t;
+      projraw[((long long)p * 4 + l) * S + s] = t;
+    }
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      T t = mk<T>(R(0), R(0));
+#pragma unroll
+      for (int j = 0; j < 4; j++) t = cadd(t, cscale(pr[j], coeff[(p * 4 + l) * 4 + j]));
+      projD[((long long)p * 4 + l) * S + s] = t;
+    }
+  }
+}
+
+template <typename R>
+void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<R> *psi, int S, C2<R> *projraw,
+                       C2<R> *projD) {
+  const Projectors &P = h.proj;
+  if (P.nproj == 0) return;
+  dim3 grid(P.nproj, (S + 31) / 32);
+  const C2<R> *gcoef;
+  const R *coeff;
+  if constexpr (sizeof(R) == 8) {
+    gcoef = P.d_gcoef;
+    coeff = P.d_coeff;
+  } else {
+    gcoef = P.d_gcoef32;
+    coeff = P.d_coeff32;
+  }
+  nl_project_kernel<R><<<grid, 256, 0, ctx.stream>>>(psi, S, P.d_pt, gcoef, P.d_npts, coeff, P.maxsph, projraw, projD);
+  LAUNCHED(ctx);
+}
+
+// out[pt][s] = nonlocal term (ks_hamiltonian::non_local, ks_hamiltonian.hpp:106-120)
+template <typename R>
+__global__ void nl_scatter_kernel(long long npoints, int S, const int *__restrict__ offs, const int *__restrict__ hit,
+                                  const C2<R> *__restrict__ hcoef, const C2<R> *__restrict__ projD, int maxsph,
+                                  C2<R> *out) {
+  using T = C2<R>;
+  const long long total = npoints * S;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long pt = e / S;
+    const int s = int(e % S);
+    T acc = mk<T>(R(0), R(0));
+    for (int hh = offs[pt]; hh < offs[pt + 1]; hh++) {
+      const int p = hit[hh] / maxsph;
+#pragma unroll
+      for (int l = 0; l < 4; l++) acc = cadd(acc, cmul(hcoef[(long long)hh * 4 + l], projD[((long long)p * 4 + l) * S + s]));
+    }
+    out[e] = acc;
+  }
+}
+
+template <typename R>
+void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out) {
+  const Projectors &P = h.proj;
+  const C2<R> *hc;
+  if constexpr (sizeof(R) == 8) hc = P.d_hcoef;
+  else hc = P.d_hcoef32;
+  nl_scatter_kernel<R><<<grid_for(b.npoints * S, 256), 256, 0, ctx.stream>>>(b.npoints, S, P.d_offs, P.d_hit, hc,
+                                                                             projD, P.maxsph, out);
+  LAUNCHED(ctx);
+}
+
+// ------------------------------------------------------------------ elementwise
+template <typename R> __global__ void fill_kernel(C2<R> *p, long long n, R re, R im) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = mk<C2<R>>(re, im);
+}
+template <typename R> void launch_fill(Ctx &ctx, C2<R> *p, long long n, double re, double im) {
+  fill_kernel<R><<<grid_for(n, 256), 256, 0, ctx.stream>>>(p, n, R(re), R(im));
+  LAUNCHED(ctx);
+}
+
+template <typename R> __global__ void axpy_kernel(C2<R> *y, const C2<R> *x, long long n, R re, R im) {
+  const C2<R> c = mk<C2<R>>(re, im);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = cadd(y[i], cmul(c, x[i]));
+}
+template <typename R> void launch_axpy(Ctx &ctx, C2<R> *y, const C2<R> *x, long long n, double re, double im) {
+  axpy_kernel<R><<<grid_for(n, 256), 256, 0, ctx.stream>>>(y, x, n, R(re), R(im));
+  LAUNCHED(ctx);
+}
+
+// y[pt][s] += scale * coef[s] * x[pt][s]   (operations::shift with a per-state factor, shift.hpp:19-31)
+template <typename R>
+__global__ void shift_vec_kernel(C2<R> *y, const C2<R> *x, int S, long long n, const double *coef, double scale) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const R c = R(scale * coef[i % S]);
+    y[i] = cadd(y[i], cscale(x[i], c));
+  }
+}
+template <typename R>
+void launch_shift_vec(Ctx &ctx, C2<R> *y, const C2<R> *x, int S, long long npoints, const double *coef_dev,
+                      double scale) {
+  shift_vec_kernel<R><<<grid_for(npoints * S, 256), 256, 0, ctx.stream>>>(y, x, S, npoints * S, coef_dev, scale);
+  LAUNCHED(ctx);
+}
+
+struct Metric {
+  int n[3];
+  double rlat[3][3];
+  double lat[3][3];
+};
+
+__device__ __forceinline__ int symi(int i, int n) { return i >= (n + 1) / 2 ? i - n : i; }
+
+__device__ __forceinline__ double lapl_at(const Metric &m, long long pt, double factor, const double *gc, double k2) {
+  const int iz = int(pt % m.n[2]);
+  const int iy = int((pt / m.n[2]) % m.n[1]);
+  const int ix = int(pt / ((long long)m.n[2] * m.n[1]));
+  const double tp = 6.283185307179586476925286766559;
+  double G0 = tp * symi(ix, m.n[0]), G1 = tp * symi(iy, m.n[1]), G2 = tp * symi(iz, m.n[2]);
+  double c0 = (m.rlat[0][0] * G0 + m.rlat[1][0] * G1) + m.rlat[2][0] * G2;
+  double c1 = (m.rlat[0][1] * G0 + m.rlat[1][1] * G1) + m.rlat[2][1] * G2;
+  double c2 = (m.rlat[0][2] * G0 + m.rlat[1][2] * G1) + m.rlat[2][2] * G2;
+  double g2 = c0 * c0 + c1 * c1 + c2 * c2;
+  return factor * (-g2 + (gc[0] * G0 + gc[1] * G1 + gc[2] * G2) + k2);
+}
+
+static Metric metric_of(const Basis &b) {
+  Metric m;
+  for (int i = 0; i < 3; i++) {
+    m.n[i] = b.n[i];
+    for (int j = 0; j < 3; j++) {
+      m.rlat[i][j] = b.rlat[i][j];
+      m.lat[i][j] = b.lat[i][j];
+    }
+  }
+  return m;
+}
+
+struct Vec3 {
+  double v[3];
+};
+
+template <typename R>
+__global__ void laplacian_kernel(Metric m, const C2<R> *in, C2<R> *out, int S, long long n, double factor, Vec3 gc) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const R f = R(lapl_at(m, i / S, factor, gc.v, 0.0));
+    out[i] = cscale(in[i], f);
+  }
+}
+template <typename R>
+void launch_laplacian(Ctx &ctx, const Basis &b, const C2<R> *in, C2<R> *out, int S, double factor, const double gc[3]) {
+  Vec3 g{{gc[0], gc[1], gc[2]}};
+  laplacian_kernel<R><<<grid_for(b.npoints * S, 256), 256, 0, ctx.stream>>>(metric_of(b), in, out, S, b.npoints * S,
+                                                                            factor, g);
+  LAUNCHED(ctx);
+}
+
+// ------------------------------------------------------------------ per-state reductions
+// Stage 1: block b handles a contiguous point range; thread t owns state s = t (blockDim >= S handled by loop)
+// and accumulates over its points in index order.  Stage 2 sums the block partials in order.
+constexpr int RED_BLOCKS = 296;
+
+template <typename R, int MODE>
+__global__ void state_reduce_kernel(const C2<R> *__restrict__ a, const C2<R> *__restrict__ b, int S, long long npoints,
+                                    Metric m, double factor, Vec3 gc, double k2, double2 *partial) {
+  const long long chunk = (npoints + gridDim.x - 1) / gridDim.x;
+  const long long p0 = blockIdx.x * chunk;
+  const long long p1 = min(npoints, p0 + chunk);
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (long long p = p0; p < p1; p++) {
+      C2<R> x = a[p * S + s];
+      if (MODE == 0) {  // conj(a) b
+        C2<R> y = b[p * S + s];
+        re += double(x.x) * double(y.x) + double(x.y) * double(y.y);
+        im += double(x.x) * double(y.y) - double(x.y) * double(y.x);
+      } else {          // conj(a) lapl a
+        double f = lapl_at(m, p, factor, gc.v, k2);
+        re += f * (double(x.x) * double(x.x) + double(x.y) * double(x.y));
+      }
+    }
+    partial[(long long)blockIdx.x * S + s] = make_double2(re, im);
+  }
+}
+
+__global__ void sum_partials_kernel(const double2 *partial, int nblk, int S, double scale, double2 *out) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < nblk; k++) {
+      re += partial[(long long)k * S + s].x;
+      im += partial[(long long)k * S + s].y;
+    }
+    out[s] = make_double2(scale * re, scale * im);
+  }
+}
+
+template <typename R>
+void launch_overlap_diag(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long long npoints, double dv, double2 *out) {
+  double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * RED_BLOCKS * S));
+  Metric m{};
+  Vec3 g{{0, 0, 0}};
+  state_reduce_kernel<R, 0><<<RED_BLOCKS, 256, 0, ctx.stream>>>(a, b, S, npoints, m, 0.0, g, 0.0, partial);
+  LAUNCHED(ctx);
+  sum_partials_kernel<<<(S + 255) / 256, 256, 0, ctx.stream>>>(partial, RED_BLOCKS, S, dv, out);
+  LAUNCHED(ctx);
+  dev_free(ctx, partial);
+}
+
+template <typename R>
+void launch_kinetic_ev(Ctx &ctx, const Basis &b, const C2<R> *fphi, int S, double factor, const double gc[3], double k2,
+                       double *out_dev) {
+  double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * (RED_BLOCKS * S + S)));
+  Vec3 g{{gc[0], gc[1], gc[2]}};
+  state_reduce_kernel<R, 1><<<RED_BLOCKS, 256, 0, ctx.stream>>>(fphi, fphi, S, b.npoints, metric_of(b), factor, g, k2,
+                                                                partial);
+  LAUNCHED(ctx);
+  double2 *sums = partial + RED_BLOCKS * S;
+  sum_partials_kernel<<<(S + 255) / 256, 256, 0, ctx.stream>>>(partial, RED_BLOCKS, S, 1.0, sums);
+  LAUNCHED(ctx);
+  INQB_CUDA(cudaMemcpy2DAsync(out_dev, sizeof(double), sums, sizeof(double2), sizeof(double), S,
+                              cudaMemcpyDeviceToDevice, ctx.stream));
+  dev_free(ctx, partial);
+}
+
+// ------------------------------------------------------------------ overlap (complex GEMM, K = npoints)
+// S[i][j] = dv * sum_p conj(a[p][i]) b[p][j].  64x64 output tile per CTA, split-K over point chunks,
+// 256 threads with a 4x4 register tile each; partial tiles summed in chunk order.
+template <typename R>
+__global__ void __launch_bounds__(256) overlap_kernel(const C2<R> *__restrict__ a, int Sa, const C2<R> *__restrict__ b,
+                                                      int Sb, long long npoints, long long chunk, double2 *partial) {
+  constexpr int TB = 64, KT = 16;
+  __shared__ double2 As[KT][TB];
+  __shared__ double2 Bs[KT][TB];
+  const int ti = blockIdx.x * TB, tj = blockIdx.y * TB;
+  const long long p0 = blockIdx.z * chunk;
+  const long long p1 = min(npoints, p0 + chunk);
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double2 acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) acc[u][v] = make_double2(0.0, 0.0);
+  for (long long k0 = p0; k0 < p1; k0 += KT) {
+    for (int e = threadIdx.x; e < KT * TB; e += 256) {
+      const int kk = e / TB, c = e % TB;
+      const long long p = k0 + kk;
+      double2 va = make_double2(0.0, 0.0), vb = make_double2(0.0, 0.0);
+      if (p < p1) {
+        if (ti + c < Sa) {
+          C2<R> x = a[p * Sa + ti + c];
+          va = make_double2(double(x.x), double(x.y));
+        }
+        if (tj + c < Sb) {
+          C2<R> y = b[p * Sb + tj + c];
+          vb = make_double2(double(y.x), double(y.y));
+        }
+      }
+      As[kk][c] = va;
+      Bs[kk][c] = vb;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < KT; kk++) {
+      double2 av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) av[u] = As[kk][ty + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 4; v++) bv[v] = Bs[kk][tx + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          acc[u][v].x += av[u].x * bv[v].x + av[u].y * bv[v].y;
+          acc[u][v].y += av[u].x * bv[v].y - av[u].y * bv[v].x;
+        }
+    }
+    __syncthreads();
+  }
+  const long long base = (long long)blockIdx.z * Sa * Sb;
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const int i = ti + ty + 16 * u, j = tj + tx + 16 * v;
+      if (i < Sa && j < Sb) partial[base + (long long)i * Sb + j] = acc[u][v];
+    }
+}
+
+__global__ void sum_tiles_kernel(const double2 *partial, int nz, long long n, double scale, double2 *out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int z = 0; z < nz; z++) {
+      re += partial[z * n + e].x;
+      im += partial[z * n + e].y;
+    }
+    out[e] = make_double2(scale * re, scale * im);
+  }
+}
+
+template <typename R>
+void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, long long npoints, double dv,
+                    double2 *out) {
+  const int gi = (Sa + 63) / 64, gj = (Sb + 63) / 64;
+  int nz = int((2LL * ctx.num_sms + gi * gj - 1) / (gi * gj));
+  if (nz < 1) nz = 1;
+  if (nz > 256) nz = 256;
+  long long chunk = (npoints + nz - 1) / nz;
+  chunk = ((chunk + 15) / 16) * 16;
+  nz = int((npoints + chunk - 1) / chunk);
+  double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * (size_t)nz * Sa * Sb));
+  overlap_kernel<R><<<dim3(gi, gj, nz), 256, 0, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, partial);
+  LAUNCHED(ctx);
+  const long long n = (long long)Sa * Sb;
+  sum_tiles_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(partial, nz, n, dv, out);
+  LAUNCHED(ctx);
+  dev_free(ctx, partial);
+}
+
+// ------------------------------------------------------------------ rotate: phi[p][:] <- phi[p][:] R
+template <typename R>
+__global__ void __launch_bounds__(256) rotate_kernel(C2<R> *phi, int S, long long npoints, const double2 *__restrict__ Rm) {
+  constexpr int ROWS = 8;
+  extern __shared__ __align__(16) unsigned char sm[];
+  double2 *rows = reinterpret_cast<double2 *>(sm);  // [ROWS][S]
+  for (long long p0 = (long long)blockIdx.x * ROWS; p0 < npoints; p0 += (long long)gridDim.x * ROWS) {
+    const int nr = int(min((long long)ROWS, npoints - p0));
+    for (int e = threadIdx.x; e < ROWS * S; e += blockDim.x) {
+      const int r = e / S, k = e % S;
+      double2 v = make_double2(0.0, 0.0);
+      if (r < nr) {
+        C2<R> x = phi[(p0 + r) * S + k];
+        v = make_double2(double(x.x), double(x.y));
+      }
+      rows[e] = v;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < S; j += blockDim.x) {
+      double2 acc[ROWS];
+#pragma unroll
+      for (int r = 0; r < ROWS; r++) acc[r] = make_double2(0.0, 0.0);
+      for (int k = 0; k < S; k++) {
+        const double2 rk = Rm[(long long)k * S + j];
+#pragma unroll
+        for (int r = 0; r < ROWS; r++) {
+          const double2 x = rows[r * S + k];
+          acc[r].x += x.x * rk.x - x.y * rk.y;
+          acc[r].y += x.x * rk.y + x.y * rk.x;
+        }
+      }
+      for (int r = 0; r < nr; r++) phi[(p0 + r) * S + j] = mk<C2<R>>(R(acc[r].x), R(acc[r].y));
+    }
+    __syncthreads();
+  }
+}
+
+template <typename R> void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev) {
+  const size_t smem = sizeof(double2) * 8 * S;
+  INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "too many states for rotate");
+  INQB_CUDA(cudaFuncSetAttribute(rotate_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  rotate_kernel<R><<<grid_for(npoints, 8, 148LL * 16), 256, smem, ctx.stream>>>(phi, S, npoints, Rdev);
+  LAUNCHED(ctx);
+}
+
+// ------------------------------------------------------------------ density n[p] (+)= sum_s occ_s |phi[p][s]|^2
+// one warp per point, lanes stride over states, fixed shuffle tree (density.hpp:24-36)
+template <typename R>
+__global__ void density_kernel(const C2<R> *__restrict__ phi, int S, long long npoints, const double *__restrict__ occ,
+                               double *dens, int accumulate) {
+  const int lane = threadIdx.x & 31;
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long p = warp; p < npoints; p += nwarps) {
+    double acc = 0.0;
+    for (int s = lane; s < S; s += 32) {
+      C2<R> x = phi[p * S + s];
+      acc += occ[s] * (double(x.x) * double(x.x) + double(x.y) * double(x.y));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) dens[p] = accumulate ? dens[p] + acc : acc;
+  }
+}
+template <typename R>
+void launch_density(Ctx &ctx, const C2<R> *phi, int S, long long npoints, const double *occ_dev, double *dens,
+                    int accumulate) {
+  density_kernel<R><<<grid_for(npoints * 32, 256), 256, 0, ctx.stream>>>(phi, S, npoints, occ_dev, dens, accumulate);
+  LAUNCHED(ctx);
+}
+
+// ------------------------------------------------------------------ kick: phi *= exp(i E_cov . r_contra)
+template <typename R>
+__global__ void kick_kernel(Metric m, C2<R> *phi, int S, long long npoints, Vec3 ecov) {
+  const long long n = npoints * S;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long pt = e / S;
+    const int iz = int(pt % m.n[2]);
+    const int iy = int((pt / m.n[2]) % m.n[1]);
+    const int ix = int(pt / ((long long)m.n[2] * m.n[1]));
+    // rvector: symmetric index times contravariant spacing 1/n (real_space.hpp:127-130)
+    const double r0 = symi(ix, m.n[0]) * (1.0 / m.n[0]);
+    const double r1 = symi(iy, m.n[1]) * (1.0 / m.n[1]);
+    const double r2 = symi(iz, m.n[2]) * (1.0 / m.n[2]);
+    const double arg = ecov.v[0] * r0 + ecov.v[1] * r1 + ecov.v[2] * r2;
+    double sn, cs;
+    sincos(arg, &sn, &cs);
+    C2<R> x = phi[e];
+    double re = double(x.x) * cs - double(x.y) * sn;
+    double im = double(x.x) * sn + double(x.y) * cs;
+    phi[e] = mk<C2<R>>(R(re), R(im));
+  }
+}
+template <typename R> void launch_kick(Ctx &ctx, const Basis &b, C2<R> *phi, int S, const double ecov[3]) {
+  Vec3 e{{ecov[0], ecov[1], ecov[2]}};
+  kick_kernel<R><<<grid_for(b.npoints * S, 256), 256, 0, ctx.stream>>>(metric_of(b), phi, S, b.npoints, e);
+  LAUNCHED(ctx);
+}
+
+// ------------------------------------------------------------------ sum |a - b| (integral_sum_absdiff)
+__global__ void absdiff_kernel(const double *a, const double *b, long long n, double *partial) {
+  __shared__ double red[256];
+  const long long chunk = (n + gridDim.x - 1) / gridDim.x;
+  const long long p0 = blockIdx.x * chunk, p1 = min(n, p0 + chunk);
+  double acc = 0.0;
+  for (long long i = p0 + threadIdx.x; i < p1; i += blockDim.x) acc += fabs(a[i] - b[i]);
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+__global__ void absdiff_final_kernel(const double *partial, int nb, double *out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < nb; i++) s += partial[i];
+    *out = s;
+  }
+}
+void launch_absdiff_sum(Ctx &ctx, const double *a, const double *b, long long n, double *out_dev) {
+  double *partial = static_cast<double *>(dev_alloc(ctx, sizeof(double) * RED_BLOCKS));
+  absdiff_kernel<<<RED_BLOCKS, 256, 0, ctx.stream>>>(a, b, n, partial);
+  LAUNCHED(ctx);
+  absdiff_final_kernel<<<1, 32, 0, ctx.stream>>>(partial, RED_BLOCKS, out_dev);
+  LAUNCHED(ctx);
+  dev_free(ctx, partial);
+}
+
+// ------------------------------------------------------------------ instantiations
+#define INST(R)                                                                                                   \
+  template void launch_nl_project<R>(Ctx &, const Basis &, const Hamiltonian &, const C2<R> *, int, C2<R> *,       \
+                                     C2<R> *);                                                                    \
+  template void launch_nl_scatter<R>(Ctx &, const Basis &, const Hamiltonian &, const C2<R> *, int, C2<R> *);     \
+  template void launch_fill<R>(Ctx &, C2<R> *, long long, double, double);                                         \
+  template void launch_axpy<R>(Ctx &, C2<R> *, const C2<R> *, long long, double, double);                          \
+  template void launch_shift_vec<R>(Ctx &, C2<R> *, const C2<R> *, int, long long, const double *, double);        \
+  template void launch_laplacian<R>(Ctx &, const Basis &, const C2<R> *, C2<R> *, int, double, const double *);    \
+  template void launch_overlap_diag<R>(Ctx &, const C2<R> *, const C2<R> *, int, long long, double, double2 *);    \
+  template void launch_kinetic_ev<R>(Ctx &, const Basis &, const C2<R> *, int, double, const double *, double,     \
+                                     double *);                                                                   \
+  template void launch_overlap<R>(Ctx &, const C2<R> *, int, const C2<R> *, int, long long, double, double2 *);   \
+  template void launch_rotate<R>(Ctx &, C2<R> *, int, long long, const double2 *);                                 \
+  template void launch_density<R>(Ctx &, const C2<R> *, int, long long, const double *, double *, int);            \
+  template void launch_kick<R>(Ctx &, const Basis &, C2<R> *, int, const double *);
+
+INST(double)
+INST(float)
+
+}  // namespace inqb
+
+namespace inqb {
+
+// ------------------------------------------------------------------ synthetic orbitals
+// SplitMix64 (Steele, Lea & Flood 2014) counter stream and the Box-Muller transform.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long seed, unsigned long long counter) {
+  unsigned long long z = seed + (counter + 1ULL) * 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ double u01(unsigned long long x) { return double(x >> 11) * (1.0 / 9007199254740992.0); }
+
+template <typename R>
+__global__ void randomize_gsphere_kernel(Metric m, C2<R> *phi, int S, long long npoints, unsigned long long seed,
+                                         double ecut) {
+  const long long n = npoints * S;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long pt = e / S;
+    const int s = int(e % S);
+    const double half_g2 = -0.5 * lapl_at(m, pt, 1.0, Vec3{{0, 0, 0}}.v, 0.0);
+    C2<R> v = mk<C2<R>>(R(0), R(0));
+    if (half_g2 < ecut) {
+      const unsigned long long c = (unsigned long long)s * (unsigned long long)npoints + (unsigned long long)pt;
+      const double a = u01(splitmix64(seed, 2 * c)), b = u01(splitmix64(seed, 2 * c + 1));
+      const double r = sqrt(-2.0 * log(1.0 - a));
+      double sn, cs;
+      sincospi(2.0 * b, &sn, &cs);
+      v = mk<C2<R>>(R(r * cs), R(r * sn));
+    }
+    phi[e] = v;
+  }
+}
+
+template <typename R>
+void launch_randomize_gsphere(Ctx &ctx, const Basis &b, C2<R> *phi, int S, unsigned long long seed, double ecut) {
+  randomize_gsphere_kernel<R><<<grid_for(b.npoints * S, 256), 256, 0, ctx.stream>>>(metric_of(b), phi, S, b.npoints,
+                                                                                     seed, ecut);
+  LAUNCHED(ctx);
+}
+
+template <typename RI, typename RO> __global__ void convert_kernel(const C2<RI> *in, C2<RO> *out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    C2<RI> x = in[i];
+    out[i] = mk<C2<RO>>(RO(x.x), RO(x.y));
+  }
+}
+
+void launch_convert(Ctx &ctx, const void *in, int in_prec, void *out, int out_prec, long long n) {
+  if (in_prec == INQB_F64 && out_prec == INQB_F32)
+    convert_kernel<double, float><<<grid_for(n, 256), 256, 0, ctx.stream>>>(static_cast<const double2 *>(in),
+                                                                            static_cast<float2 *>(out), n);
+  else if (in_prec == INQB_F32 && out_prec == INQB_F64)
+    convert_kernel<float, double><<<grid_for(n, 256), 256, 0, ctx.stream>>>(static_cast<const float2 *>(in),
+                                                                            static_cast<double2 *>(out), n);
+  else
+    throw Error(INQB_ERR_ARG, "conversion needs two different precisions");
+  LAUNCHED(ctx);
+}
+
+template void launch_randomize_gsphere<double>(Ctx &, const Basis &, double2 *, int, unsigned long long, double);
+template void launch_randomize_gsphere<float>(Ctx &, const Basis &, float2 *, int, unsigned long long, double);
+
+}  // namespace inqb

@@ -1,0 +1,242 @@
+"""Pin the CPU oracle against the reference's own known-answer unit tests.
+
+Each test restates one reference Catch2 TEST_CASE (file:line in its docstring)
+with the same inputs and the same tolerance, so the oracle that later checks the
+CUDA path is itself anchored to the reference.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+# Catch::Approx default (the `_a` literal): epsilon = 100 * float epsilon, relative
+APPROX = 100 * np.finfo(np.float32).eps
+
+
+def approx(a, b):
+    return abs(a - b) <= APPROX * (max(abs(a), abs(b)) + 1.0) if b == 0 else abs(a - b) <= APPROX * abs(b)
+
+
+# ---------------------------------------------------------------- spherical_grid.hpp:258-399
+
+def _pw10():
+    return O.RealSpace.from_spacing(O.Cell.cubic(10.0), 0.49672941)
+
+
+@pytest.mark.parametrize("center", [(0.0, 0.0, 0.0), (-5.0, 0.0, 0.0), (5.0, 0.0, 0.0), (-5.0, -5.0, -5.0),
+                                    (5.0, 5.0, 5.0), (2.5, 2.5, 2.5)])
+def test_sphere_size_cubic(center):
+    """spherical_grid.hpp:269-358: radius-2 spheres on the 20^3 grid of a 10 bohr cube hold 257 points."""
+    rs = _pw10()
+    assert rs.sizes == (20, 20, 20)
+    sph = O.spherical_grid(rs, np.array(center), 2.0)
+    assert sph.size == 257
+    theo = 4.0 / 3.0 * math.pi * 2.0 ** 3
+    assert approx(sph.size * rs.volume_element() / theo, 0.9586598525)
+
+
+def test_sphere_gather_scatter_counts():
+    """spherical_grid.hpp:286-322: gather of ones over 20 states sums to 20*257; scatter of -1 leaves 20*(N-257)."""
+    rs = _pw10()
+    sph = O.spherical_grid(rs, np.array([-5.0, 0.0, 0.0]), 2.0)
+    grid = np.ones(rs.sizes + (20,), complex)
+    sub = grid[sph.points[:, 0], sph.points[:, 1], sph.points[:, 2], :]
+    assert np.isclose(np.sum(sub.real), 20.0 * 257)
+    np.add.at(grid, (sph.points[:, 0], sph.points[:, 1], sph.points[:, 2]), -np.ones_like(sub))
+    assert np.isclose(np.sum(grid.real), 20.0 * (rs.npoints - sph.size))
+    # no grid point appears twice
+    flat = (sph.points[:, 0] * 20 + sph.points[:, 1]) * 20 + sph.points[:, 2]
+    assert len(np.unique(flat)) == len(flat)
+
+
+def test_sphere_size_noncubic():
+    """spherical_grid.hpp:382-397: hexagonal-like cell, radius 5.71 -> 15963 points, ratio 1.0013282291."""
+    cell = O.Cell([[7.57325, 0.0, 0.0], [-3.78662, 6.55862, 0.0], [5.78917e-16, 1.00271e-15, 9.45443]])
+    rs = O.RealSpace.from_spacing(cell, 0.405578)
+    sph = O.spherical_grid(rs, np.array([3.78659, -2.18619, 1.65434]), 5.71)
+    assert sph.size == 15963
+    theo = 4.0 / 3.0 * math.pi * 5.71 ** 3
+    assert approx(sph.size * rs.volume_element() / theo, 1.0013282291)
+
+
+# ---------------------------------------------------------------- real_space.hpp / ks_hamiltonian.hpp:297-536
+
+def test_real_space_basis():
+    """real_space.hpp unit test + ks_hamiltonian.hpp:304-311: 20^3 points, spacing 0.5, dV 0.125."""
+    rs = _pw10()
+    assert rs.npoints == 8000
+    assert np.allclose(rs.rspacing, 0.5)
+    assert approx(rs.volume_element(), 0.125)
+
+
+def _ham_free(rs):
+    return O.Hamiltonian(rs, np.zeros(rs.sizes))
+
+
+NST = 6  # ks_states(UNPOLARIZED, 11 electrons)
+
+
+def test_hamiltonian_constant():
+    """ks_hamiltonian.hpp:324-357: H of a constant is zero (mean |H phi| < 1e-14)."""
+    rs = _pw10()
+    phi = np.ones(rs.sizes + (NST,), complex)
+    h = _ham_free(rs).apply_real(phi)
+    assert np.sum(np.abs(h)) / h.size < 1e-14
+
+
+def _plane_waves(rs):
+    kk = 2.0 * math.pi / rs.rlength[0]
+    x = rs.rvector_cartesian()[..., 0]
+    s = np.arange(NST)
+    return np.exp(1j * s[None, None, None, :] * kk * x[..., None]), kk
+
+
+def test_hamiltonian_plane_wave():
+    """ks_hamiltonian.hpp:359-402: H e^{i s k x} = (s k)^2/2 e^{i s k x} (< 1e-14)."""
+    rs = _pw10()
+    phi, kk = _plane_waves(rs)
+    h = _ham_free(rs).apply_real(phi)
+    s = np.arange(NST)
+    diff = np.sum(np.abs(h - 0.5 * (s * kk) ** 2 * phi)) / h.size
+    assert diff < 1e-14
+
+
+def _oscillator(rs, ww=2.0):
+    r2 = rs.r2()
+    ham = O.Hamiltonian(rs, 0.5 * ww * ww * r2)
+    phi = np.repeat(np.exp(-ww * r2)[..., None], NST, axis=-1).astype(complex)
+    return ham, phi
+
+
+def test_hamiltonian_harmonic_oscillator():
+    """ks_hamiltonian.hpp:404-445: mean |H phi - 1.5 w phi| == 0.0051420503 (Approx)."""
+    rs = _pw10()
+    ham, phi = _oscillator(rs)
+    h = ham.apply_real(phi)
+    diff = np.sum(np.abs(h - 1.5 * 2.0 * phi)) / h.size
+    assert approx(diff, 0.0051420503)
+
+
+def test_hamiltonian_fourier_forms():
+    """ks_hamiltonian.hpp:448-536: the plane-wave and oscillator checks through the Fourier-space operator."""
+    rs = _pw10()
+    phi, kk = _plane_waves(rs)
+    h = O.to_real(_ham_free(rs).apply_fourier(O.to_fourier(phi)))
+    s = np.arange(NST)
+    assert np.sum(np.abs(h - 0.5 * (s * kk) ** 2 * phi)) / h.size < 1e-14
+    ham, phi = _oscillator(rs)
+    h = O.to_real(ham.apply_fourier(O.to_fourier(phi)))
+    assert approx(np.sum(np.abs(h - 3.0 * phi)) / h.size, 0.0051420503)
+
+
+# ---------------------------------------------------------------- transform.hpp:273-415
+
+def _rs1666(rotated=False):
+    aa = 16.66
+    if rotated:
+        cell = O.Cell([[aa / math.sqrt(2.0), aa / 2, aa / 2], [-aa / math.sqrt(2), aa / 2, aa / 2],
+                       [0.0, -aa / math.sqrt(2.0), aa / math.sqrt(2.0)]])
+    else:
+        cell = O.Cell.cubic(aa)
+    return O.RealSpace.from_spacing(cell, 0.306320257)
+
+
+def test_zero_outside_sphere():
+    """transform.hpp:273-287: fs volume 0.0293659268; zeroing outside the sphere keeps 0.5240308896."""
+    rs = _rs1666()
+    vol = rs.fourier_volume_element() * rs.npoints
+    assert approx(vol, 0.0293659268)
+    inside = ~rs.outside_sphere()
+    assert approx(rs.fourier_volume_element() * np.sum(inside) / vol, 0.5240308896)
+
+
+@pytest.mark.parametrize("rotated", [False, True])
+def test_gaussian_transform(rotated):
+    """transform.hpp:289-415: FT of exp(-s r^2) vs (pi/s)^{3/2}/fs_vol exp(-G^2/4s) (mean < 1e-3); round trip < 1e-15."""
+    rs = _rs1666(rotated)
+    r2 = rs.r2()
+    sig = 0.5 * (np.arange(7) + 1)
+    phi = np.exp(-sig[None, None, None, :] * r2[..., None]).astype(complex)
+    fphi = O.to_fourier(phi)
+    fs_vol = rs.npoints * rs.fourier_volume_element()
+    assert approx(fs_vol, 0.0293659268)
+    g2 = rs.g2()
+    an = (math.pi / sig) ** 1.5 / fs_vol * np.exp(-0.25 * g2[..., None] / sig)
+    assert np.sum(np.abs(fphi - an)) / rs.npoints < 1e-3
+    back = O.to_real(fphi)
+    assert np.sum(np.abs(phi - back)) / phi.size < 1e-15
+
+
+# ---------------------------------------------------------------- laplacian.hpp:143-336
+
+def _lap_cells():
+    ll = 9.0
+    ll2 = 5.89
+    yield O.Cell([[9.0, 0, 0], [0, 12.0, 0], [0, 0, 10.0]]), None, 1e-8
+    yield O.Cell([[ll / math.sqrt(2), ll / math.sqrt(2), 0.0], [-ll / math.sqrt(2), ll / math.sqrt(2), 0.0],
+                  [0.0, 0.0, ll]]), "rot", 1e-8
+    yield O.Cell([[0.0, ll2, ll2], [ll2, 0.0, ll2], [ll2, ll2, 0.0]]), "fcc", 1e-7
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+def test_laplacian_plane_wave(which):
+    """laplacian.hpp:143-336: laplacian / in-place / add of (s+1) e^{ik.r}, three lattices."""
+    cell, kind, tol = list(_lap_cells())[which]
+    rs = O.RealSpace.from_spacing(cell, 0.49672941)
+    if kind is None:
+        kvec = 2.0 * math.pi * np.array([1.0 / 9, 1.0 / 12, 1.0 / 10])
+    elif kind == "rot":
+        kvec = 2.0 * math.pi * np.array([math.sqrt(2.0) / 9, math.sqrt(2.0) / 9, 0.0])
+    else:
+        rec = cell.reciprocal[2]
+        kvec = 2.0 * rec + 3.0 * rec - 1.0 * rec
+    r = rs.rvector_cartesian()
+    ff = np.exp(1j * (kvec[0] * r[..., 0] + kvec[1] * r[..., 1] + kvec[2] * r[..., 2]))
+    s1 = np.arange(13) + 1.0
+    func = s1[None, None, None, :] * ff[..., None]
+    factor = 0.673214
+    an = s1[None, None, None, :] * factor * (-np.dot(kvec, kvec)) * ff[..., None]
+    lap = O.to_real(O.laplacian(rs, O.to_fourier(func), factor))
+    assert np.sum(np.abs(lap - an)) < tol
+    fs = O.laplacian(rs, O.to_fourier(func), factor)
+    lap_add = O.to_real(fs + O.laplacian(rs, O.to_fourier(func), factor))
+    assert np.sum(np.abs(lap_add - 2 * an)) < 5e-7
+
+
+# ---------------------------------------------------------------- exponential.hpp:89-140
+
+def test_exponential_diagonal():
+    """exponential.hpp:89-140: exp(-0.1 D) of unit vectors for D = diag(0..99), order 16."""
+    npoint, nvec = 100, 12
+    d = np.arange(npoint, dtype=float)
+    phi = np.zeros((npoint, nvec), complex)
+    for i in range(nvec):
+        phi[i, i] = 1.0
+    out = O.exponential_in_place(lambda x: d[:, None] * x, -0.1, phi, 16)
+    for i in range(nvec):
+        assert approx(out[i, i].real, math.exp(-0.1 * i))
+    mask = np.ones_like(out, bool)
+    mask[np.arange(nvec), np.arange(nvec)] = False
+    assert np.max(np.abs(out[mask])) < 1e-12
+    e1, e2 = O.exponential_2_for_1(lambda x: d[:, None] * x, -0.05, -0.1, phi, 16)
+    for i in range(nvec):
+        assert approx(e1[i, i].real, math.exp(-0.05 * i))
+        assert approx(e2[i, i].real, math.exp(-0.1 * i))
+
+
+# ---------------------------------------------------------------- orthogonalize.hpp:72-130
+
+@pytest.mark.parametrize("nst", [3, 100])
+def test_orthogonalize_identity(nst, rng):
+    """orthogonalize.hpp:72-130: after orthogonalize, S = I (off-diagonal < 1e-14)."""
+    rs = O.RealSpace.from_spacing(O.Cell.cubic(6.3), 0.44428829)
+    phi = rng.standard_normal(rs.sizes + (nst,)) + 1j * rng.standard_normal(rs.sizes + (nst,))
+    phi = O.orthogonalize(rs, phi)
+    S = O.overlap(rs, phi)
+    assert np.allclose(np.diag(S).real, 1.0, atol=1e-13)
+    assert np.max(np.abs(np.diag(S).imag)) < 1e-14
+    off = S - np.diag(np.diag(S))
+    assert np.max(np.abs(off)) < 1e-13
