@@ -339,6 +339,25 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile_case(args):
+    """Small case for ncu captures: the C2 grid and atoms with 32 orbitals (226 MB per FP32 set, above L2).
+
+    Sequence: FP64 build (3 FFT passes), then ``--steps`` mixed-form and ``--steps`` FP64 applications
+    (each: 1 projection + 5 FFT passes)."""
+    import inq_b200 as ib
+    from inq_b200 import synthetic
+    sysm = synthetic.config("c2", nst=32)
+    basis, ham, phi64 = synthetic.build(sysm)
+    phi32 = phi64.converted(ib.F32)
+    out32, out64 = phi32.skeleton(), phi64.skeleton()
+    for _ in range(args.steps):
+        ham.apply(phi32, out32)
+    for _ in range(args.steps):
+        ham.apply(phi64, out64)
+    basis.ctx.synchronize()
+    print(json.dumps({"profile_case": "c2 grid, 32 states", "launches": basis.ctx.launch_count()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,10 +365,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true", help="small workload for ncu captures")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -46,11 +46,16 @@ typedef struct inqb_hamiltonian inqb_hamiltonian;
 int inqb_ctx_create(int device, inqb_ctx **out);
 int inqb_ctx_destroy(inqb_ctx *ctx);
 const char *inqb_last_error(const inqb_ctx *ctx);
+/* Waits for the context's stream; returns INQB_ERR_TIMEOUT if a kernel's bounded device-side
+ * wait expired since the last call (the flag is then cleared). */
 int inqb_ctx_synchronize(inqb_ctx *ctx);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own work. */
 int inqb_ctx_stream(inqb_ctx *ctx, void **stream);
 /* Number of kernels this library launched on the context so far. */
 int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
+/* Tuning options: "fft_impl" = 0 (specialised persistent TMA kernels where a line length
+ * has one, the default) or 1 (generic kernel for every length). */
+int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Free and total device memory in bytes (admission control for serving). */
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
 

@@ -42,6 +42,7 @@ SIGNATURES = {
     "inqb_ctx_synchronize": (I, [P]),
     "inqb_ctx_stream": (I, [P, C.POINTER(P)]),
     "inqb_ctx_launch_count": (I, [P, C.POINTER(LL)]),
+    "inqb_ctx_set_option": (I, [P, C.c_char_p, LL]),
     "inqb_ctx_mem_info": (I, [P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "inqb_basis_create": (I, [P, DP, I, I, I, C.POINTER(P)]),
     "inqb_basis_destroy": (I, [P]),

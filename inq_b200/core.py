@@ -67,6 +67,9 @@ class Context:
         self.check(self.lib.inqb_ctx_launch_count(self.handle, C.byref(n)))
         return n.value
 
+    def set_option(self, key: str, value: int):
+        self.check(self.lib.inqb_ctx_set_option(self.handle, key.encode(), int(value)))
+
     def mem_info(self):
         f, t = C.c_size_t(), C.c_size_t()
         self.check(self.lib.inqb_ctx_mem_info(self.handle, C.byref(f), C.byref(t)))

@@ -512,6 +512,8 @@ int inqb_ctx_create(int device, inqb_ctx **out) {
     c->num_sms = prop.multiProcessorCount;
     c->max_smem_optin = prop.sharedMemPerBlockOptin;
     INQB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    INQB_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
+    INQB_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
       uint64_t thr = UINT64_MAX;
@@ -526,6 +528,7 @@ int inqb_ctx_destroy(inqb_ctx *ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   cudaStreamDestroy(ctx->stream);
+  if (ctx->d_err) cudaFree(ctx->d_err);
   delete ctx;
   return INQB_OK;
 }
@@ -536,6 +539,26 @@ int inqb_ctx_synchronize(inqb_ctx *ctx) {
   return guarded(ctx, [&] {
     set_device(*ctx);
     INQB_CUDA(cudaStreamSynchronize(ctx->stream));
+    int flag = 0;
+    INQB_CUDA(cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      INQB_CUDA(cudaMemset(ctx->d_err, 0, sizeof(int)));
+      throw Error(INQB_ERR_TIMEOUT, "a device-side wait exceeded its time limit; the results of the calls since the "
+                                    "last synchronize are invalid");
+    }
+  });
+}
+
+int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && key, INQB_ERR_ARG, "null argument");
+    const std::string k(key);
+    if (k == "fft_impl") {
+      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_impl is 0 (specialised) or 1 (generic)");
+      ctx->fft_impl = int(value);
+    } else {
+      throw Error(INQB_ERR_ARG, "unknown option " + k);
+    }
   });
 }
 

@@ -1,0 +1,547 @@
+// Persistent, TMA-pipelined batched FFT pass for compile-time line lengths.
+//
+// Same tile as fft.cu -- one grid line of N points times W consecutive states,
+// 256-byte rows -- but:
+//   * tiles stream through an NS-stage shared-memory ring: one elected thread
+//     issues cp.async.bulk.tensor (TMA) loads NS tiles ahead and a TMA store per
+//     finished tile, so HBM traffic overlaps the arithmetic of the other stages;
+//   * the line DFT is a two-level Cooley-Tukey N = N1 x N2 done in registers
+//     (N1- and N2-point codelets, composite ones from radix 2,3,4,5,8 with
+//     twiddles from a shared-memory copy of the line's table), with one
+//     shared-memory exchange instead of one per radix;
+//   * all index arithmetic is compile-time except the per-tile line decomposition.
+// Every mbarrier wait is bounded (about 2 s by %globaltimer); on expiry the CTA
+// raises the context's error flag and leaves its tile loop.
+
+#pragma once
+
+#include <cuda.h>
+
+#include "fft_common.cuh"
+
+namespace inqb {
+namespace v2 {
+
+enum Variant { FWD_STORE = 0, INV_STORE = 1, MID_KIN = 2, INV_FINAL = 3, FWD_VPSI = 4, FWD_LAPLADD = 5 };
+
+constexpr bool has_aux(int v) { return v == INV_FINAL || v == FWD_LAPLADD; }
+
+template <int N> struct Split { static constexpr int N1 = 0, N2 = 0; };
+template <> struct Split<24> { static constexpr int N1 = 8, N2 = 3; };
+template <> struct Split<32> { static constexpr int N1 = 8, N2 = 4; };
+template <> struct Split<40> { static constexpr int N1 = 8, N2 = 5; };
+template <> struct Split<48> { static constexpr int N1 = 8, N2 = 6; };
+template <> struct Split<64> { static constexpr int N1 = 8, N2 = 8; };
+template <> struct Split<72> { static constexpr int N1 = 8, N2 = 9; };
+template <> struct Split<96> { static constexpr int N1 = 8, N2 = 12; };
+template <> struct Split<120> { static constexpr int N1 = 8, N2 = 15; };
+template <> struct Split<128> { static constexpr int N1 = 8, N2 = 16; };
+
+constexpr int first_factor(int M) {
+  const int f[6] = {8, 4, 2, 3, 5, 7};
+  for (int i = 0; i < 6; i++)
+    if (M % f[i] == 0 && M != f[i]) return f[i];
+  return M;
+}
+
+// ------------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::
+          "r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void *src, int c0, int c1, int c2, int c3) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// ------------------------------------------------------------------ register codelets (compile-time size)
+
+template <int DIR, typename T> __device__ __forceinline__ T mmi(T a) {  // a * (-i * DIR)
+  if constexpr (DIR > 0) return mk<T>(a.y, -a.x);
+  else return mk<T>(-a.y, a.x);
+}
+template <int DIR, typename T> __device__ __forceinline__ T twid(T t) {
+  if constexpr (DIR < 0) t.y = -t.y;
+  return t;
+}
+
+// cos(2 pi m / r) and sin(2 pi m / r), m = 1..(r-1)/2, for the odd prime codelets
+template <int RR> __host__ __device__ constexpr double odd_cos(int m) {
+  if (RR == 3) return -0.5;
+  if (RR == 5) return m == 1 ? 0.30901699437494742410229341718281905886 : -0.80901699437494742410229341718281905886;
+  return m == 1 ? 0.62348980185873353052500488400423981063
+                : (m == 2 ? -0.22252093395631440428890256449679475947 : -0.90096886790241912623610231950744505117);
+}
+template <int RR> __host__ __device__ constexpr double odd_sin(int m) {
+  if (RR == 3) return 0.86602540378443864676372317075293618347;
+  if (RR == 5) return m == 1 ? 0.95105651629515357211643933337938214341 : 0.58778525229247312916870595463907276860;
+  return m == 1 ? 0.78183148246802980870844452667405775023
+                : (m == 2 ? 0.97492791218182360701813168299393121723 : 0.43388373911755812047576833284835875461);
+}
+
+template <int M, int DIR, int N, typename T>
+__device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
+  using R = decltype(T::x);
+  if constexpr (M == 1) {
+  } else if constexpr (M == 2) {
+    T a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (M == 4) {
+    T t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    T t2 = cadd(v[1], v[3]), t3 = mmi<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  } else if constexpr (M == 8) {
+    const R h = R(0.70710678118654752440084436210484903928);
+    T e[4] = {v[0], v[2], v[4], v[6]};
+    T o[4] = {v[1], v[3], v[5], v[7]};
+    dft<4, DIR, N>(e, tw);
+    dft<4, DIR, N>(o, tw);
+    T w1, w3;
+    if constexpr (DIR > 0) {
+      w1 = mk<T>((o[1].x + o[1].y) * h, (o[1].y - o[1].x) * h);
+      w3 = mk<T>((o[3].y - o[3].x) * h, (-o[3].x - o[3].y) * h);
+    } else {
+      w1 = mk<T>((o[1].x - o[1].y) * h, (o[1].y + o[1].x) * h);
+      w3 = mk<T>((-o[3].x - o[3].y) * h, (o[3].x - o[3].y) * h);
+    }
+    T w2 = mmi<DIR>(o[2]);
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], w1);
+    v[5] = csub(e[1], w1);
+    v[2] = cadd(e[2], w2);
+    v[6] = csub(e[2], w2);
+    v[3] = cadd(e[3], w3);
+    v[7] = csub(e[3], w3);
+  } else if constexpr (M == 3 || M == 5 || M == 7) {
+    constexpr int H = (M - 1) / 2;
+    T a[H], b[H];
+#pragma unroll
+    for (int m = 1; m <= H; m++) {
+      a[m - 1] = cadd(v[m], v[M - m]);
+      b[m - 1] = csub(v[m], v[M - m]);
+    }
+    const T x0 = v[0];
+    T s = x0;
+#pragma unroll
+    for (int m = 0; m < H; m++) s = cadd(s, a[m]);
+    T y[M];
+    y[0] = s;
+#pragma unroll
+    for (int k = 1; k <= H; k++) {
+      T re = x0, im = mk<T>(R(0), R(0));
+#pragma unroll
+      for (int m = 1; m <= H; m++) {
+        const int idx = (m * k) % M;
+        const R c = idx <= H ? R(odd_cos<M>(idx)) : R(odd_cos<M>(M - idx));
+        const R sn = idx <= H ? R(odd_sin<M>(idx)) : -R(odd_sin<M>(M - idx));
+        re = cadd(re, cscale(a[m - 1], c));
+        im = cadd(im, cscale(b[m - 1], sn));
+      }
+      const T t = mmi<DIR>(im);
+      y[k] = cadd(re, t);
+      y[M - k] = csub(re, t);
+    }
+#pragma unroll
+    for (int k = 0; k < M; k++) v[k] = y[k];
+  } else {
+    // composite: Cooley-Tukey M = A * B, twiddles W_M^t = tw[t * N / M]
+    constexpr int A = first_factor(M);
+    constexpr int B = M / A;
+    T tmp[M];
+#pragma unroll
+    for (int j2 = 0; j2 < B; j2++) {
+      T s[A];
+#pragma unroll
+      for (int j1 = 0; j1 < A; j1++) s[j1] = v[j2 + B * j1];
+      dft<A, DIR, N>(s, tw);
+#pragma unroll
+      for (int k1 = 0; k1 < A; k1++) {
+        if (j2 * k1 == 0) tmp[k1 * B + j2] = s[k1];
+        else tmp[k1 * B + j2] = cmul(s[k1], twid<DIR>(tw[(j2 * k1) * (N / M)]));
+      }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; k1++) {
+      T s[B];
+#pragma unroll
+      for (int j2 = 0; j2 < B; j2++) s[j2] = tmp[k1 * B + j2];
+      dft<B, DIR, N>(s, tw);
+#pragma unroll
+      for (int k2 = 0; k2 < B; k2++) v[k1 + A * k2] = s[k2];
+    }
+  }
+}
+
+// Two-level in-place transform of a [N][W] tile (rows = points, natural order in and out).
+template <int N, int DIR, int W, int NT, typename T>
+__device__ __forceinline__ void tile_dft(T *__restrict__ buf, const T *__restrict__ tw) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  // step A: N1-point DFTs down the columns j2 (stride N2), twiddle W_N^{j2 k1}, in place
+  for (int it = threadIdx.x; it < W * N2; it += NT) {
+    const int w = it % W, j2 = it / W;
+    T s[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) s[j1] = buf[(j2 + N2 * j1) * W + w];
+    dft<N1, DIR, N>(s, tw);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; k1++) s[k1] = cmul(s[k1], twid<DIR>(tw[j2 * k1]));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) buf[(j2 + N2 * k1) * W + w] = s[k1];
+  }
+  __syncthreads();
+  // step B: N2-point DFTs along the rows k1, written back in natural order k1 + N1 k2
+  constexpr int IB = (W * N1 + NT - 1) / NT;
+  T r[IB][N2];
+#pragma unroll
+  for (int b = 0; b < IB; b++) {
+    const int it = threadIdx.x + b * NT;
+    if (it < W * N1) {
+      const int w = it % W, k1 = it / W;
+#pragma unroll
+      for (int j2 = 0; j2 < N2; j2++) r[b][j2] = buf[(j2 + N2 * k1) * W + w];
+      dft<N2, DIR, N>(r[b], tw);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < IB; b++) {
+    const int it = threadIdx.x + b * NT;
+    if (it < W * N1) {
+      const int w = it % W, k1 = it / W;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) buf[(k1 + N1 * k2) * W + w] = r[b][k2];
+    }
+  }
+  __syncthreads();
+}
+
+struct Geom2 {
+  Geom g;           // grid and line decomposition (point strides)
+  int axis;
+  int nsb;          // state blocks per line
+  long long ntiles;
+  int stages;
+  int cwords;       // 32-bit words per complex element
+};
+
+template <int VAR> constexpr int dir_first() { return (VAR == INV_STORE || VAR == INV_FINAL) ? -1 : +1; }
+
+template <typename R, int N, int VAR>
+__global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
+                                                   const __grid_constant__ CUtensorMap map_out,
+                                                   const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
+                                                   const C2<R> *__restrict__ twg, int *err) {
+  using T = C2<R>;
+  constexpr int NT = 128;
+  constexpr int W = 256 / int(sizeof(T));
+  constexpr int TILE = N * W;                       // complex elements per tile
+  constexpr uint32_t TILE_BYTES = TILE * sizeof(T);
+  constexpr bool AUX = has_aux(VAR);
+  const int NS = gg.stages;
+
+  extern __shared__ __align__(1024) unsigned char smem[];
+  T *stage_in = reinterpret_cast<T *>(smem);                         // NS tiles
+  T *stage_aux = stage_in + size_t(NS) * TILE;                       // NS tiles when AUX
+  T *tw = stage_aux + (AUX ? size_t(NS) * TILE : 0);                // N twiddles
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N + (N & 1));    // NS barriers (8-byte aligned)
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bar + NS);
+
+  const Geom &g = gg.g;
+  for (int i = threadIdx.x; i < N; i += NT) tw[i] = twg[i];
+  if (threadIdx.x == 0) {
+    *abort_flag = 0;
+    for (int s = 0; s < NS; s++) mbar_init(&bar[s], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+
+  auto coords = [&](long long t, int &c0, int &c1, int &c2, int &c3) {
+    const long long L = t / gg.nsb;
+    const int s0 = int(t % gg.nsb) * W;
+    const int la = int(L / g.nb), lb = int(L % g.nb);
+    c0 = s0 * gg.cwords;
+    if (gg.axis == 2) { c1 = 0; c2 = lb; c3 = la; }        // z-lines: (x, y) fixed
+    else if (gg.axis == 1) { c1 = lb; c2 = 0; c3 = la; }   // y-lines: (x, z) fixed
+    else { c1 = lb; c2 = la; c3 = 0; }                     // x-lines: (y, z) fixed
+  };
+  auto issue = [&](int st, long long t) {
+    int c0, c1, c2, c3;
+    coords(t, c0, c1, c2, c3);
+    mbar_expect_tx(&bar[st], AUX ? 2 * TILE_BYTES : TILE_BYTES);
+    tma_load_4d(stage_in + size_t(st) * TILE, &map_in, &bar[st], c0, c1, c2, c3);
+    if constexpr (AUX) tma_load_4d(stage_aux + size_t(st) * TILE, &map_aux, &bar[st], c0, c1, c2, c3);
+  };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS; s++) {
+      const long long t = blockIdx.x + (long long)s * gridDim.x;
+      if (t < gg.ntiles) issue(s, t);
+    }
+  }
+
+  int i = 0;
+  for (long long t = blockIdx.x; t < gg.ntiles; t += gridDim.x, i++) {
+    const int st = i % NS;
+    const uint32_t par = uint32_t(i / NS) & 1u;
+    // bounded wait for this stage's TMA load
+    {
+      const uint64_t t0 = global_ns();
+      while (!mbar_try_wait(&bar[st], par)) {
+        if (*abort_flag) break;
+        if (global_ns() - t0 > 2000000000ull) {
+          *abort_flag = 1;
+          atomicExch(err, 1);
+          break;
+        }
+      }
+    }
+    __syncthreads();
+    if (*abort_flag) break;
+
+    T *buf = stage_in + size_t(st) * TILE;
+    const T *aux = stage_aux + size_t(st) * TILE;
+    const long long L = t / gg.nsb;
+    const int s0 = int(t % gg.nsb) * W;
+    const int la = int(L / g.nb), lb = int(L % g.nb);
+    const long long pbase = la * g.sa + lb * g.sb;
+
+    if constexpr (VAR == FWD_VPSI) {
+      for (int e = threadIdx.x; e < TILE; e += NT) {
+        const int m = e / W, w = e % W, s = s0 + w;
+        if (s < a.S) {
+          const long long pt = pbase + m * g.sp;
+          T v = cscale(buf[e], a.V[pt * a.nspin + a.spin] + a.vshift);
+          if (a.nl_offs) v = cadd(v, nl_term<R>(a, pt, s));
+          buf[e] = v;
+        }
+      }
+      __syncthreads();
+    }
+
+    tile_dft<N, dir_first<VAR>(), W, NT>(buf, tw);
+
+    if constexpr (VAR == MID_KIN) {
+      for (int e = threadIdx.x; e < TILE; e += NT) {
+        const int m = e / W;
+        int ix, iy, iz;
+        line_coords(gg.axis, la, lb, m, ix, iy, iz);
+        buf[e] = cscale(buf[e], R(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc)));
+      }
+      __syncthreads();
+      tile_dft<N, -1, W, NT>(buf, tw);
+    }
+
+    // epilogue in shared memory, then one TMA store of the tile
+    {
+      const bool scaled = a.scale != R(1);
+      const bool accum = (a.acc1 != nullptr) || (a.acc2 != nullptr);
+      if (scaled || AUX || accum) {
+        for (int e = threadIdx.x; e < TILE; e += NT) {
+          const int m = e / W, w = e % W, s = s0 + w;
+          if (s >= a.S) continue;
+          const long long pt = pbase + m * g.sp;
+          T v = buf[e];
+          if (scaled) v = cscale(v, a.scale);
+          if constexpr (VAR == INV_FINAL) {
+            v = cadd(v, cscale(aux[e], a.V[pt * a.nspin + a.spin] + a.vshift));
+            if (a.nl_offs) v = cadd(v, nl_term<R>(a, pt, s));
+          } else if constexpr (VAR == FWD_LAPLADD) {
+            int ix, iy, iz;
+            line_coords(gg.axis, la, lb, m, ix, iy, iz);
+            v = cadd(v, cscale(aux[e], R(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc))));
+          }
+          if (accum) {
+            const long long ge = pt * a.S + s;
+            if (a.acc1) a.acc1[ge] = cadd(a.acc1[ge], cmul(a.c1, v));
+            if (a.acc2) a.acc2[ge] = cadd(a.acc2[ge], cmul(a.c2, v));
+          }
+          buf[e] = v;
+        }
+      }
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int c0, c1, c2, c3;
+      coords(t, c0, c1, c2, c3);
+      tma_store_4d(&map_out, buf, c0, c1, c2, c3);
+      bulk_commit();
+      bulk_wait_read0();  // the stage may be refilled once the store has read it
+      const long long tn = t + (long long)NS * gridDim.x;
+      if (tn < gg.ntiles) issue(st, tn);
+    }
+  }
+  if (threadIdx.x == 0) bulk_wait0();
+}
+
+}  // namespace v2
+}  // namespace inqb
+
+// ------------------------------------------------------------------ host side
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+namespace inqb {
+namespace v2 {
+
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  INQB_REQUIRE(fn != nullptr, INQB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  return fn;
+}
+
+// 4-D map of a [nx][ny][nz][S] complex array as 32-bit words; box = W states x N points along `axis`.
+inline CUtensorMap orbital_map(const void *base, const Basis &b, int S, int cwords, int axis, int W) {
+  CUtensorMap m;
+  const cuuint64_t row = cuuint64_t(S) * cwords * 4;
+  cuuint64_t dims[4] = {cuuint64_t(S) * cwords, cuuint64_t(b.n[2]), cuuint64_t(b.n[1]), cuuint64_t(b.n[0])};
+  cuuint64_t strides[3] = {row, row * b.n[2], row * b.n[2] * b.n[1]};
+  cuuint32_t box[4] = {cuuint32_t(W * cwords), cuuint32_t(axis == 2 ? b.n[2] : 1), cuuint32_t(axis == 1 ? b.n[1] : 1),
+                       cuuint32_t(axis == 0 ? b.n[0] : 1)};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, const_cast<void *>(base), dims, strides, box,
+                                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  INQB_REQUIRE(r == CUDA_SUCCESS, INQB_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+  return m;
+}
+
+template <typename R, int N, int VAR>
+void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
+  using T = C2<R>;
+  constexpr int W = 256 / int(sizeof(T));
+  constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
+  const int nbuf = has_aux(VAR) ? 2 : 1;
+  const size_t fixed = N * sizeof(T) + 64 + 16 * 8;
+  // two CTAs per SM: stay below ~113 KB of shared memory per CTA
+  int ns = int((113 * 1024 - fixed) / (TILE_BYTES * nbuf));
+  ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
+  gg.stages = ns;
+  const size_t smem = TILE_BYTES * nbuf * ns + fixed;
+  INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
+  auto kern = fft2_kernel<R, N, VAR>;
+  static int attr_set = 0;  // per instantiation
+  static int per_sm = 0;
+  if (attr_set != int(smem)) {
+    INQB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    INQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
+    attr_set = int(smem);
+  }
+  long long grid = (long long)(per_sm < 1 ? 1 : per_sm) * ctx.num_sms;
+  if (grid > gg.ntiles) grid = gg.ntiles;
+  const int cwords = int(sizeof(T) / 4);
+  CUtensorMap mi = orbital_map(a.in, b, a.S, cwords, gg.axis, W);
+  CUtensorMap mo = orbital_map(a.out, b, a.S, cwords, gg.axis, W);
+  CUtensorMap mx = has_aux(VAR) ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W) : mi;
+  const T *tw = reinterpret_cast<const T *>(sizeof(R) == 8 ? b.tw64[gg.axis] : b.tw32[gg.axis]);
+  kern<<<unsigned(grid), 128, smem, ctx.stream>>>(mi, mo, mx, a, gg, tw, ctx.d_err);
+  INQB_CUDA(cudaGetLastError());
+  ctx.launches++;
+}
+
+template <typename R, int N>
+void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var) {
+  switch (var) {
+    case FWD_STORE: launch_kernel<R, N, FWD_STORE>(ctx, b, a, gg); break;
+    case INV_STORE: launch_kernel<R, N, INV_STORE>(ctx, b, a, gg); break;
+    case MID_KIN: launch_kernel<R, N, MID_KIN>(ctx, b, a, gg); break;
+    case INV_FINAL: launch_kernel<R, N, INV_FINAL>(ctx, b, a, gg); break;
+    case FWD_VPSI: launch_kernel<R, N, FWD_VPSI>(ctx, b, a, gg); break;
+    default: launch_kernel<R, N, FWD_LAPLADD>(ctx, b, a, gg); break;
+  }
+}
+
+// Returns false (and does nothing) when the pass is not covered by a specialised kernel.
+template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue) {
+  using T = C2<R>;
+  if (ctx.fft_impl == 1) return false;
+  const int n = b.n[a.axis];
+  if (n != 24 && n != 32 && n != 40 && n != 48 && n != 64 && n != 72 && n != 96 && n != 120 && n != 128) return false;
+  if ((size_t(a.S) * sizeof(T)) % 16 != 0) return false;
+  if (a.S < 256 / int(sizeof(T))) return false;  // fewer states than one 256-byte row: generic kernel
+  int var;
+  if (a.mid_kinetic) var = MID_KIN;
+  else if (prologue == PRO_VPSI) var = FWD_VPSI;
+  else if (epilogue == EPI_FINAL_REAL) var = INV_FINAL;
+  else if (epilogue == EPI_LAPL_ADD) var = FWD_LAPLADD;
+  else var = a.dir > 0 ? FWD_STORE : INV_STORE;
+  if ((var == INV_FINAL && a.dir > 0) || ((var == FWD_VPSI || var == FWD_LAPLADD) && a.dir < 0)) return false;
+
+  constexpr int W = 256 / int(sizeof(T));
+  Geom2 gg;
+  for (int i = 0; i < 3; i++) gg.g.n[i] = b.n[i];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) gg.g.rlat[i][j] = b.rlat[i][j];
+  const long long ny = b.n[1], nz = b.n[2];
+  if (a.axis == 2) { gg.g.nb = int(ny); gg.g.sa = ny * nz; gg.g.sb = nz; gg.g.sp = 1; }
+  else if (a.axis == 1) { gg.g.nb = int(nz); gg.g.sa = ny * nz; gg.g.sb = 1; gg.g.sp = nz; }
+  else { gg.g.nb = int(nz); gg.g.sa = nz; gg.g.sb = 1; gg.g.sp = ny * nz; }
+  gg.axis = a.axis;
+  gg.nsb = (a.S + W - 1) / W;
+  gg.ntiles = (b.npoints / n) * gg.nsb;
+  gg.cwords = int(sizeof(T) / 4);
+  gg.stages = 2;
+  switch (n) {
+    case 24: launch_n<R, 24>(ctx, b, a, gg, var); break;
+    case 32: launch_n<R, 32>(ctx, b, a, gg, var); break;
+    case 40: launch_n<R, 40>(ctx, b, a, gg, var); break;
+    case 48: launch_n<R, 48>(ctx, b, a, gg, var); break;
+    case 64: launch_n<R, 64>(ctx, b, a, gg, var); break;
+    case 72: launch_n<R, 72>(ctx, b, a, gg, var); break;
+    case 96: launch_n<R, 96>(ctx, b, a, gg, var); break;
+    case 120: launch_n<R, 120>(ctx, b, a, gg, var); break;
+    default: launch_n<R, 128>(ctx, b, a, gg, var); break;
+  }
+  return true;
+}
+
+}  // namespace v2
+}  // namespace inqb

@@ -66,6 +66,8 @@ struct Ctx {
   long long launches = 0;
   int num_sms = 0;
   size_t max_smem_optin = 0;
+  int *d_err = nullptr;      // device flag raised by a kernel whose bounded wait expired
+  int fft_impl = 0;          // 0: specialised TMA kernels where available, 1: generic kernel only
 };
 
 struct Basis {
@@ -167,6 +169,10 @@ template <typename R> struct PassArgs {
 
 template <typename R>
 void launch_fft_pass(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue);
+// specialised persistent TMA kernels (fft2.cuh); false when the pass is not covered
+template <typename R> bool launch_fft2(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue);
+template <> bool launch_fft2<float>(Ctx &ctx, const Basis &b, const PassArgs<float> &a, int prologue, int epilogue);
+template <> bool launch_fft2<double>(Ctx &ctx, const Basis &b, const PassArgs<double> &a, int prologue, int epilogue);
 
 template <typename R>
 void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<R> *psi, int S, C2<R> *projraw,

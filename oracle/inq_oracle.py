@@ -515,13 +515,21 @@ class Hamiltonian:
     def kA(self, kpoint_cov):
         return np.asarray(kpoint_cov, dtype=np.float64) + self.A_cov
 
+    def _kinetic_factor(self, kA):
+        # the per-point factor -0.5*(-|G|^2 + gc.G) depends only on k + A: keep the last one
+        key = tuple(float(v) for v in kA)
+        if getattr(self, "_kin_key", None) != key:
+            gradcoeff = -2.0 * self.rs.cell.cov_to_contra(kA)
+            self._kin = laplacian_factor(self.rs, -0.5, gradcoeff)[..., None]
+            self._kin_key = key
+        return self._kin
+
     def apply_real(self, psi, kpoint_cov=(0.0, 0.0, 0.0)):
         """ks_hamiltonian::operator()(orbital_set<real_space>) (ks_hamiltonian.hpp:137-156)."""
         kA = self.kA(kpoint_cov)
         sphere = project(self.rs, self.pa, psi, kA) if self.pa is not None and self.pa.nproj else None
         fpsi = to_fourier(psi)
-        gradcoeff = -2.0 * self.rs.cell.cov_to_contra(kA)
-        hf = laplacian(self.rs, fpsi, -0.5, gradcoeff)
+        hf = self._kinetic_factor(kA) * fpsi
         hpsi = to_real(hf)
         shift = 0.5 * float(self.rs.cell.norm_cov(kA))
         hpsi = hpsi + (self.V[..., None] + shift) * psi

@@ -37,20 +37,43 @@ def _random_orbitals(rng, sizes, nst):
 
 # ------------------------------------------------------------------ transforms
 
+@pytest.mark.parametrize("impl", [0, 1])
 @pytest.mark.parametrize("sizes,nst", [((20, 20, 20), 6), ((32, 32, 32), 16), ((18, 24, 20), 13), ((54, 54, 54), 7),
-                                       ((14, 21, 28), 3), ((24, 40, 30), 33), ((96, 96, 96), 8), ((120, 8, 10), 40)])
-def test_fft_roundtrip_and_parity(ib, rng, sizes, nst):
-    """to_fourier / to_real (transform.hpp:52-249) vs numpy's FFT; radices 2,3,4,5,7,8."""
+                                       ((14, 21, 28), 3), ((24, 40, 30), 33), ((96, 96, 96), 18), ((120, 8, 10), 40),
+                                       ((64, 72, 48), 32), ((128, 24, 40), 17)])
+def test_fft_roundtrip_and_parity(ib, rng, sizes, nst, impl):
+    """to_fourier / to_real (transform.hpp:52-249) vs numpy's FFT; radices 2,3,4,5,7,8; both FFT kernels."""
     cell = ib.Cell.orthorhombic(9.0, 12.0, 10.0)
     rs = ib.RealSpace(cell, sizes=sizes)
-    x = _random_orbitals(rng, sizes, nst)
-    phi = ib.OrbitalSet.from_array(rs, x)
-    f = ib.to_fourier(phi)
-    assert rel(f.hypercubic(), O.to_fourier(x)) < TOL64
-    back = ib.to_real(f)
-    assert rel(back.hypercubic(), x) < TOL64
-    un = ib.to_real(f, normalize=False)
-    assert rel(un.hypercubic(), x * np.prod(sizes)) < TOL64
+    rs.ctx.set_option("fft_impl", impl)
+    try:
+        x = _random_orbitals(rng, sizes, nst)
+        phi = ib.OrbitalSet.from_array(rs, x)
+        f = ib.to_fourier(phi)
+        assert rel(f.hypercubic(), O.to_fourier(x)) < TOL64
+        back = ib.to_real(f)
+        assert rel(back.hypercubic(), x) < TOL64
+        un = ib.to_real(f, normalize=False)
+        assert rel(un.hypercubic(), x * np.prod(sizes)) < TOL64
+        rs.ctx.synchronize()
+    finally:
+        rs.ctx.set_option("fft_impl", 0)
+
+
+@pytest.mark.parametrize("impl", [0, 1])
+@pytest.mark.parametrize("sizes,nst", [((48, 40, 36), 64), ((96, 96, 96), 32), ((24, 32, 72), 40)])
+def test_fft_mixed_precision_kernels(ib, rng, sizes, nst, impl):
+    """FP32 transforms through both kernels: relative error <= 2e-6 against the FP64 oracle."""
+    rs = ib.RealSpace(ib.Cell.cubic(10.0), sizes=sizes)
+    rs.ctx.set_option("fft_impl", impl)
+    try:
+        x = _random_orbitals(rng, sizes, nst)
+        phi = ib.OrbitalSet.from_array(rs, x, precision=ib.F32)
+        f = ib.to_fourier(phi)
+        assert rel(f.hypercubic(), O.to_fourier(x)) < TOL32
+        assert rel(ib.to_real(f).hypercubic(), x) < TOL32
+    finally:
+        rs.ctx.set_option("fft_impl", 0)
 
 
 def test_fft_mixed_precision(ib, rng):
@@ -180,6 +203,40 @@ def test_hamiltonian_fourier_parity(ib, c1):
     fph = ib.OrbitalSet.from_array(basis, fx, kpoint=kp, space=ib.FOURIER_SPACE)
     h = ham(fph).hypercubic()
     assert rel(h, oh.apply_fourier(fx, kp)) < TOL64
+
+
+@pytest.fixture(scope="module")
+def c1big(ib):
+    """C1 construction with 64 states: every FFT axis and state count goes through the TMA kernels."""
+    from inq_b200 import synthetic
+    sysm = synthetic.config("c1", nst=64)
+    basis, ham, phi = synthetic.build(sysm)
+    oh, ors = _oracle_system(sysm)
+    return sysm, basis, ham, phi, oh, ors
+
+
+@pytest.mark.parametrize("impl", [0, 1])
+def test_hamiltonian_kernels_both_paths(ib, c1big, impl):
+    """Real- and Fourier-form H through the specialised (0) and generic (1) FFT kernels, FP64 and FP32."""
+    sysm, basis, ham, phi, oh, ors = c1big
+    basis.ctx.set_option("fft_impl", impl)
+    try:
+        x = phi.hypercubic()
+        kp = (0.2, -0.1, 0.05)
+        ref = oh.apply_real(x, kp)
+        h = ham(ib.OrbitalSet.from_array(basis, x, kpoint=kp)).hypercubic()
+        assert rel(h, ref) < TOL64
+        h32 = ham(ib.OrbitalSet.from_array(basis, x, kpoint=kp, precision=ib.F32)).hypercubic()
+        assert rel(h32, ref) < TOL32
+        fx = O.to_fourier(x)
+        hf = ham(ib.OrbitalSet.from_array(basis, fx, kpoint=kp, space=ib.FOURIER_SPACE)).hypercubic()
+        assert rel(hf, oh.apply_fourier(fx, kp)) < TOL64
+        p = phi.copy()
+        ib.exponential_in_place(ham, complex(0.0, -0.025), p)
+        assert rel(p.hypercubic(), O.exponential_in_place(oh.apply_real, complex(0.0, -0.025), x)) < TOL64
+        basis.ctx.synchronize()
+    finally:
+        basis.ctx.set_option("fft_impl", 0)
 
 
 def test_hamiltonian_deterministic(ib, c1):
