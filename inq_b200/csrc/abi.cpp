@@ -165,19 +165,13 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   a.nspin = h.nspin;
   a.spin = in.spin_index;
   a.vshift = R(0.5 * norm_cov(b, kA));
-  if (h.proj.nproj > 0) {
-    a.nl_offs = h.proj.d_offs;
-    a.nl_hit = h.proj.d_hit;
-    if constexpr (sizeof(R) == 8) a.nl_hcoef = h.proj.d_hcoef;
-    else a.nl_hcoef = h.proj.d_hcoef32;
-    a.projD = projD;
-    a.maxsph = h.proj.maxsph;
-  }
   a.acc1 = static_cast<C2<R> *>(acc.acc1);
   a.acc2 = static_cast<C2<R> *>(acc.acc2);
   a.c1 = mk<C2<R>>(R(acc.c1[0]), R(acc.c1[1]));
   a.c2 = mk<C2<R>>(R(acc.c2[0]), R(acc.c2[1]));
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_FINAL_REAL);
+  // nonlocal term added at the sphere points (and to the Taylor accumulators) by its own kernel
+  if (h.proj.nproj > 0) launch_nl_apply<R>(ctx, h, projD, S, hpsi, a.acc1, a.c1, a.acc2, a.c2);
 }
 
 template <typename R> void apply_fourier(Hamiltonian &h, const Orbitals &in, Orbitals &out) {
@@ -402,7 +396,7 @@ template <typename T> std::vector<T> download(Ctx &ctx, const void *dev, size_t 
 }
 
 void free_projectors(Projectors &P) {
-  void *ptrs[] = {P.d_pt, P.d_pos, P.d_mat, P.d_coeff, P.d_coeff32, P.d_npts, P.d_offs, P.d_hit,
+  void *ptrs[] = {P.d_pt, P.d_pos, P.d_mat, P.d_coeff, P.d_coeff32, P.d_npts, P.d_offs, P.d_hit, P.d_hitpts,
                   P.d_gcoef, P.d_hcoef, P.d_gcoef32, P.d_hcoef32};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -473,6 +467,10 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
     hit[k] = hits[k].second;
   }
   for (long long i = 0; i < b.npoints; i++) offs[size_t(i) + 1] += offs[size_t(i)];
+  std::vector<int> hitpts;
+  for (size_t k = 0; k < hits.size(); k++)
+    if (k == 0 || hits[k].first != hits[k - 1].first) hitpts.push_back(int(hits[k].first));
+  P.nhitpts = (long long)hitpts.size();
 
   P.d_pt = upload_vec(flat);
   P.d_pos = upload_vec(P.h_pos);
@@ -482,6 +480,7 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
   P.d_npts = upload_vec(P.h_npts);
   P.d_offs = upload_vec(offs);
   P.d_hit = upload_vec(hit);
+  P.d_hitpts = upload_vec(hitpts);
   INQB_CUDA(cudaMalloc(&P.d_gcoef, sizeof(double2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4)));
   INQB_CUDA(cudaMalloc(&P.d_gcoef32, sizeof(float2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4)));
   INQB_CUDA(cudaMalloc(&P.d_hcoef, sizeof(double2) * std::max<size_t>(1, size_t(P.total) * 4)));
@@ -556,6 +555,9 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     if (k == "fft_impl") {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_impl is 0 (specialised) or 1 (generic)");
       ctx->fft_impl = int(value);
+    } else if (k == "mixed_compute") {
+      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "mixed_compute is 0 (FP32 arithmetic) or 1 (FP64)");
+      ctx->mixed_compute = int(value);
     } else {
       throw Error(INQB_ERR_ARG, "unknown option " + k);
     }

@@ -212,32 +212,36 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
 }
 
 // Two-level in-place transform of a [N][W] tile (rows = points, natural order in and out).
-template <int N, int DIR, int W, int NT, typename T>
-__device__ __forceinline__ void tile_dft(T *__restrict__ buf, const T *__restrict__ tw) {
+template <typename TO, typename TI> __device__ __forceinline__ TO conv(TI x) { return mk<TO>(decltype(TO::x)(x.x), decltype(TO::x)(x.y)); }
+
+// The tile is stored in shared memory as T (the orbital precision); the arithmetic runs in TC
+// registers (equal to T, or double2 for single-precision orbitals with double-precision butterflies).
+template <int N, int DIR, int W, int NT, typename T, typename TC>
+__device__ __forceinline__ void tile_dft(T *__restrict__ buf, const TC *__restrict__ tw) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   // step A: N1-point DFTs down the columns j2 (stride N2), twiddle W_N^{j2 k1}, in place
   for (int it = threadIdx.x; it < W * N2; it += NT) {
     const int w = it % W, j2 = it / W;
-    T s[N1];
+    TC s[N1];
 #pragma unroll
-    for (int j1 = 0; j1 < N1; j1++) s[j1] = buf[(j2 + N2 * j1) * W + w];
+    for (int j1 = 0; j1 < N1; j1++) s[j1] = conv<TC>(buf[(j2 + N2 * j1) * W + w]);
     dft<N1, DIR, N>(s, tw);
 #pragma unroll
     for (int k1 = 1; k1 < N1; k1++) s[k1] = cmul(s[k1], twid<DIR>(tw[j2 * k1]));
 #pragma unroll
-    for (int k1 = 0; k1 < N1; k1++) buf[(j2 + N2 * k1) * W + w] = s[k1];
+    for (int k1 = 0; k1 < N1; k1++) buf[(j2 + N2 * k1) * W + w] = conv<T>(s[k1]);
   }
   __syncthreads();
   // step B: N2-point DFTs along the rows k1, written back in natural order k1 + N1 k2
   constexpr int IB = (W * N1 + NT - 1) / NT;
-  T r[IB][N2];
+  TC r[IB][N2];
 #pragma unroll
   for (int b = 0; b < IB; b++) {
     const int it = threadIdx.x + b * NT;
     if (it < W * N1) {
       const int w = it % W, k1 = it / W;
 #pragma unroll
-      for (int j2 = 0; j2 < N2; j2++) r[b][j2] = buf[(j2 + N2 * k1) * W + w];
+      for (int j2 = 0; j2 < N2; j2++) r[b][j2] = conv<TC>(buf[(j2 + N2 * k1) * W + w]);
       dft<N2, DIR, N>(r[b], tw);
     }
   }
@@ -248,7 +252,7 @@ __device__ __forceinline__ void tile_dft(T *__restrict__ buf, const T *__restric
     if (it < W * N1) {
       const int w = it % W, k1 = it / W;
 #pragma unroll
-      for (int k2 = 0; k2 < N2; k2++) buf[(k1 + N1 * k2) * W + w] = r[b][k2];
+      for (int k2 = 0; k2 < N2; k2++) buf[(k1 + N1 * k2) * W + w] = conv<T>(r[b][k2]);
     }
   }
   __syncthreads();
@@ -265,12 +269,13 @@ struct Geom2 {
 
 template <int VAR> constexpr int dir_first() { return (VAR == INV_STORE || VAR == INV_FINAL) ? -1 : +1; }
 
-template <typename R, int N, int VAR>
+template <typename R, typename CR, int N, int VAR>
 __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
                                                    const __grid_constant__ CUtensorMap map_out,
                                                    const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
-                                                   const C2<R> *__restrict__ twg, int *err) {
+                                                   const C2<CR> *__restrict__ twg, int *err) {
   using T = C2<R>;
+  using TC = C2<CR>;
   constexpr int NT = 128;
   constexpr int W = 256 / int(sizeof(T));
   constexpr int TILE = N * W;                       // complex elements per tile
@@ -281,8 +286,9 @@ __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUten
   extern __shared__ __align__(1024) unsigned char smem[];
   T *stage_in = reinterpret_cast<T *>(smem);                         // NS tiles
   T *stage_aux = stage_in + size_t(NS) * TILE;                       // NS tiles when AUX
-  T *tw = stage_aux + (AUX ? size_t(NS) * TILE : 0);                // N twiddles
-  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N + (N & 1));    // NS barriers (8-byte aligned)
+  TC *tw = reinterpret_cast<TC *>(stage_aux + (AUX ? size_t(NS) * TILE : 0));  // N twiddles
+  CR *linev = reinterpret_cast<CR *>(tw + N);                        // N per-point factors of the current line
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N + N);          // NS barriers (8-byte aligned)
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar + NS);
 
   const Geom &g = gg.g;
@@ -344,12 +350,24 @@ __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUten
     const int la = int(L / g.nb), lb = int(L % g.nb);
     const long long pbase = la * g.sa + lb * g.sb;
 
+    // per-point factors of this line, computed once per tile (consumed after the next barrier)
+    if constexpr (VAR == MID_KIN || VAR == FWD_LAPLADD) {
+      for (int m = threadIdx.x; m < N; m += NT) {
+        int ix, iy, iz;
+        line_coords(gg.axis, la, lb, m, ix, iy, iz);
+        linev[m] = CR(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc));
+      }
+    } else if constexpr (VAR == INV_FINAL || VAR == FWD_VPSI) {
+      for (int m = threadIdx.x; m < N; m += NT)
+        linev[m] = CR(a.V[(pbase + m * g.sp) * a.nspin + a.spin]) + CR(a.vshift);
+    }
     if constexpr (VAR == FWD_VPSI) {
+      __syncthreads();
       for (int e = threadIdx.x; e < TILE; e += NT) {
         const int m = e / W, w = e % W, s = s0 + w;
         if (s < a.S) {
           const long long pt = pbase + m * g.sp;
-          T v = cscale(buf[e], a.V[pt * a.nspin + a.spin] + a.vshift);
+          T v = conv<T>(cscale(conv<TC>(buf[e]), linev[m]));
           if (a.nl_offs) v = cadd(v, nl_term<R>(a, pt, s));
           buf[e] = v;
         }
@@ -357,17 +375,12 @@ __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUten
       __syncthreads();
     }
 
-    tile_dft<N, dir_first<VAR>(), W, NT>(buf, tw);
+    tile_dft<N, dir_first<VAR>(), W, NT, T, TC>(buf, tw);
 
     if constexpr (VAR == MID_KIN) {
-      for (int e = threadIdx.x; e < TILE; e += NT) {
-        const int m = e / W;
-        int ix, iy, iz;
-        line_coords(gg.axis, la, lb, m, ix, iy, iz);
-        buf[e] = cscale(buf[e], R(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc)));
-      }
+      for (int e = threadIdx.x; e < TILE; e += NT) buf[e] = conv<T>(cscale(conv<TC>(buf[e]), linev[e / W]));
       __syncthreads();
-      tile_dft<N, -1, W, NT>(buf, tw);
+      tile_dft<N, -1, W, NT, T, TC>(buf, tw);
     }
 
     // epilogue in shared memory, then one TMA store of the tile
@@ -379,15 +392,12 @@ __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUten
           const int m = e / W, w = e % W, s = s0 + w;
           if (s >= a.S) continue;
           const long long pt = pbase + m * g.sp;
-          T v = buf[e];
-          if (scaled) v = cscale(v, a.scale);
+          TC vc = conv<TC>(buf[e]);
+          if (scaled) vc = cscale(vc, CR(a.scale));
+          if constexpr (VAR == INV_FINAL || VAR == FWD_LAPLADD) vc = cadd(vc, cscale(conv<TC>(aux[e]), linev[m]));
+          T v = conv<T>(vc);
           if constexpr (VAR == INV_FINAL) {
-            v = cadd(v, cscale(aux[e], a.V[pt * a.nspin + a.spin] + a.vshift));
             if (a.nl_offs) v = cadd(v, nl_term<R>(a, pt, s));
-          } else if constexpr (VAR == FWD_LAPLADD) {
-            int ix, iy, iz;
-            line_coords(gg.axis, la, lb, m, ix, iy, iz);
-            v = cadd(v, cscale(aux[e], R(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc))));
           }
           if (accum) {
             const long long ge = pt * a.S + s;
@@ -454,20 +464,21 @@ inline CUtensorMap orbital_map(const void *base, const Basis &b, int S, int cwor
   return m;
 }
 
-template <typename R, int N, int VAR>
+template <typename R, typename CR, int N, int VAR>
 void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   using T = C2<R>;
+  using TC = C2<CR>;
   constexpr int W = 256 / int(sizeof(T));
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
   const int nbuf = has_aux(VAR) ? 2 : 1;
-  const size_t fixed = N * sizeof(T) + 64 + 16 * 8;
+  const size_t fixed = 2 * N * sizeof(TC) + 64 + 16 * 8;
   // two CTAs per SM: stay below ~113 KB of shared memory per CTA
   int ns = int((113 * 1024 - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   gg.stages = ns;
   const size_t smem = TILE_BYTES * nbuf * ns + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
-  auto kern = fft2_kernel<R, N, VAR>;
+  auto kern = fft2_kernel<R, CR, N, VAR>;
   static int attr_set = 0;  // per instantiation
   static int per_sm = 0;
   if (attr_set != int(smem)) {
@@ -481,22 +492,34 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   CUtensorMap mi = orbital_map(a.in, b, a.S, cwords, gg.axis, W);
   CUtensorMap mo = orbital_map(a.out, b, a.S, cwords, gg.axis, W);
   CUtensorMap mx = has_aux(VAR) ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W) : mi;
-  const T *tw = reinterpret_cast<const T *>(sizeof(R) == 8 ? b.tw64[gg.axis] : b.tw32[gg.axis]);
+  const TC *tw = reinterpret_cast<const TC *>(sizeof(CR) == 8 ? b.tw64[gg.axis] : b.tw32[gg.axis]);
   kern<<<unsigned(grid), 128, smem, ctx.stream>>>(mi, mo, mx, a, gg, tw, ctx.d_err);
   INQB_CUDA(cudaGetLastError());
   ctx.launches++;
 }
 
+template <typename R, typename CR, int N>
+void launch_nc(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var) {
+  switch (var) {
+    case FWD_STORE: launch_kernel<R, CR, N, FWD_STORE>(ctx, b, a, gg); break;
+    case INV_STORE: launch_kernel<R, CR, N, INV_STORE>(ctx, b, a, gg); break;
+    case MID_KIN: launch_kernel<R, CR, N, MID_KIN>(ctx, b, a, gg); break;
+    case INV_FINAL: launch_kernel<R, CR, N, INV_FINAL>(ctx, b, a, gg); break;
+    case FWD_VPSI: launch_kernel<R, CR, N, FWD_VPSI>(ctx, b, a, gg); break;
+    default: launch_kernel<R, CR, N, FWD_LAPLADD>(ctx, b, a, gg); break;
+  }
+}
+
+// single-precision orbitals run their butterflies in double unless the context asks for single
 template <typename R, int N>
 void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var) {
-  switch (var) {
-    case FWD_STORE: launch_kernel<R, N, FWD_STORE>(ctx, b, a, gg); break;
-    case INV_STORE: launch_kernel<R, N, INV_STORE>(ctx, b, a, gg); break;
-    case MID_KIN: launch_kernel<R, N, MID_KIN>(ctx, b, a, gg); break;
-    case INV_FINAL: launch_kernel<R, N, INV_FINAL>(ctx, b, a, gg); break;
-    case FWD_VPSI: launch_kernel<R, N, FWD_VPSI>(ctx, b, a, gg); break;
-    default: launch_kernel<R, N, FWD_LAPLADD>(ctx, b, a, gg); break;
+  if constexpr (sizeof(R) == 4) {
+    if (ctx.mixed_compute == 0) {
+      launch_nc<R, float, N>(ctx, b, a, gg, var);
+      return;
+    }
   }
+  launch_nc<R, double, N>(ctx, b, a, gg, var);
 }
 
 // Returns false (and does nothing) when the pass is not covered by a specialised kernel.

@@ -68,6 +68,7 @@ struct Ctx {
   size_t max_smem_optin = 0;
   int *d_err = nullptr;      // device flag raised by a kernel whose bounded wait expired
   int fft_impl = 0;          // 0: specialised TMA kernels where available, 1: generic kernel only
+  int mixed_compute = 1;     // single-precision orbitals: 1 = double-precision arithmetic, 0 = single
 };
 
 struct Basis {
@@ -115,6 +116,8 @@ struct Projectors {
   int *d_npts = nullptr;
   int *d_offs = nullptr;                 // [npoints + 1] CSR of sphere hits per grid point
   int *d_hit = nullptr;                  // [total] (p * maxsph + i) for each hit, sorted by point then p
+  int *d_hitpts = nullptr;               // [nhitpts] grid points with at least one hit, ascending
+  long long nhitpts = 0;
   // (k+A)-dependent coefficient tables
   double kA[3] = {1e300, 1e300, 1e300};
   double2 *d_gcoef = nullptr;            // [nproj][maxsph][4]  dV e^{+ik.r} M
@@ -180,6 +183,9 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
 void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[3]);
 template <typename R>
 void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out);
+template <typename R>
+void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out, C2<R> *acc1, C2<R> c1,
+                     C2<R> *acc2, C2<R> c2);
 
 template <typename R> void launch_fill(Ctx &ctx, C2<R> *p, long long n, double re, double im);
 template <typename R>

@@ -88,31 +88,35 @@ void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[
 // (projector_all.hpp:113-211).  CTA = (projector p, 32 states); 8 warps stride over
 // the sphere points; lanes are consecutive states so each warp load is one contiguous
 // row segment of the state-fastest layout.  The 8 warp partials are summed in order.
-template <typename R>
+template <typename R, typename A>
 __global__ void __launch_bounds__(256) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
-                                                         const int *__restrict__ pt, const C2<R> *__restrict__ gcoef,
-                                                         const int *__restrict__ npts, const R *__restrict__ coeff,
+                                                         const int *__restrict__ pt, const C2<A> *__restrict__ gcoef,
+                                                         const int *__restrict__ npts, const A *__restrict__ coeff,
                                                          int maxsph, C2<R> *projraw, C2<R> *projD) {
   using T = C2<R>;
-  __shared__ T part[8][4][32];
+  using TA = C2<A>;
+  __shared__ TA part[8][4][32];
   const int p = blockIdx.x;
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const int s = blockIdx.y * 32 + lane;
   const bool active = s < S;
   const int np = npts[p];
-  T acc[4];
+  TA acc[4];
 #pragma unroll
-  for (int l = 0; l < 4; l++) acc[l] = mk<T>(R(0), R(0));
+  for (int l = 0; l < 4; l++) acc[l] = mk<TA>(A(0), A(0));
   const long long rowbase = (long long)p * maxsph;
   int i = wp;
 #pragma unroll 1
   for (; i + 8 * 3 < np; i += 8 * 4) {
-    T v[4];
+    TA v[4];
     int q[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) q[u] = __ldg(&pt[rowbase + i + 8 * u]);
 #pragma unroll
-    for (int u = 0; u < 4; u++) v[u] = active ? psi[(long long)q[u] * S + s] : mk<T>(R(0), R(0));
+    for (int u = 0; u < 4; u++) {
+      T x = active ? psi[(long long)q[u] * S + s] : mk<T>(R(0), R(0));
+      v[u] = mk<TA>(A(x.x), A(x.y));
+    }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
 #pragma unroll
@@ -121,7 +125,8 @@ __global__ void __launch_bounds__(256) nl_project_kernel(const C2<R> *__restrict
   }
   for (; i < np; i += 8) {
     const int q = __ldg(&pt[rowbase + i]);
-    T v = active ? psi[(long long)q * S + s] : mk<T>(R(0), R(0));
+    T x = active ? psi[(long long)q * S + s] : mk<T>(R(0), R(0));
+    const TA v = mk<TA>(A(x.x), A(x.y));
 #pragma unroll
     for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(gcoef[(rowbase + i) * 4 + l], v));
   }
@@ -129,20 +134,20 @@ __global__ void __launch_bounds__(256) nl_project_kernel(const C2<R> *__restrict
   for (int l = 0; l < 4; l++) part[wp][l][lane] = acc[l];
   __syncthreads();
   if (wp == 0 && active) {
-    T pr[4];
+    TA pr[4];
 #pragma unroll
     for (int l = 0; l < 4; l++) {
-      T t = part[0][l][lane];
+      TA t = part[0][l][lane];
       for (int k = 1; k < 8; k++) t = cadd(t, part[k][l][lane]);
       pr[l] = t;
-      projraw[((long long)p * 4 + l) * S + s] = t;
+      projraw[((long long)p * 4 + l) * S + s] = mk<T>(R(t.x), R(t.y));
     }
 #pragma unroll
     for (int l = 0; l < 4; l++) {
-      T t = mk<T>(R(0), R(0));
+      TA t = mk<TA>(A(0), A(0));
 #pragma unroll
       for (int j = 0; j < 4; j++) t = cadd(t, cscale(pr[j], coeff[(p * 4 + l) * 4 + j]));
-      projD[((long long)p * 4 + l) * S + s] = t;
+      projD[((long long)p * 4 + l) * S + s] = mk<T>(R(t.x), R(t.y));
     }
   }
 }
@@ -153,16 +158,14 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   const Projectors &P = h.proj;
   if (P.nproj == 0) return;
   dim3 grid(P.nproj, (S + 31) / 32);
-  const C2<R> *gcoef;
-  const R *coeff;
-  if constexpr (sizeof(R) == 8) {
-    gcoef = P.d_gcoef;
-    coeff = P.d_coeff;
+  if (sizeof(R) == 8 || ctx.mixed_compute == 1) {
+    // double-precision coefficients and accumulation
+    nl_project_kernel<R, double><<<grid, 256, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef, P.d_npts, P.d_coeff,
+                                                                P.maxsph, projraw, projD);
   } else {
-    gcoef = P.d_gcoef32;
-    coeff = P.d_coeff32;
+    nl_project_kernel<R, float><<<grid, 256, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef32, P.d_npts, P.d_coeff32,
+                                                               P.maxsph, projraw, projD);
   }
-  nl_project_kernel<R><<<grid, 256, 0, ctx.stream>>>(psi, S, P.d_pt, gcoef, P.d_npts, coeff, P.maxsph, projraw, projD);
   LAUNCHED(ctx);
 }
 
@@ -195,6 +198,55 @@ void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   else hc = P.d_hcoef32;
   nl_scatter_kernel<R><<<grid_for(b.npoints * S, 256), 256, 0, ctx.stream>>>(b.npoints, S, P.d_offs, P.d_hit, hc,
                                                                              projD, P.maxsph, out);
+  LAUNCHED(ctx);
+}
+
+// out[pt][s] += nonlocal term at the grid points that lie in a sphere (ks_hamiltonian.hpp:153,
+// projector_all.hpp:276-288), owner computes: one thread per (hit point, state), hits of a point summed
+// in projector order, no atomics.  Optional Taylor accumulators acc += c * term (linear in the term).
+template <typename R>
+__global__ void __launch_bounds__(256) nl_apply_kernel(long long nhp, int S, const int *__restrict__ hitpts,
+                                                       const int *__restrict__ offs, const int *__restrict__ hit,
+                                                       const C2<R> *__restrict__ hcoef, const C2<R> *__restrict__ projD,
+                                                       int maxsph, C2<R> *out, C2<R> *acc1, C2<R> c1, C2<R> *acc2,
+                                                       C2<R> c2) {
+  using T = C2<R>;
+  const int lane = threadIdx.x & 31;
+  const long long row0 = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const long long rstride = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = row0; r < nhp; r += rstride) {
+    const long long pt = hitpts[r];
+    const int h0 = offs[pt], h1 = offs[pt + 1];
+    for (int s = blockIdx.y * 32 + lane; s < S; s += gridDim.y * 32) {
+      T acc = mk<T>(R(0), R(0));
+      for (int h = h0; h < h1; h++) {
+        const int p = hit[h] / maxsph;
+#pragma unroll
+        for (int l = 0; l < 4; l++) acc = cadd(acc, cmul(hcoef[(long long)h * 4 + l], projD[((long long)p * 4 + l) * S + s]));
+      }
+      const long long e = pt * S + s;
+      out[e] = cadd(out[e], acc);
+      if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, acc));
+      if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, acc));
+    }
+  }
+}
+
+template <typename R>
+void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out, C2<R> *acc1, C2<R> c1,
+                     C2<R> *acc2, C2<R> c2) {
+  const Projectors &P = h.proj;
+  if (P.nhitpts == 0) return;
+  const C2<R> *hc;
+  if constexpr (sizeof(R) == 8) hc = P.d_hcoef;
+  else hc = P.d_hcoef32;
+  const int sblocks = (S + 31) / 32;
+  long long rows = (P.nhitpts + 7) / 8;
+  long long cap = (148LL * 32 + sblocks - 1) / sblocks;
+  if (rows > cap) rows = cap;
+  dim3 grid(unsigned(rows < 1 ? 1 : rows), unsigned(sblocks));
+  nl_apply_kernel<R><<<grid, 256, 0, ctx.stream>>>(P.nhitpts, S, P.d_hitpts, P.d_offs, P.d_hit, hc, projD, P.maxsph, out,
+                                                   acc1, c1, acc2, c2);
   LAUNCHED(ctx);
 }
 
@@ -581,6 +633,8 @@ void launch_absdiff_sum(Ctx &ctx, const double *a, const double *b, long long n,
   template void launch_nl_project<R>(Ctx &, const Basis &, const Hamiltonian &, const C2<R> *, int, C2<R> *,       \
                                      C2<R> *);                                                                    \
   template void launch_nl_scatter<R>(Ctx &, const Basis &, const Hamiltonian &, const C2<R> *, int, C2<R> *);     \
+  template void launch_nl_apply<R>(Ctx &, const Hamiltonian &, const C2<R> *, int, C2<R> *, C2<R> *, C2<R>,       \
+                                   C2<R> *, C2<R>);                                                              \
   template void launch_fill<R>(Ctx &, C2<R> *, long long, double, double);                                         \
   template void launch_axpy<R>(Ctx &, C2<R> *, const C2<R> *, long long, double, double);                          \
   template void launch_shift_vec<R>(Ctx &, C2<R> *, const C2<R> *, int, long long, const double *, double);        \

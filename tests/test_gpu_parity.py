@@ -60,12 +60,14 @@ def test_fft_roundtrip_and_parity(ib, rng, sizes, nst, impl):
         rs.ctx.set_option("fft_impl", 0)
 
 
+@pytest.mark.parametrize("mixed_compute", [1, 0])
 @pytest.mark.parametrize("impl", [0, 1])
 @pytest.mark.parametrize("sizes,nst", [((48, 40, 36), 64), ((96, 96, 96), 32), ((24, 32, 72), 40)])
-def test_fft_mixed_precision_kernels(ib, rng, sizes, nst, impl):
+def test_fft_mixed_precision_kernels(ib, rng, sizes, nst, impl, mixed_compute):
     """FP32 transforms through both kernels: relative error <= 2e-6 against the FP64 oracle."""
     rs = ib.RealSpace(ib.Cell.cubic(10.0), sizes=sizes)
     rs.ctx.set_option("fft_impl", impl)
+    rs.ctx.set_option("mixed_compute", mixed_compute)
     try:
         x = _random_orbitals(rng, sizes, nst)
         phi = ib.OrbitalSet.from_array(rs, x, precision=ib.F32)
@@ -74,6 +76,7 @@ def test_fft_mixed_precision_kernels(ib, rng, sizes, nst, impl):
         assert rel(ib.to_real(f).hypercubic(), x) < TOL32
     finally:
         rs.ctx.set_option("fft_impl", 0)
+        rs.ctx.set_option("mixed_compute", 1)
 
 
 def test_fft_mixed_precision(ib, rng):
@@ -261,12 +264,25 @@ def test_nonlocal_pieces(ib, c1):
     assert np.max(np.abs(res - ores)) < 1e-9
 
 
-def test_hamiltonian_mixed_precision(ib, c1):
-    sysm, basis, ham, phi, oh, ors = c1
-    x = phi.hypercubic()
-    ph32 = phi.converted(ib.F32)
-    h = ham(ph32).hypercubic()
-    assert rel(h, oh.apply_real(x)) < TOL32
+@pytest.mark.parametrize("mixed_compute", [1, 0])
+def test_hamiltonian_mixed_precision(ib, c1big, mixed_compute):
+    """Mixed form (FP32 orbitals; FP64 or FP32 butterflies): H|psi> within 2e-6 relative and eigenvalues
+    within 1e-6 Ha (FP64 butterflies) of the FP64 oracle."""
+    sysm, basis, ham, phi, oh, ors = c1big
+    basis.ctx.set_option("mixed_compute", mixed_compute)
+    try:
+        x = phi.hypercubic()
+        ph32 = phi.converted(ib.F32)
+        h = ham(ph32).hypercubic()
+        ref = oh.apply_real(x)
+        assert rel(h, ref) < TOL32
+        eig, _ = ham.eigenvalues(ph32)
+        oeig, _ = O.eigenvalues(oh, x)
+        if mixed_compute == 1:
+            assert np.max(np.abs(eig - oeig)) < 1e-6
+            assert rel(h, ref) < 5e-7
+    finally:
+        basis.ctx.set_option("mixed_compute", 1)
 
 
 # ------------------------------------------------------------------ real time
