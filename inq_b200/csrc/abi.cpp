@@ -396,7 +396,7 @@ template <typename T> std::vector<T> download(Ctx &ctx, const void *dev, size_t 
 }
 
 void free_projectors(Projectors &P) {
-  void *ptrs[] = {P.d_pt, P.d_pos, P.d_mat, P.d_coeff, P.d_coeff32, P.d_npts, P.d_offs, P.d_hit, P.d_hitpts,
+  void *ptrs[] = {P.d_pt, P.d_pos, P.d_mat, P.d_coeff, P.d_coeff32, P.d_npts, P.d_offs, P.d_hit, P.d_hitpts, P.d_hitp,
                   P.d_gcoef, P.d_hcoef, P.d_gcoef32, P.d_hcoef32};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -467,6 +467,8 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
     hit[k] = hits[k].second;
   }
   for (long long i = 0; i < b.npoints; i++) offs[size_t(i) + 1] += offs[size_t(i)];
+  std::vector<int> hitp(hits.size());
+  for (size_t k = 0; k < hits.size(); k++) hitp[k] = hits[k].second / maxsph;
   std::vector<int> hitpts;
   for (size_t k = 0; k < hits.size(); k++)
     if (k == 0 || hits[k].first != hits[k - 1].first) hitpts.push_back(int(hits[k].first));
@@ -481,6 +483,7 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
   P.d_offs = upload_vec(offs);
   P.d_hit = upload_vec(hit);
   P.d_hitpts = upload_vec(hitpts);
+  P.d_hitp = upload_vec(hitp);
   INQB_CUDA(cudaMalloc(&P.d_gcoef, sizeof(double2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4)));
   INQB_CUDA(cudaMalloc(&P.d_gcoef32, sizeof(float2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4)));
   INQB_CUDA(cudaMalloc(&P.d_hcoef, sizeof(double2) * std::max<size_t>(1, size_t(P.total) * 4)));

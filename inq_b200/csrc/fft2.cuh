@@ -214,45 +214,64 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
 // Two-level in-place transform of a [N][W] tile (rows = points, natural order in and out).
 template <typename TO, typename TI> __device__ __forceinline__ TO conv(TI x) { return mk<TO>(decltype(TO::x)(x.x), decltype(TO::x)(x.y)); }
 
-// The tile is stored in shared memory as T (the orbital precision); the arithmetic runs in TC
-// registers (equal to T, or double2 for single-precision orbitals with double-precision butterflies).
-template <int N, int DIR, int W, int NT, typename T, typename TC>
-__device__ __forceinline__ void tile_dft(T *__restrict__ buf, const TC *__restrict__ tw) {
+// Two-level transform of one [N][W] tile.
+//   step A: N1-point DFTs down the columns j2 (points j2 + N2 j1), twiddle W_N^{j2 k1};
+//   step B: N2-point DFTs along the rows k1, outputs in natural order m = k1 + N1 k2.
+// Step A reads `asrc` (times an optional per-point factor `pre`, applied on load) and writes
+// `adst`; step B reads `adst` and hands every output value to `put(m, w, value)`.  When
+// HOLD is set (step B writes into the buffer it reads), all step-B inputs are read into
+// registers before a barrier and only then stored.
+template <int N, int DIR, int W, int NT, bool HOLD, typename TC, typename SA, typename DA, typename Put>
+__device__ __forceinline__ void tile_dft(const SA *asrc, DA *adst, const TC *__restrict__ tw,
+                                         const decltype(TC::x) *pre, Put put) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
-  // step A: N1-point DFTs down the columns j2 (stride N2), twiddle W_N^{j2 k1}, in place
   for (int it = threadIdx.x; it < W * N2; it += NT) {
     const int w = it % W, j2 = it / W;
     TC s[N1];
 #pragma unroll
-    for (int j1 = 0; j1 < N1; j1++) s[j1] = conv<TC>(buf[(j2 + N2 * j1) * W + w]);
+    for (int j1 = 0; j1 < N1; j1++) {
+      s[j1] = conv<TC>(asrc[(j2 + N2 * j1) * W + w]);
+      if (pre) s[j1] = cscale(s[j1], pre[j2 + N2 * j1]);
+    }
     dft<N1, DIR, N>(s, tw);
 #pragma unroll
     for (int k1 = 1; k1 < N1; k1++) s[k1] = cmul(s[k1], twid<DIR>(tw[j2 * k1]));
 #pragma unroll
-    for (int k1 = 0; k1 < N1; k1++) buf[(j2 + N2 * k1) * W + w] = conv<T>(s[k1]);
+    for (int k1 = 0; k1 < N1; k1++) adst[(j2 + N2 * k1) * W + w] = conv<DA>(s[k1]);
   }
   __syncthreads();
-  // step B: N2-point DFTs along the rows k1, written back in natural order k1 + N1 k2
-  constexpr int IB = (W * N1 + NT - 1) / NT;
-  TC r[IB][N2];
+  if constexpr (HOLD) {
+    constexpr int IB = (W * N1 + NT - 1) / NT;
+    TC r[IB][N2];
 #pragma unroll
-  for (int b = 0; b < IB; b++) {
-    const int it = threadIdx.x + b * NT;
-    if (it < W * N1) {
-      const int w = it % W, k1 = it / W;
+    for (int b = 0; b < IB; b++) {
+      const int it = threadIdx.x + b * NT;
+      if (it < W * N1) {
+        const int w = it % W, k1 = it / W;
 #pragma unroll
-      for (int j2 = 0; j2 < N2; j2++) r[b][j2] = conv<TC>(buf[(j2 + N2 * k1) * W + w]);
-      dft<N2, DIR, N>(r[b], tw);
+        for (int j2 = 0; j2 < N2; j2++) r[b][j2] = conv<TC>(adst[(j2 + N2 * k1) * W + w]);
+        dft<N2, DIR, N>(r[b], tw);
+      }
     }
-  }
-  __syncthreads();
+    __syncthreads();
 #pragma unroll
-  for (int b = 0; b < IB; b++) {
-    const int it = threadIdx.x + b * NT;
-    if (it < W * N1) {
+    for (int b = 0; b < IB; b++) {
+      const int it = threadIdx.x + b * NT;
+      if (it < W * N1) {
+        const int w = it % W, k1 = it / W;
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) put(k1 + N1 * k2, w, r[b][k2]);
+      }
+    }
+  } else {
+    for (int it = threadIdx.x; it < W * N1; it += NT) {
       const int w = it % W, k1 = it / W;
+      TC r[N2];
 #pragma unroll
-      for (int k2 = 0; k2 < N2; k2++) buf[(k1 + N1 * k2) * W + w] = conv<T>(r[b][k2]);
+      for (int j2 = 0; j2 < N2; j2++) r[j2] = conv<TC>(adst[(j2 + N2 * k1) * W + w]);
+      dft<N2, DIR, N>(r, tw);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) put(k1 + N1 * k2, w, r[k2]);
     }
   }
   __syncthreads();
@@ -269,14 +288,19 @@ struct Geom2 {
 
 template <int VAR> constexpr int dir_first() { return (VAR == INV_STORE || VAR == INV_FINAL) ? -1 : +1; }
 
+// threads per CTA: 256 when the butterflies run in a wider type than the storage (exchange buffer in
+// shared memory, more warps to cover the double-precision latency), 128 otherwise
+template <typename R, typename CR> constexpr int threads_of() { return sizeof(CR) > sizeof(R) ? 256 : 128; }
+
 template <typename R, typename CR, int N, int VAR>
-__global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
+__global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
                                                    const __grid_constant__ CUtensorMap map_out,
                                                    const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
                                                    const C2<CR> *__restrict__ twg, int *err) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr int NT = 128;
+  constexpr int NT = threads_of<R, CR>();
+  constexpr bool SPLIT = sizeof(CR) > sizeof(R);    // exchange buffer in the arithmetic type
   constexpr int W = 256 / int(sizeof(T));
   constexpr int TILE = N * W;                       // complex elements per tile
   constexpr uint32_t TILE_BYTES = TILE * sizeof(T);
@@ -286,7 +310,8 @@ __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUten
   extern __shared__ __align__(1024) unsigned char smem[];
   T *stage_in = reinterpret_cast<T *>(smem);                         // NS tiles
   T *stage_aux = stage_in + size_t(NS) * TILE;                       // NS tiles when AUX
-  TC *tw = reinterpret_cast<TC *>(stage_aux + (AUX ? size_t(NS) * TILE : 0));  // N twiddles
+  TC *exch = reinterpret_cast<TC *>(stage_aux + (AUX ? size_t(NS) * TILE : 0));  // one tile when SPLIT
+  TC *tw = exch + (SPLIT ? TILE : 0);                                // N twiddles
   CR *linev = reinterpret_cast<CR *>(tw + N);                        // N per-point factors of the current line
   uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N + N);          // NS barriers (8-byte aligned)
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar + NS);
@@ -324,6 +349,8 @@ __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUten
     }
   }
 
+  const bool scaled = a.scale != R(1);
+  const bool accum = (a.acc1 != nullptr) || (a.acc2 != nullptr);
   int i = 0;
   for (long long t = blockIdx.x; t < gg.ntiles; t += gridDim.x, i++) {
     const int st = i % NS;
@@ -350,7 +377,7 @@ __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUten
     const int la = int(L / g.nb), lb = int(L % g.nb);
     const long long pbase = la * g.sa + lb * g.sb;
 
-    // per-point factors of this line, computed once per tile (consumed after the next barrier)
+    // per-point factors of this line (consumed after the first barrier of the transform)
     if constexpr (VAR == MID_KIN || VAR == FWD_LAPLADD) {
       for (int m = threadIdx.x; m < N; m += NT) {
         int ix, iy, iz;
@@ -363,51 +390,52 @@ __global__ void __launch_bounds__(128) fft2_kernel(const __grid_constant__ CUten
     }
     if constexpr (VAR == FWD_VPSI) {
       __syncthreads();
-      for (int e = threadIdx.x; e < TILE; e += NT) {
-        const int m = e / W, w = e % W, s = s0 + w;
-        if (s < a.S) {
-          const long long pt = pbase + m * g.sp;
-          T v = conv<T>(cscale(conv<TC>(buf[e]), linev[m]));
-          if (a.nl_offs) v = cadd(v, nl_term<R>(a, pt, s));
-          buf[e] = v;
-        }
-      }
-      __syncthreads();
-    }
-
-    tile_dft<N, dir_first<VAR>(), W, NT, T, TC>(buf, tw);
-
-    if constexpr (VAR == MID_KIN) {
-      for (int e = threadIdx.x; e < TILE; e += NT) buf[e] = conv<T>(cscale(conv<TC>(buf[e]), linev[e / W]));
-      __syncthreads();
-      tile_dft<N, -1, W, NT, T, TC>(buf, tw);
-    }
-
-    // epilogue in shared memory, then one TMA store of the tile
-    {
-      const bool scaled = a.scale != R(1);
-      const bool accum = (a.acc1 != nullptr) || (a.acc2 != nullptr);
-      if (scaled || AUX || accum) {
+      if (a.nl_offs) {
+        // Fourier-form operator: (V + shift) psi + nonlocal(psi) formed in shared memory before the transform
         for (int e = threadIdx.x; e < TILE; e += NT) {
           const int m = e / W, w = e % W, s = s0 + w;
-          if (s >= a.S) continue;
-          const long long pt = pbase + m * g.sp;
-          TC vc = conv<TC>(buf[e]);
-          if (scaled) vc = cscale(vc, CR(a.scale));
-          if constexpr (VAR == INV_FINAL || VAR == FWD_LAPLADD) vc = cadd(vc, cscale(conv<TC>(aux[e]), linev[m]));
-          T v = conv<T>(vc);
-          if constexpr (VAR == INV_FINAL) {
-            if (a.nl_offs) v = cadd(v, nl_term<R>(a, pt, s));
+          if (s < a.S) {
+            const long long pt = pbase + m * g.sp;
+            T v = conv<T>(cscale(conv<TC>(buf[e]), linev[m]));
+            buf[e] = cadd(v, nl_term<R>(a, pt, s));
           }
-          if (accum) {
-            const long long ge = pt * a.S + s;
-            if (a.acc1) a.acc1[ge] = cadd(a.acc1[ge], cmul(a.c1, v));
-            if (a.acc2) a.acc2[ge] = cadd(a.acc2[ge], cmul(a.c2, v));
-          }
-          buf[e] = v;
         }
+        __syncthreads();
       }
     }
+
+    // final store of one output value: epilogue terms, Taylor accumulators, write into the stage
+    auto put_out = [&](int m, int w, TC v) {
+      const int s = s0 + w;
+      if (scaled) v = cscale(v, CR(a.scale));
+      if constexpr (VAR == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
+      const T o = conv<T>(v);
+      if (accum && s < a.S) {
+        const long long ge = (pbase + m * g.sp) * a.S + s;
+        if (a.acc1) a.acc1[ge] = cadd(a.acc1[ge], cmul(a.c1, o));
+        if (a.acc2) a.acc2[ge] = cadd(a.acc2[ge], cmul(a.c2, o));
+      }
+      buf[m * W + w] = o;
+    };
+    const CR *pre = (VAR == FWD_VPSI && !a.nl_offs) ? linev : nullptr;
+    constexpr int D = dir_first<VAR>();
+
+    if constexpr (VAR == MID_KIN) {
+      // forward, multiply by the kinetic factor, backward
+      if constexpr (SPLIT) {
+        tile_dft<N, +1, W, NT, true, TC>(buf, exch, tw, (const CR *)nullptr,
+                                         [&](int m, int w, TC v) { exch[m * W + w] = cscale(v, linev[m]); });
+        tile_dft<N, -1, W, NT, false, TC>(exch, exch, tw, (const CR *)nullptr, put_out);
+      } else {
+        tile_dft<N, +1, W, NT, true, TC>(buf, buf, tw, (const CR *)nullptr,
+                                         [&](int m, int w, TC v) { buf[m * W + w] = conv<T>(cscale(v, linev[m])); });
+        tile_dft<N, -1, W, NT, true, TC>(buf, buf, tw, (const CR *)nullptr, put_out);
+      }
+    } else {
+      if constexpr (SPLIT) tile_dft<N, D, W, NT, false, TC>(buf, exch, tw, pre, put_out);
+      else tile_dft<N, D, W, NT, true, TC>(buf, buf, tw, pre, put_out);
+    }
+
     fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -471,7 +499,9 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   constexpr int W = 256 / int(sizeof(T));
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
   const int nbuf = has_aux(VAR) ? 2 : 1;
-  const size_t fixed = 2 * N * sizeof(TC) + 64 + 16 * 8;
+  constexpr bool SPLIT = sizeof(CR) > sizeof(R);
+  constexpr int NT = threads_of<R, CR>();
+  const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + 2 * N * sizeof(TC) + 64 + 16 * 8;
   // two CTAs per SM: stay below ~113 KB of shared memory per CTA
   int ns = int((113 * 1024 - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
@@ -483,7 +513,7 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   static int per_sm = 0;
   if (attr_set != int(smem)) {
     INQB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    INQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
+    INQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
     attr_set = int(smem);
   }
   long long grid = (long long)(per_sm < 1 ? 1 : per_sm) * ctx.num_sms;
@@ -493,7 +523,7 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   CUtensorMap mo = orbital_map(a.out, b, a.S, cwords, gg.axis, W);
   CUtensorMap mx = has_aux(VAR) ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W) : mi;
   const TC *tw = reinterpret_cast<const TC *>(sizeof(CR) == 8 ? b.tw64[gg.axis] : b.tw32[gg.axis]);
-  kern<<<unsigned(grid), 128, smem, ctx.stream>>>(mi, mo, mx, a, gg, tw, ctx.d_err);
+  kern<<<unsigned(grid), NT, smem, ctx.stream>>>(mi, mo, mx, a, gg, tw, ctx.d_err);
   INQB_CUDA(cudaGetLastError());
   ctx.launches++;
 }

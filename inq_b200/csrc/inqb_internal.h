@@ -117,6 +117,7 @@ struct Projectors {
   int *d_offs = nullptr;                 // [npoints + 1] CSR of sphere hits per grid point
   int *d_hit = nullptr;                  // [total] (p * maxsph + i) for each hit, sorted by point then p
   int *d_hitpts = nullptr;               // [nhitpts] grid points with at least one hit, ascending
+  int *d_hitp = nullptr;                 // [total] projector index of each hit
   long long nhitpts = 0;
   // (k+A)-dependent coefficient tables
   double kA[3] = {1e300, 1e300, 1e300};

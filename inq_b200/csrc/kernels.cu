@@ -89,13 +89,14 @@ void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[
 // the sphere points; lanes are consecutive states so each warp load is one contiguous
 // row segment of the state-fastest layout.  The 8 warp partials are summed in order.
 template <typename R, typename A>
-__global__ void __launch_bounds__(256) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
+__global__ void __launch_bounds__(512) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
                                                          const int *__restrict__ pt, const C2<A> *__restrict__ gcoef,
                                                          const int *__restrict__ npts, const A *__restrict__ coeff,
                                                          int maxsph, C2<R> *projraw, C2<R> *projD) {
   using T = C2<R>;
   using TA = C2<A>;
-  __shared__ TA part[8][4][32];
+  constexpr int NW = 16;  // warps per CTA, each striding over the sphere points
+  __shared__ TA part[NW][4][32];
   const int p = blockIdx.x;
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const int s = blockIdx.y * 32 + lane;
@@ -107,11 +108,11 @@ __global__ void __launch_bounds__(256) nl_project_kernel(const C2<R> *__restrict
   const long long rowbase = (long long)p * maxsph;
   int i = wp;
 #pragma unroll 1
-  for (; i + 8 * 3 < np; i += 8 * 4) {
+  for (; i + NW * 3 < np; i += NW * 4) {
     TA v[4];
     int q[4];
 #pragma unroll
-    for (int u = 0; u < 4; u++) q[u] = __ldg(&pt[rowbase + i + 8 * u]);
+    for (int u = 0; u < 4; u++) q[u] = __ldg(&pt[rowbase + i + NW * u]);
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       T x = active ? psi[(long long)q[u] * S + s] : mk<T>(R(0), R(0));
@@ -120,10 +121,10 @@ __global__ void __launch_bounds__(256) nl_project_kernel(const C2<R> *__restrict
 #pragma unroll
     for (int u = 0; u < 4; u++) {
 #pragma unroll
-      for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(gcoef[(rowbase + i + 8 * u) * 4 + l], v[u]));
+      for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(gcoef[(rowbase + i + NW * u) * 4 + l], v[u]));
     }
   }
-  for (; i < np; i += 8) {
+  for (; i < np; i += NW) {
     const int q = __ldg(&pt[rowbase + i]);
     T x = active ? psi[(long long)q * S + s] : mk<T>(R(0), R(0));
     const TA v = mk<TA>(A(x.x), A(x.y));
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(256) nl_project_kernel(const C2<R> *__restrict
 #pragma unroll
     for (int l = 0; l < 4; l++) {
       TA t = part[0][l][lane];
-      for (int k = 1; k < 8; k++) t = cadd(t, part[k][l][lane]);
+      for (int k = 1; k < NW; k++) t = cadd(t, part[k][l][lane]);
       pr[l] = t;
       projraw[((long long)p * 4 + l) * S + s] = mk<T>(R(t.x), R(t.y));
     }
@@ -160,10 +161,10 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   dim3 grid(P.nproj, (S + 31) / 32);
   if (sizeof(R) == 8 || ctx.mixed_compute == 1) {
     // double-precision coefficients and accumulation
-    nl_project_kernel<R, double><<<grid, 256, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef, P.d_npts, P.d_coeff,
+    nl_project_kernel<R, double><<<grid, 512, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef, P.d_npts, P.d_coeff,
                                                                 P.maxsph, projraw, projD);
   } else {
-    nl_project_kernel<R, float><<<grid, 256, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef32, P.d_npts, P.d_coeff32,
+    nl_project_kernel<R, float><<<grid, 512, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef32, P.d_npts, P.d_coeff32,
                                                                P.maxsph, projraw, projD);
   }
   LAUNCHED(ctx);
@@ -206,28 +207,63 @@ void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
 // in projector order, no atomics.  Optional Taylor accumulators acc += c * term (linear in the term).
 template <typename R>
 __global__ void __launch_bounds__(256) nl_apply_kernel(long long nhp, int S, const int *__restrict__ hitpts,
-                                                       const int *__restrict__ offs, const int *__restrict__ hit,
+                                                       const int *__restrict__ offs, const int *__restrict__ hitp,
                                                        const C2<R> *__restrict__ hcoef, const C2<R> *__restrict__ projD,
-                                                       int maxsph, C2<R> *out, C2<R> *acc1, C2<R> c1, C2<R> *acc2,
-                                                       C2<R> c2) {
+                                                       C2<R> *out, C2<R> *acc1, C2<R> c1, C2<R> *acc2, C2<R> c2) {
   using T = C2<R>;
+  constexpr int MAXH = 2;  // hits of a point kept in registers; more are read again per state chunk
   const int lane = threadIdx.x & 31;
-  const long long row0 = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const long long rstride = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long r = row0; r < nhp; r += rstride) {
+  const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = warp; r < nhp; r += nwarps) {
     const long long pt = hitpts[r];
     const int h0 = offs[pt], h1 = offs[pt + 1];
-    for (int s = blockIdx.y * 32 + lane; s < S; s += gridDim.y * 32) {
-      T acc = mk<T>(R(0), R(0));
-      for (int h = h0; h < h1; h++) {
-        const int p = hit[h] / maxsph;
+    const int nh = h1 - h0;
+    int ph[MAXH];
+    T hc[MAXH][4];
 #pragma unroll
-        for (int l = 0; l < 4; l++) acc = cadd(acc, cmul(hcoef[(long long)h * 4 + l], projD[((long long)p * 4 + l) * S + s]));
+    for (int k = 0; k < MAXH; k++) {
+      if (k < nh) {
+        ph[k] = hitp[h0 + k];
+#pragma unroll
+        for (int l = 0; l < 4; l++) hc[k][l] = hcoef[(long long)(h0 + k) * 4 + l];
       }
-      const long long e = pt * S + s;
-      out[e] = cadd(out[e], acc);
-      if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, acc));
-      if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, acc));
+    }
+    for (int s0 = 0; s0 < S; s0 += 32 * 4) {
+      T accv[4];
+      long long e[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        accv[u] = mk<T>(R(0), R(0));
+        e[u] = -1;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int s = s0 + u * 32 + lane;
+        if (s >= S) continue;
+        e[u] = pt * S + s;
+#pragma unroll
+        for (int k = 0; k < MAXH; k++) {
+          if (k < nh) {
+#pragma unroll
+            for (int l = 0; l < 4; l++)
+              accv[u] = cadd(accv[u], cmul(hc[k][l], projD[((long long)ph[k] * 4 + l) * S + s]));
+          }
+        }
+        for (int k = MAXH; k < nh; k++) {
+          const int p = hitp[h0 + k];
+#pragma unroll
+          for (int l = 0; l < 4; l++)
+            accv[u] = cadd(accv[u], cmul(hcoef[(long long)(h0 + k) * 4 + l], projD[((long long)p * 4 + l) * S + s]));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (e[u] < 0) continue;
+        out[e[u]] = cadd(out[e[u]], accv[u]);
+        if (acc1) acc1[e[u]] = cadd(acc1[e[u]], cmul(c1, accv[u]));
+        if (acc2) acc2[e[u]] = cadd(acc2[e[u]], cmul(c2, accv[u]));
+      }
     }
   }
 }
@@ -240,13 +276,10 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
   const C2<R> *hc;
   if constexpr (sizeof(R) == 8) hc = P.d_hcoef;
   else hc = P.d_hcoef32;
-  const int sblocks = (S + 31) / 32;
-  long long rows = (P.nhitpts + 7) / 8;
-  long long cap = (148LL * 32 + sblocks - 1) / sblocks;
-  if (rows > cap) rows = cap;
-  dim3 grid(unsigned(rows < 1 ? 1 : rows), unsigned(sblocks));
-  nl_apply_kernel<R><<<grid, 256, 0, ctx.stream>>>(P.nhitpts, S, P.d_hitpts, P.d_offs, P.d_hit, hc, projD, P.maxsph, out,
-                                                   acc1, c1, acc2, c2);
+  long long blocks = (P.nhitpts + 7) / 8;
+  if (blocks > 148LL * 16) blocks = 148LL * 16;
+  nl_apply_kernel<R><<<unsigned(blocks), 256, 0, ctx.stream>>>(P.nhitpts, S, P.d_hitpts, P.d_offs, P.d_hitp, hc, projD,
+                                                               out, acc1, c1, acc2, c2);
   LAUNCHED(ctx);
 }
 
