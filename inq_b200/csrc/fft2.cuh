@@ -277,6 +277,47 @@ __device__ __forceinline__ void tile_dft(const SA *asrc, DA *adst, const TC *__r
   __syncthreads();
 }
 
+// In-place two-level transform of a [N][W] tile when storage and arithmetic types agree.
+template <int N, int DIR, int W, int NT, typename T>
+__device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *__restrict__ tw) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  for (int it = threadIdx.x; it < W * N2; it += NT) {
+    const int w = it % W, j2 = it / W;
+    T s[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) s[j1] = buf[(j2 + N2 * j1) * W + w];
+    dft<N1, DIR, N>(s, tw);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; k1++) s[k1] = cmul(s[k1], twid<DIR>(tw[j2 * k1]));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) buf[(j2 + N2 * k1) * W + w] = s[k1];
+  }
+  __syncthreads();
+  constexpr int IB = (W * N1 + NT - 1) / NT;
+  T r[IB][N2];
+#pragma unroll
+  for (int b = 0; b < IB; b++) {
+    const int it = threadIdx.x + b * NT;
+    if (it < W * N1) {
+      const int w = it % W, k1 = it / W;
+#pragma unroll
+      for (int j2 = 0; j2 < N2; j2++) r[b][j2] = buf[(j2 + N2 * k1) * W + w];
+      dft<N2, DIR, N>(r[b], tw);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < IB; b++) {
+    const int it = threadIdx.x + b * NT;
+    if (it < W * N1) {
+      const int w = it % W, k1 = it / W;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) buf[(k1 + N1 * k2) * W + w] = r[b][k2];
+    }
+  }
+  __syncthreads();
+}
+
 struct Geom2 {
   Geom g;           // grid and line decomposition (point strides)
   int axis;
@@ -288,9 +329,13 @@ struct Geom2 {
 
 template <int VAR> constexpr int dir_first() { return (VAR == INV_STORE || VAR == INV_FINAL) ? -1 : +1; }
 
-// threads per CTA: 256 when the butterflies run in a wider type than the storage (exchange buffer in
-// shared memory, more warps to cover the double-precision latency), 128 otherwise
-template <typename R, typename CR> constexpr int threads_of() { return sizeof(CR) > sizeof(R) ? 256 : 128; }
+// 128 threads per CTA; tiles of 256-byte rows, or 128-byte rows when the butterflies run in a wider
+// type than the storage (the tile then also needs an exchange buffer of that type, and smaller tiles
+// let three CTAs share an SM to cover the double-precision latency)
+template <typename R, typename CR> constexpr int threads_of() { return 128; }
+template <typename R, typename CR> constexpr int tile_w() {
+  return (sizeof(CR) > sizeof(R) ? 128 : 256) / int(2 * sizeof(R));
+}
 
 template <typename R, typename CR, int N, int VAR>
 __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
@@ -301,7 +346,7 @@ __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_
   using TC = C2<CR>;
   constexpr int NT = threads_of<R, CR>();
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);    // exchange buffer in the arithmetic type
-  constexpr int W = 256 / int(sizeof(T));
+  constexpr int W = tile_w<R, CR>();
   constexpr int TILE = N * W;                       // complex elements per tile
   constexpr uint32_t TILE_BYTES = TILE * sizeof(T);
   constexpr bool AUX = has_aux(VAR);
@@ -420,20 +465,32 @@ __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_
     const CR *pre = (VAR == FWD_VPSI && !a.nl_offs) ? linev : nullptr;
     constexpr int D = dir_first<VAR>();
 
-    if constexpr (VAR == MID_KIN) {
-      // forward, multiply by the kinetic factor, backward
-      if constexpr (SPLIT) {
+    if constexpr (SPLIT) {
+      if constexpr (VAR == MID_KIN) {
+        // forward, multiply by the kinetic factor, backward
         tile_dft<N, +1, W, NT, true, TC>(buf, exch, tw, (const CR *)nullptr,
                                          [&](int m, int w, TC v) { exch[m * W + w] = cscale(v, linev[m]); });
         tile_dft<N, -1, W, NT, false, TC>(exch, exch, tw, (const CR *)nullptr, put_out);
       } else {
-        tile_dft<N, +1, W, NT, true, TC>(buf, buf, tw, (const CR *)nullptr,
-                                         [&](int m, int w, TC v) { buf[m * W + w] = conv<T>(cscale(v, linev[m])); });
-        tile_dft<N, -1, W, NT, true, TC>(buf, buf, tw, (const CR *)nullptr, put_out);
+        tile_dft<N, D, W, NT, false, TC>(buf, exch, tw, pre, put_out);
       }
     } else {
-      if constexpr (SPLIT) tile_dft<N, D, W, NT, false, TC>(buf, exch, tw, pre, put_out);
-      else tile_dft<N, D, W, NT, true, TC>(buf, buf, tw, pre, put_out);
+      if constexpr (VAR == FWD_VPSI) {
+        if (!a.nl_offs) {
+          for (int e = threadIdx.x; e < TILE; e += NT) buf[e] = cscale(buf[e], linev[e / W]);
+          __syncthreads();
+        }
+      }
+      tile_dft_inplace<N, D, W, NT, T>(buf, reinterpret_cast<const T *>(tw));
+      if constexpr (VAR == MID_KIN) {
+        for (int e = threadIdx.x; e < TILE; e += NT) buf[e] = cscale(buf[e], linev[e / W]);
+        __syncthreads();
+        tile_dft_inplace<N, -1, W, NT, T>(buf, reinterpret_cast<const T *>(tw));
+      }
+      if (scaled || AUX || accum) {
+        for (int e = threadIdx.x; e < TILE; e += NT) put_out(e / W, e % W, buf[e]);
+        __syncthreads();
+      }
     }
 
     fence_proxy_async();
@@ -496,16 +553,19 @@ template <typename R, typename CR, int N, int VAR>
 void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr int W = 256 / int(sizeof(T));
+  constexpr int W = tile_w<R, CR>();
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
   const int nbuf = has_aux(VAR) ? 2 : 1;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
   constexpr int NT = threads_of<R, CR>();
   const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + 2 * N * sizeof(TC) + 64 + 16 * 8;
-  // two CTAs per SM: stay below ~113 KB of shared memory per CTA
-  int ns = int((113 * 1024 - fixed) / (TILE_BYTES * nbuf));
+  // shared memory per CTA: ~113 KB (two CTAs per SM), ~74 KB for the wide-arithmetic kernels (three)
+  const size_t budget = SPLIT ? 74 * 1024 : 113 * 1024;
+  int ns = int((budget - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   gg.stages = ns;
+  gg.nsb = (a.S + W - 1) / W;
+  gg.ntiles = (b.npoints / b.n[gg.axis]) * gg.nsb;
   const size_t smem = TILE_BYTES * nbuf * ns + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
   auto kern = fft2_kernel<R, CR, N, VAR>;
