@@ -559,7 +559,7 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_impl is 0 (specialised) or 1 (generic)");
       ctx->fft_impl = int(value);
     } else if (k == "mixed_compute") {
-      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "mixed_compute is 0 (FP32 arithmetic) or 1 (FP64)");
+      INQB_REQUIRE(value >= 0 && value <= 3, INQB_ERR_ARG, "mixed_compute is 0, 1, 2 or 3");
       ctx->mixed_compute = int(value);
     } else {
       throw Error(INQB_ERR_ARG, "unknown option " + k);

@@ -600,11 +600,17 @@ void launch_nc(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var
   }
 }
 
-// single-precision orbitals run their butterflies in double unless the context asks for single
+// Arithmetic of the passes over single-precision orbitals (context option mixed_compute):
+//   0 single precision everywhere; 1 double precision everywhere;
+//   2 double except the final (inverse, epilogue) pass of the real-space operator;
+//   3 as 2 and the first forward pass (z) of every transform also single.
 template <typename R, int N>
 void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var) {
   if constexpr (sizeof(R) == 4) {
-    if (ctx.mixed_compute == 0) {
+    const int mode = ctx.mixed_compute;
+    const bool single = mode == 0 || (mode >= 2 && var == INV_FINAL) ||
+                        (mode == 3 && a.axis == 2 && (var == FWD_STORE || var == FWD_VPSI));
+    if (single) {
       launch_nc<R, float, N>(ctx, b, a, gg, var);
       return;
     }
