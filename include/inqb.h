@@ -161,6 +161,17 @@ int inqb_kinetic_expectation_value(const inqb_hamiltonian *ham, const inqb_orbit
 int inqb_overlap(const inqb_orbitals *a, const inqb_orbitals *b, double *out);
 /* operations::overlap_diagonal (overlap_diagonal.hpp:25-55): host out [nst] complex128. */
 int inqb_overlap_diagonal(const inqb_orbitals *a, const inqb_orbitals *b, double *out);
+/* No counterpart in the reference: inqb_overlap_diagonal for callers that cannot let the
+ * library allocate device memory (a serving loop whose admission control has handed all
+ * device memory to resident orbital sets; latency-sensitive code that must not risk the
+ * implicit synchronisation of cudaMalloc/cudaFree).  Allocates nothing: out_dev is a
+ * caller-owned device buffer of nst complex128 (2*nst doubles) on the sets' device, and the
+ * reduction's partial sums use a fixed 2.3 MiB array inside the library (held by every GPU
+ * that loads it).  At most 512 states; larger sets get INQB_ERR_ARG.  Asynchronous on the
+ * context's stream.  The first call on a device looks up that array's device address; make
+ * it before any stream capture.  All calls share the array: calls that overlap on the GPU
+ * (different streams or contexts) race. */
+int inqb_overlap_diagonal_noalloc(const inqb_orbitals *a, const inqb_orbitals *b, double *out_dev);
 /* operations::orthogonalize (orthogonalize.hpp:25-31): FP64 overlap, FP64 Cholesky
  * (matrix/cholesky.hpp:28-99), phi <- phi U^-1 (rotate.hpp:147-156). */
 int inqb_orthogonalize(inqb_orbitals *phi);

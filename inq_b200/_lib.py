@@ -76,6 +76,7 @@ SIGNATURES = {
     "inqb_kinetic_expectation_value": (I, [P, P, DP]),
     "inqb_overlap": (I, [P, P, DP]),
     "inqb_overlap_diagonal": (I, [P, P, DP]),
+    "inqb_overlap_diagonal_noalloc": (I, [P, P, P]),
     "inqb_orthogonalize": (I, [P]),
     "inqb_shift": (I, [D, D, P, P]),
     "inqb_rotate": (I, [P, DP]),
