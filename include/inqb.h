@@ -55,9 +55,9 @@ int inqb_ctx_stream(inqb_ctx *ctx, void **stream);
 int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
 /* Tuning options: "fft_impl" = 0 (specialised persistent TMA kernels where a line length
  * has one, the default) or 1 (generic kernel for every length); "mixed_compute" selects
- * the butterfly arithmetic of single-precision orbitals: 1 double everywhere (default),
- * 0 single everywhere, 2 double except the last inverse pass of H, 3 as 2 and single for
- * the first forward pass too. */
+ * the butterfly arithmetic of single-precision orbitals: 0 single everywhere, 1 double
+ * everywhere, 2 double except the last inverse pass of H, 3 (default) as 2 and single for
+ * the first forward pass of every transform too. */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Free and total device memory in bytes (admission control for serving). */
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);

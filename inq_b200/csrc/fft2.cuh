@@ -559,8 +559,8 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
   constexpr int NT = threads_of<R, CR>();
   const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + 2 * N * sizeof(TC) + 64 + 16 * 8;
-  // shared memory per CTA: ~113 KB (two CTAs per SM), ~74 KB for the wide-arithmetic kernels (three)
-  const size_t budget = SPLIT ? 74 * 1024 : 113 * 1024;
+  // shared memory per CTA: ~113 KB (two CTAs per SM), ~56 KB for the wide-arithmetic kernels (four)
+  const size_t budget = SPLIT ? 56 * 1024 : 113 * 1024;
   int ns = int((budget - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   gg.stages = ns;

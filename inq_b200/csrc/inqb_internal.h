@@ -68,7 +68,7 @@ struct Ctx {
   size_t max_smem_optin = 0;
   int *d_err = nullptr;      // device flag raised by a kernel whose bounded wait expired
   int fft_impl = 0;          // 0: specialised TMA kernels where available, 1: generic kernel only
-  int mixed_compute = 1;     // single-precision orbitals: 1 = double-precision arithmetic, 0 = single
+  int mixed_compute = 3;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
 };
 
 struct Basis {
