@@ -57,7 +57,8 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * has one, the default) or 1 (generic kernel for every length); "mixed_compute" selects
  * the butterfly arithmetic of single-precision orbitals: 0 single everywhere, 1 double
  * everywhere, 2 double except the last inverse pass of H, 3 (default) as 2 and single for
- * the first forward pass of every transform too. */
+ * the first forward pass of every transform too; "fft_stages" = 0 (ring depth of the TMA
+ * kernels from their shared-memory budget, the default) or 2..8 stages. */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Free and total device memory in bytes (admission control for serving). */
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
@@ -182,6 +183,24 @@ int inqb_rotate(inqb_orbitals *phi, const double *R);
 /* energy::calculate eigenvalue part (energy.hpp:83-89): eig[s] = Re<phi|H phi>/<phi|phi>,
  * normres[s] = <r|r> with r = H phi - eig phi.  Host outputs [nst]. */
 int inqb_eigenvalues(const inqb_hamiltonian *ham, const inqb_orbitals *phi, double *eig, double *normres);
+
+/* ---- batches of systems and CUDA graphs ------------------------------------ */
+/* H|psi> for n independent systems sharing one context: system i runs
+ * ks_hamiltonian::operator() of hams[i] on ins[i] -> outs[i].  The systems' operator
+ * chains are forked onto up to `nstreams` auxiliary streams and joined back into the
+ * context's stream, so small systems run concurrently; inside a stream capture the
+ * call records one graph with parallel branches.  Batched execution has no counterpart
+ * in the reference (INQ applies one ks_hamiltonian per call, ks_hamiltonian.hpp:137). */
+int inqb_batch_apply(inqb_ctx *ctx, int n, inqb_hamiltonian *const *hams, const inqb_orbitals *const *ins,
+                     inqb_orbitals *const *outs, int nstreams);
+/* Stream capture of the context's stream into a CUDA graph: begin, then any calls on
+ * the context, then end (returns an instantiated cudaGraphExec_t); launch replays it
+ * on the context's stream.  Calls made during capture must not allocate: run them once
+ * eagerly first (tables, projection buffers and kernel attributes are then set up). */
+int inqb_graph_capture_begin(inqb_ctx *ctx);
+int inqb_graph_capture_end(inqb_ctx *ctx, void **graph_exec);
+int inqb_graph_launch(inqb_ctx *ctx, void *graph_exec);
+int inqb_graph_destroy(void *graph_exec);
 
 /* ---- real time ------------------------------------------------------------ */
 /* operations::exponential_in_place (exponential.hpp:21-34): phi <- sum_n (f H)^n/n! phi, f = re + i im. */

@@ -86,6 +86,11 @@ SIGNATURES = {
     "inqb_density": (I, [C.POINTER(P), I, C.POINTER(DP), DP]),
     "inqb_kick": (I, [P, DP]),
     "inqb_dipole": (I, [P, DP, DP]),
+    "inqb_batch_apply": (I, [P, I, C.POINTER(P), C.POINTER(P), C.POINTER(P), I]),
+    "inqb_graph_capture_begin": (I, [P]),
+    "inqb_graph_capture_end": (I, [P, C.POINTER(P)]),
+    "inqb_graph_launch": (I, [P, P]),
+    "inqb_graph_destroy": (I, [P]),
     "inqb_etrs_step": (I, [P, C.POINTER(P), I, C.POINTER(DP), D, I, D, DP, DP, C.POINTER(I)]),
 }
 

@@ -529,6 +529,11 @@ int inqb_ctx_destroy(inqb_ctx *ctx) {
   if (!ctx) return INQB_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  for (cudaStream_t st : ctx->aux) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (cudaEvent_t ev : ctx->aux_events) cudaEventDestroy(ev);
   cudaStreamDestroy(ctx->stream);
   if (ctx->d_err) cudaFree(ctx->d_err);
   delete ctx;
@@ -558,6 +563,9 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     if (k == "fft_impl") {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_impl is 0 (specialised) or 1 (generic)");
       ctx->fft_impl = int(value);
+    } else if (k == "fft_stages") {
+      INQB_REQUIRE(value >= 0 && value <= 8, INQB_ERR_ARG, "fft_stages is 0 (automatic) or 1..8");
+      ctx->fft_stages = int(value);
     } else if (k == "mixed_compute") {
       INQB_REQUIRE(value >= 0 && value <= 3, INQB_ERR_ARG, "mixed_compute is 0, 1, 2 or 3");
       ctx->mixed_compute = int(value);
@@ -1237,6 +1245,92 @@ int inqb_dipole(const inqb_basis *b, const double *density_host, double dipole[3
     INQB_REQUIRE(b && density_host && dipole, INQB_ERR_ARG, "null argument");
     dipole_host(*b, density_host, dipole);
   });
+}
+
+int inqb_batch_apply(inqb_ctx *ctx, int n, inqb_hamiltonian *const *hams, const inqb_orbitals *const *ins,
+                     inqb_orbitals *const *outs, int nstreams) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && n >= 0 && (n == 0 || (hams && ins && outs)), INQB_ERR_ARG, "null argument");
+    set_device(*ctx);
+    if (n == 0) return;
+    const int K = std::max(1, std::min({nstreams, n, 32}));
+    while (int(ctx->aux.size()) < K) {
+      cudaStream_t st;
+      INQB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      ctx->aux.push_back(st);
+    }
+    while (int(ctx->aux_events.size()) < K + 1) {
+      cudaEvent_t ev;
+      INQB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      ctx->aux_events.push_back(ev);
+    }
+    for (int i = 0; i < n; i++)
+      INQB_REQUIRE(hams[i] && ins[i] && outs[i] && hams[i]->ctx == ctx && ins[i]->ctx == ctx && outs[i]->ctx == ctx,
+                   INQB_ERR_ARG, "every system of a batch must use the batch's context");
+    cudaStream_t main = ctx->stream;
+    // fork: every auxiliary stream starts after the work already queued on the context's stream
+    INQB_CUDA(cudaEventRecord(ctx->aux_events[0], main));
+    for (int k = 0; k < K; k++) INQB_CUDA(cudaStreamWaitEvent(ctx->aux[k], ctx->aux_events[0], 0));
+    try {
+      // systems that share a Hamiltonian share its projection buffers: keep them on one stream
+      std::vector<const inqb_hamiltonian *> seen;
+      for (int i = 0; i < n; i++) {
+        int slot = -1;
+        for (size_t j = 0; j < seen.size(); j++)
+          if (seen[j] == hams[i]) slot = int(j);
+        if (slot < 0) {
+          slot = int(seen.size());
+          seen.push_back(hams[i]);
+        }
+        ctx->stream = ctx->aux[slot % K];
+        apply_any(*hams[i], *ins[i], *outs[i]);
+      }
+    } catch (...) {
+      ctx->stream = main;
+      throw;
+    }
+    ctx->stream = main;
+    // join
+    for (int k = 0; k < K; k++) {
+      INQB_CUDA(cudaEventRecord(ctx->aux_events[k + 1], ctx->aux[k]));
+      INQB_CUDA(cudaStreamWaitEvent(main, ctx->aux_events[k + 1], 0));
+    }
+  });
+}
+
+int inqb_graph_capture_begin(inqb_ctx *ctx) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx, INQB_ERR_ARG, "null argument");
+    set_device(*ctx);
+    INQB_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  });
+}
+
+int inqb_graph_capture_end(inqb_ctx *ctx, void **graph_exec) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && graph_exec, INQB_ERR_ARG, "null argument");
+    set_device(*ctx);
+    cudaGraph_t g = nullptr;
+    INQB_CUDA(cudaStreamEndCapture(ctx->stream, &g));
+    cudaGraphExec_t ge = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    INQB_CUDA(e);
+    *graph_exec = reinterpret_cast<void *>(ge);
+  });
+}
+
+int inqb_graph_launch(inqb_ctx *ctx, void *graph_exec) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && graph_exec, INQB_ERR_ARG, "null argument");
+    set_device(*ctx);
+    INQB_CUDA(cudaGraphLaunch(reinterpret_cast<cudaGraphExec_t>(graph_exec), ctx->stream));
+  });
+}
+
+int inqb_graph_destroy(void *graph_exec) {
+  if (graph_exec) cudaGraphExecDestroy(reinterpret_cast<cudaGraphExec_t>(graph_exec));
+  return INQB_OK;
 }
 
 int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int nsets, const double *const *occ,

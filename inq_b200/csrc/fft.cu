@@ -135,7 +135,7 @@ void launch_fft_pass(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologu
   const T *tw = reinterpret_cast<const T *>(sizeof(R) == 8 ? b.tw64[axis] : b.tw32[axis]);
 
   auto go = [&](auto kern) {
-    INQB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    ensure_smem_attr(reinterpret_cast<const void *>(kern), smem);
     kern<<<unsigned(tiles), threads, smem, ctx.stream>>>(a, g, rad, tw, W);
     INQB_CUDA(cudaGetLastError());
     ctx.launches++;

@@ -563,18 +563,26 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   const size_t budget = SPLIT ? 56 * 1024 : 113 * 1024;
   int ns = int((budget - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
+  if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;
   gg.stages = ns;
   gg.nsb = (a.S + W - 1) / W;
   gg.ntiles = (b.npoints / b.n[gg.axis]) * gg.nsb;
   const size_t smem = TILE_BYTES * nbuf * ns + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
   auto kern = fft2_kernel<R, CR, N, VAR>;
-  static int attr_set = 0;  // per instantiation
-  static int per_sm = 0;
-  if (attr_set != int(smem)) {
-    INQB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    INQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
-    attr_set = int(smem);
+  // per instantiation: shared-memory attribute and occupancy, computed under a lock (several host
+  // threads may drive contexts at once); the attribute only ever grows
+  static std::mutex mtx;
+  static int occ_smem = -1, occ_per_sm = 1;
+  int per_sm;
+  ensure_smem_attr(reinterpret_cast<const void *>(kern), smem);
+  {
+    std::lock_guard<std::mutex> lock(mtx);
+    if (occ_smem != int(smem)) {
+      INQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_per_sm, kern, NT, smem));
+      occ_smem = int(smem);
+    }
+    per_sm = occ_per_sm;
   }
   long long grid = (long long)(per_sm < 1 ? 1 : per_sm) * ctx.num_sms;
   if (grid > gg.ntiles) grid = gg.ntiles;

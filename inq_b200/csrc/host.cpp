@@ -6,7 +6,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
+#include <unordered_map>
 
 #include "inqb_internal.h"
 
@@ -54,6 +56,22 @@ std::vector<int> fft_radices(int n) {
   INQB_REQUIRE(m == 1, INQB_ERR_UNSUPPORTED,
                "grid size " + std::to_string(n) + " is not a product of 2, 3, 5 and 7");
   return r;
+}
+
+// ------------------------------------------------------------------ kernel attributes
+
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`.  Host threads driving
+// different contexts may launch the same kernel; the limit only ever grows, under a lock, so a
+// launch never finds it lowered by another thread.
+void ensure_smem_attr(const void *kernel, size_t bytes) {
+  static std::mutex mtx;
+  static std::unordered_map<const void *, size_t> current;
+  std::lock_guard<std::mutex> lock(mtx);
+  size_t &cur = current[kernel];
+  if (bytes > cur) {
+    INQB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    cur = bytes;
+  }
 }
 
 // ------------------------------------------------------------------ scratch memory

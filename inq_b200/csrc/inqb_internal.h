@@ -67,7 +67,10 @@ struct Ctx {
   int num_sms = 0;
   size_t max_smem_optin = 0;
   int *d_err = nullptr;      // device flag raised by a kernel whose bounded wait expired
+  std::vector<cudaStream_t> aux;        // fork streams of batched calls
+  std::vector<cudaEvent_t> aux_events;  // [0] fork point, [1..] joins
   int fft_impl = 0;          // 0: specialised TMA kernels where available, 1: generic kernel only
+  int fft_stages = 0;        // shared-memory ring depth of the TMA FFT kernels (0: from the memory budget)
   int mixed_compute = 3;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
 };
 
@@ -221,6 +224,8 @@ void launch_convert(Ctx &ctx, const void *in, int in_prec, void *out, int out_pr
 
 std::vector<int> fft_radices(int n);
 void basis_metric(const double lattice[9], double lat[3][3], double rec[3][3], double rlat[3][3], double &volume);
+
+void ensure_smem_attr(const void *kernel, size_t bytes);
 
 // scratch allocation on the context stream (stream-ordered pool)
 void *dev_alloc(Ctx &ctx, size_t bytes);

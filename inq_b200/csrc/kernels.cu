@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(256) rotate_kernel(C2<R> *phi, int S, long lon
 template <typename R> void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev) {
   const size_t smem = sizeof(double2) * 8 * S;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "too many states for rotate");
-  INQB_CUDA(cudaFuncSetAttribute(rotate_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  ensure_smem_attr(reinterpret_cast<const void *>(rotate_kernel<R>), smem);
   rotate_kernel<R><<<grid_for(npoints, 8, 148LL * 16), 256, smem, ctx.stream>>>(phi, S, npoints, Rdev);
   LAUNCHED(ctx);
 }
