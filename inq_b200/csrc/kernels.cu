@@ -159,7 +159,7 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   const Projectors &P = h.proj;
   if (P.nproj == 0) return;
   dim3 grid(P.nproj, (S + 31) / 32);
-  if (sizeof(R) == 8 || ctx.mixed_compute == 1) {
+  if (sizeof(R) == 8 || ctx.mixed_compute != 0) {
     // double-precision coefficients and accumulation
     nl_project_kernel<R, double><<<grid, 512, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef, P.d_npts, P.d_coeff,
                                                                 P.maxsph, projraw, projD);
