@@ -181,6 +181,70 @@ def run_reference(args):
 # ---------------------------------------------------------------- GPU arm
 
 
+def batch_leg(ctx, nsys=64, reps=5):
+    """C4: 64 uneven systems (grids 24..72^3, 8..128 states, 2..32 atoms), mixed form; eager fork/join
+    over streams and the replayed CUDA graph of the same batch."""
+    import time as _t
+    import inq_b200 as ib
+    import torch
+    from inq_b200 import synthetic
+    from inq_b200.batch import Batch, autotune
+    t0 = _t.perf_counter()
+    sy = synthetic.batch_systems(nsys)
+    built = [synthetic.build(s, precision=ib.F32, ctx=ctx) for s in sy]
+    setup_s = _t.perf_counter() - t0
+    hams = [b[1] for b in built]
+    ins = [b[2] for b in built]
+    outs = [p.skeleton() for p in ins]
+    states = sum(s.nst for s in sy)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+
+    def timed(fn):
+        fn()
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_serial = timed(lambda: [h.apply(i, o) for h, i, o in zip(hams, ins, outs)])
+    tuning = autotune(list(zip(hams, ins)), reps=2)
+    b = Batch(ctx, hams, ins, outs, nstreams=16, tuning=tuning)
+    ms_eager = timed(b.apply)
+    b.capture()
+    ms_graph = timed(b.launch)
+    b.close()
+    grids = sorted({s.sizes[0] for s in sy})
+    return {"workload": f"c4: {nsys} systems, grids {grids}^3, {states} states in total, "
+                        f"{min(s.natoms for s in sy)}-{max(s.natoms for s in sy)} atoms, mixed form",
+            "state_applications_per_s_graph": states / (ms_graph / 1000.0),
+            "state_applications_per_s_eager_streams": states / (ms_eager / 1000.0),
+            "state_applications_per_s_one_by_one": states / (ms_serial / 1000.0),
+            "ms_per_batch_graph": ms_graph, "ms_per_batch_eager": ms_eager, "ms_per_batch_one_by_one": ms_serial,
+            "autotuned_shapes": len(tuning.table), "setup_s": setup_s}
+
+
+def serving_leg(ctx, rates=(100.0, 1000.0), nreq=120):
+    """C5: Poisson stream of H|psi> and 10-step ETRS requests over C4-like systems plus 10% at 96^3 / 256
+    states, admitted by free device memory, four slots (streams); p50 / p99 latency and throughput."""
+    import inq_b200 as ib
+    from inq_b200 import serving, synthetic
+    pool = [serving.make_payload(s, ib.F32, ctx) for s in synthetic.batch_systems(12, seed=99)]
+    large = serving.make_payload(synthetic.config("c2"), ib.F32, ctx)
+    out = {}
+    srv = serving.Server(slots=4, precision=ib.F32)
+    for rate in rates:
+        reqs = serving.poisson_requests(pool, nreq, rate, seed=int(rate), large=large)
+        st = srv.run(reqs)
+        out[f"{int(rate)}_req_s"] = {k: st[k] for k in ("completed", "rejected", "throughput_req_s",
+                                                        "state_applications_per_s", "p50_ms", "p99_ms", "max_ms")}
+    srv.close()
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -322,6 +386,11 @@ def run_ours(args):
         e2e_s = float(t.item())
     e2e_v = world * S * e2e_steps / e2e_s
 
+    legs = {}
+    if world == 1 and not args.skip_legs:
+        legs["batch"] = batch_leg(ctx)
+        legs["serving"] = serving_leg(ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nsample = 8
@@ -362,6 +431,10 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
+        line.update(legs)
+        if "serving" in legs:
+            line["serving_p50_ms"] = legs["serving"]["100_req_s"]["p50_ms"]
+            line["serving_p99_ms"] = legs["serving"]["100_req_s"]["p99_ms"]
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -396,6 +469,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-legs", action="store_true", help="skip the batched-systems and serving legs")
     ap.add_argument("--profile-case", action="store_true", help="small workload for ncu captures")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -1,0 +1,197 @@
+"""Continuous-batching request loop for H|psi> and short ETRS propagations.
+
+A request carries one system (cell, grid, atoms, potential, orbitals) and asks for either
+one H application or ``steps`` ETRS steps.  The server:
+
+* admits a request when a slot is free and its device-memory footprint fits in the budget
+  (the free device memory at start-up minus a reserve; the sum of the admitted footprints
+  never exceeds it), in arrival order -- requests that arrive while others run are admitted
+  as soon as a slot and memory free up;
+* gives each slot its own library context (one CUDA stream) and host thread, so the work of
+  different requests overlaps on the device, and keeps a request's orbitals and potential
+  resident on the device across all its steps;
+* records every request's latency (completion minus arrival) and result, and reports
+  p50 / p99 latency beside throughput.
+
+Results do not depend on what else runs: every kernel is deterministic and requests share no
+device state, which ``tests/test_serving.py`` checks by comparing results alone and in a mix.
+"""
+
+from __future__ import annotations
+
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import core, synthetic
+from ._lib import F32, F64
+
+
+@dataclass
+class Payload:
+    """Host-side inputs of one system: what a client sends."""
+    system: synthetic.System
+    potential: np.ndarray          # [npoint] float64
+    orbitals: np.ndarray           # [npoint][nst] complex (orthonormal), complex64 or complex128
+
+    @property
+    def nbytes(self):
+        return self.orbitals.nbytes
+
+
+@dataclass
+class Request:
+    rid: int
+    kind: str                      # "apply" | "etrs"
+    payload: Payload
+    steps: int = 1
+    dt: float = 0.05
+    arrival: float = 0.0           # seconds after the start of the run
+    # filled by the server
+    admitted: float = -1.0
+    finished: float = -1.0
+    result: dict = field(default_factory=dict)
+    error: str = ""
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+    def footprint(self, precision) -> int:
+        """Device bytes the request holds while it runs."""
+        n = self.payload.system.npoints
+        s = self.payload.system.nst
+        cb = 16 if precision == F64 else 8
+        sets = 2 if self.kind == "apply" else 5   # in/out; ETRS: phi, saved half step, two H^n buffers, spare
+        tables = n * 8 * 4 + self.payload.system.natoms * 4000 * 64   # potential, CSR, projector tables
+        return sets * n * s * cb + tables + (64 << 20)
+
+
+def make_payload(sysm: synthetic.System, precision=F32, ctx: core.Context | None = None) -> Payload:
+    """Generate a system's inputs (on the device, then copied to the host as a client would hold them)."""
+    basis, ham, phi = synthetic.build(sysm, precision=precision, ctx=ctx)
+    orb = phi.matrix()
+    return Payload(sysm, sysm.local_potential().reshape(-1), orb)
+
+
+class Server:
+    """``contexts`` and ``execute`` default to one library context per slot and the library
+    operators; tests of the admission logic inject stand-ins for both."""
+
+    def __init__(self, device: int = 0, slots: int = 4, precision=F32, reserve_bytes: int = 8 << 30,
+                 mixed_compute: int = 3, budget_bytes: int | None = None, contexts=None, execute=None):
+        self.device = device
+        self.precision = precision
+        if contexts is None:
+            contexts = [core.Context(device) for _ in range(slots)]
+            for c in contexts:
+                c.set_option("mixed_compute", mixed_compute)
+        self.contexts = list(contexts)
+        if budget_bytes is None:
+            free, _ = self.contexts[0].mem_info()
+            budget_bytes = max(0, free - reserve_bytes)
+        self.budget = budget_bytes
+        self.execute = execute or self._execute
+        self.committed = 0
+        self.peak_committed = 0
+        self.lock = threading.Condition()
+        self.free_slots = list(range(len(self.contexts)))
+
+    # ------------------------------------------------------------------ one request on one slot
+    def _execute(self, req: Request, ctx: core.Context):
+        sysm = req.payload.system
+        basis = core.RealSpace(core.Cell(sysm.lattice), sizes=sysm.sizes, ctx=ctx)
+        ham = core.KSHamiltonian(basis)
+        ham.set_scalar_potential(req.payload.potential)
+        ham.update_projectors_gaussian(sysm.positions, sysm.radius, sysm.rc, sysm.kb)
+        phi = core.OrbitalSet(basis, sysm.nst, precision=self.precision).upload(req.payload.orbitals)
+        if req.kind == "apply":
+            out = phi.skeleton()
+            ham.apply(phi, out)
+            h = out.matrix()
+            req.result = {"hphi": h, "norm": float(np.linalg.norm(h)), "happs": sysm.nst}
+        else:
+            occ = np.full(sysm.nst, 2.0)
+            dips = []
+            happs = 0
+            for _ in range(req.steps):
+                _, dip, iters = core.etrs(ham, [phi], [occ], req.dt)
+                dips.append(dip)
+                happs += (4 + 4 * iters) * sysm.nst   # exponential_2_for_1 + one exponential per SCF pass
+            req.result = {"dipoles": np.array(dips), "phi": phi.matrix(), "happs": happs}
+        ctx.synchronize()
+
+    def _worker(self, slot: int, req: Request, t0: float, fp: int):
+        try:
+            self.execute(req, self.contexts[slot])
+        except Exception as e:  # a failing request is reported, the server goes on
+            req.error = f"{type(e).__name__}: {e}"
+        finally:
+            req.finished = time.perf_counter() - t0
+            with self.lock:
+                self.committed -= fp
+                self.free_slots.append(slot)
+                self.lock.notify_all()
+
+    # ------------------------------------------------------------------ the loop
+    def run(self, requests: list[Request], realtime: bool = True) -> dict:
+        """Serve ``requests`` (sorted by arrival); returns latency / throughput statistics."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        threads = []
+        t0 = time.perf_counter()
+        for req in reqs:
+            fp = req.footprint(self.precision)
+            if fp > self.budget:
+                req.error = f"rejected: needs {fp} bytes, the budget is {self.budget}"
+                req.finished = req.admitted = time.perf_counter() - t0
+                continue
+            if realtime:
+                wait = req.arrival - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+            with self.lock:
+                while not self.free_slots or self.committed + fp > self.budget:
+                    self.lock.wait()
+                slot = self.free_slots.pop(0)
+                self.committed += fp
+                self.peak_committed = max(self.peak_committed, self.committed)
+            req.admitted = time.perf_counter() - t0
+            th = threading.Thread(target=self._worker, args=(slot, req, t0, fp), daemon=True)
+            th.start()
+            threads.append(th)
+        for th in threads:
+            th.join()
+        wall = time.perf_counter() - t0
+        done = [r for r in reqs if not r.error]
+        lat = np.array([r.latency for r in done]) if done else np.zeros(1)
+        happs = sum(r.result.get("happs", 0) for r in done)
+        return {"requests": len(reqs), "completed": len(done), "rejected": len(reqs) - len(done),
+                "wall_s": wall, "throughput_req_s": len(done) / wall,
+                "state_applications_per_s": happs / wall,
+                "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000),
+                "max_ms": float(lat.max() * 1000), "peak_committed_bytes": self.peak_committed,
+                "budget_bytes": self.budget}
+
+    def close(self):
+        for c in self.contexts:
+            if hasattr(c, "close"):
+                c.close()
+
+
+def poisson_requests(payloads: list[Payload], n: int, rate: float, seed: int = 7, etrs_fraction: float = 0.3,
+                     etrs_steps: int = 10, large: Payload | None = None, large_fraction: float = 0.1):
+    """A Poisson arrival stream over the given payloads (the C5 request mix)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        if large is not None and rng.random() < large_fraction:
+            p = large
+        else:
+            p = payloads[int(rng.integers(len(payloads)))]
+        kind = "etrs" if rng.random() < etrs_fraction else "apply"
+        out.append(Request(i, kind, p, steps=etrs_steps if kind == "etrs" else 1, arrival=t))
+    return out
