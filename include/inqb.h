@@ -202,6 +202,12 @@ int inqb_graph_capture_end(inqb_ctx *ctx, void **graph_exec);
 int inqb_graph_launch(inqb_ctx *ctx, void *graph_exec);
 int inqb_graph_destroy(void *graph_exec);
 
+/* ground_state::subspace_diagonalization (subspace_diagonalization.hpp:21-29): H_sub =
+ * <phi|H|phi> (FP64 overlap), Hermitian eigen-decomposition in FP64 (matrix::diagonalize,
+ * diagonalize.hpp:100-190; here cyclic Jacobi on the host), phi rotated onto the
+ * eigenvectors; eigenvalues host [nst], ascending. */
+int inqb_subspace_diagonalization(const inqb_hamiltonian *ham, inqb_orbitals *phi, double *eigenvalues);
+
 /* ---- real time ------------------------------------------------------------ */
 /* operations::exponential_in_place (exponential.hpp:21-34): phi <- sum_n (f H)^n/n! phi, f = re + i im. */
 int inqb_exponential_in_place(const inqb_hamiltonian *ham, double re, double im, inqb_orbitals *phi, int order);

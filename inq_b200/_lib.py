@@ -81,6 +81,7 @@ SIGNATURES = {
     "inqb_shift": (I, [D, D, P, P]),
     "inqb_rotate": (I, [P, DP]),
     "inqb_eigenvalues": (I, [P, P, DP, DP]),
+    "inqb_subspace_diagonalization": (I, [P, P, DP]),
     "inqb_exponential_in_place": (I, [P, D, D, P, I]),
     "inqb_exponential_2_for_1": (I, [P, D, D, D, D, P, P, I]),
     "inqb_density": (I, [C.POINTER(P), I, C.POINTER(DP), DP]),

@@ -430,6 +430,12 @@ class KSHamiltonian:
         self.ctx.check(self.ctx.lib.inqb_eigenvalues(self.handle, phi.handle, dptr(eig), dptr(res)))
         return eig, res
 
+    def subspace_diagonalization(self, phi: OrbitalSet):
+        """ground_state::subspace_diagonalization: rotates phi onto the subspace eigenvectors, returns eigenvalues."""
+        eig = np.zeros(phi.nst)
+        self.ctx.check(self.ctx.lib.inqb_subspace_diagonalization(self.handle, phi.handle, dptr(eig)))
+        return eig
+
     def __del__(self):
         try:
             if getattr(self, "handle", None) and self.ctx.handle:

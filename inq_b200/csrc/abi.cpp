@@ -357,6 +357,73 @@ void cholesky_inverse(int n, const std::complex<double> *S, std::complex<double>
   }
 }
 
+// Eigen-decomposition of a Hermitian matrix (matrix::diagonalize, diagonalize.hpp:100-190) by cyclic
+// Jacobi rotations in FP64.  A is [n][n] row-major and read from its upper triangle (the reference
+// passes "U" to zheev / Zheevd); on return w holds the eigenvalues in ascending order and column k of
+// the row-major V the eigenvector of w[k].
+void hermitian_eigen(int n, const std::complex<double> *Ain, double *w, std::complex<double> *V) {
+  using cd = std::complex<double>;
+  std::vector<cd> A(size_t(n) * n);
+  for (int i = 0; i < n; i++)
+    for (int j = i; j < n; j++) {
+      A[size_t(i) * n + j] = Ain[size_t(i) * n + j];
+      A[size_t(j) * n + i] = std::conj(Ain[size_t(i) * n + j]);
+    }
+  for (int i = 0; i < n; i++) A[size_t(i) * n + i] = A[size_t(i) * n + i].real();
+  std::vector<cd> Vm(size_t(n) * n, 0.0);
+  for (int i = 0; i < n; i++) Vm[size_t(i) * n + i] = 1.0;
+  auto off = [&] {
+    double s = 0.0;
+    for (int i = 0; i < n; i++)
+      for (int j = i + 1; j < n; j++) s += std::norm(A[size_t(i) * n + j]);
+    return s;
+  };
+  double total = 0.0;
+  for (auto &x : A) total += std::norm(x);
+  for (int sweep = 0; sweep < 60 && off() > 1e-30 * total; sweep++) {
+    for (int p = 0; p < n - 1; p++)
+      for (int q = p + 1; q < n; q++) {
+        const cd b = A[size_t(p) * n + q];
+        const double r = std::abs(b);
+        if (r < 1e-300) continue;
+        const double a = A[size_t(p) * n + p].real(), d = A[size_t(q) * n + q].real();
+        const cd ph = b / r;  // e^{i phi}
+        // real rotation zeroing [[a, r], [r, d]]
+        const double theta = 0.5 * std::atan2(2.0 * r, d - a);
+        const double c = std::cos(theta), sn = std::sin(theta);
+        // U = diag(1, conj(ph)) * [[c, s], [-s, c]]: columns p, q
+        const cd upp = c, upq = sn, uqp = -sn * std::conj(ph), uqq = c * std::conj(ph);
+        for (int k = 0; k < n; k++) {  // A <- A U
+          const cd akp = A[size_t(k) * n + p], akq = A[size_t(k) * n + q];
+          A[size_t(k) * n + p] = akp * upp + akq * uqp;
+          A[size_t(k) * n + q] = akp * upq + akq * uqq;
+        }
+        for (int k = 0; k < n; k++) {  // A <- U^H A
+          const cd apk = A[size_t(p) * n + k], aqk = A[size_t(q) * n + k];
+          A[size_t(p) * n + k] = std::conj(upp) * apk + std::conj(uqp) * aqk;
+          A[size_t(q) * n + k] = std::conj(upq) * apk + std::conj(uqq) * aqk;
+        }
+        A[size_t(p) * n + q] = 0.0;
+        A[size_t(q) * n + p] = 0.0;
+        A[size_t(p) * n + p] = A[size_t(p) * n + p].real();
+        A[size_t(q) * n + q] = A[size_t(q) * n + q].real();
+        for (int k = 0; k < n; k++) {  // V <- V U
+          const cd vkp = Vm[size_t(k) * n + p], vkq = Vm[size_t(k) * n + q];
+          Vm[size_t(k) * n + p] = vkp * upp + vkq * uqp;
+          Vm[size_t(k) * n + q] = vkp * upq + vkq * uqq;
+        }
+      }
+  }
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return A[size_t(x) * n + x].real() < A[size_t(y) * n + y].real(); });
+  for (int k = 0; k < n; k++) {
+    w[k] = A[size_t(order[k]) * n + order[k]].real();
+    for (int i = 0; i < n; i++) V[size_t(i) * n + k] = Vm[size_t(i) * n + order[k]];
+  }
+}
+
 void overlap_dev(const Orbitals &a, const Orbitals &b, double2 *out_dev) {
   Ctx &ctx = *a.ctx;
   INQB_REQUIRE(a.basis == b.basis && a.precision == b.precision, INQB_ERR_ARG, "overlap of incompatible sets");
@@ -1189,6 +1256,32 @@ int inqb_eigenvalues(const inqb_hamiltonian *hc, const inqb_orbitals *phi, doubl
       dev_free(ctx, de);
     }
     dev_free(ctx, d);
+  });
+}
+
+int inqb_subspace_diagonalization(const inqb_hamiltonian *hc, inqb_orbitals *phi, double *eigenvalues) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && phi && eigenvalues, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(phi->space == INQB_REAL_SPACE, INQB_ERR_ARG, "subspace diagonalization needs a real-space set");
+    set_device(*h->ctx);
+    Ctx &ctx = *h->ctx;
+    const int S = phi->nst;
+    // subspace Hamiltonian <phi_i|H|phi_j> (overlap(phi, ham(phi)), subspace_diagonalization.hpp:25)
+    double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * S * S));
+    {
+      TempSet hp(*phi);
+      apply_any(*h, *phi, hp.o);
+      overlap_dev(*phi, hp.o, d);
+    }
+    auto Hs = download<std::complex<double>>(ctx, d, size_t(S) * S);
+    std::vector<std::complex<double>> V(size_t(S) * S);
+    hermitian_eigen(S, Hs.data(), eigenvalues, V.data());
+    // phi_k <- sum_j V[j][k] phi_j (operations::rotate with the eigenvectors, rotate.hpp:27-62)
+    INQB_CUDA(cudaMemcpyAsync(d, V.data(), sizeof(double2) * S * S, cudaMemcpyHostToDevice, ctx.stream));
+    rotate_dev(*phi, d);
+    dev_free(ctx, d);
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
   });
 }
 

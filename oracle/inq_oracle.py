@@ -597,6 +597,15 @@ def orthogonalize(rs, phi):
     return (phi.reshape(-1, shp[-1]) @ Uinv).reshape(shp)
 
 
+def subspace_diagonalization(ham: Hamiltonian, phi, kpoint_cov=(0.0, 0.0, 0.0)):
+    """subspace_diagonalization.hpp:21-29: H_sub = <phi|H phi>, Hermitian eigenproblem (upper triangle),
+    phi rotated onto the eigenvectors; eigenvalues ascending."""
+    Hs = overlap(ham.rs, phi, ham.apply_real(phi, kpoint_cov))
+    w, U = np.linalg.eigh(Hs, UPLO="U")
+    shp = phi.shape
+    return w, (phi.reshape(-1, shp[-1]) @ U).reshape(shp)
+
+
 def eigenvalues(ham: Hamiltonian, phi, kpoint_cov=(0.0, 0.0, 0.0)):
     """energy::calculate eigenvalue part (energy.hpp:83-89): Re<phi|H phi>/<phi|phi>, residual norms."""
     hphi = ham.apply_real(phi, kpoint_cov)

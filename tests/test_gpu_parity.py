@@ -327,6 +327,20 @@ def test_etrs_step_parity(ib, c1):
     assert np.max(np.abs(dip - O.dipole_electronic(ors, rdens))) < 1e-10
 
 
+def test_subspace_diagonalization(ib, c1):
+    """subspace_diagonalization.hpp:21-29 vs the oracle: eigenvalues within 1e-10 Ha, rotated set diagonalises H."""
+    sysm, basis, ham, phi, oh, ors = c1
+    x = phi.hypercubic()
+    p = phi.copy()
+    w = ham.subspace_diagonalization(p)
+    ow, ox = O.subspace_diagonalization(oh, x)
+    assert np.max(np.abs(w - ow)) < 1e-10
+    y = p.hypercubic()
+    Hs = O.overlap(ors, y, oh.apply_real(y))
+    assert np.max(np.abs(Hs - np.diag(ow))) < 1e-9
+    assert np.max(np.abs(O.overlap(ors, y) - np.eye(sysm.nst))) < 1e-11
+
+
 def test_orthogonalize_random(ib, rng):
     rs = ib.RealSpace(ib.Cell.cubic(6.3), spacing=0.44428829)
     x = _random_orbitals(rng, rs.sizes, 40)
