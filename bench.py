@@ -235,13 +235,46 @@ def serving_leg(ctx, rates=(100.0, 1000.0), nreq=120):
     pool = [serving.make_payload(s, ib.F32, ctx) for s in synthetic.batch_systems(12, seed=99)]
     large = serving.make_payload(synthetic.config("c2"), ib.F32, ctx)
     out = {}
-    srv = serving.Server(slots=4, precision=ib.F32)
+    srv = serving.Server(slots=4, precision=ib.F32, keep_results=False)
     for rate in rates:
         reqs = serving.poisson_requests(pool, nreq, rate, seed=int(rate), large=large)
         st = srv.run(reqs)
         out[f"{int(rate)}_req_s"] = {k: st[k] for k in ("completed", "rejected", "throughput_req_s",
                                                         "state_applications_per_s", "p50_ms", "p99_ms", "max_ms")}
     srv.close()
+    return out
+
+
+def etrs_leg(ctx, steps=10):
+    """C3: ETRS propagation at 120^3 / 256 states / 128 atoms after a 0.01 a.u. kick along x (phase
+    exp(i 0.01 x)), dt = 0.05, FP64 density every step; plain FP64 and mixed dipole series."""
+    import numpy as np
+    import torch
+    import inq_b200 as ib
+    from inq_b200 import synthetic
+    sysm = synthetic.config("c3")
+    basis, ham, phi64 = synthetic.build(sysm, ctx=ctx)
+    ib.apply_phase_kick(phi64, [0.01, 0.0, 0.0])
+    phi32 = phi64.converted(ib.F32)
+    occ = np.full(sysm.nst, 2.0)
+    out = {}
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    for name, phi in (("fp64", phi64), ("mixed", phi32)):
+        dips = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            _, dip, _ = ib.etrs(ham, [phi], [occ], 0.05)
+            dips.append(dip.tolist())
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"steps_per_s": steps / (ms / 1000.0), "ms_per_step": ms / steps, "dipole_series": dips}
+    d64 = np.array(out["fp64"]["dipole_series"])
+    d32 = np.array(out["mixed"]["dipole_series"])
+    out["max_dipole_diff_mixed_vs_fp64"] = float(np.max(np.abs(d64 - d32)))
+    out["workload"] = f"c3: 120^3, {sysm.nst} states, {sysm.natoms} atoms, kick 0.01 x, dt 0.05, {steps} steps"
     return out
 
 
@@ -390,6 +423,8 @@ def run_ours(args):
     if world == 1 and not args.skip_legs:
         legs["batch"] = batch_leg(ctx)
         legs["serving"] = serving_leg(ctx)
+        if args.etrs_steps > 0:
+            legs["etrs"] = etrs_leg(ctx, args.etrs_steps)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -469,7 +504,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--skip-legs", action="store_true", help="skip the batched-systems and serving legs")
+    ap.add_argument("--skip-legs", action="store_true", help="skip the batched-systems, serving and ETRS legs")
+    ap.add_argument("--etrs-steps", type=int, default=10, help="ETRS steps of the 120^3 real-time leg (0: skip)")
     ap.add_argument("--profile-case", action="store_true", help="small workload for ncu captures")
     args = ap.parse_args()
     if args.warmup < 3:

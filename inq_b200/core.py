@@ -307,6 +307,12 @@ class OrbitalSet:
         self.ctx.check(self.ctx.lib.inqb_orbitals_download(self.handle, out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def download_into(self, out: np.ndarray) -> np.ndarray:
+        """Copy the set into a caller-provided contiguous host array (pinned memory copies fastest)."""
+        assert out.dtype == self.dtype and out.flags.c_contiguous and out.size == self.basis.size() * self.nst
+        self.ctx.check(self.ctx.lib.inqb_orbitals_download(self.handle, out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def hypercubic(self) -> np.ndarray:
         """Host copy [nx][ny][nz][nst] (field_set::hypercubic())."""
         return self.matrix().reshape(self.basis.sizes + (self.nst,))

@@ -93,12 +93,12 @@ void fft3d(Ctx &ctx, const Basis &b, const C2<R> *in, C2<R> *out, int S, int dir
 template <typename R> C2<R> *proj_buf(Hamiltonian &h, int S, int which) {
   const size_t need = size_t(std::max(1, h.proj.nproj)) * 4 * S * sizeof(C2<double>);
   if (need > h.proj_bytes) {
-    if (h.d_projraw) INQB_CUDA(cudaFree(h.d_projraw));
-    if (h.d_projD) INQB_CUDA(cudaFree(h.d_projD));
+    if (h.d_projraw) INQB_CUDA(cudaFreeAsync(h.d_projraw, h.ctx->stream));
+    if (h.d_projD) INQB_CUDA(cudaFreeAsync(h.d_projD, h.ctx->stream));
     h.d_projraw = h.d_projD = nullptr;
     h.proj_bytes = 0;
-    INQB_CUDA(cudaMalloc(&h.d_projraw, need));
-    INQB_CUDA(cudaMalloc(&h.d_projD, need));
+    INQB_CUDA(cudaMallocAsync(&h.d_projraw, need, h.ctx->stream));
+    INQB_CUDA(cudaMallocAsync(&h.d_projD, need, h.ctx->stream));
     h.proj_bytes = need;
   }
   return static_cast<C2<R> *>(which == 0 ? h.d_projraw : h.d_projD);
@@ -462,19 +462,23 @@ template <typename T> std::vector<T> download(Ctx &ctx, const void *dev, size_t 
   return h;
 }
 
-void free_projectors(Projectors &P) {
+// all device memory of the library is stream-ordered (cudaMallocAsync / cudaFreeAsync on the owning
+// context's stream): releasing an object never synchronises the device, so contexts driven by
+// different host threads (the serving slots) do not stall one another
+void free_projectors(Projectors &P, cudaStream_t st) {
   void *ptrs[] = {P.d_pt, P.d_pos, P.d_mat, P.d_coeff, P.d_coeff32, P.d_npts, P.d_offs, P.d_hit, P.d_hitpts, P.d_hitp,
                   P.d_gcoef, P.d_hcoef, P.d_gcoef32, P.d_hcoef32};
   for (void *p : ptrs)
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
   P = Projectors();
 }
 
-template <typename T> T *upload_vec(const std::vector<T> &v) {
+// the caller synchronises the stream before the host vector goes away
+template <typename T> T *upload_vec(const std::vector<T> &v, cudaStream_t st) {
   T *d = nullptr;
   const size_t bytes = std::max<size_t>(sizeof(T), v.size() * sizeof(T));
-  INQB_CUDA(cudaMalloc(&d, bytes));
-  if (!v.empty()) INQB_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  INQB_CUDA(cudaMallocAsync(&d, bytes, st));
+  if (!v.empty()) INQB_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   return d;
 }
 
@@ -484,8 +488,8 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
   const Basis &b = *h.basis;
   INQB_REQUIRE(nproj >= 0 && maxsph >= 0, INQB_ERR_ARG, "negative projector table size");
   INQB_REQUIRE(maxnlm >= 0 && maxnlm <= 4, INQB_ERR_UNSUPPORTED, "at most 4 (l <= 1) projector functions per atom");
-  INQB_CUDA(cudaStreamSynchronize(h.ctx->stream));
-  free_projectors(h.proj);
+  cudaStream_t st = h.ctx->stream;
+  free_projectors(h.proj, st);
   Projectors &P = h.proj;
   P.nproj = nproj;
   P.maxsph = maxsph;
@@ -541,20 +545,21 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
     if (k == 0 || hits[k].first != hits[k - 1].first) hitpts.push_back(int(hits[k].first));
   P.nhitpts = (long long)hitpts.size();
 
-  P.d_pt = upload_vec(flat);
-  P.d_pos = upload_vec(P.h_pos);
-  P.d_mat = upload_vec(mat4);
-  P.d_coeff = upload_vec(coeff4);
-  P.d_coeff32 = upload_vec(coeff4f);
-  P.d_npts = upload_vec(P.h_npts);
-  P.d_offs = upload_vec(offs);
-  P.d_hit = upload_vec(hit);
-  P.d_hitpts = upload_vec(hitpts);
-  P.d_hitp = upload_vec(hitp);
-  INQB_CUDA(cudaMalloc(&P.d_gcoef, sizeof(double2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4)));
-  INQB_CUDA(cudaMalloc(&P.d_gcoef32, sizeof(float2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4)));
-  INQB_CUDA(cudaMalloc(&P.d_hcoef, sizeof(double2) * std::max<size_t>(1, size_t(P.total) * 4)));
-  INQB_CUDA(cudaMalloc(&P.d_hcoef32, sizeof(float2) * std::max<size_t>(1, size_t(P.total) * 4)));
+  P.d_pt = upload_vec(flat, st);
+  P.d_pos = upload_vec(P.h_pos, st);
+  P.d_mat = upload_vec(mat4, st);
+  P.d_coeff = upload_vec(coeff4, st);
+  P.d_coeff32 = upload_vec(coeff4f, st);
+  P.d_npts = upload_vec(P.h_npts, st);
+  P.d_offs = upload_vec(offs, st);
+  P.d_hit = upload_vec(hit, st);
+  P.d_hitpts = upload_vec(hitpts, st);
+  P.d_hitp = upload_vec(hitp, st);
+  INQB_CUDA(cudaMallocAsync(&P.d_gcoef, sizeof(double2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4), st));
+  INQB_CUDA(cudaMallocAsync(&P.d_gcoef32, sizeof(float2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4), st));
+  INQB_CUDA(cudaMallocAsync(&P.d_hcoef, sizeof(double2) * std::max<size_t>(1, size_t(P.total) * 4), st));
+  INQB_CUDA(cudaMallocAsync(&P.d_hcoef32, sizeof(float2) * std::max<size_t>(1, size_t(P.total) * 4), st));
+  INQB_CUDA(cudaStreamSynchronize(st));  // the host tables above go out of scope
   P.kA[0] = P.kA[1] = P.kA[2] = 1e300;  // tables are built on first use for a given k + A
 }
 
@@ -681,15 +686,16 @@ int inqb_basis_create(inqb_ctx *ctx, const double lattice[9], int nx, int ny, in
           t64[t] = make_double2(double(cosl(ang)), double(-sinl(ang)));
           t32[t] = make_float2(float(cosl(ang)), float(-sinl(ang)));
         }
-        INQB_CUDA(cudaMalloc(&b->tw64[ax], sizeof(double2) * n));
-        INQB_CUDA(cudaMalloc(&b->tw32[ax], sizeof(float2) * n));
-        INQB_CUDA(cudaMemcpy(b->tw64[ax], t64.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
-        INQB_CUDA(cudaMemcpy(b->tw32[ax], t32.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+        INQB_CUDA(cudaMallocAsync(&b->tw64[ax], sizeof(double2) * n, ctx->stream));
+        INQB_CUDA(cudaMallocAsync(&b->tw32[ax], sizeof(float2) * n, ctx->stream));
+        INQB_CUDA(cudaMemcpyAsync(b->tw64[ax], t64.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, ctx->stream));
+        INQB_CUDA(cudaMemcpyAsync(b->tw32[ax], t32.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, ctx->stream));
+        INQB_CUDA(cudaStreamSynchronize(ctx->stream));
       }
     } catch (...) {
       for (int ax = 0; ax < 3; ax++) {
-        if (b->tw64[ax]) cudaFree(b->tw64[ax]);
-        if (b->tw32[ax]) cudaFree(b->tw32[ax]);
+        if (b->tw64[ax]) cudaFreeAsync(b->tw64[ax], ctx->stream);
+        if (b->tw32[ax]) cudaFreeAsync(b->tw32[ax], ctx->stream);
       }
       delete b;
       throw;
@@ -701,10 +707,9 @@ int inqb_basis_create(inqb_ctx *ctx, const double lattice[9], int nx, int ny, in
 int inqb_basis_destroy(inqb_basis *b) {
   if (!b) return INQB_OK;
   cudaSetDevice(b->ctx->device);
-  cudaStreamSynchronize(b->ctx->stream);
   for (int ax = 0; ax < 3; ax++) {
-    if (b->tw64[ax]) cudaFree(b->tw64[ax]);
-    if (b->tw32[ax]) cudaFree(b->tw32[ax]);
+    if (b->tw64[ax]) cudaFreeAsync(b->tw64[ax], b->ctx->stream);
+    if (b->tw32[ax]) cudaFreeAsync(b->tw32[ax], b->ctx->stream);
   }
   delete b;
   return INQB_OK;
@@ -735,7 +740,8 @@ int inqb_orbitals_create(inqb_ctx *ctx, const inqb_basis *basis, int nst, int sp
     o->spin_index = spin_index;
     o->space = space;
     o->precision = precision;
-    cudaError_t e = cudaMalloc(&o->data, o->bytes());
+    cudaError_t e = cudaMallocAsync(&o->data, o->bytes(), ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // usable from any stream on return
     if (e != cudaSuccess) {
       (void)cudaGetLastError();
       delete o;
@@ -748,8 +754,7 @@ int inqb_orbitals_create(inqb_ctx *ctx, const inqb_basis *basis, int nst, int sp
 int inqb_orbitals_destroy(inqb_orbitals *o) {
   if (!o) return INQB_OK;
   cudaSetDevice(o->ctx->device);
-  cudaStreamSynchronize(o->ctx->stream);
-  if (o->data) cudaFree(o->data);
+  if (o->data) cudaFreeAsync(o->data, o->ctx->stream);
   delete o;
   return INQB_OK;
 }
@@ -906,8 +911,8 @@ int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, i
     h->basis = basis;
     h->nspin = nspin;
     const size_t nv = size_t(basis->npoints) * nspin;
-    INQB_CUDA(cudaMalloc(&h->d_V, sizeof(double) * nv));
-    INQB_CUDA(cudaMalloc(&h->d_V32, sizeof(float) * nv));
+    INQB_CUDA(cudaMallocAsync(&h->d_V, sizeof(double) * nv, ctx->stream));
+    INQB_CUDA(cudaMallocAsync(&h->d_V32, sizeof(float) * nv, ctx->stream));
     INQB_CUDA(cudaMemsetAsync(h->d_V, 0, sizeof(double) * nv, ctx->stream));
     INQB_CUDA(cudaMemsetAsync(h->d_V32, 0, sizeof(float) * nv, ctx->stream));
     INQB_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -918,12 +923,12 @@ int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, i
 int inqb_hamiltonian_destroy(inqb_hamiltonian *h) {
   if (!h) return INQB_OK;
   cudaSetDevice(h->ctx->device);
-  cudaStreamSynchronize(h->ctx->stream);
-  free_projectors(h->proj);
-  if (h->d_V) cudaFree(h->d_V);
-  if (h->d_V32) cudaFree(h->d_V32);
-  if (h->d_projraw) cudaFree(h->d_projraw);
-  if (h->d_projD) cudaFree(h->d_projD);
+  cudaStream_t st = h->ctx->stream;
+  free_projectors(h->proj, st);
+  if (h->d_V) cudaFreeAsync(h->d_V, st);
+  if (h->d_V32) cudaFreeAsync(h->d_V32, st);
+  if (h->d_projraw) cudaFreeAsync(h->d_projraw, st);
+  if (h->d_projD) cudaFreeAsync(h->d_projD, st);
   delete h;
   return INQB_OK;
 }
@@ -934,9 +939,9 @@ int inqb_potential_set(inqb_hamiltonian *h, const double *V) {
     set_device(*h->ctx);
     const size_t nv = size_t(h->basis->npoints) * h->nspin;
     std::vector<float> v32(V, V + nv);
+    INQB_CUDA(cudaMemcpyAsync(h->d_V, V, sizeof(double) * nv, cudaMemcpyHostToDevice, h->ctx->stream));
+    INQB_CUDA(cudaMemcpyAsync(h->d_V32, v32.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, h->ctx->stream));
     INQB_CUDA(cudaStreamSynchronize(h->ctx->stream));
-    INQB_CUDA(cudaMemcpy(h->d_V, V, sizeof(double) * nv, cudaMemcpyHostToDevice));
-    INQB_CUDA(cudaMemcpy(h->d_V32, v32.data(), sizeof(float) * nv, cudaMemcpyHostToDevice));
   });
 }
 
