@@ -227,7 +227,7 @@ def batch_leg(ctx, nsys=64, reps=5):
             "autotuned_shapes": len(tuning.table), "setup_s": setup_s}
 
 
-def serving_leg(ctx, rates=(100.0, 1000.0), nreq=120):
+def serving_leg(ctx, rates=(50.0, 200.0, 1000.0, 2000.0), nreq=120):
     """C5: Poisson stream of H|psi> and 10-step ETRS requests over C4-like systems plus 10% at 96^3 / 256
     states, admitted by free device memory, four slots (streams); p50 / p99 latency and throughput."""
     import inq_b200 as ib
@@ -240,14 +240,20 @@ def serving_leg(ctx, rates=(100.0, 1000.0), nreq=120):
         reqs = serving.poisson_requests(pool, nreq, rate, seed=int(rate), large=large)
         st = srv.run(reqs)
         out[f"{int(rate)}_req_s"] = {k: st[k] for k in ("completed", "rejected", "throughput_req_s",
-                                                        "state_applications_per_s", "p50_ms", "p99_ms", "max_ms")}
+                                                        "state_applications_per_s", "p50_ms", "p99_ms", "max_ms",
+                                                        "mean_phase_ms")}
     srv.close()
     return out
 
 
-def etrs_leg(ctx, steps=10):
+def etrs_leg(ctx, steps=10, dt=0.005):
     """C3: ETRS propagation at 120^3 / 256 states / 128 atoms after a 0.01 a.u. kick along x (phase
-    exp(i 0.01 x)), dt = 0.05, FP64 density every step; plain FP64 and mixed dipole series."""
+    exp(i 0.01 x)), FP64 density every step; plain FP64 and mixed dipole series.
+
+    The time step: the order-4 Taylor exponential (exponential.hpp:21-69) is stable only for
+    dt * E_max < 2 sqrt(2), and the grid's kinetic energy reaches E_max = 3/2 (pi n / a)^2 = 325 Ha at
+    120^3 / a = 25.6 bohr, so dt must stay below 0.0087 a.u.; at dt = 0.05 the norm grows without bound
+    (the reference algorithm does the same).  The leg runs at dt = 0.005."""
     import numpy as np
     import torch
     import inq_b200 as ib
@@ -257,24 +263,34 @@ def etrs_leg(ctx, steps=10):
     ib.apply_phase_kick(phi64, [0.01, 0.0, 0.0])
     phi32 = phi64.converted(ib.F32)
     occ = np.full(sysm.nst, 2.0)
+    emax = 1.5 * (np.pi * sysm.sizes[0] / sysm.lattice[0][0]) ** 2
     out = {}
     stream = torch.cuda.ExternalStream(ctx.stream())
     for name, phi in (("fp64", phi64), ("mixed", phi32)):
         dips = []
+        iters = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ctx.synchronize()
         e0.record(stream)
         for _ in range(steps):
-            _, dip, _ = ib.etrs(ham, [phi], [occ], 0.05)
+            _, dip, it = ib.etrs(ham, [phi], [occ], dt)
             dips.append(dip.tolist())
+            iters.append(it)
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
-        out[name] = {"steps_per_s": steps / (ms / 1000.0), "ms_per_step": ms / steps, "dipole_series": dips}
+        norm = ib.overlap_diagonal(phi).real
+        out[name] = {"steps_per_s": steps / (ms / 1000.0), "ms_per_step": ms / steps,
+                     "scf_iterations": iters, "max_norm_drift": float(np.max(np.abs(norm - 1.0))),
+                     "dipole_series": dips}
     d64 = np.array(out["fp64"]["dipole_series"])
     d32 = np.array(out["mixed"]["dipole_series"])
     out["max_dipole_diff_mixed_vs_fp64"] = float(np.max(np.abs(d64 - d32)))
-    out["workload"] = f"c3: 120^3, {sysm.nst} states, {sysm.natoms} atoms, kick 0.01 x, dt 0.05, {steps} steps"
+    out["max_rel_dipole_change_fp64"] = float(np.max(np.abs(d64 - d64[0])))
+    out["dt"] = dt
+    out["dt_stability_bound"] = float(2 * np.sqrt(2) / emax)
+    out["workload"] = (f"c3: 120^3, {sysm.nst} states, {sysm.natoms} atoms, kick 0.01 x, dt {dt} "
+                       f"(0.05 exceeds the Taylor-4 stability bound {2 * np.sqrt(2) / emax:.4f}), {steps} steps")
     return out
 
 
@@ -424,7 +440,7 @@ def run_ours(args):
         legs["batch"] = batch_leg(ctx)
         legs["serving"] = serving_leg(ctx)
         if args.etrs_steps > 0:
-            legs["etrs"] = etrs_leg(ctx, args.etrs_steps)
+            legs["etrs"] = etrs_leg(ctx, args.etrs_steps, args.etrs_dt)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -468,8 +484,8 @@ def run_ours(args):
         }
         line.update(legs)
         if "serving" in legs:
-            line["serving_p50_ms"] = legs["serving"]["100_req_s"]["p50_ms"]
-            line["serving_p99_ms"] = legs["serving"]["100_req_s"]["p99_ms"]
+            line["serving_p50_ms"] = legs["serving"]["50_req_s"]["p50_ms"]
+            line["serving_p99_ms"] = legs["serving"]["50_req_s"]["p99_ms"]
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -506,6 +522,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-legs", action="store_true", help="skip the batched-systems, serving and ETRS legs")
     ap.add_argument("--etrs-steps", type=int, default=10, help="ETRS steps of the 120^3 real-time leg (0: skip)")
+    ap.add_argument("--etrs-dt", type=float, default=0.005, help="time step of the 120^3 real-time leg (a.u.)")
     ap.add_argument("--profile-case", action="store_true", help="small workload for ncu captures")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -358,7 +358,8 @@ __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_
   TC *exch = reinterpret_cast<TC *>(stage_aux + (AUX ? size_t(NS) * TILE : 0));  // one tile when SPLIT
   TC *tw = exch + (SPLIT ? TILE : 0);                                // N twiddles
   CR *linev = reinterpret_cast<CR *>(tw + N);                        // N per-point factors of the current line
-  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N + N);          // NS barriers (8-byte aligned)
+  int2 *lineh = reinterpret_cast<int2 *>(tw + N + N);                // N hit ranges of the current line's points
+  uint64_t *bar = reinterpret_cast<uint64_t *>(lineh + N);           // NS barriers (8-byte aligned)
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar + NS);
 
   const Geom &g = gg.g;
@@ -432,6 +433,13 @@ __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_
     } else if constexpr (VAR == INV_FINAL || VAR == FWD_VPSI) {
       for (int m = threadIdx.x; m < N; m += NT)
         linev[m] = CR(a.V[(pbase + m * g.sp) * a.nspin + a.spin]) + CR(a.vshift);
+      if constexpr (VAR == INV_FINAL) {
+        if (a.nl_offs)
+          for (int m = threadIdx.x; m < N; m += NT) {
+            const long long pt = pbase + m * g.sp;
+            lineh[m] = make_int2(__ldg(&a.nl_offs[pt]), __ldg(&a.nl_offs[pt + 1]));
+          }
+      }
     }
     if constexpr (VAR == FWD_VPSI) {
       __syncthreads();
@@ -454,6 +462,18 @@ __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_
       const int s = s0 + w;
       if (scaled) v = cscale(v, CR(a.scale));
       if constexpr (VAR == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
+      if constexpr (VAR == INV_FINAL) {
+        // nonlocal term: sum over the projectors whose sphere holds this point
+        if (a.nl_offs && s < a.S) {
+          const int2 hr = lineh[m];
+          for (int h = hr.x; h < hr.y; h++) {
+            const long long pl = (long long)__ldg(&a.nl_hitp[h]) * 4;
+#pragma unroll
+            for (int l = 0; l < 4; l++)
+              v = cadd(v, cmul(conv<TC>(a.nl_hcoef[h * 4 + l]), conv<TC>(a.projD[(pl + l) * a.S + s])));
+          }
+        }
+      }
       const T o = conv<T>(v);
       if (accum && s < a.S) {
         const long long ge = (pbase + m * g.sp) * a.S + s;
@@ -558,9 +578,10 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   const int nbuf = has_aux(VAR) ? 2 : 1;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
   constexpr int NT = threads_of<R, CR>();
-  const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + 2 * N * sizeof(TC) + 64 + 16 * 8;
-  // shared memory per CTA: ~113 KB (two CTAs per SM), ~56 KB for the wide-arithmetic kernels (four)
-  const size_t budget = SPLIT ? 56 * 1024 : 113 * 1024;
+  const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + 2 * N * sizeof(TC) + N * sizeof(int2) + 64 + 16 * 8;
+  // shared memory per CTA: ~113 KB (two CTAs per SM) for the streaming passes; ~56 KB (four per SM)
+  // for the wide-arithmetic and the kinetic passes, whose arithmetic needs more warps to hide latency
+  const size_t budget = (SPLIT || VAR == MID_KIN) ? 56 * 1024 : 113 * 1024;
   int ns = int((budget - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;

@@ -203,7 +203,7 @@ __device__ __forceinline__ C2<R> nl_term(const PassArgs<R> &a, long long pt, int
   T acc = mk<T>(R(0), R(0));
   const int h0 = __ldg(&a.nl_offs[pt]), h1 = __ldg(&a.nl_offs[pt + 1]);
   for (int h = h0; h < h1; h++) {
-    const int p = __ldg(&a.nl_hit[h]) / a.maxsph;
+    const int p = __ldg(&a.nl_hitp[h]);
 #pragma unroll
     for (int l = 0; l < 4; l++) {
       T c = a.nl_hcoef[h * 4 + l];

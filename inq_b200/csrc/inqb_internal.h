@@ -165,10 +165,9 @@ template <typename R> struct PassArgs {
   int nspin = 1, spin = 0;
   R vshift = R(0);
   const int *nl_offs = nullptr;
-  const int *nl_hit = nullptr;
+  const int *nl_hitp = nullptr;     // projector index of each hit
   const C2<R> *nl_hcoef = nullptr;
   const C2<R> *projD = nullptr;
-  int maxsph = 0;
   // Taylor accumulators: acc1 += c1 * out, acc2 += c2 * out
   C2<R> *acc1 = nullptr, *acc2 = nullptr;
   C2<R> c1, c2;

@@ -47,7 +47,7 @@ class Request:
     kind: str                      # "apply" | "etrs"
     payload: Payload
     steps: int = 1
-    dt: float = 0.05
+    dt: float | None = None        # None: 0.05 a.u., or less where the grid needs it (synthetic.taylor_stable_dt)
     arrival: float = 0.0           # seconds after the start of the run
     # filled by the server
     admitted: float = -1.0
@@ -125,26 +125,35 @@ class Server:
 
     # ------------------------------------------------------------------ one request on one slot
     def _execute(self, req: Request, ctx: core.Context):
+        t0 = time.perf_counter()
         sysm = req.payload.system
         basis = core.RealSpace(core.Cell(sysm.lattice), sizes=sysm.sizes, ctx=ctx)
         ham = core.KSHamiltonian(basis)
         ham.set_scalar_potential(req.payload.potential)
         ham.update_projectors_gaussian(sysm.positions, sysm.radius, sysm.rc, sysm.kb)
         phi = core.OrbitalSet(basis, sysm.nst, precision=self.precision).upload(req.payload.orbitals)
+        ctx.synchronize()
+        t1 = time.perf_counter()
         if req.kind == "apply":
             out = phi.skeleton()
             ham.apply(phi, out)
+            ctx.synchronize()
+            t2 = time.perf_counter()
             req.result = {"hphi": self._fetch(ctx, out), "happs": sysm.nst}
         else:
             occ = np.full(sysm.nst, 2.0)
+            dt = req.dt if req.dt is not None else min(0.05, synthetic.taylor_stable_dt(sysm))
             dips = []
             happs = 0
             for _ in range(req.steps):
-                _, dip, iters = core.etrs(ham, [phi], [occ], req.dt)
+                _, dip, iters = core.etrs(ham, [phi], [occ], dt)
                 dips.append(dip)
                 happs += (4 + 4 * iters) * sysm.nst   # exponential_2_for_1 + one exponential per SCF pass
+            ctx.synchronize()
+            t2 = time.perf_counter()
             req.result = {"dipoles": np.array(dips), "phi": self._fetch(ctx, phi), "happs": happs}
         ctx.synchronize()
+        req.result["phases_ms"] = ((t1 - t0) * 1e3, (t2 - t1) * 1e3, (time.perf_counter() - t2) * 1e3)
 
     def _worker(self, slot: int, req: Request, t0: float, fp: int):
         try:
@@ -190,11 +199,15 @@ class Server:
         done = [r for r in reqs if not r.error]
         lat = np.array([r.latency for r in done]) if done else np.zeros(1)
         happs = sum(r.result.get("happs", 0) for r in done)
+        ph = np.array([r.result["phases_ms"] for r in done if "phases_ms" in r.result]).reshape(-1, 3)
+        phases = {k: float(ph[:, i].mean()) if len(ph) else 0.0
+                  for i, k in enumerate(("setup_ms", "compute_ms", "fetch_ms"))}
         return {"requests": len(reqs), "completed": len(done), "rejected": len(reqs) - len(done),
                 "wall_s": wall, "throughput_req_s": len(done) / wall,
                 "state_applications_per_s": happs / wall,
                 "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000),
-                "max_ms": float(lat.max() * 1000), "peak_committed_bytes": self.peak_committed,
+                "max_ms": float(lat.max() * 1000), "mean_phase_ms": phases,
+                "peak_committed_bytes": self.peak_committed,
                 "budget_bytes": self.budget}
 
     def close(self):

@@ -153,6 +153,28 @@ def config(name: str, seed: int = 20240601, nst: int | None = None, n: int | Non
     raise ValueError(f"unknown configuration {name}")
 
 
+def max_kinetic_energy(sysm: System) -> float:
+    """Largest kinetic energy 1/2 |G|^2 (Ha) on the system's grid: the corners of the symmetric G range."""
+    rec = 2.0 * np.pi * np.linalg.inv(sysm.lattice).T     # rows: reciprocal vectors b_i (a_i . b_j = 2 pi delta_ij)
+    half = np.array(sysm.sizes, dtype=np.float64) / 2.0
+    best = 0.0
+    for sx in (-1, 1):
+        for sy in (-1, 1):
+            for sz in (-1, 1):
+                g = (np.array([sx, sy, sz]) * half) @ rec
+                best = max(best, 0.5 * float(g @ g))
+    return best
+
+
+def taylor_stable_dt(sysm: System, margin: float = 0.5) -> float:
+    """A time step at which the order-4 Taylor propagator (exponential.hpp:21-69) stays bounded.
+
+    |sum_{n<=4} (-i x)^n / n!|^2 = 1 - x^6/72 + x^8/576 exceeds 1 for x = dt * E > 2 sqrt(2), so
+    the spectrum's top (the grid's largest kinetic energy) fixes dt < 2 sqrt(2) / E_max; ``margin``
+    scales that bound."""
+    return margin * 2.0 * np.sqrt(2.0) / max_kinetic_energy(sysm)
+
+
 BATCH_GRIDS = (24, 32, 40, 48, 64, 72)
 
 
