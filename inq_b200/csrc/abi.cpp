@@ -169,15 +169,11 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   a.acc2 = static_cast<C2<R> *>(acc.acc2);
   a.c1 = mk<C2<R>>(R(acc.c1[0]), R(acc.c1[1]));
   a.c2 = mk<C2<R>>(R(acc.c2[0]), R(acc.c2[1]));
-  // the nonlocal term joins the epilogue at the sphere points (before the Taylor accumulators)
-  if (h.proj.nproj > 0) {
-    a.nl_offs = h.proj.d_offs;
-    a.nl_hitp = h.proj.d_hitp;
-    if constexpr (sizeof(R) == 8) a.nl_hcoef = h.proj.d_hcoef;
-    else a.nl_hcoef = h.proj.d_hcoef32;
-    a.projD = projD;
-  }
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_FINAL_REAL);
+  // nonlocal term added at the sphere points (and to the Taylor accumulators) by its own kernel: as a
+  // fully occupied kernel of its own it hides the latency of the hit-table and projection reads, which
+  // stall the FFT epilogue
+  if (h.proj.nproj > 0) launch_nl_apply<R>(ctx, h, projD, S, hpsi, a.acc1, a.c1, a.acc2, a.c2);
 }
 
 template <typename R> void apply_fourier(Hamiltonian &h, const Orbitals &in, Orbitals &out) {

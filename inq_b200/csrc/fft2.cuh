@@ -329,22 +329,30 @@ struct Geom2 {
 
 template <int VAR> constexpr int dir_first() { return (VAR == INV_STORE || VAR == INV_FINAL) ? -1 : +1; }
 
-// 128 threads per CTA; tiles of 256-byte rows, or 128-byte rows when the butterflies run in a wider
-// type than the storage (the tile then also needs an exchange buffer of that type, and smaller tiles
-// let three CTAs share an SM to cover the double-precision latency)
-template <typename R, typename CR> constexpr int threads_of() { return 128; }
+// Tiles of 256-byte rows, or 128-byte rows when the butterflies run in a wider type than the storage
+// (the tile then also needs an exchange buffer of that type, and smaller tiles let several CTAs share
+// an SM to cover the double-precision latency).
 template <typename R, typename CR> constexpr int tile_w() {
   return (sizeof(CR) > sizeof(R) ? 128 : 256) / int(2 * sizeof(R));
 }
+// Threads per CTA.  The two steps of a tile transform have W*N2 and W*N1 independent line pieces; with
+// 128 threads and 16-state tiles (N1 = 8) the first step of N = 72, 96, 120, 128 takes two rounds in
+// which part of the CTA idles at the next barrier, so those tiles get one thread per first-step piece.
+template <typename R, typename CR, int N> constexpr int threads_of() {
+  constexpr int W = tile_w<R, CR>();
+  constexpr int A = W * Split<N>::N2, B = W * Split<N>::N1;
+  constexpr int M = A > B ? A : B;
+  return (W == 16 && M > 128 && M <= 256) ? (M + 31) / 32 * 32 : 128;
+}
 
 template <typename R, typename CR, int N, int VAR>
-__global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
+__global__ void __launch_bounds__(threads_of<R, CR, N>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
                                                    const __grid_constant__ CUtensorMap map_out,
                                                    const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
                                                    const C2<CR> *__restrict__ twg, int *err) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr int NT = threads_of<R, CR>();
+  constexpr int NT = threads_of<R, CR, N>();
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);    // exchange buffer in the arithmetic type
   constexpr int W = tile_w<R, CR>();
   constexpr int TILE = N * W;                       // complex elements per tile
@@ -358,8 +366,7 @@ __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_
   TC *exch = reinterpret_cast<TC *>(stage_aux + (AUX ? size_t(NS) * TILE : 0));  // one tile when SPLIT
   TC *tw = exch + (SPLIT ? TILE : 0);                                // N twiddles
   CR *linev = reinterpret_cast<CR *>(tw + N);                        // N per-point factors of the current line
-  int2 *lineh = reinterpret_cast<int2 *>(tw + N + N);                // N hit ranges of the current line's points
-  uint64_t *bar = reinterpret_cast<uint64_t *>(lineh + N);           // NS barriers (8-byte aligned)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N + N);          // NS barriers (8-byte aligned)
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar + NS);
 
   const Geom &g = gg.g;
@@ -433,13 +440,6 @@ __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_
     } else if constexpr (VAR == INV_FINAL || VAR == FWD_VPSI) {
       for (int m = threadIdx.x; m < N; m += NT)
         linev[m] = CR(a.V[(pbase + m * g.sp) * a.nspin + a.spin]) + CR(a.vshift);
-      if constexpr (VAR == INV_FINAL) {
-        if (a.nl_offs)
-          for (int m = threadIdx.x; m < N; m += NT) {
-            const long long pt = pbase + m * g.sp;
-            lineh[m] = make_int2(__ldg(&a.nl_offs[pt]), __ldg(&a.nl_offs[pt + 1]));
-          }
-      }
     }
     if constexpr (VAR == FWD_VPSI) {
       __syncthreads();
@@ -462,18 +462,6 @@ __global__ void __launch_bounds__(threads_of<R, CR>()) fft2_kernel(const __grid_
       const int s = s0 + w;
       if (scaled) v = cscale(v, CR(a.scale));
       if constexpr (VAR == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
-      if constexpr (VAR == INV_FINAL) {
-        // nonlocal term: sum over the projectors whose sphere holds this point
-        if (a.nl_offs && s < a.S) {
-          const int2 hr = lineh[m];
-          for (int h = hr.x; h < hr.y; h++) {
-            const long long pl = (long long)__ldg(&a.nl_hitp[h]) * 4;
-#pragma unroll
-            for (int l = 0; l < 4; l++)
-              v = cadd(v, cmul(conv<TC>(a.nl_hcoef[h * 4 + l]), conv<TC>(a.projD[(pl + l) * a.S + s])));
-          }
-        }
-      }
       const T o = conv<T>(v);
       if (accum && s < a.S) {
         const long long ge = (pbase + m * g.sp) * a.S + s;
@@ -577,8 +565,8 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
   const int nbuf = has_aux(VAR) ? 2 : 1;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
-  constexpr int NT = threads_of<R, CR>();
-  const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + 2 * N * sizeof(TC) + N * sizeof(int2) + 64 + 16 * 8;
+  constexpr int NT = threads_of<R, CR, N>();
+  const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + 2 * N * sizeof(TC) + 64 + 16 * 8;
   // shared memory per CTA: ~113 KB (two CTAs per SM) for the streaming passes; ~56 KB (four per SM)
   // for the wide-arithmetic and the kinetic passes, whose arithmetic needs more warps to hide latency
   const size_t budget = (SPLIT || VAR == MID_KIN) ? 56 * 1024 : 113 * 1024;
