@@ -246,6 +246,31 @@ def serving_leg(ctx, rates=(50.0, 200.0, 1000.0, 2000.0), nreq=120):
     return out
 
 
+def overlap_leg(ctx, phi32, phi64, time_loop, reps=5):
+    """Subspace overlap S = dV phi^H phi of the 96^3 / 256-state set: the mixed form's split-BF16
+    tensor-core kernel against the FP64 overlap of the FP64 set (tensor roofline: the executed
+    BF16 products are 3 x 8 N S^2 flop)."""
+    import numpy as np
+    import inq_b200 as ib
+    N = phi32.basis.size()
+    S = phi32.nst
+    ref = ib.overlap(phi64)
+    got = ib.overlap(phi32)
+    ms_tc = time_loop(lambda: ib.overlap(phi32), reps) / reps
+    ms_64 = time_loop(lambda: ib.overlap(phi64), 1)
+    flop = 3.0 * 8.0 * N * S * S
+    peak = float(json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                             "MEASURED_PEAKS.json")))["bf16_tflops"]) \
+        if os.path.exists(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) else 1590.0
+    return {"workload": f"overlap of the c2 set: {N} points, {S} x {S} states",
+            "ms_tensor_core_split_bf16": ms_tc, "ms_fp64_simt": ms_64,
+            "rel_err_vs_fp64": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+            "max_abs_err_vs_fp64": float(np.max(np.abs(got - ref))),
+            "roofline": {"bound": "tensor", "achieved": flop / (ms_tc / 1000.0) / 1e12, "peak": peak,
+                         "unit": "TFLOP/s", "frac": flop / (ms_tc / 1000.0) / 1e12 / peak,
+                         "flop_per_call": flop}}
+
+
 def etrs_leg(ctx, steps=10, dt=0.005):
     """C3: ETRS propagation at 120^3 / 256 states / 128 atoms after a 0.01 a.u. kick along x (phase
     exp(i 0.01 x)), FP64 density every step; plain FP64 and mixed dipole series.
@@ -437,6 +462,7 @@ def run_ours(args):
 
     legs = {}
     if world == 1 and not args.skip_legs:
+        legs["overlap"] = overlap_leg(ctx, phi32, phi64, time_loop)
         legs["batch"] = batch_leg(ctx)
         legs["serving"] = serving_leg(ctx)
         if args.etrs_steps > 0:

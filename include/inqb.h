@@ -58,7 +58,11 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * the butterfly arithmetic of single-precision orbitals: 0 single everywhere, 1 double
  * everywhere, 2 double except the last inverse pass of H, 3 (default) as 2 and single for
  * the first forward pass of every transform too; "fft_stages" = 0 (ring depth of the TMA
- * kernels from their shared-memory budget, the default) or 2..8 stages. */
+ * kernels from their shared-memory budget, the default) or 2..8 stages; "overlap_tc" = 1
+ * (default: overlaps of single-precision sets -- inqb_overlap, and the ones inside
+ * inqb_orthogonalize and inqb_subspace_diagonalization -- on the tensor cores as split-BF16
+ * products with FP32 accumulation and an FP64 sum of the per-SM partials) or 0 (FP64 SIMT
+ * products, as for double-precision sets). */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Free and total device memory in bytes (admission control for serving). */
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
@@ -158,7 +162,8 @@ int inqb_kinetic_expectation_value(const inqb_hamiltonian *ham, const inqb_orbit
 
 /* ---- orbital-set linear algebra ------------------------------------------- */
 /* operations::overlap (overlap.hpp:26-95): S[i][j] = dV sum_r conj(a[r][i]) b[r][j]; host out
- * [nst_a][nst_b] complex128. */
+ * [nst_a][nst_b] complex128.  Single-precision sets use the tensor cores unless the context
+ * option "overlap_tc" is 0. */
 int inqb_overlap(const inqb_orbitals *a, const inqb_orbitals *b, double *out);
 /* operations::overlap_diagonal (overlap_diagonal.hpp:25-55): host out [nst] complex128. */
 int inqb_overlap_diagonal(const inqb_orbitals *a, const inqb_orbitals *b, double *out);

@@ -72,7 +72,7 @@ void check_same_shape(const Orbitals &a, const Orbitals &b) {
 // ------------------------------------------------------------------ transforms
 
 template <typename R>
-void fft3d(Ctx &ctx, const Basis &b, const C2<R> *in, C2<R> *out, int S, int dir, R scale) {
+void fft3d(Ctx &ctx, const Basis &b, const C2<R> *in, C2<R> *out, int S, int dir, double scale) {
   PassArgs<R> a;
   a.S = S;
   a.dir = dir;
@@ -83,7 +83,7 @@ void fft3d(Ctx &ctx, const Basis &b, const C2<R> *in, C2<R> *out, int S, int dir
     a.axis = order[k];
     a.in = (k == 0) ? in : out;
     a.out = out;
-    a.scale = (k == 2) ? scale : R(1);
+    a.scale = (k == 2) ? scale : 1.0;
     launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   }
 }
@@ -146,10 +146,11 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   a.axis = 1;
   a.in = hpsi;
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
-  // x: forward, kinetic factor -0.5*(-|G|^2 + gc.G), gc = -2 (k+A)^contra, backward
+  // x: forward, kinetic factor -0.5*(-|G|^2 + gc.G), gc = -2 (k+A)^contra, backward; the 1/N of the
+  // inverse transform is folded into the per-point factor (formed in double, rounded once)
   a.axis = 0;
   a.mid_kinetic = 1;
-  a.lap_factor = -0.5;
+  a.lap_factor = -0.5 / double(b.npoints);
   for (int i = 0; i < 3; i++) a.gc[i] = -2.0 * kc[i];
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   a.mid_kinetic = 0;
@@ -158,7 +159,6 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   a.axis = 1;
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   a.axis = 2;
-  a.scale = R(1.0 / double(b.npoints));
   a.psi = psi;
   if constexpr (sizeof(R) == 8) a.V = h.d_V;
   else a.V = h.d_V32;
@@ -188,7 +188,7 @@ template <typename R> void apply_fourier(Hamiltonian &h, const Orbitals &in, Orb
   cart_to_contra(b, ktmp, kc);
 
   // psi_rs = to_real(fpsi) in the output buffer
-  fft3d<R>(ctx, b, fpsi, w, S, -1, R(1.0 / double(b.npoints)));
+  fft3d<R>(ctx, b, fpsi, w, S, -1, 1.0 / double(b.npoints));
   C2<R> *projD = nullptr;
   if (h.proj.nproj > 0) {
     ensure_tables(h, kA);
@@ -432,6 +432,9 @@ void overlap_dev(const Orbitals &a, const Orbitals &b, double2 *out_dev) {
   if (a.precision == INQB_F64)
     launch_overlap<double>(ctx, static_cast<const double2 *>(a.data), a.nst, static_cast<const double2 *>(b.data),
                            b.nst, a.basis->npoints, dv, out_dev);
+  else if (ctx.overlap_tc)
+    launch_overlap_tc(ctx, static_cast<const float2 *>(a.data), a.nst, static_cast<const float2 *>(b.data), b.nst,
+                      a.basis->npoints, dv, out_dev);
   else
     launch_overlap<float>(ctx, static_cast<const float2 *>(a.data), a.nst, static_cast<const float2 *>(b.data), b.nst,
                           a.basis->npoints, dv, out_dev);
@@ -642,6 +645,9 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     } else if (k == "mixed_compute") {
       INQB_REQUIRE(value >= 0 && value <= 3, INQB_ERR_ARG, "mixed_compute is 0, 1, 2 or 3");
       ctx->mixed_compute = int(value);
+    } else if (k == "overlap_tc") {
+      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "overlap_tc is 0 (FP64 SIMT) or 1 (tensor cores)");
+      ctx->overlap_tc = int(value);
     } else {
       throw Error(INQB_ERR_ARG, "unknown option " + k);
     }
@@ -680,17 +686,19 @@ int inqb_basis_create(inqb_ctx *ctx, const double lattice[9], int nx, int ny, in
         const int n = b->n[ax];
         b->radices[ax] = fft_radices(n);
         std::vector<double2> t64(n);
-        std::vector<float2> t32(n);
+        std::vector<float2> t32(2 * n);  // float parts, then the remainders (cos - float(cos), ...)
         const long double two_pi = 6.283185307179586476925286766559005768L;
         for (int t = 0; t < n; t++) {
           const long double ang = two_pi * (long double)t / (long double)n;
           t64[t] = make_double2(double(cosl(ang)), double(-sinl(ang)));
-          t32[t] = make_float2(float(cosl(ang)), float(-sinl(ang)));
+          const long double c = cosl(ang), sn = -sinl(ang);
+          t32[t] = make_float2(float(c), float(sn));
+          t32[n + t] = make_float2(float(c - (long double)t32[t].x), float(sn - (long double)t32[t].y));
         }
         INQB_CUDA(cudaMallocAsync(&b->tw64[ax], sizeof(double2) * n, ctx->stream));
-        INQB_CUDA(cudaMallocAsync(&b->tw32[ax], sizeof(float2) * n, ctx->stream));
+        INQB_CUDA(cudaMallocAsync(&b->tw32[ax], sizeof(float2) * 2 * n, ctx->stream));
         INQB_CUDA(cudaMemcpyAsync(b->tw64[ax], t64.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, ctx->stream));
-        INQB_CUDA(cudaMemcpyAsync(b->tw32[ax], t32.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, ctx->stream));
+        INQB_CUDA(cudaMemcpyAsync(b->tw32[ax], t32.data(), sizeof(float2) * 2 * n, cudaMemcpyHostToDevice, ctx->stream));
         INQB_CUDA(cudaStreamSynchronize(ctx->stream));
       }
     } catch (...) {
@@ -876,7 +884,7 @@ int inqb_to_real(const inqb_orbitals *in, inqb_orbitals *out, int normalize) {
                     in->nst, -1, sc);
     else
       fft3d<float>(*in->ctx, *in->basis, static_cast<const float2 *>(in->data), static_cast<float2 *>(out->data),
-                   in->nst, -1, float(sc));
+                   in->nst, -1, sc);
     out->space = INQB_REAL_SPACE;
     for (int i = 0; i < 3; i++) out->kpoint[i] = in->kpoint[i];
     out->spin_index = in->spin_index;

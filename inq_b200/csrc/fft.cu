@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(PassArgs<R> a, Geom g, Ra
     const long long pt = pbase + p * g.sp;
     const long long e = pt * a.S + s;
     T v = res[p * W + w];
-    if (a.scale != R(1)) v = cscale(v, a.scale);
+    if (a.scale != 1.0) v = cscale(v, R(a.scale));
     if (EPI == EPI_FINAL_REAL) {
       R vv = a.V[pt * a.nspin + a.spin] + a.vshift;
       v = cadd(v, cscale(a.psi[e], vv));

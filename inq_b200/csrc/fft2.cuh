@@ -18,6 +18,7 @@
 #include <cuda.h>
 
 #include "fft_common.cuh"
+#include "ptx.cuh"
 
 namespace inqb {
 namespace v2 {
@@ -46,28 +47,13 @@ constexpr int first_factor(int M) {
 
 // ------------------------------------------------------------------ PTX helpers
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+using ptx::global_ns;
+using ptx::mbar_init;
+using ptx::mbar_init_fence;
+using ptx::mbar_try_wait;
+using ptx::smem_u32;
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
 }
 __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
                                             int c3) {
@@ -86,7 +72,7 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+using ptx::fence_proxy_async;
 
 // ------------------------------------------------------------------ register codelets (compile-time size)
 
@@ -100,6 +86,35 @@ template <int DIR, typename T> __device__ __forceinline__ T twid(T t) {
 }
 
 // cos(2 pi m / r) and sin(2 pi m / r), m = 1..(r-1)/2, for the odd prime codelets
+// Single-precision products by a constant or a twiddle factor.  The float roundings of sqrt(1/2),
+// sin(pi/3) and of many table twiddles fall on the same side often enough to shrink every transform
+// by ~2e-8 (an energy bias that reaches ~1e-6 Ha in <psi|H|psi>).  With c = c_hi + c_lo (c_lo the
+// float rounding remainder), fma(x, c_hi, x * c_lo) leaves only an unbiased rounding; double products
+// need no correction.
+template <typename T> __device__ __forceinline__ T kscale(T a, double c) {
+  using R = decltype(T::x);
+  if constexpr (sizeof(R) == 4) {
+    const float hi = float(c), lo = float(c - double(float(c)));
+    if (lo == 0.0f) return mk<T>(a.x * hi, a.y * hi);
+    return mk<T>(__fmaf_rn(a.x, hi, a.x * lo), __fmaf_rn(a.y, hi, a.y * lo));
+  } else {
+    return mk<T>(a.x * R(c), a.y * R(c));
+  }
+}
+// a times twiddle `idx` of the line table; single-precision tables hold N high parts then N low parts.
+template <int DIR, int N, typename T> __device__ __forceinline__ T twmul(T a, const T *__restrict__ tw, int idx) {
+  using R = decltype(T::x);
+  if constexpr (sizeof(R) == 4) {
+    const T h = twid<DIR>(tw[idx]), l = twid<DIR>(tw[idx + N]);
+    const R lr = __fmaf_rn(-a.y, l.y, a.x * l.x), li = __fmaf_rn(a.y, l.x, a.x * l.y);
+    return mk<T>(__fmaf_rn(a.x, h.x, __fmaf_rn(-a.y, h.y, lr)), __fmaf_rn(a.x, h.y, __fmaf_rn(a.y, h.x, li)));
+  } else {
+    return cmul(a, twid<DIR>(tw[idx]));
+  }
+}
+// entries of the line's twiddle table in shared memory: N, or 2N for single precision
+template <typename R> constexpr int tw_entries(int N) { return sizeof(R) == 4 ? 2 * N : N; }
+
 template <int RR> __host__ __device__ constexpr double odd_cos(int m) {
   if (RR == 3) return -0.5;
   if (RR == 5) return m == 1 ? 0.30901699437494742410229341718281905886 : -0.80901699437494742410229341718281905886;
@@ -129,18 +144,18 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
     v[1] = cadd(t1, t3);
     v[3] = csub(t1, t3);
   } else if constexpr (M == 8) {
-    const R h = R(0.70710678118654752440084436210484903928);
+    constexpr double h = 0.70710678118654752440084436210484903928;
     T e[4] = {v[0], v[2], v[4], v[6]};
     T o[4] = {v[1], v[3], v[5], v[7]};
     dft<4, DIR, N>(e, tw);
     dft<4, DIR, N>(o, tw);
     T w1, w3;
     if constexpr (DIR > 0) {
-      w1 = mk<T>((o[1].x + o[1].y) * h, (o[1].y - o[1].x) * h);
-      w3 = mk<T>((o[3].y - o[3].x) * h, (-o[3].x - o[3].y) * h);
+      w1 = kscale(mk<T>(o[1].x + o[1].y, o[1].y - o[1].x), h);
+      w3 = kscale(mk<T>(o[3].y - o[3].x, -o[3].x - o[3].y), h);
     } else {
-      w1 = mk<T>((o[1].x - o[1].y) * h, (o[1].y + o[1].x) * h);
-      w3 = mk<T>((-o[3].x - o[3].y) * h, (o[3].x - o[3].y) * h);
+      w1 = kscale(mk<T>(o[1].x - o[1].y, o[1].y + o[1].x), h);
+      w3 = kscale(mk<T>(-o[3].x - o[3].y, o[3].x - o[3].y), h);
     }
     T w2 = mmi<DIR>(o[2]);
     v[0] = cadd(e[0], o[0]);
@@ -171,10 +186,10 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
 #pragma unroll
       for (int m = 1; m <= H; m++) {
         const int idx = (m * k) % M;
-        const R c = idx <= H ? R(odd_cos<M>(idx)) : R(odd_cos<M>(M - idx));
-        const R sn = idx <= H ? R(odd_sin<M>(idx)) : -R(odd_sin<M>(M - idx));
-        re = cadd(re, cscale(a[m - 1], c));
-        im = cadd(im, cscale(b[m - 1], sn));
+        const double c = idx <= H ? odd_cos<M>(idx) : odd_cos<M>(M - idx);
+        const double sn = idx <= H ? odd_sin<M>(idx) : -odd_sin<M>(M - idx);
+        re = cadd(re, kscale(a[m - 1], c));
+        im = cadd(im, kscale(b[m - 1], sn));
       }
       const T t = mmi<DIR>(im);
       y[k] = cadd(re, t);
@@ -196,7 +211,7 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
 #pragma unroll
       for (int k1 = 0; k1 < A; k1++) {
         if (j2 * k1 == 0) tmp[k1 * B + j2] = s[k1];
-        else tmp[k1 * B + j2] = cmul(s[k1], twid<DIR>(tw[(j2 * k1) * (N / M)]));
+        else tmp[k1 * B + j2] = twmul<DIR, N>(s[k1], tw, (j2 * k1) * (N / M));
       }
     }
 #pragma unroll
@@ -235,7 +250,7 @@ __device__ __forceinline__ void tile_dft(const SA *asrc, DA *adst, const TC *__r
     }
     dft<N1, DIR, N>(s, tw);
 #pragma unroll
-    for (int k1 = 1; k1 < N1; k1++) s[k1] = cmul(s[k1], twid<DIR>(tw[j2 * k1]));
+    for (int k1 = 1; k1 < N1; k1++) s[k1] = twmul<DIR, N>(s[k1], tw, j2 * k1);
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) adst[(j2 + N2 * k1) * W + w] = conv<DA>(s[k1]);
   }
@@ -288,7 +303,7 @@ __device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *_
     for (int j1 = 0; j1 < N1; j1++) s[j1] = buf[(j2 + N2 * j1) * W + w];
     dft<N1, DIR, N>(s, tw);
 #pragma unroll
-    for (int k1 = 1; k1 < N1; k1++) s[k1] = cmul(s[k1], twid<DIR>(tw[j2 * k1]));
+    for (int k1 = 1; k1 < N1; k1++) s[k1] = twmul<DIR, N>(s[k1], tw, j2 * k1);
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) buf[(j2 + N2 * k1) * W + w] = s[k1];
   }
@@ -338,21 +353,23 @@ template <typename R, typename CR> constexpr int tile_w() {
 // Threads per CTA.  The two steps of a tile transform have W*N2 and W*N1 independent line pieces; with
 // 128 threads and 16-state tiles (N1 = 8) the first step of N = 72, 96, 120, 128 takes two rounds in
 // which part of the CTA idles at the next barrier, so those tiles get one thread per first-step piece.
-template <typename R, typename CR, int N> constexpr int threads_of() {
+// The kinetic pass (two transforms, the second with two idle thirds in its second step either way)
+// keeps 128 threads and more CTAs per SM.
+template <typename R, typename CR, int N, int VAR> constexpr int threads_of() {
   constexpr int W = tile_w<R, CR>();
   constexpr int A = W * Split<N>::N2, B = W * Split<N>::N1;
   constexpr int M = A > B ? A : B;
-  return (W == 16 && M > 128 && M <= 256) ? (M + 31) / 32 * 32 : 128;
+  return (VAR != MID_KIN && W == 16 && M > 128 && M <= 256) ? (M + 31) / 32 * 32 : 128;
 }
 
 template <typename R, typename CR, int N, int VAR>
-__global__ void __launch_bounds__(threads_of<R, CR, N>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
+__global__ void __launch_bounds__(threads_of<R, CR, N, VAR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
                                                    const __grid_constant__ CUtensorMap map_out,
                                                    const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
                                                    const C2<CR> *__restrict__ twg, int *err) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr int NT = threads_of<R, CR, N>();
+  constexpr int NT = threads_of<R, CR, N, VAR>();
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);    // exchange buffer in the arithmetic type
   constexpr int W = tile_w<R, CR>();
   constexpr int TILE = N * W;                       // complex elements per tile
@@ -364,13 +381,14 @@ __global__ void __launch_bounds__(threads_of<R, CR, N>()) fft2_kernel(const __gr
   T *stage_in = reinterpret_cast<T *>(smem);                         // NS tiles
   T *stage_aux = stage_in + size_t(NS) * TILE;                       // NS tiles when AUX
   TC *exch = reinterpret_cast<TC *>(stage_aux + (AUX ? size_t(NS) * TILE : 0));  // one tile when SPLIT
-  TC *tw = exch + (SPLIT ? TILE : 0);                                // N twiddles
-  CR *linev = reinterpret_cast<CR *>(tw + N);                        // N per-point factors of the current line
-  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + N + N);          // NS barriers (8-byte aligned)
+  constexpr int TWN = tw_entries<CR>(N);
+  TC *tw = exch + (SPLIT ? TILE : 0);                                // twiddles (high, then low parts)
+  CR *linev = reinterpret_cast<CR *>(tw + TWN);                      // N per-point factors of the current line
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + TWN + N);        // NS barriers (8-byte aligned)
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar + NS);
 
   const Geom &g = gg.g;
-  for (int i = threadIdx.x; i < N; i += NT) tw[i] = twg[i];
+  for (int i = threadIdx.x; i < TWN; i += NT) tw[i] = twg[i];
   if (threadIdx.x == 0) {
     *abort_flag = 0;
     for (int s = 0; s < NS; s++) mbar_init(&bar[s], 1);
@@ -402,7 +420,7 @@ __global__ void __launch_bounds__(threads_of<R, CR, N>()) fft2_kernel(const __gr
     }
   }
 
-  const bool scaled = a.scale != R(1);
+  const bool scaled = a.scale != 1.0;
   const bool accum = (a.acc1 != nullptr) || (a.acc2 != nullptr);
   int i = 0;
   for (long long t = blockIdx.x; t < gg.ntiles; t += gridDim.x, i++) {
@@ -460,7 +478,7 @@ __global__ void __launch_bounds__(threads_of<R, CR, N>()) fft2_kernel(const __gr
     // final store of one output value: epilogue terms, Taylor accumulators, write into the stage
     auto put_out = [&](int m, int w, TC v) {
       const int s = s0 + w;
-      if (scaled) v = cscale(v, CR(a.scale));
+      if (scaled) v = kscale(v, a.scale);
       if constexpr (VAR == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
       const T o = conv<T>(v);
       if (accum && s < a.S) {
@@ -565,8 +583,8 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
   const int nbuf = has_aux(VAR) ? 2 : 1;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
-  constexpr int NT = threads_of<R, CR, N>();
-  const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + 2 * N * sizeof(TC) + 64 + 16 * 8;
+  constexpr int NT = threads_of<R, CR, N, VAR>();
+  const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + size_t(tw_entries<CR>(N) + N) * sizeof(TC) + 64 + 16 * 8;
   // shared memory per CTA: ~113 KB (two CTAs per SM) for the streaming passes; ~56 KB (four per SM)
   // for the wide-arithmetic and the kinetic passes, whose arithmetic needs more warps to hide latency
   const size_t budget = (SPLIT || VAR == MID_KIN) ? 56 * 1024 : 113 * 1024;

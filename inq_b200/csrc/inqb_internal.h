@@ -72,6 +72,7 @@ struct Ctx {
   int fft_impl = 0;          // 0: specialised TMA kernels where available, 1: generic kernel only
   int fft_stages = 0;        // shared-memory ring depth of the TMA FFT kernels (0: from the memory budget)
   int mixed_compute = 3;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
+  int overlap_tc = 1;        // overlaps of single-precision sets on the tensor cores (split BF16)
 };
 
 struct Basis {
@@ -156,7 +157,7 @@ template <typename R> struct PassArgs {
   int axis = 0;
   int dir = +1;                 // +1 forward (e^{-i}), -1 backward
   int mid_kinetic = 0;          // forward, multiply by lapl factor, backward (same axis)
-  R scale = R(1);               // applied at the store
+  double scale = 1.0;           // applied at the store
   // lapl factor data: factor*(-|G|^2 + gc.G)
   double lap_factor = 0.0, gc[3] = {0, 0, 0};
   // final-real / prologue data
@@ -225,6 +226,9 @@ std::vector<int> fft_radices(int n);
 void basis_metric(const double lattice[9], double lat[3][3], double rec[3][3], double rlat[3][3], double &volume);
 
 void ensure_smem_attr(const void *kernel, size_t bytes);
+// S = dv a^H b of single-precision sets on the tensor cores (overlap_tc.cu); out [Sa][Sb] on the device
+void launch_overlap_tc(Ctx &ctx, const float2 *a, int Sa, const float2 *b, int Sb, long long npoints, double dv,
+                       double2 *out);
 
 // scratch allocation on the context stream (stream-ordered pool)
 void *dev_alloc(Ctx &ctx, size_t bytes);

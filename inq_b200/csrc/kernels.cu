@@ -206,14 +206,14 @@ void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
 // projector_all.hpp:276-288), owner computes: one thread per (hit point, state), hits of a point summed
 // in projector order, no atomics.  Optional Taylor accumulators acc += c * term (linear in the term).
 template <typename R>
-__global__ void __launch_bounds__(256, 2) nl_apply_kernel(long long nhp, int S, const int *__restrict__ hitpts,
+__global__ void __launch_bounds__(256) nl_apply_kernel(long long nhp, int S, const int *__restrict__ hitpts,
                                                        const int *__restrict__ offs, const int *__restrict__ hitp,
                                                        const C2<R> *__restrict__ hcoef, const C2<R> *__restrict__ projD,
                                                        C2<R> *__restrict__ out, C2<R> *__restrict__ acc1, C2<R> c1,
                                                        C2<R> *__restrict__ acc2, C2<R> c2) {
   using T = C2<R>;
-  constexpr int MAXH = 2;   // hits of a point kept in registers; more are read again per state chunk
-  constexpr int U = 32 / sizeof(R);   // states per lane and chunk (8 single, 4 double): 64 registers of chunk data
+  constexpr int MAXH = 2;  // hits of a point kept in registers; more are read again per state chunk
+  constexpr int U = 4;     // states per lane and chunk
   const int lane = threadIdx.x & 31;
   const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -232,21 +232,10 @@ __global__ void __launch_bounds__(256, 2) nl_apply_kernel(long long nhp, int S, 
       }
     }
     for (int s0 = 0; s0 < S; s0 += 32 * U) {
-      // issue every read of this chunk before any write: out (and the accumulators) are read once
-      T o[U], a1[U], a2[U], accv[U];
+      T accv[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const int s = s0 + u * 32 + lane;
         accv[u] = mk<T>(R(0), R(0));
-        if (s < S) {
-          const long long e = pt * S + s;
-          o[u] = out[e];
-          if (acc1) a1[u] = acc1[e];
-          if (acc2) a2[u] = acc2[e];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; u++) {
         const int s = s0 + u * 32 + lane;
         if (s >= S) continue;
 #pragma unroll
@@ -269,9 +258,9 @@ __global__ void __launch_bounds__(256, 2) nl_apply_kernel(long long nhp, int S, 
         const int s = s0 + u * 32 + lane;
         if (s >= S) continue;
         const long long e = pt * S + s;
-        out[e] = cadd(o[u], accv[u]);
-        if (acc1) acc1[e] = cadd(a1[u], cmul(c1, accv[u]));
-        if (acc2) acc2[e] = cadd(a2[u], cmul(c2, accv[u]));
+        out[e] = cadd(out[e], accv[u]);
+        if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, accv[u]));
+        if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, accv[u]));
       }
     }
   }
