@@ -151,6 +151,18 @@ int inqb_projectors_get(const inqb_hamiltonian *ham, int32_t *points, float *pos
 /* ks_hamiltonian::operator() (ks_hamiltonian.hpp:137-180): out = H in.  Real- or
  * Fourier-space form from in's space tag; out must be a distinct set of the same shape. */
 int inqb_apply(const inqb_hamiltonian *ham, const inqb_orbitals *in, inqb_orbitals *out);
+/* ks_hamiltonian::operator() (ks_hamiltonian.hpp:137-156) for a real-space set held in host memory:
+ * host_out = H host_in, both [npoint][nst] complex of `precision` (complex128 for INQB_F64, complex64
+ * for INQB_F32), with k-point kpoint_cov (NULL: Gamma) and spin spin_index.  The states go through
+ * the device in blocks of block_states (0: 512-byte rows, 32 double or 64 single states): the upload
+ * of the next block and the download of the previous one overlap the operator on the current block
+ * (two copy streams beside the context's stream).  Page-locked host buffers give that overlap;
+ * pageable ones are copied correctly but without it.  Returns when host_out is complete.  Holds two
+ * input and two output blocks of device memory during the call.  The reference returns a new
+ * device-resident set instead (operator() allocates its result); this is the host-buffer form of
+ * the same operator. */
+int inqb_apply_host(const inqb_hamiltonian *ham, int nst, const double kpoint_cov[3], int spin_index, int precision,
+                    const void *host_in, void *host_out, int block_states);
 /* ks_hamiltonian::non_local (ks_hamiltonian.hpp:106-120). */
 int inqb_non_local(const inqb_hamiltonian *ham, const inqb_orbitals *in, inqb_orbitals *out);
 /* ks_hamiltonian::non_local_energy (ks_hamiltonian.hpp:124-133, projector_all.hpp:306-327);

@@ -414,6 +414,30 @@ class KSHamiltonian:
         self.ctx.check(self.ctx.lib.inqb_apply(self.handle, phi.handle, out.handle))
         return out
 
+    def apply_host(self, host_in: np.ndarray, host_out: np.ndarray, kpoint=(0.0, 0.0, 0.0), spin_index: int = 0,
+                   block_states: int = 0) -> np.ndarray:
+        """H applied to a real-space set held in host memory ([npoint][nst] complex128 or complex64,
+        C-contiguous); the result is written into ``host_out``.  States stream through the device in
+        blocks with the copies overlapping the operator (page-locked arrays overlap, others are copied
+        without overlap)."""
+        if host_in.dtype != host_out.dtype or host_in.shape != host_out.shape or host_in.ndim != 2:
+            raise ValueError("host_in and host_out must be [npoint][nst] arrays of one complex type")
+        if host_in.dtype == np.complex128:
+            prec = F64
+        elif host_in.dtype == np.complex64:
+            prec = F32
+        else:
+            raise ValueError("complex128 or complex64 arrays expected")
+        if not (host_in.flags.c_contiguous and host_out.flags.c_contiguous):
+            raise ValueError("host arrays must be C-contiguous")
+        if host_in.shape[0] != self.basis.size():
+            raise ValueError("host arrays must have one row per grid point")
+        kp = np.asarray(kpoint, dtype=np.float64).copy()
+        self.ctx.check(self.ctx.lib.inqb_apply_host(self.handle, int(host_in.shape[1]), kp.ctypes.data_as(_lib.DP),
+                                                    int(spin_index), prec, host_in.ctypes.data, host_out.ctypes.data,
+                                                    int(block_states)))
+        return host_out
+
     def non_local(self, phi: OrbitalSet) -> OrbitalSet:
         out = phi.skeleton()
         self.ctx.check(self.ctx.lib.inqb_non_local(self.handle, phi.handle, out.handle))

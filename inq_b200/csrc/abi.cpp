@@ -1058,6 +1058,107 @@ int inqb_apply(const inqb_hamiltonian *hc, const inqb_orbitals *in, inqb_orbital
   });
 }
 
+// Streams, events and device blocks of one inqb_apply_host call; released after every copy and
+// kernel of the call has finished (also when the call fails half-way).
+struct HostApplyRes {
+  Ctx *ctx = nullptr;
+  cudaStream_t up = nullptr, down = nullptr;
+  cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {}, ev_join = nullptr;
+  void *bin[2] = {}, *bout[2] = {};
+  ~HostApplyRes() {
+    if (up) cudaStreamSynchronize(up);
+    if (down) cudaStreamSynchronize(down);
+    if (ctx) cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < 2; i++) {
+      if (bin[i]) cudaFree(bin[i]);
+      if (bout[i]) cudaFree(bout[i]);
+      for (cudaEvent_t e : {ev_in[i], ev_comp[i], ev_out[i]})
+        if (e) cudaEventDestroy(e);
+    }
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (up) cudaStreamDestroy(up);
+    if (down) cudaStreamDestroy(down);
+  }
+};
+
+int inqb_apply_host(const inqb_hamiltonian *hc, int nst, const double kpoint_cov[3], int spin_index, int precision,
+                    const void *host_in, void *host_out, int block_states) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && host_in && host_out, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(nst > 0 && block_states >= 0, INQB_ERR_ARG, "bad state count");
+    INQB_REQUIRE(precision == INQB_F64 || precision == INQB_F32, INQB_ERR_ARG, "bad precision tag");
+    INQB_REQUIRE(spin_index >= 0 && spin_index < h->nspin, INQB_ERR_ARG, "spin index out of range");
+    INQB_REQUIRE(host_in != host_out, INQB_ERR_ARG, "H|psi> needs distinct input and output buffers");
+    set_device(*h->ctx);
+    Ctx &ctx = *h->ctx;
+    const size_t cs = precision == INQB_F64 ? 16 : 8;
+    const size_t npts = size_t(h->basis->npoints);
+    int B = block_states > 0 ? block_states : int(512 / cs);  // 512-byte rows of a block by default
+    if (B > nst) B = nst;
+    const int nblocks = (nst + B - 1) / B;
+    HostApplyRes r;
+    r.ctx = &ctx;
+    INQB_CUDA(cudaStreamCreateWithFlags(&r.up, cudaStreamNonBlocking));
+    INQB_CUDA(cudaStreamCreateWithFlags(&r.down, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; i++) {
+      INQB_CUDA(cudaEventCreateWithFlags(&r.ev_in[i], cudaEventDisableTiming));
+      INQB_CUDA(cudaEventCreateWithFlags(&r.ev_comp[i], cudaEventDisableTiming));
+      INQB_CUDA(cudaEventCreateWithFlags(&r.ev_out[i], cudaEventDisableTiming));
+      for (void **p : {&r.bin[i], &r.bout[i]}) {
+        if (i == 1 && nblocks == 1) continue;
+        cudaError_t e = cudaMalloc(p, npts * B * cs);
+        if (e != cudaSuccess) {
+          (void)cudaGetLastError();
+          throw Error(INQB_ERR_MEMORY, "device allocation of a state block failed: " + std::string(cudaGetErrorString(e)));
+        }
+      }
+    }
+    INQB_CUDA(cudaEventCreateWithFlags(&r.ev_join, cudaEventDisableTiming));
+    // the copies start after the work already queued on the context's stream
+    INQB_CUDA(cudaEventRecord(r.ev_join, ctx.stream));
+    INQB_CUDA(cudaStreamWaitEvent(r.up, r.ev_join, 0));
+    const char *hin = static_cast<const char *>(host_in);
+    char *hout = static_cast<char *>(host_out);
+    for (int i = 0; i < nblocks; i++) {
+      const int slot = i & 1, s0 = i * B, nb = std::min(B, nst - s0);
+      // block i reuses the buffers of block i - 2: its upload waits for that block's operator, its
+      // operator for that block's download
+      if (i >= 2) INQB_CUDA(cudaStreamWaitEvent(r.up, r.ev_comp[slot], 0));
+      INQB_CUDA(cudaMemcpy2DAsync(r.bin[slot], nb * cs, hin + s0 * cs, nst * cs, nb * cs, npts, cudaMemcpyHostToDevice,
+                                  r.up));
+      INQB_CUDA(cudaEventRecord(r.ev_in[slot], r.up));
+      INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_in[slot], 0));
+      if (i >= 2) INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_out[slot], 0));
+      Orbitals in, out;
+      in.ctx = out.ctx = &ctx;
+      in.basis = out.basis = h->basis;
+      in.nst = out.nst = nb;
+      for (int k = 0; k < 3; k++) in.kpoint[k] = out.kpoint[k] = kpoint_cov ? kpoint_cov[k] : 0.0;
+      in.spin_index = out.spin_index = spin_index;
+      in.space = out.space = INQB_REAL_SPACE;
+      in.precision = out.precision = precision;
+      in.data = r.bin[slot];
+      out.data = r.bout[slot];
+      apply_any(*h, in, out);
+      INQB_CUDA(cudaEventRecord(r.ev_comp[slot], ctx.stream));
+      INQB_CUDA(cudaStreamWaitEvent(r.down, r.ev_comp[slot], 0));
+      INQB_CUDA(cudaMemcpy2DAsync(hout + s0 * cs, nst * cs, r.bout[slot], nb * cs, nb * cs, npts,
+                                  cudaMemcpyDeviceToHost, r.down));
+      INQB_CUDA(cudaEventRecord(r.ev_out[slot], r.down));
+    }
+    INQB_CUDA(cudaEventRecord(r.ev_join, r.down));
+    INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_join, 0));
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+    int flag = 0;
+    INQB_CUDA(cudaMemcpy(&flag, ctx.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      INQB_CUDA(cudaMemset(ctx.d_err, 0, sizeof(int)));
+      throw Error(INQB_ERR_TIMEOUT, "a device-side wait exceeded its time limit; host_out is invalid");
+    }
+  });
+}
+
 int inqb_non_local(const inqb_hamiltonian *hc, const inqb_orbitals *in, inqb_orbitals *out) {
   auto *h = const_cast<inqb_hamiltonian *>(hc);
   return guarded(h ? h->ctx : nullptr, [&] {

@@ -4,10 +4,11 @@
 //                                                 a ZGEMM a^H b over the grid points)
 //
 // Split-BF16 compensated products: every FP32 component x is held as hi + lo with hi = bf16(x) and
-// lo = bf16(x - hi) (16 significant bits), and a product is formed as hi*hi + hi*lo + lo*hi; the lo*lo
-// term (2^-18 relative) is dropped.  The complex product is four real ones,
+// lo = bf16(x - hi) (16 significant bits), and a product is formed as hi*hi + hi*lo + lo*hi + lo*lo.
+// The lo*lo term is kept: |lo| reaches 2^-8 |x|, and in a norm (a = b) the dropped squares would all
+// have the same sign, a bias of ~4e-6 on the diagonal.  The complex product is four real ones,
 //   Re S = ar.br + ai.bi,   Im S = ar.bi - ai.br   (the minus by the instruction's negate-A bit),
-// so one 16-point chunk costs 12 MMAs of 128 x N x 16 (kind::f16, BF16 in, FP32 accumulate).
+// so one 16-point chunk costs 16 MMAs of 128 x N x 16 (kind::f16, BF16 in, FP32 accumulate).
 //
 // One CTA per SM holds a 128-state block of a (tensor-memory lanes) against up to 256 states of b: the
 // real and imaginary FP32 accumulators take N + N of the 512 tensor-memory columns.  The points are
@@ -154,18 +155,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
       const bool acc = c > 0;
       // planes: 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo
-      ptx::mma_bf16(d_re, da[0], db[0], id, acc);
+      // smallest products first into each accumulator's chunk sum
+      ptx::mma_bf16(d_re, da[1], db[1], id, acc);
+      ptx::mma_bf16(d_re, da[3], db[3], id, true);
       ptx::mma_bf16(d_re, da[0], db[1], id, true);
       ptx::mma_bf16(d_re, da[1], db[0], id, true);
-      ptx::mma_bf16(d_re, da[2], db[2], id, true);
       ptx::mma_bf16(d_re, da[2], db[3], id, true);
       ptx::mma_bf16(d_re, da[3], db[2], id, true);
-      ptx::mma_bf16(d_im, da[0], db[2], id, acc);
+      ptx::mma_bf16(d_re, da[0], db[0], id, true);
+      ptx::mma_bf16(d_re, da[2], db[2], id, true);
+      ptx::mma_bf16(d_im, da[1], db[3], id, acc);
+      ptx::mma_bf16(d_im, da[3], db[1], idn, true);
       ptx::mma_bf16(d_im, da[0], db[3], id, true);
       ptx::mma_bf16(d_im, da[1], db[2], id, true);
-      ptx::mma_bf16(d_im, da[2], db[0], idn, true);
       ptx::mma_bf16(d_im, da[2], db[1], idn, true);
       ptx::mma_bf16(d_im, da[3], db[0], idn, true);
+      ptx::mma_bf16(d_im, da[0], db[2], id, true);
+      ptx::mma_bf16(d_im, da[2], db[0], idn, true);
       ptx::mma_commit(&done[bsel]);
     }
     issued = c + 1;
