@@ -61,7 +61,8 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * kernels from their shared-memory budget, the default) or 2..8 stages; "overlap_tc" = 1
  * (default: overlaps of single-precision sets -- inqb_overlap, and the ones inside
  * inqb_orthogonalize and inqb_subspace_diagonalization -- on the tensor cores as split-BF16
- * products with FP32 accumulation and an FP64 sum of the per-SM partials) or 0 (FP64 SIMT
+ * products with FP32 accumulation and an FP64 sum of the per-SM partials; 16 significant bits
+ * per value, so |error of S_ij| stays near 2^-16 |a_i| |b_j| / sqrt(npoint)) or 0 (FP64 SIMT
  * products, as for double-precision sets). */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Free and total device memory in bytes (admission control for serving). */

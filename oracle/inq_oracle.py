@@ -714,3 +714,86 @@ def etrs_step(ham: Hamiltonian, phis, occs, dt, kpoints=None, nscf=5, scf_thresh
         if done:
             break
     return cur, dens, iters
+
+
+# ---------------------------------------------------------------------------
+# interacting Hamiltonian update (solvers/poisson.hpp, hamiltonian/xc_term.hpp,
+# hamiltonian/self_consistency.hpp)
+# ---------------------------------------------------------------------------
+
+
+def poisson_solve(rs: RealSpace, density):
+    """solvers::poisson::solve for a periodic cell (poisson.hpp:98-104 with poisson_apply_kernel
+    :72-87 and poisson_kernel_3d :29-35): V(G) = 4 pi n(G) / |G|^2 (cartesian |G|^2), the G with
+    |G|^2 < 1e-6 set to the zero term 0, unnormalised backward transform.  A real density gives a
+    real potential (the real part, poisson.hpp:207-212)."""
+    real_in = np.isrealobj(density)
+    d = np.asarray(density, dtype=np.complex128)[..., None]
+    fd = to_fourier(d)
+    g2 = rs.g2()
+    scal = (-4.0 * math.pi) / rs.npoints
+    kern = np.where(g2 < 1e-6, 0.0, -1.0 / np.where(g2 < 1e-6, 1.0, g2))
+    fd = fd * (scal * kern)[..., None]
+    v = to_real(fd, normalize=False)[..., 0]
+    return v.real if real_in else v
+
+
+LDA_X_FACTOR = -0.75 * (3.0 / math.pi) ** (1.0 / 3.0)   # eps_x = LDA_X_FACTOR n^(1/3)
+PZ_GAMMA, PZ_BETA1, PZ_BETA2 = -0.1423, 1.0529, 0.3334  # Perdew-Zunger 1981, rs >= 1
+PZ_A, PZ_B, PZ_C, PZ_D = 0.0311, -0.048, 0.0020, -0.0116  # rs < 1
+DENS_THRESHOLD = 1e-15
+
+
+def lda_x(n):
+    """Slater exchange of an unpolarised density (libxc XC_LDA_X): energy per particle and potential."""
+    n = np.asarray(n, dtype=np.float64)
+    ok = n > DENS_THRESHOLD
+    nc = np.where(ok, n, 1.0)
+    eps = np.where(ok, LDA_X_FACTOR * np.cbrt(nc), 0.0)
+    return eps, 4.0 / 3.0 * eps
+
+
+def lda_c_pz(n):
+    """Perdew-Zunger 1981 correlation of an unpolarised density (libxc XC_LDA_C_PZ, the published
+    parametrisation): energy per particle and potential v = eps - rs/3 deps/drs."""
+    n = np.asarray(n, dtype=np.float64)
+    ok = n > DENS_THRESHOLD
+    rs = np.cbrt(3.0 / (4.0 * math.pi * np.where(ok, n, 1.0)))
+    sq = np.sqrt(rs)
+    den = 1.0 + PZ_BETA1 * sq + PZ_BETA2 * rs
+    eps_hi = PZ_GAMMA / den
+    v_hi = eps_hi * (1.0 + 7.0 / 6.0 * PZ_BETA1 * sq + 4.0 / 3.0 * PZ_BETA2 * rs) / den
+    lr = np.log(rs)
+    eps_lo = PZ_A * lr + PZ_B + PZ_C * rs * lr + PZ_D * rs
+    v_lo = PZ_A * lr + (PZ_B - PZ_A / 3.0) + 2.0 / 3.0 * PZ_C * rs * lr + (2.0 * PZ_D - PZ_C) / 3.0 * rs
+    eps = np.where(rs >= 1.0, eps_hi, eps_lo)
+    v = np.where(rs >= 1.0, v_hi, v_lo)
+    return np.where(ok, eps, 0.0), np.where(ok, v, 0.0)
+
+
+def xc_lda(rs: RealSpace, n):
+    """xc_term with the LDA (options::theory::lda, theory.hpp:48-54: Slater exchange + PZ
+    correlation), unpolarised: returns (v_xc, E_xc = int n eps_xc, int n v_xc) (xc_term.hpp:186-236)."""
+    ex, vx = lda_x(n)
+    ec, vc = lda_c_pz(n)
+    v = vx + vc
+    dv = rs.volume_element()
+    return v, dv * float(np.sum(n * (ex + ec))), dv * float(np.sum(n * v))
+
+
+def update_hamiltonian(ham: Hamiltonian, vion, n, hartree=True, xc=True):
+    """self_consistency::update_hamiltonian (self_consistency.hpp:88-170), unpolarised, static ions, no
+    external fields: V = V_ion + V_H[n] + V_xc[n]; returns the energies (external, Hartree, xc, nvxc)."""
+    dv = ham.rs.volume_element()
+    v = np.array(vion, dtype=np.float64, copy=True)
+    energies = {"external": dv * float(np.sum(n * vion)), "hartree": 0.0, "xc": 0.0, "nvxc": 0.0}
+    if hartree:
+        vh = poisson_solve(ham.rs, n)
+        energies["hartree"] = 0.5 * dv * float(np.sum(n * vh))
+        v = v + vh
+    if xc:
+        vxc, exc, nvxc = xc_lda(ham.rs, n)
+        energies["xc"], energies["nvxc"] = exc, nvxc
+        v = v + vxc
+    ham.V = v
+    return energies

@@ -240,3 +240,74 @@ def test_orthogonalize_identity(nst, rng):
     assert np.max(np.abs(np.diag(S).imag)) < 1e-14
     off = S - np.diag(np.diag(S))
     assert np.max(np.abs(off)) < 1e-13
+
+
+# ---------------------------------------------------------------- solvers/poisson.hpp:236-340
+
+def _poisson_rs():
+    rs = O.RealSpace.from_spacing(O.Cell(np.diag([10.0, 10.0, 13.7])), 0.1)
+    assert rs.sizes == (100, 100, 140)
+    return rs
+
+
+def test_poisson_point_charge():
+    """poisson.hpp:256-299: a -1 point charge at the origin; sum |Re V| = 82.9383793318 (Catch Approx),
+    V(0) = -0.0238339212, Im V = 0."""
+    rs = _poisson_rs()
+    d = np.zeros(rs.sizes, np.complex128)
+    d[0, 0, 0] = -1.0
+    v = O.poisson_solve(rs, d)
+    assert approx(float(np.sum(np.abs(v.real))), 82.9383793318)
+    assert approx(float(v[0, 0, 0].real), -0.0238339212)
+    assert float(np.sum(np.abs(v.imag))) <= 5e-12
+
+
+def test_poisson_plane_waves():
+    """poisson.hpp:301-340: V = 4 pi / k^2 n for n = e^{ikx} (mean |diff| < 1e-13) and for the real
+    n = cos(k' y) (< 1e-8)."""
+    rs = _poisson_rs()
+    r = rs.rvector_cartesian()
+    kk = 2.0 * math.pi / 10.0
+    n = np.exp(1j * kk * r[..., 0])
+    v = O.poisson_solve(rs, n)
+    assert np.mean(np.abs(v - 4 * math.pi / kk ** 2 * n)) < 1e-13
+    ky = 8.0 * math.pi / 10.0
+    nr = np.cos(ky * r[..., 1])
+    vr = O.poisson_solve(rs, nr)
+    assert np.isrealobj(vr)
+    assert np.mean(np.abs(vr - 4 * math.pi / ky ** 2 * nr)) < 1e-8
+
+
+# ---------------------------------------------------------------- hamiltonian/xc_term.hpp:335-446
+
+def test_lda_exchange():
+    """xc_term.hpp:346-446, LDA_X unpolarised: on the 25x35x12 grid of a 10.3 x 13.8 x 4.5 cell the
+    density max(0, cos(k.r) + 1) normalised to 42 has n(20,8,4) = 0.0232053167 and n(1,27,3) =
+    0.1264954137; E_x = -14.0558385758, v_x = -0.2808792311 and -0.494328201 there."""
+    rs = O.RealSpace.from_spacing(O.Cell(np.diag([10.3, 13.8, 4.5])), 0.40557787)
+    assert rs.sizes == (25, 35, 12)
+    k = 2.0 * math.pi * np.array([1 / 10.3, 1 / 13.8, 1 / 4.5])
+    n = np.maximum(0.0, np.cos(rs.rvector_cartesian() @ k) + 1.0)
+    n *= 42.0 / (rs.volume_element() * n.sum())
+    assert approx(float(n[20, 8, 4]), 0.0232053167)
+    assert approx(float(n[1, 27, 3]), 0.1264954137)
+    ex, vx = O.lda_x(n)
+    assert approx(rs.volume_element() * float(np.sum(n * ex)), -14.0558385758)
+    assert approx(float(vx[20, 8, 4]), -0.2808792311)
+    assert approx(float(vx[1, 27, 3]), -0.494328201)
+
+
+def test_pz_correlation_branches():
+    """Perdew-Zunger 1981 correlation (no reference test pins it; libxc is absent): the two branches
+    meet at rs = 1 to the published parameters' accuracy, and v = eps - rs/3 deps/drs holds."""
+    rs_vals = np.array([0.3, 0.99999, 1.00001, 2.0, 8.0])
+    n = 3.0 / (4.0 * math.pi * rs_vals ** 3)
+    eps, v = O.lda_c_pz(n)
+    assert abs(eps[1] - eps[2]) < 1e-4
+    h = 1e-6
+    for i, r in enumerate(rs_vals[[0, 3, 4]]):
+        e1, _ = O.lda_c_pz(3.0 / (4.0 * math.pi * (r + h) ** 3))
+        e0, _ = O.lda_c_pz(3.0 / (4.0 * math.pi * (r - h) ** 3))
+        de = (e1 - e0) / (2 * h)
+        e, vv = O.lda_c_pz(3.0 / (4.0 * math.pi * r ** 3))
+        assert abs(vv - (e - r / 3.0 * de)) < 1e-8
