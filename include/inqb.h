@@ -122,6 +122,19 @@ int inqb_hamiltonian_destroy(inqb_hamiltonian *ham);
 int inqb_potential_set(inqb_hamiltonian *ham, const double *V);
 /* ks_hamiltonian::uniform_vector_potential() assignment (covariant, ks_hamiltonian.hpp:259-264). */
 int inqb_vector_potential_set(inqb_hamiltonian *ham, const double A_cov[3]);
+/* The interacting part of self_consistency::update_hamiltonian (self_consistency.hpp:88-170),
+ * unpolarised, static ions, no external fields.  set_interaction stores the ionic potential
+ * vion [npoint] (float64) and which terms follow the density: hartree != 0 adds the Hartree
+ * potential of solvers::poisson (poisson.hpp:98-104, periodic cell: 4 pi n(G)/|G|^2, G = 0
+ * dropped), xc = 1 the LDA of options::theory::lda (theory.hpp:48-54: Slater exchange and
+ * Perdew-Zunger 1981 correlation; xc_term.hpp:186-236), xc = 0 none.  From then on
+ * inqb_etrs_step rebuilds the potential V = vion + V_H[n] + V_xc[n] from every density it forms
+ * (etrs.hpp:51 and :75), so its self-consistency loop is a real one.  inqb_update_hamiltonian
+ * does the same for a given density [npoint] (host, float64) and returns energies[4] = {external
+ * int n vion, Hartree 1/2 int n V_H, xc int n eps_xc, int n v_xc} (NULL: not wanted).
+ * set_interaction with vion = NULL removes the interaction (the potential in place stays). */
+int inqb_hamiltonian_set_interaction(inqb_hamiltonian *ham, const double *vion, int hartree, int xc);
+int inqb_update_hamiltonian(inqb_hamiltonian *ham, const double *density, double energies[4]);
 /* projector_all packing (projector_all.hpp:40-109): padded host tables
  *   points   [nproj][maxsph][3] int32 grid indices (-1 for padding)
  *   pos      [nproj][maxsph][3] float32 contravariant offsets from the atom

@@ -65,6 +65,8 @@ SIGNATURES = {
     "inqb_hamiltonian_destroy": (I, [P]),
     "inqb_potential_set": (I, [P, DP]),
     "inqb_vector_potential_set": (I, [P, DP]),
+    "inqb_hamiltonian_set_interaction": (I, [P, DP, I, I]),
+    "inqb_update_hamiltonian": (I, [P, DP, DP]),
     "inqb_projectors_set": (I, [P, I, I, I, P, P, P, P, P, P]),
     "inqb_projectors_build_gaussian": (I, [P, I, DP, D, D, DP]),
     "inqb_projectors_info": (I, [P, C.POINTER(I), C.POINTER(I), C.POINTER(LL)]),

@@ -359,6 +359,28 @@ class KSHamiltonian:
         v = np.ascontiguousarray(np.asarray(V, dtype=np.float64).reshape(self.basis.size(), self.nspin))
         self.ctx.check(self.ctx.lib.inqb_potential_set(self.handle, dptr(v)))
 
+    def set_interaction(self, vion, hartree: bool = True, xc: str | None = "lda"):
+        """The density-dependent part of the Kohn-Sham potential (self_consistency::update_hamiltonian):
+        ionic potential ``vion`` [npoint], Hartree term, and ``xc`` = "lda" (Slater + PZ81) or None.
+        ETRS steps then rebuild the potential from every density they form."""
+        if xc not in ("lda", None):
+            raise ValueError("xc is 'lda' or None")
+        v = np.ascontiguousarray(np.asarray(vion, dtype=np.float64).reshape(-1))
+        self._vion = v
+        self.ctx.check(self.ctx.lib.inqb_hamiltonian_set_interaction(self.handle, dptr(v), int(bool(hartree)),
+                                                                     1 if xc == "lda" else 0))
+
+    def clear_interaction(self):
+        """Back to a fixed potential (the one in place stays until set_scalar_potential)."""
+        self.ctx.check(self.ctx.lib.inqb_hamiltonian_set_interaction(self.handle, None, 0, 0))
+
+    def update_hamiltonian(self, density) -> dict:
+        """V = V_ion + V_H[n] + V_xc[n] for the density ``density`` [npoint]; returns the energies."""
+        n = np.ascontiguousarray(np.asarray(density, dtype=np.float64).reshape(-1))
+        e = np.zeros(4)
+        self.ctx.check(self.ctx.lib.inqb_update_hamiltonian(self.handle, dptr(n), dptr(e)))
+        return {"external": float(e[0]), "hartree": float(e[1]), "xc": float(e[2]), "nvxc": float(e[3])}
+
     @property
     def uniform_vector_potential(self):
         return self._A.copy()
@@ -601,7 +623,8 @@ def apply_phase_kick(phi: OrbitalSet, efield_cart):
 
 def etrs(ham: KSHamiltonian, phis: Sequence[OrbitalSet], occupations: Sequence, dt: float, nscf: int = 5,
          scf_threshold: float = 5e-5, want_density: bool = False):
-    """One ETRS step (real_time/etrs.hpp:22-79) with a fixed Hamiltonian.
+    """One ETRS step (real_time/etrs.hpp:22-79); a Hamiltonian with an interaction
+    (KSHamiltonian.set_interaction) is rebuilt from every density the step forms.
 
     Returns (density or None, electronic dipole [3], number of SCF iterations)."""
     hs, optrs, keep = _ptr_arrays(phis, occupations)

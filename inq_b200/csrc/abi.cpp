@@ -301,6 +301,42 @@ template <typename R> double *occ_to_device(Ctx &ctx, const double *occ, int S) 
   return d;
 }
 
+// self_consistency::update_hamiltonian (self_consistency.hpp:88-170), unpolarised, static ions, no
+// external fields: V = V_ion + V_H[n] + V_xc[n] from a device density, left in the Hamiltonian's
+// potential; energies (if given) = {external, Hartree, xc, int n v_xc}.
+void update_hamiltonian_dev(Hamiltonian &h, const double *d_dens, double *energies) {
+  Ctx &ctx = *h.ctx;
+  const Basis &b = *h.basis;
+  INQB_REQUIRE(h.d_vion, INQB_ERR_ARG, "the Hamiltonian has no interaction (inqb_hamiltonian_set_interaction)");
+  INQB_REQUIRE(h.nspin == 1, INQB_ERR_UNSUPPORTED, "the interacting update is implemented for one spin channel");
+  double2 *vh = nullptr;
+  if (h.hartree) {
+    // solvers::poisson::solve (poisson.hpp:98-104): forward transform, 4 pi / |G|^2, unnormalised backward
+    vh = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * b.npoints));
+    launch_real_to_complex(ctx, d_dens, vh, b.npoints);
+    fft3d<double>(ctx, b, vh, vh, 1, +1, 1.0);
+    launch_poisson_factor(ctx, b, vh);
+    fft3d<double>(ctx, b, vh, vh, 1, -1, 1.0);
+  }
+  double *partial = static_cast<double *>(dev_alloc(ctx, sizeof(double) * KS_BLOCKS * 4));
+  launch_ks_potential(ctx, d_dens, h.d_vion, vh, h.xc, b.npoints, h.d_V, h.d_V32, partial);
+  if (energies) {
+    std::vector<double> hp(size_t(KS_BLOCKS) * 4);
+    INQB_CUDA(cudaMemcpyAsync(hp.data(), partial, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, ctx.stream));
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+    double e[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int blk = 0; blk < KS_BLOCKS; blk++)
+      for (int k = 0; k < 4; k++) e[k] += hp[size_t(blk) * 4 + k];
+    const double dv = b.volume / double(b.npoints);
+    energies[0] = dv * e[0];
+    energies[1] = h.hartree ? 0.5 * dv * e[1] : 0.0;
+    energies[2] = h.xc ? dv * e[2] : 0.0;
+    energies[3] = h.xc ? dv * e[3] : 0.0;
+  }
+  dev_free(ctx, partial);
+  if (vh) dev_free(ctx, vh);
+}
+
 void density_dev(Ctx &ctx, inqb_orbitals *const *phis, int nsets, const double *const *occ, double *dens) {
   for (int k = 0; k < nsets; k++) {
     const Orbitals &o = *phis[k];
@@ -938,6 +974,7 @@ int inqb_hamiltonian_destroy(inqb_hamiltonian *h) {
   if (h->d_V32) cudaFreeAsync(h->d_V32, st);
   if (h->d_projraw) cudaFreeAsync(h->d_projraw, st);
   if (h->d_projD) cudaFreeAsync(h->d_projD, st);
+  if (h->d_vion) cudaFreeAsync(h->d_vion, st);
   delete h;
   return INQB_OK;
 }
@@ -951,6 +988,45 @@ int inqb_potential_set(inqb_hamiltonian *h, const double *V) {
     INQB_CUDA(cudaMemcpyAsync(h->d_V, V, sizeof(double) * nv, cudaMemcpyHostToDevice, h->ctx->stream));
     INQB_CUDA(cudaMemcpyAsync(h->d_V32, v32.data(), sizeof(float) * nv, cudaMemcpyHostToDevice, h->ctx->stream));
     INQB_CUDA(cudaStreamSynchronize(h->ctx->stream));
+  });
+}
+
+int inqb_hamiltonian_set_interaction(inqb_hamiltonian *h, const double *vion, int hartree, int xc) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h, INQB_ERR_ARG, "null argument");
+    set_device(*h->ctx);
+    if (!vion) {  // back to a fixed potential
+      if (h->d_vion) dev_free(*h->ctx, h->d_vion);
+      h->d_vion = nullptr;
+      h->hartree = h->xc = 0;
+      return;
+    }
+    INQB_REQUIRE(xc == 0 || xc == 1, INQB_ERR_ARG, "xc is 0 (none) or 1 (LDA: Slater exchange, PZ81 correlation)");
+    INQB_REQUIRE(h->nspin == 1, INQB_ERR_UNSUPPORTED, "the interacting update is implemented for one spin channel");
+    set_device(*h->ctx);
+    const size_t n = size_t(h->basis->npoints);
+    if (!h->d_vion) h->d_vion = static_cast<double *>(dev_alloc(*h->ctx, sizeof(double) * n));
+    INQB_CUDA(cudaMemcpyAsync(h->d_vion, vion, sizeof(double) * n, cudaMemcpyHostToDevice, h->ctx->stream));
+    INQB_CUDA(cudaStreamSynchronize(h->ctx->stream));
+    h->hartree = hartree ? 1 : 0;
+    h->xc = xc;
+  });
+}
+
+int inqb_update_hamiltonian(inqb_hamiltonian *h, const double *density, double energies[4]) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && density, INQB_ERR_ARG, "null argument");
+    set_device(*h->ctx);
+    Ctx &ctx = *h->ctx;
+    const size_t n = size_t(h->basis->npoints);
+    double *d = static_cast<double *>(dev_alloc(ctx, sizeof(double) * n));
+    INQB_CUDA(cudaMemcpyAsync(d, density, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.stream));
+    double e[4];
+    update_hamiltonian_dev(*h, d, e);
+    if (energies)
+      for (int k = 0; k < 4; k++) energies[k] = e[k];
+    dev_free(ctx, d);
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
   });
 }
 
@@ -1561,7 +1637,9 @@ int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int n
     double *old = static_cast<double *>(dev_alloc(ctx, sizeof(double) * b.npoints));
     double *delta_dev = static_cast<double *>(dev_alloc(ctx, sizeof(double)));
     density_dev(ctx, phis, nsets, occ, dens);
-    // (the Hamiltonian is fixed: update_hamiltonian of etrs.hpp:51 has nothing to update)
+    // etrs.hpp:51: H(t + dt) from the predicted density (nothing to update for a fixed Hamiltonian)
+    const bool interacting = h->d_vion != nullptr;
+    if (interacting) update_hamiltonian_dev(*h, dens, nullptr);
     int it = 0;
     for (int iscf = 0; iscf < nscf_max; iscf++) {
       for (int k = 0; k < nsets; k++) {
@@ -1576,6 +1654,7 @@ int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int n
       INQB_CUDA(cudaStreamSynchronize(ctx.stream));
       delta *= b.volume / double(b.npoints);
       it = iscf + 1;
+      if (interacting) update_hamiltonian_dev(*h, dens, nullptr);  // etrs.hpp:75
       if (delta < scf_threshold || iscf == nscf_max - 1) break;
     }
     if (iterations) *iterations = it;

@@ -142,6 +142,9 @@ struct Hamiltonian {
   // device scratch for the projections of the current apply
   void *d_projraw = nullptr, *d_projD = nullptr;
   size_t proj_bytes = 0;
+  // interaction (self_consistency::update_hamiltonian): ionic potential, Hartree and LDA terms
+  double *d_vion = nullptr;              // [npoints]
+  int hartree = 0, xc = 0;
 };
 
 // ------------------------------------------------------------------ launchers (kernels.cu)
@@ -226,6 +229,13 @@ std::vector<int> fft_radices(int n);
 void basis_metric(const double lattice[9], double lat[3][3], double rec[3][3], double rlat[3][3], double &volume);
 
 void ensure_smem_attr(const void *kernel, size_t bytes);
+// interacting potential (kernels.cu): real -> complex copy, Poisson factor on the Fourier grid,
+// V = V_ion + V_H + V_xc with per-block energy sums (KS_BLOCKS x 4 doubles)
+constexpr int KS_BLOCKS = 148;
+void launch_real_to_complex(Ctx &ctx, const double *in, double2 *out, long long n);
+void launch_poisson_factor(Ctx &ctx, const Basis &b, double2 *f);
+void launch_ks_potential(Ctx &ctx, const double *n, const double *vion, const double2 *vh, int xc, long long np,
+                         double *V, float *V32, double *partial_dev);
 // S = dv a^H b of single-precision sets on the tensor cores (overlap_tc.cu); out [Sa][Sb] on the device
 void launch_overlap_tc(Ctx &ctx, const float2 *a, int Sa, const float2 *b, int Sb, long long npoints, double dv,
                        double2 *out);

@@ -659,6 +659,103 @@ void launch_absdiff_sum(Ctx &ctx, const double *a, const double *b, long long n,
   dev_free(ctx, partial);
 }
 
+// ------------------------------------------------------------------ interacting potential
+// (solvers/poisson.hpp, hamiltonian/xc_term.hpp, hamiltonian/self_consistency.hpp)
+
+__global__ void real_to_complex_kernel(const double *__restrict__ in, double2 *__restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = make_double2(in[i], 0.0);
+}
+
+// poisson_apply_kernel with poisson_kernel_3d (poisson.hpp:29-35, 72-87): times scal * kern,
+// scal = -4 pi / N, kern = -1/|G|^2 (cartesian), 0 for |G|^2 < 1e-6
+__global__ void poisson_factor_kernel(Metric m, double2 *__restrict__ f, long long n, double scal) {
+  const double zero[3] = {0.0, 0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double g2 = lapl_at(m, i, -1.0, zero, 0.0);
+    const double k = g2 < 1e-6 ? 0.0 : -1.0 / g2;
+    const double c = scal * k;
+    f[i] = make_double2(f[i].x * c, f[i].y * c);
+  }
+}
+
+// Slater exchange and Perdew-Zunger 1981 correlation of an unpolarised density (the published
+// parametrisation, libxc's XC_LDA_X and XC_LDA_C_PZ): energy per particle and potential.
+__device__ __forceinline__ void lda_xc(double n, double &eps, double &v) {
+  if (!(n > 1e-15)) {
+    eps = 0.0;
+    v = 0.0;
+    return;
+  }
+  const double pi = 3.14159265358979323846;
+  const double cx = -0.75 * cbrt(3.0 / pi);
+  const double ex = cx * cbrt(n);
+  const double rs = cbrt(3.0 / (4.0 * pi * n));
+  double ec, vc;
+  if (rs >= 1.0) {
+    const double sq = sqrt(rs);
+    const double den = 1.0 + 1.0529 * sq + 0.3334 * rs;
+    ec = -0.1423 / den;
+    vc = ec * (1.0 + 7.0 / 6.0 * 1.0529 * sq + 4.0 / 3.0 * 0.3334 * rs) / den;
+  } else {
+    const double lr = log(rs);
+    ec = 0.0311 * lr - 0.048 + 0.0020 * rs * lr - 0.0116 * rs;
+    vc = 0.0311 * lr + (-0.048 - 0.0311 / 3.0) + 2.0 / 3.0 * 0.0020 * rs * lr + (2.0 * -0.0116 - 0.0020) / 3.0 * rs;
+  }
+  eps = ex + ec;
+  v = 4.0 / 3.0 * ex + vc;
+}
+
+// V = V_ion + Re V_H + V_xc (double and single copies) and the block sums, in a fixed order, of
+// n V_ion, n V_H, n eps_xc, n v_xc
+__global__ void ks_potential_kernel(const double *__restrict__ n, const double *__restrict__ vion,
+                                    const double2 *__restrict__ vh, int xc, long long np, double *__restrict__ V,
+                                    float *__restrict__ V32, double *__restrict__ partial) {
+  __shared__ double red[4][256];
+  const long long chunk = (np + gridDim.x - 1) / gridDim.x;
+  const long long p0 = blockIdx.x * chunk, p1 = min(np, p0 + chunk);
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long long i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+    const double d = n[i];
+    const double h = vh ? vh[i].x : 0.0;
+    double eps = 0.0, vx = 0.0;
+    if (xc) lda_xc(d, eps, vx);
+    const double v = (vion[i] + h) + vx;
+    V[i] = v;
+    V32[i] = float(v);
+    s[0] += d * vion[i];
+    s[1] += d * h;
+    s[2] += d * eps;
+    s[3] += d * vx;
+  }
+  for (int k = 0; k < 4; k++) red[k][threadIdx.x] = s[k];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 4; k++) red[k][threadIdx.x] += red[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) partial[blockIdx.x * 4 + k] = red[k][0];
+}
+
+void launch_real_to_complex(Ctx &ctx, const double *in, double2 *out, long long n) {
+  real_to_complex_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(in, out, n);
+  LAUNCHED(ctx);
+}
+
+void launch_poisson_factor(Ctx &ctx, const Basis &b, double2 *f) {
+  poisson_factor_kernel<<<grid_for(b.npoints, 256), 256, 0, ctx.stream>>>(metric_of(b), f, b.npoints,
+                                                                         -4.0 * 3.14159265358979323846 / double(b.npoints));
+  LAUNCHED(ctx);
+}
+
+void launch_ks_potential(Ctx &ctx, const double *n, const double *vion, const double2 *vh, int xc, long long np,
+                         double *V, float *V32, double *partial_dev) {
+  ks_potential_kernel<<<KS_BLOCKS, 256, 0, ctx.stream>>>(n, vion, vh, xc, np, V, V32, partial_dev);
+  LAUNCHED(ctx);
+}
+
 // ------------------------------------------------------------------ instantiations
 #define INST(R)                                                                                                   \
   template void launch_nl_project<R>(Ctx &, const Basis &, const Hamiltonian &, const C2<R> *, int, C2<R> *,       \
