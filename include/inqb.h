@@ -55,9 +55,11 @@ int inqb_ctx_stream(inqb_ctx *ctx, void **stream);
 int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
 /* Tuning options: "fft_impl" = 0 (specialised persistent TMA kernels where a line length
  * has one, the default) or 1 (generic kernel for every length); "mixed_compute" selects
- * the butterfly arithmetic of single-precision orbitals: 0 single everywhere, 1 double
- * everywhere, 2 double except the last inverse pass of H, 3 (default) as 2 and single for
- * the first forward pass of every transform too; "fft_stages" = 0 (ring depth of the TMA
+ * the butterfly arithmetic of single-precision orbitals: 0 (default) single everywhere, with
+ * the products by constants and twiddles compensated (fma with the float remainder) so that
+ * they carry no rounding bias, and single-precision projector sums; 1 double everywhere; 2
+ * double except the last inverse pass of H; 3 as 2 and single for the first forward pass of
+ * every transform too (1-3 sum the projections in double); "fft_stages" = 0 (ring depth of the TMA
  * kernels from their shared-memory budget, the default) or 2..8 stages; "overlap_tc" = 1
  * (default: overlaps of single-precision sets -- inqb_overlap, and the ones inside
  * inqb_orthogonalize and inqb_subspace_diagonalization -- on the tensor cores as split-BF16

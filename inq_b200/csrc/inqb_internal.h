@@ -71,7 +71,7 @@ struct Ctx {
   std::vector<cudaEvent_t> aux_events;  // [0] fork point, [1..] joins
   int fft_impl = 0;          // 0: specialised TMA kernels where available, 1: generic kernel only
   int fft_stages = 0;        // shared-memory ring depth of the TMA FFT kernels (0: from the memory budget)
-  int mixed_compute = 3;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
+  int mixed_compute = 0;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
   int overlap_tc = 1;        // overlaps of single-precision sets on the tensor cores (split BF16)
 };
 

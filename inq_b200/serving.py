@@ -89,7 +89,7 @@ class Server:
     operators; tests of the admission logic inject stand-ins for both."""
 
     def __init__(self, device: int = 0, slots: int = 4, precision=F32, reserve_bytes: int = 8 << 30,
-                 mixed_compute: int = 3, budget_bytes: int | None = None, contexts=None, execute=None,
+                 mixed_compute: int = 0, budget_bytes: int | None = None, contexts=None, execute=None,
                  keep_results: bool = True):
         self.device = device
         self.precision = precision

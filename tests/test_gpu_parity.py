@@ -76,7 +76,7 @@ def test_fft_mixed_precision_kernels(ib, rng, sizes, nst, impl, mixed_compute):
         assert rel(ib.to_real(f).hypercubic(), x) < TOL32
     finally:
         rs.ctx.set_option("fft_impl", 0)
-        rs.ctx.set_option("mixed_compute", 1)
+        rs.ctx.set_option("mixed_compute", 0)
 
 
 def test_fft_mixed_precision(ib, rng):
@@ -266,8 +266,8 @@ def test_nonlocal_pieces(ib, c1):
 
 @pytest.mark.parametrize("mixed_compute", [1, 0])
 def test_hamiltonian_mixed_precision(ib, c1big, mixed_compute):
-    """Mixed form (FP32 orbitals; FP64 or FP32 butterflies): H|psi> within 2e-6 relative and eigenvalues
-    within 1e-6 Ha (FP64 butterflies) of the FP64 oracle."""
+    """Mixed form (FP32 orbitals; FP64 or compensated FP32 butterflies): H|psi> within 2e-6 relative and
+    eigenvalues within 1e-6 Ha of the FP64 oracle in both."""
     sysm, basis, ham, phi, oh, ors = c1big
     basis.ctx.set_option("mixed_compute", mixed_compute)
     try:
@@ -278,11 +278,11 @@ def test_hamiltonian_mixed_precision(ib, c1big, mixed_compute):
         assert rel(h, ref) < TOL32
         eig, _ = ham.eigenvalues(ph32)
         oeig, _ = O.eigenvalues(oh, x)
+        assert np.max(np.abs(eig - oeig)) < 1e-6
         if mixed_compute == 1:
-            assert np.max(np.abs(eig - oeig)) < 1e-6
             assert rel(h, ref) < 5e-7
     finally:
-        basis.ctx.set_option("mixed_compute", 1)
+        basis.ctx.set_option("mixed_compute", 0)
 
 
 # ------------------------------------------------------------------ real time
