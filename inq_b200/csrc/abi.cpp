@@ -507,7 +507,7 @@ template <typename T> std::vector<T> download(Ctx &ctx, const void *dev, size_t 
 // different host threads (the serving slots) do not stall one another
 void free_projectors(Projectors &P, cudaStream_t st) {
   void *ptrs[] = {P.d_pt, P.d_pos, P.d_mat, P.d_coeff, P.d_coeff32, P.d_npts, P.d_offs, P.d_hit, P.d_hitpts, P.d_hitp,
-                  P.d_gcoef, P.d_hcoef, P.d_gcoef32, P.d_hcoef32};
+                  P.d_hrec, P.d_gcoef, P.d_hcoef, P.d_gcoef32, P.d_hcoef32};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, st);
   P = Projectors();
@@ -584,6 +584,12 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
   for (size_t k = 0; k < hits.size(); k++)
     if (k == 0 || hits[k].first != hits[k - 1].first) hitpts.push_back(int(hits[k].first));
   P.nhitpts = (long long)hitpts.size();
+  // one record per hit point: (point, first hit, hit count, projector of the first hit)
+  std::vector<int4> hrec(hitpts.size());
+  for (size_t r = 0; r < hitpts.size(); r++) {
+    const int pt = hitpts[r], h0 = offs[size_t(pt)];
+    hrec[r] = make_int4(pt, h0, offs[size_t(pt) + 1] - h0, hitp[size_t(h0)]);
+  }
 
   P.d_pt = upload_vec(flat, st);
   P.d_pos = upload_vec(P.h_pos, st);
@@ -595,6 +601,7 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
   P.d_hit = upload_vec(hit, st);
   P.d_hitpts = upload_vec(hitpts, st);
   P.d_hitp = upload_vec(hitp, st);
+  P.d_hrec = upload_vec(hrec, st);
   INQB_CUDA(cudaMallocAsync(&P.d_gcoef, sizeof(double2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4), st));
   INQB_CUDA(cudaMallocAsync(&P.d_gcoef32, sizeof(float2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4), st));
   INQB_CUDA(cudaMallocAsync(&P.d_hcoef, sizeof(double2) * std::max<size_t>(1, size_t(P.total) * 4), st));

@@ -362,8 +362,15 @@ template <typename R, typename CR, int N, int VAR> constexpr int threads_of() {
   return (VAR != MID_KIN && W == 16 && M > 128 && M <= 256) ? (M + 31) / 32 * 32 : 128;
 }
 
+// CTAs per SM the register allocation must allow: four for the single-precision kinetic pass of lines
+// up to 96 points (two transforms per tile, latency-bound with fewer warps; longer lines would spill),
+// otherwise what the shared memory allows.
+template <typename R, typename CR, int N, int VAR> constexpr int min_ctas_of() {
+  return (VAR == MID_KIN && sizeof(R) == 4 && sizeof(CR) == 4 && N <= 96) ? 4 : 1;
+}
+
 template <typename R, typename CR, int N, int VAR>
-__global__ void __launch_bounds__(threads_of<R, CR, N, VAR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
+__global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR, N, VAR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
                                                    const __grid_constant__ CUtensorMap map_out,
                                                    const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
                                                    const C2<CR> *__restrict__ twg, int *err) {

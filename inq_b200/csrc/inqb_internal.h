@@ -122,6 +122,7 @@ struct Projectors {
   int *d_hit = nullptr;                  // [total] (p * maxsph + i) for each hit, sorted by point then p
   int *d_hitpts = nullptr;               // [nhitpts] grid points with at least one hit, ascending
   int *d_hitp = nullptr;                 // [total] projector index of each hit
+  int4 *d_hrec = nullptr;                // [nhitpts] (point, first hit, hit count, first hit's projector)
   long long nhitpts = 0;
   // (k+A)-dependent coefficient tables
   double kA[3] = {1e300, 1e300, 1e300};

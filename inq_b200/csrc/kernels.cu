@@ -205,62 +205,56 @@ void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
 // out[pt][s] += nonlocal term at the grid points that lie in a sphere (ks_hamiltonian.hpp:153,
 // projector_all.hpp:276-288), owner computes: one thread per (hit point, state), hits of a point summed
 // in projector order, no atomics.  Optional Taylor accumulators acc += c * term (linear in the term).
+// Owner computes: one warp per grid point with sphere hits, lanes over states.  The point's record
+// gives its first hit and projector in one load, so the coefficient, projection and output reads are
+// all issued together (a two-level dependency instead of point -> CSR -> hit -> projection).
 template <typename R>
-__global__ void __launch_bounds__(256) nl_apply_kernel(long long nhp, int S, const int *__restrict__ hitpts,
-                                                       const int *__restrict__ offs, const int *__restrict__ hitp,
-                                                       const C2<R> *__restrict__ hcoef, const C2<R> *__restrict__ projD,
-                                                       C2<R> *__restrict__ out, C2<R> *__restrict__ acc1, C2<R> c1,
-                                                       C2<R> *__restrict__ acc2, C2<R> c2) {
+__global__ void __launch_bounds__(256, 2) nl_apply_kernel(long long nhp, int S, const int4 *__restrict__ hrec,
+                                                       const int *__restrict__ hitp, const C2<R> *__restrict__ hcoef,
+                                                       const C2<R> *__restrict__ projD, C2<R> *__restrict__ out,
+                                                       C2<R> *__restrict__ acc1, C2<R> c1, C2<R> *__restrict__ acc2,
+                                                       C2<R> c2) {
   using T = C2<R>;
-  constexpr int MAXH = 2;  // hits of a point kept in registers; more are read again per state chunk
-  constexpr int U = 4;     // states per lane and chunk
+  constexpr int U = 16 / sizeof(R);  // states per lane and chunk: 4 single, 2 double
   const int lane = threadIdx.x & 31;
   const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long r = warp; r < nhp; r += nwarps) {
-    const long long pt = hitpts[r];
-    const int h0 = offs[pt], h1 = offs[pt + 1];
-    const int nh = h1 - h0;
-    int ph[MAXH];
-    T hc[MAXH][4];
+    const int4 rec = hrec[r];
+    const long long pt = rec.x;
+    const int h0 = rec.y, nh = rec.z, p0 = rec.w;
+    T hc[4];
 #pragma unroll
-    for (int k = 0; k < MAXH; k++) {
-      if (k < nh) {
-        ph[k] = hitp[h0 + k];
-#pragma unroll
-        for (int l = 0; l < 4; l++) hc[k][l] = hcoef[(long long)(h0 + k) * 4 + l];
-      }
-    }
+    for (int l = 0; l < 4; l++) hc[l] = hcoef[(long long)h0 * 4 + l];
     for (int s0 = 0; s0 < S; s0 += 32 * U) {
-      T accv[U];
+      T o[U], pd[4][U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        accv[u] = mk<T>(R(0), R(0));
+        const int s = s0 + u * 32 + lane;
+        if (s < S) {
+          o[u] = out[pt * S + s];
+#pragma unroll
+          for (int l = 0; l < 4; l++) pd[l][u] = projD[((long long)p0 * 4 + l) * S + s];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
         const int s = s0 + u * 32 + lane;
         if (s >= S) continue;
+        T accv = mk<T>(R(0), R(0));
 #pragma unroll
-        for (int k = 0; k < MAXH; k++) {
-          if (k < nh) {
-#pragma unroll
-            for (int l = 0; l < 4; l++)
-              accv[u] = cadd(accv[u], cmul(hc[k][l], projD[((long long)ph[k] * 4 + l) * S + s]));
-          }
-        }
-        for (int k = MAXH; k < nh; k++) {
-          const int p = hitp[h0 + k];
+        for (int l = 0; l < 4; l++) accv = cadd(accv, cmul(hc[l], pd[l][u]));
+        for (int k = 1; k < nh; k++) {
+          const int h = h0 + k;
+          const int p = hitp[h];
 #pragma unroll
           for (int l = 0; l < 4; l++)
-            accv[u] = cadd(accv[u], cmul(hcoef[(long long)(h0 + k) * 4 + l], projD[((long long)p * 4 + l) * S + s]));
+            accv = cadd(accv, cmul(hcoef[(long long)h * 4 + l], projD[((long long)p * 4 + l) * S + s]));
         }
-      }
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int s = s0 + u * 32 + lane;
-        if (s >= S) continue;
         const long long e = pt * S + s;
-        out[e] = cadd(out[e], accv[u]);
-        if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, accv[u]));
-        if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, accv[u]));
+        out[e] = cadd(o[u], accv);
+        if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, accv));
+        if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, accv));
       }
     }
   }
@@ -276,8 +270,8 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
   else hc = P.d_hcoef32;
   long long blocks = (P.nhitpts + 7) / 8;
   if (blocks > 148LL * 16) blocks = 148LL * 16;
-  nl_apply_kernel<R><<<unsigned(blocks), 256, 0, ctx.stream>>>(P.nhitpts, S, P.d_hitpts, P.d_offs, P.d_hitp, hc, projD,
-                                                               out, acc1, c1, acc2, c2);
+  nl_apply_kernel<R><<<unsigned(blocks), 256, 0, ctx.stream>>>(P.nhitpts, S, P.d_hrec, P.d_hitp, hc, projD, out, acc1,
+                                                               c1, acc2, c2);
   LAUNCHED(ctx);
 }
 
