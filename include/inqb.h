@@ -209,6 +209,11 @@ int inqb_overlap_diagonal_noalloc(const inqb_orbitals *a, const inqb_orbitals *b
 /* operations::orthogonalize (orthogonalize.hpp:25-31): FP64 overlap, FP64 Cholesky
  * (matrix/cholesky.hpp:28-99), phi <- phi U^-1 (rotate.hpp:147-156). */
 int inqb_orthogonalize(inqb_orbitals *phi);
+/* eigensolvers::steepest_descent (steepest_descent.hpp:23-86) with operations::preconditioner
+ * (preconditioner.hpp:24-46, Teter-Payne-Allan) on a Fourier-space set, as the ground-state loop
+ * calls it (ground_state/calculator.hpp:161-174): five preconditioned line-minimisation steps per
+ * state, then orthogonalize.  fphi is updated in place. */
+int inqb_steepest_descent(const inqb_hamiltonian *ham, inqb_orbitals *fphi);
 /* operations::shift (shift.hpp:33-43): phi += (re + i im) * chi. */
 int inqb_shift(double re, double im, const inqb_orbitals *chi, inqb_orbitals *phi);
 /* operations::rotate (rotate.hpp:27-62): phi <- phi R, R host [nst][nst] complex128 row-major. */

@@ -74,6 +74,7 @@ SIGNATURES = {
     "inqb_projectors_get": (I, [P, P, P, P, P]),
     "inqb_apply": (I, [P, P, P]),
     "inqb_apply_host": (I, [P, I, DP, I, I, P, P, I]),
+    "inqb_steepest_descent": (I, [P, P]),
     "inqb_non_local": (I, [P, P, P]),
     "inqb_non_local_energy": (I, [P, P, DP, DP]),
     "inqb_kinetic_expectation_value": (I, [P, P, DP]),

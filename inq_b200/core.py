@@ -370,6 +370,12 @@ class KSHamiltonian:
         self.ctx.check(self.ctx.lib.inqb_hamiltonian_set_interaction(self.handle, dptr(v), int(bool(hartree)),
                                                                      1 if xc == "lda" else 0))
 
+    def steepest_descent(self, fphi: OrbitalSet) -> OrbitalSet:
+        """eigensolvers::steepest_descent with the TPA preconditioner on a Fourier-space set (in place),
+        followed by orthogonalize, as one iteration of the ground-state loop calls it."""
+        self.ctx.check(self.ctx.lib.inqb_steepest_descent(self.handle, fphi.handle))
+        return fphi
+
     def clear_interaction(self):
         """Back to a fixed potential (the one in place stays until set_scalar_potential)."""
         self.ctx.check(self.ctx.lib.inqb_hamiltonian_set_interaction(self.handle, None, 0, 0))

@@ -464,7 +464,8 @@ void hermitian_eigen(int n, const std::complex<double> *Ain, double *w, std::com
 void overlap_dev(const Orbitals &a, const Orbitals &b, double2 *out_dev) {
   Ctx &ctx = *a.ctx;
   INQB_REQUIRE(a.basis == b.basis && a.precision == b.precision, INQB_ERR_ARG, "overlap of incompatible sets");
-  const double dv = a.basis->volume / double(a.basis->npoints);
+  INQB_REQUIRE(a.space == b.space, INQB_ERR_ARG, "overlap of sets in different spaces");
+  const double dv = set_volume_element(a);
   if (a.precision == INQB_F64)
     launch_overlap<double>(ctx, static_cast<const double2 *>(a.data), a.nst, static_cast<const double2 *>(b.data),
                            b.nst, a.basis->npoints, dv, out_dev);
@@ -479,7 +480,7 @@ void overlap_dev(const Orbitals &a, const Orbitals &b, double2 *out_dev) {
 void ovdiag_dev(const Orbitals &a, const Orbitals &b, double2 *out_dev) {
   check_same_shape(a, b);
   Ctx &ctx = *a.ctx;
-  const double dv = a.basis->volume / double(a.basis->npoints);
+  const double dv = set_volume_element(a);
   if (a.precision == INQB_F64)
     launch_overlap_diag<double>(ctx, static_cast<const double2 *>(a.data), static_cast<const double2 *>(b.data), a.nst,
                                 a.basis->npoints, dv, out_dev);
@@ -613,6 +614,82 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
 }  // namespace
 
 // ============================================================================ C ABI
+
+// operations::orthogonalize (orthogonalize.hpp:25-31)
+void orthogonalize_dev(Orbitals &phi) {
+  Ctx &ctx = *phi.ctx;
+  const int S = phi.nst;
+  double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * S * S));
+  overlap_dev(phi, phi, d);
+  auto Sh = download<std::complex<double>>(ctx, d, size_t(S) * S);
+  std::vector<std::complex<double>> X(size_t(S) * S);
+  cholesky_inverse(S, Sh.data(), X.data());
+  INQB_CUDA(cudaMemcpyAsync(d, X.data(), sizeof(double2) * S * S, cudaMemcpyHostToDevice, ctx.stream));
+  rotate_dev(phi, d);
+  dev_free(ctx, d);
+  INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+// eigensolvers::steepest_descent (steepest_descent.hpp:23-86) with the Teter-Payne-Allan preconditioner
+// (preconditioner.hpp:24-46) on a Fourier-space set: five line-minimisation steps per state along the
+// preconditioned residual, then orthogonalize.  The per-state overlaps are FP64 reductions; the step
+// lengths are formed on the host.
+template <typename R> void steepest_descent_t(Hamiltonian &h, Orbitals &phi) {
+  Ctx &ctx = *h.ctx;
+  const Basis &b = *h.basis;
+  const int S = phi.nst;
+  const long long np = b.npoints;
+  using T = C2<R>;
+  constexpr int num_steps = 5;
+  TempSet hphi(phi), res(phi), hres(phi), lap(phi);
+  auto D = [](Orbitals &o) { return static_cast<T *>(o.data); };
+  auto CD = [](const Orbitals &o) { return static_cast<const T *>(o.data); };
+  double2 *dov = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * S));
+  double2 *dcoef = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * S));
+  double *dkin = static_cast<double *>(dev_alloc(ctx, sizeof(double) * S));
+  auto ovd = [&](const Orbitals &x, const Orbitals &y) {
+    ovdiag_dev(x, y, dov);
+    return download<std::complex<double>>(ctx, dov, size_t(S));
+  };
+  apply_any(h, phi, hphi.o);
+  std::vector<double2> coef(S);
+  std::vector<double> kin(S);
+  const double zero[3] = {0.0, 0.0, 0.0};
+  for (int istep = 0; istep < num_steps; istep++) {
+    copy_set(hphi.o, res.o);
+    const auto ev = ovd(res.o, phi);
+    const auto nrm = ovd(phi, phi);
+    for (int s = 0; s < S; s++) {
+      const std::complex<double> e = ev[s] / nrm[s].real();
+      coef[s] = make_double2(e.real(), e.imag());
+    }
+    INQB_CUDA(cudaMemcpyAsync(dcoef, coef.data(), sizeof(double2) * S, cudaMemcpyHostToDevice, ctx.stream));
+    launch_shift_cvec<R>(ctx, D(res.o), CD(phi), S, np, dcoef, -1.0);
+    // preconditioner: kinetic energy per state, then K(0.5 |G|^2 / T_s)
+    launch_laplacian<R>(ctx, b, CD(res.o), D(lap.o), S, -0.5, zero);
+    const auto tv = ovd(lap.o, res.o);
+    const auto tn = ovd(res.o, res.o);
+    for (int s = 0; s < S; s++) kin[s] = (tv[s] / tn[s]).real();
+    INQB_CUDA(cudaMemcpyAsync(dkin, kin.data(), sizeof(double) * S, cudaMemcpyHostToDevice, ctx.stream));
+    launch_tpa_precondition<R>(ctx, b, D(res.o), S, dkin);
+    apply_any(h, res.o, hres.o);
+    const auto m0 = ovd(res.o, res.o), m1 = ovd(phi, res.o), m2 = ovd(res.o, hres.o), m3 = ovd(phi, hres.o);
+    for (int s = 0; s < S; s++) {
+      const double ca = (m0[s] * m3[s] - m2[s] * m1[s]).real();
+      const double cb = (nrm[s] * m2[s] - ev[s] * m0[s]).real();
+      const double cc = (ev[s] * m1[s] - m3[s] * nrm[s]).real();
+      const double den = cb + std::sqrt(cb * cb - 4.0 * ca * cc);
+      coef[s] = make_double2(std::fabs(den) < 1e-15 ? 0.0 : 2.0 * cc / den, 0.0);
+    }
+    INQB_CUDA(cudaMemcpyAsync(dcoef, coef.data(), sizeof(double2) * S, cudaMemcpyHostToDevice, ctx.stream));
+    launch_shift_cvec<R>(ctx, D(phi), CD(res.o), S, np, dcoef, 1.0);
+    if (istep != num_steps - 1) launch_shift_cvec<R>(ctx, D(hphi.o), CD(hres.o), S, np, dcoef, 1.0);
+  }
+  INQB_CUDA(cudaStreamSynchronize(ctx.stream));  // the host factors above go out of scope
+  dev_free(ctx, dov);
+  dev_free(ctx, dcoef);
+  dev_free(ctx, dkin);
+}
 
 extern "C" {
 
@@ -1380,17 +1457,20 @@ int inqb_orthogonalize(inqb_orbitals *phi) {
   return guarded(phi ? phi->ctx : nullptr, [&] {
     INQB_REQUIRE(phi, INQB_ERR_ARG, "null argument");
     set_device(*phi->ctx);
-    Ctx &ctx = *phi->ctx;
-    const int S = phi->nst;
-    double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * S * S));
-    overlap_dev(*phi, *phi, d);
-    auto Sh = download<std::complex<double>>(ctx, d, size_t(S) * S);
-    std::vector<std::complex<double>> X(size_t(S) * S);
-    cholesky_inverse(S, Sh.data(), X.data());
-    INQB_CUDA(cudaMemcpyAsync(d, X.data(), sizeof(double2) * S * S, cudaMemcpyHostToDevice, ctx.stream));
-    rotate_dev(*phi, d);
-    dev_free(ctx, d);
-    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+    orthogonalize_dev(*phi);
+  });
+}
+
+int inqb_steepest_descent(const inqb_hamiltonian *hc, inqb_orbitals *fphi) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && fphi, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(fphi->space == INQB_FOURIER_SPACE, INQB_ERR_ARG, "steepest_descent needs a Fourier-space set");
+    INQB_REQUIRE(fphi->basis == h->basis, INQB_ERR_ARG, "orbitals and Hamiltonian live on different bases");
+    set_device(*h->ctx);
+    if (fphi->precision == INQB_F64) steepest_descent_t<double>(*h, *fphi);
+    else steepest_descent_t<float>(*h, *fphi);
+    orthogonalize_dev(*fphi);
   });
 }
 

@@ -363,10 +363,10 @@ template <typename R, typename CR, int N, int VAR> constexpr int threads_of() {
 }
 
 // CTAs per SM the register allocation must allow: four for the single-precision kinetic pass of lines
-// up to 96 points (two transforms per tile, latency-bound with fewer warps; longer lines would spill),
-// otherwise what the shared memory allows.
+// up to 96 points (two transforms per tile, latency-bound with fewer warps; longer lines would spill);
+// 0 (no constraint: the compiler's own register choice) otherwise.
 template <typename R, typename CR, int N, int VAR> constexpr int min_ctas_of() {
-  return (VAR == MID_KIN && sizeof(R) == 4 && sizeof(CR) == 4 && N <= 96) ? 4 : 1;
+  return (VAR == MID_KIN && sizeof(R) == 4 && sizeof(CR) == 4 && N <= 96) ? 4 : 0;
 }
 
 template <typename R, typename CR, int N, int VAR>

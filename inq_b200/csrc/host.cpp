@@ -74,6 +74,13 @@ void ensure_smem_attr(const void *kernel, size_t bytes) {
   }
 }
 
+// volume element of a set's basis: Omega / N in real space (real_space.hpp:216-218), Omega / N^2 in
+// Fourier space (fourier_space.hpp:48-50, the forward transform being unnormalised)
+double set_volume_element(const Orbitals &o) {
+  const double n = double(o.basis->npoints);
+  return o.space == INQB_FOURIER_SPACE ? o.basis->volume / (n * n) : o.basis->volume / n;
+}
+
 // ------------------------------------------------------------------ scratch memory
 
 void *dev_alloc(Ctx &ctx, size_t bytes) {

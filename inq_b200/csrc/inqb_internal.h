@@ -214,6 +214,10 @@ void launch_density(Ctx &ctx, const C2<R> *phi, int S, long long npoints, const 
                     int accumulate);
 template <typename R> void launch_kick(Ctx &ctx, const Basis &b, C2<R> *phi, int S, const double ecov[3]);
 template <typename R>
+void launch_shift_cvec(Ctx &ctx, C2<R> *y, const C2<R> *x, int S, long long npoints, const double2 *coef_dev,
+                       double scale);
+template <typename R> void launch_tpa_precondition(Ctx &ctx, const Basis &b, C2<R> *x, int S, const double *kin_dev);
+template <typename R>
 void launch_shift_vec(Ctx &ctx, C2<R> *y, const C2<R> *x, int S, long long npoints, const double *coef_dev,
                       double scale);
 template <typename R>
@@ -230,6 +234,8 @@ std::vector<int> fft_radices(int n);
 void basis_metric(const double lattice[9], double lat[3][3], double rec[3][3], double rlat[3][3], double &volume);
 
 void ensure_smem_attr(const void *kernel, size_t bytes);
+// volume element of a set's basis: Omega / N (real space) or Omega / N^2 (Fourier space)
+double set_volume_element(const Orbitals &o);
 // interacting potential (kernels.cu): real -> complex copy, Poisson factor on the Fourier grid,
 // V = V_ion + V_H + V_xc with per-block energy sums (KS_BLOCKS x 4 doubles)
 constexpr int KS_BLOCKS = 148;

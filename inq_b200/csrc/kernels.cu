@@ -653,6 +653,46 @@ void launch_absdiff_sum(Ctx &ctx, const double *a, const double *b, long long n,
   dev_free(ctx, partial);
 }
 
+// ------------------------------------------------------------------ eigensolver pieces
+// y[pt][s] += scale * (coef[s] * x[pt][s]) with complex per-state factors (operations::shift, shift.hpp:19-31)
+template <typename R>
+__global__ void shift_cvec_kernel(C2<R> *__restrict__ y, const C2<R> *__restrict__ x, int S, long long n,
+                                  const double2 *__restrict__ coef, double scale) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double2 c = coef[i % S];
+    const C2<R> xv = x[i];
+    const double tr = c.x * double(xv.x) - c.y * double(xv.y), ti = c.x * double(xv.y) + c.y * double(xv.x);
+    y[i] = mk<C2<R>>(R(double(y[i].x) + scale * tr), R(double(y[i].y) + scale * ti));
+  }
+}
+template <typename R>
+void launch_shift_cvec(Ctx &ctx, C2<R> *y, const C2<R> *x, int S, long long npoints, const double2 *coef_dev,
+                       double scale) {
+  shift_cvec_kernel<R><<<grid_for(npoints * S, 256), 256, 0, ctx.stream>>>(y, x, S, npoints * S, coef_dev, scale);
+  LAUNCHED(ctx);
+}
+
+// Teter-Payne-Allan preconditioner on a Fourier-space set (preconditioner.hpp:24-46):
+// x[G][s] *= K(0.5 |G|^2 / kin[s]), K(t) = (((8t + 12)t + 18)t + 27) / ((((16t + 8)t + 12)t + 18)t + 27)
+template <typename R>
+__global__ void tpa_precondition_kernel(Metric m, C2<R> *__restrict__ x, int S, long long n,
+                                        const double *__restrict__ kin) {
+  const double zero[3] = {0.0, 0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double lapl = -0.5 * lapl_at(m, i / S, 1.0, zero, 0.0);  // -0.5 * (-|G|^2)
+    const double t = lapl / kin[i % S];
+    const double num = ((8.0 * t + 12.0) * t + 18.0) * t + 27.0;
+    const double den = (((16.0 * t + 8.0) * t + 12.0) * t + 18.0) * t + 27.0;
+    const double k = num / den;
+    x[i] = mk<C2<R>>(R(double(x[i].x) * k), R(double(x[i].y) * k));
+  }
+}
+template <typename R> void launch_tpa_precondition(Ctx &ctx, const Basis &b, C2<R> *x, int S, const double *kin_dev) {
+  tpa_precondition_kernel<R><<<grid_for(b.npoints * S, 256), 256, 0, ctx.stream>>>(metric_of(b), x, S,
+                                                                                   b.npoints * S, kin_dev);
+  LAUNCHED(ctx);
+}
+
 // ------------------------------------------------------------------ interacting potential
 // (solvers/poisson.hpp, hamiltonian/xc_term.hpp, hamiltonian/self_consistency.hpp)
 
@@ -760,6 +800,8 @@ void launch_ks_potential(Ctx &ctx, const double *n, const double *vion, const do
   template void launch_fill<R>(Ctx &, C2<R> *, long long, double, double);                                         \
   template void launch_axpy<R>(Ctx &, C2<R> *, const C2<R> *, long long, double, double);                          \
   template void launch_shift_vec<R>(Ctx &, C2<R> *, const C2<R> *, int, long long, const double *, double);        \
+  template void launch_shift_cvec<R>(Ctx &, C2<R> *, const C2<R> *, int, long long, const double2 *, double);      \
+  template void launch_tpa_precondition<R>(Ctx &, const Basis &, C2<R> *, int, const double *);                    \
   template void launch_laplacian<R>(Ctx &, const Basis &, const C2<R> *, C2<R> *, int, double, const double *);    \
   template void launch_overlap_diag<R>(Ctx &, const C2<R> *, const C2<R> *, int, long long, double, double2 *);    \
   template void launch_kinetic_ev<R>(Ctx &, const Basis &, const C2<R> *, int, double, const double *, double,     \

@@ -90,7 +90,7 @@ extern "C" int inqb_overlap_diagonal_noalloc(const inqb_orbitals *a, const inqb_
     double2 *partial = partial_address(ctx->device);
     const int S = a->nst;
     const long long np = a->basis->npoints;
-    const double dv = a->basis->volume / double(np);
+    const double dv = set_volume_element(*a);
     if (a->precision == INQB_F64)
       noalloc_partial_kernel<double><<<NOALLOC_BLOCKS, 256, 0, ctx->stream>>>(
           static_cast<const double2 *>(a->data), static_cast<const double2 *>(b->data), S, np, partial);

@@ -797,3 +797,69 @@ def update_hamiltonian(ham: Hamiltonian, vion, n, hartree=True, xc=True):
         v = v + vxc
     ham.V = v
     return energies
+
+
+# ---------------------------------------------------------------------------
+# Fourier-space eigensolver (eigensolvers/steepest_descent.hpp, operations/preconditioner.hpp)
+# ---------------------------------------------------------------------------
+
+
+def tpa_k(x):
+    """Teter-Payne-Allan preconditioner function (preconditioner.hpp:24-30)."""
+    num = ((8.0 * x + 12.0) * x + 18.0) * x + 27.0
+    den = (((16.0 * x + 8.0) * x + 12.0) * x + 18.0) * x + 27.0
+    return num / den
+
+
+def precondition(rs: RealSpace, fphi):
+    """preconditioner::operator()(orbital_set<fourier_space>) (preconditioner.hpp:32-46): each state times
+    K(0.5 |G|^2 / T_s), T_s = Re <-0.5 lapl phi_s | phi_s> / <phi_s | phi_s>."""
+    lap = laplacian(rs, fphi, -0.5)
+    kin = np.real(np.sum(np.conj(lap) * fphi, axis=(0, 1, 2)) / np.sum(np.conj(fphi) * fphi, axis=(0, 1, 2)))
+    lapl = 0.5 * rs.g2()
+    return fphi * tpa_k(lapl[..., None] / kin[None, None, None, :])
+
+
+def overlap_diagonal_fs(rs: RealSpace, a, b=None):
+    """overlap_diagonal of Fourier-space sets: the Fourier volume element Omega / N^2."""
+    if b is None:
+        b = a
+    return rs.fourier_volume_element() * np.sum(np.conj(a) * b, axis=(0, 1, 2))
+
+
+def orthogonalize_fs(rs: RealSpace, fphi):
+    """orthogonalize.hpp:25-31 on a Fourier-space set (overlap with Omega / N^2)."""
+    S = rs.fourier_volume_element() * np.einsum("xyzi,xyzj->ij", np.conj(fphi), fphi)
+    U = np.linalg.cholesky(S).conj().T
+    shp = fphi.shape
+    return (fphi.reshape(-1, shp[-1]) @ np.linalg.inv(U)).reshape(shp)
+
+
+def steepest_descent(ham: Hamiltonian, fphi, kpoint_cov=(0.0, 0.0, 0.0), num_steps=5):
+    """eigensolvers::steepest_descent (steepest_descent.hpp:23-86) with the TPA preconditioner on a
+    Fourier-space set; returns the new set (orthonormalised)."""
+    rs = ham.rs
+    phi = fphi.copy()
+    hphi = ham.apply_fourier(phi, kpoint_cov)
+    for istep in range(num_steps):
+        res = hphi.copy()
+        ev = overlap_diagonal_fs(rs, res, phi)
+        norm = overlap_diagonal_fs(rs, phi)
+        evnorm = ev / np.real(norm)
+        res = res - evnorm[None, None, None, :] * phi            # shift(-1, evnorm, phi, residual)
+        res = precondition(rs, res)
+        hres = ham.apply_fourier(res, kpoint_cov)
+        m0 = overlap_diagonal_fs(rs, res, res)
+        m1 = overlap_diagonal_fs(rs, phi, res)
+        m2 = overlap_diagonal_fs(rs, res, hres)
+        m3 = overlap_diagonal_fs(rs, phi, hres)
+        m4, m5 = ev, norm
+        ca = np.real(m0 * m3 - m2 * m1)
+        cb = np.real(m5 * m2 - m4 * m0)
+        cc = np.real(m4 * m1 - m3 * m5)
+        den = cb + np.sqrt(cb * cb - 4.0 * ca * cc)
+        lam = np.where(np.abs(den) < 1e-15, 0.0, 2.0 * cc / np.where(np.abs(den) < 1e-15, 1.0, den))
+        phi = phi + lam[None, None, None, :] * res
+        if istep != num_steps - 1:
+            hphi = hphi + lam[None, None, None, :] * hres
+    return orthogonalize_fs(rs, phi)
