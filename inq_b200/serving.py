@@ -202,7 +202,14 @@ class Server:
         ph = np.array([r.result["phases_ms"] for r in done if "phases_ms" in r.result]).reshape(-1, 3)
         phases = {k: float(ph[:, i].mean()) if len(ph) else 0.0
                   for i, k in enumerate(("setup_ms", "compute_ms", "fetch_ms"))}
+        def pct(rs, q):
+            return float(np.percentile([r.latency for r in rs], q) * 1000) if rs else 0.0
+        big = max((r.payload.system.npoints * r.payload.system.nst for r in done), default=0)
+        large = [r for r in done if r.payload.system.npoints * r.payload.system.nst == big]
+        small = [r for r in done if r.payload.system.npoints * r.payload.system.nst != big]
         return {"requests": len(reqs), "completed": len(done), "rejected": len(reqs) - len(done),
+                "by_size": {"largest_system": {"n": len(large), "p50_ms": pct(large, 50), "p99_ms": pct(large, 99)},
+                            "others": {"n": len(small), "p50_ms": pct(small, 50), "p99_ms": pct(small, 99)}},
                 "wall_s": wall, "throughput_req_s": len(done) / wall,
                 "state_applications_per_s": happs / wall,
                 "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000),
