@@ -542,13 +542,16 @@ def run_ours(args):
 
 
 def run_profile_case(args):
-    """Small case for ncu captures: the C2 grid and atoms with 32 orbitals (226 MB per FP32 set, above L2).
+    """Small case for ncu captures: the C2 grid and atoms with ``--profile-states`` orbitals (32: 226 MB
+    per FP32 set, above L2; 128: 0.9 GB).
 
     Sequence: FP64 build (3 FFT passes), then ``--steps`` mixed-form and ``--steps`` FP64 applications
-    (each: 1 projection + 5 FFT passes)."""
+    (each: 1 projection + 5 FFT passes + 1 nonlocal apply), then ``--steps`` tensor-core overlaps of the
+    FP32 set."""
     import inq_b200 as ib
     from inq_b200 import synthetic
-    sysm = synthetic.config("c2", nst=32)
+    S = args.profile_states
+    sysm = synthetic.config("c2", nst=S)
     basis, ham, phi64 = synthetic.build(sysm)
     phi32 = phi64.converted(ib.F32)
     out32, out64 = phi32.skeleton(), phi64.skeleton()
@@ -556,8 +559,10 @@ def run_profile_case(args):
         ham.apply(phi32, out32)
     for _ in range(args.steps):
         ham.apply(phi64, out64)
+    for _ in range(args.steps):
+        ib.overlap(phi32)
     basis.ctx.synchronize()
-    print(json.dumps({"profile_case": "c2 grid, 32 states", "launches": basis.ctx.launch_count()}))
+    print(json.dumps({"profile_case": f"c2 grid, {S} states", "launches": basis.ctx.launch_count()}))
 
 
 def main():
@@ -571,6 +576,7 @@ def main():
     ap.add_argument("--etrs-steps", type=int, default=10, help="ETRS steps of the 120^3 real-time leg (0: skip)")
     ap.add_argument("--etrs-dt", type=float, default=0.005, help="time step of the 120^3 real-time leg (a.u.)")
     ap.add_argument("--profile-case", action="store_true", help="small workload for ncu captures")
+    ap.add_argument("--profile-states", type=int, default=32, help="orbitals of the --profile-case workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

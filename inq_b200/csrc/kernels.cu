@@ -85,51 +85,53 @@ void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[
 
 // ------------------------------------------------------------------ nonlocal projection
 // proj[p][l][s] = sum_i gcoef[p][i][l] * psi[pt_i][s]; projD = coeff[p] . proj
-// (projector_all.hpp:113-211).  CTA = (projector p, 32 states); 8 warps stride over
-// the sphere points; lanes are consecutive states so each warp load is one contiguous
-// row segment of the state-fastest layout.  The 8 warp partials are summed in order.
+// (projector_all.hpp:113-211).  CTA = (projector p, 32 states); each of 16 warps takes a
+// contiguous run of the sphere points, reads 32 point indices with one coalesced load and
+// hands them out by shuffles, keeping 8 row loads in flight; lanes are consecutive states
+// so each row load is one contiguous segment of the state-fastest layout.  The 16 warp
+// partials are summed in order.
 template <typename R, typename A>
-__global__ void __launch_bounds__(512) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
+__global__ void __launch_bounds__(512, 2) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
                                                          const int *__restrict__ pt, const C2<A> *__restrict__ gcoef,
                                                          const int *__restrict__ npts, const A *__restrict__ coeff,
                                                          int maxsph, C2<R> *projraw, C2<R> *projD) {
   using T = C2<R>;
   using TA = C2<A>;
-  constexpr int NW = 16;  // warps per CTA, each striding over the sphere points
+  constexpr int NW = 16;  // warps per CTA, each over a contiguous run of the sphere points
+  constexpr int UN = 8;   // independent row loads in flight per warp
   __shared__ TA part[NW][4][32];
   const int p = blockIdx.x;
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const int s = blockIdx.y * 32 + lane;
   const bool active = s < S;
   const int np = npts[p];
+  const int per = (np + NW - 1) / NW;
+  const int i0 = wp * per, i1 = min(np, i0 + per);
   TA acc[4];
 #pragma unroll
   for (int l = 0; l < 4; l++) acc[l] = mk<TA>(A(0), A(0));
   const long long rowbase = (long long)p * maxsph;
-  int i = wp;
-#pragma unroll 1
-  for (; i + NW * 3 < np; i += NW * 4) {
-    TA v[4];
-    int q[4];
+  for (int base = i0; base < i1; base += 32) {
+    // 32 point indices with one coalesced load, handed out by shuffles
+    const int cnt = min(32, i1 - base);
+    const int qv = lane < cnt ? __ldg(&pt[rowbase + base + lane]) : 0;
+    for (int j = 0; j < cnt; j += UN) {
+      T x[UN];
 #pragma unroll
-    for (int u = 0; u < 4; u++) q[u] = __ldg(&pt[rowbase + i + NW * u]);
+      for (int u = 0; u < UN; u++) {
+        const int q = __shfl_sync(0xffffffffu, qv, (j + u) & 31);
+        x[u] = (active && j + u < cnt) ? psi[(long long)q * S + s] : mk<T>(R(0), R(0));
+      }
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      T x = active ? psi[(long long)q[u] * S + s] : mk<T>(R(0), R(0));
-      v[u] = mk<TA>(A(x.x), A(x.y));
+      for (int u = 0; u < UN; u++) {
+        if (j + u < cnt) {
+          const TA v = mk<TA>(A(x[u].x), A(x[u].y));
+          const TA *g = gcoef + (rowbase + base + j + u) * 4;
+#pragma unroll
+          for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(g[l], v));
+        }
+      }
     }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-#pragma unroll
-      for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(gcoef[(rowbase + i + NW * u) * 4 + l], v[u]));
-    }
-  }
-  for (; i < np; i += NW) {
-    const int q = __ldg(&pt[rowbase + i]);
-    T x = active ? psi[(long long)q * S + s] : mk<T>(R(0), R(0));
-    const TA v = mk<TA>(A(x.x), A(x.y));
-#pragma unroll
-    for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(gcoef[(rowbase + i) * 4 + l], v));
   }
 #pragma unroll
   for (int l = 0; l < 4; l++) part[wp][l][lane] = acc[l];
@@ -203,59 +205,60 @@ void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
 }
 
 // out[pt][s] += nonlocal term at the grid points that lie in a sphere (ks_hamiltonian.hpp:153,
-// projector_all.hpp:276-288), owner computes: one thread per (hit point, state), hits of a point summed
-// in projector order, no atomics.  Optional Taylor accumulators acc += c * term (linear in the term).
-// Owner computes: one warp per grid point with sphere hits, lanes over states.  The point's record
-// gives its first hit and projector in one load, so the coefficient, projection and output reads are
-// all issued together (a two-level dependency instead of point -> CSR -> hit -> projection).
+// projector_all.hpp:276-288), hits of a point summed in projector order, no atomics; optional Taylor
+// accumulators acc += c * term (linear in the term).
+// Owner computes: one warp per (grid point with sphere hits, chunk of 32 * U states), lanes over states.
+// The point's record gives its first hit and projector in one load, so the coefficient, projection and
+// output reads are all issued together (a two-level dependency instead of point -> CSR -> hit ->
+// projection); splitting the states into chunks keeps the registers low and many warps resident.
 template <typename R>
-__global__ void __launch_bounds__(256, 2) nl_apply_kernel(long long nhp, int S, const int4 *__restrict__ hrec,
-                                                       const int *__restrict__ hitp, const C2<R> *__restrict__ hcoef,
-                                                       const C2<R> *__restrict__ projD, C2<R> *__restrict__ out,
-                                                       C2<R> *__restrict__ acc1, C2<R> c1, C2<R> *__restrict__ acc2,
-                                                       C2<R> c2) {
+__global__ void __launch_bounds__(128) nl_apply_kernel(long long nitems, int nchunks, int S,
+                                                          const int4 *__restrict__ hrec, const int *__restrict__ hitp,
+                                                          const C2<R> *__restrict__ hcoef,
+                                                          const C2<R> *__restrict__ projD, C2<R> *__restrict__ out,
+                                                          C2<R> *__restrict__ acc1, C2<R> c1,
+                                                          C2<R> *__restrict__ acc2, C2<R> c2) {
   using T = C2<R>;
-  constexpr int U = 16 / sizeof(R);  // states per lane and chunk: 4 single, 2 double
+  constexpr int U = 16 / sizeof(R);  // states per lane: 4 single, 2 double
   const int lane = threadIdx.x & 31;
   const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long r = warp; r < nhp; r += nwarps) {
+  for (long long it = warp; it < nitems; it += nwarps) {
+    const long long r = it / nchunks;
+    const int s0 = int(it % nchunks) * (32 * U);
     const int4 rec = hrec[r];
     const long long pt = rec.x;
     const int h0 = rec.y, nh = rec.z, p0 = rec.w;
-    T hc[4];
+    T hc[4], o[U], pd[4][U];
 #pragma unroll
     for (int l = 0; l < 4; l++) hc[l] = hcoef[(long long)h0 * 4 + l];
-    for (int s0 = 0; s0 < S; s0 += 32 * U) {
-      T o[U], pd[4][U];
 #pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int s = s0 + u * 32 + lane;
-        if (s < S) {
-          o[u] = out[pt * S + s];
+    for (int u = 0; u < U; u++) {
+      const int s = s0 + u * 32 + lane;
+      if (s < S) {
+        o[u] = out[pt * S + s];
 #pragma unroll
-          for (int l = 0; l < 4; l++) pd[l][u] = projD[((long long)p0 * 4 + l) * S + s];
-        }
+        for (int l = 0; l < 4; l++) pd[l][u] = projD[((long long)p0 * 4 + l) * S + s];
       }
+    }
 #pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int s = s0 + u * 32 + lane;
-        if (s >= S) continue;
-        T accv = mk<T>(R(0), R(0));
+    for (int u = 0; u < U; u++) {
+      const int s = s0 + u * 32 + lane;
+      if (s >= S) continue;
+      T accv = mk<T>(R(0), R(0));
 #pragma unroll
-        for (int l = 0; l < 4; l++) accv = cadd(accv, cmul(hc[l], pd[l][u]));
-        for (int k = 1; k < nh; k++) {
-          const int h = h0 + k;
-          const int p = hitp[h];
+      for (int l = 0; l < 4; l++) accv = cadd(accv, cmul(hc[l], pd[l][u]));
+      for (int k = 1; k < nh; k++) {
+        const int h = h0 + k;
+        const int p = hitp[h];
 #pragma unroll
-          for (int l = 0; l < 4; l++)
-            accv = cadd(accv, cmul(hcoef[(long long)h * 4 + l], projD[((long long)p * 4 + l) * S + s]));
-        }
-        const long long e = pt * S + s;
-        out[e] = cadd(o[u], accv);
-        if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, accv));
-        if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, accv));
+        for (int l = 0; l < 4; l++)
+          accv = cadd(accv, cmul(hcoef[(long long)h * 4 + l], projD[((long long)p * 4 + l) * S + s]));
       }
+      const long long e = pt * S + s;
+      out[e] = cadd(o[u], accv);
+      if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, accv));
+      if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, accv));
     }
   }
 }
@@ -268,10 +271,13 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
   const C2<R> *hc;
   if constexpr (sizeof(R) == 8) hc = P.d_hcoef;
   else hc = P.d_hcoef32;
-  long long blocks = (P.nhitpts + 7) / 8;
-  if (blocks > 148LL * 16) blocks = 148LL * 16;
-  nl_apply_kernel<R><<<unsigned(blocks), 256, 0, ctx.stream>>>(P.nhitpts, S, P.d_hrec, P.d_hitp, hc, projD, out, acc1,
-                                                               c1, acc2, c2);
+  const int chunk = 32 * int(16 / sizeof(R));
+  const int nchunks = (S + chunk - 1) / chunk;
+  const long long nitems = P.nhitpts * nchunks;
+  long long blocks = (nitems + 3) / 4;
+  if (blocks > 148LL * 48) blocks = 148LL * 48;
+  nl_apply_kernel<R><<<unsigned(blocks), 128, 0, ctx.stream>>>(nitems, nchunks, S, P.d_hrec, P.d_hitp, hc, projD, out,
+                                                               acc1, c1, acc2, c2);
   LAUNCHED(ctx);
 }
 
