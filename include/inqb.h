@@ -246,6 +246,25 @@ int inqb_graph_destroy(void *graph_exec);
  * eigenvectors; eigenvalues host [nst], ascending. */
 int inqb_subspace_diagonalization(const inqb_hamiltonian *ham, inqb_orbitals *phi, double *eigenvalues);
 
+/* ---- restart files (operations/io.hpp, systems/electrons.hpp:323-380) ----------- */
+/* operations::io::save(dirname, orbital_set) (io.hpp:172-189): dirname is created and gets one
+ * file per state, "<state %010d>_<spinor %010d>", each holding the state's npoint complex128
+ * values in grid order (x slowest), native byte order -- the layout the reference reads back.
+ * Single-precision sets are widened to complex128. */
+int inqb_orbitals_save(const inqb_orbitals *phi, const char *dirname);
+/* operations::io::load(dirname, orbital_set) (io.hpp:192-215): reads those files into phi
+ * (narrowed for single precision); INQB_ERR_ARG when the directory or a file is missing or short. */
+int inqb_orbitals_load(inqb_orbitals *phi, const char *dirname);
+/* io::save / io::load of a field_set<real_space, double> (io.hpp:129-169): one file per
+ * component, "<component %010d>", npoint float64; data is [npoint][ncomp] on the host (the
+ * spin density of electrons::save). */
+int inqb_field_save(const char *dirname, const double *data, long long npoint, int ncomp);
+int inqb_field_load(const char *dirname, double *data, long long npoint, int ncomp);
+/* io::save / io::load of a plain array (io.hpp:112-127): dirname/array, n float64 (the
+ * occupations of electrons::save). */
+int inqb_array_save(const char *dirname, const double *data, long long n);
+int inqb_array_load(const char *dirname, double *data, long long n);
+
 /* ---- real time ------------------------------------------------------------ */
 /* operations::exponential_in_place (exponential.hpp:21-34): phi <- sum_n (f H)^n/n! phi, f = re + i im. */
 int inqb_exponential_in_place(const inqb_hamiltonian *ham, double re, double im, inqb_orbitals *phi, int order);

@@ -75,6 +75,12 @@ SIGNATURES = {
     "inqb_apply": (I, [P, P, P]),
     "inqb_apply_host": (I, [P, I, DP, I, I, P, P, I]),
     "inqb_steepest_descent": (I, [P, P]),
+    "inqb_orbitals_save": (I, [P, C.c_char_p]),
+    "inqb_orbitals_load": (I, [P, C.c_char_p]),
+    "inqb_field_save": (I, [C.c_char_p, DP, LL, I]),
+    "inqb_field_load": (I, [C.c_char_p, DP, LL, I]),
+    "inqb_array_save": (I, [C.c_char_p, DP, LL]),
+    "inqb_array_load": (I, [C.c_char_p, DP, LL]),
     "inqb_non_local": (I, [P, P, P]),
     "inqb_non_local_energy": (I, [P, P, DP, DP]),
     "inqb_kinetic_expectation_value": (I, [P, P, DP]),

@@ -301,6 +301,16 @@ class OrbitalSet:
         self.ctx.check(self.ctx.lib.inqb_orbitals_upload(self.handle, a.ctypes.data_as(C.c_void_p)))
         return self
 
+    def save(self, dirname: str) -> "OrbitalSet":
+        """operations::io::save: one complex128 file per state in ``dirname`` (the reference's layout)."""
+        self.ctx.check(self.ctx.lib.inqb_orbitals_save(self.handle, str(dirname).encode()))
+        return self
+
+    def load(self, dirname: str) -> "OrbitalSet":
+        """operations::io::load: the states of ``dirname`` into this set."""
+        self.ctx.check(self.ctx.lib.inqb_orbitals_load(self.handle, str(dirname).encode()))
+        return self
+
     def matrix(self) -> np.ndarray:
         """Host copy [npoint][nst] (field_set::matrix())."""
         out = np.empty((self.basis.size(), self.nst), dtype=self.dtype)
@@ -580,6 +590,37 @@ def _ptr_arrays(phis, occs):
     occ_arrays = [np.ascontiguousarray(o, dtype=np.float64) for o in occs]
     optrs = (_lib.DP * len(occs))(*[dptr(o) for o in occ_arrays])
     return hs, optrs, occ_arrays
+
+
+def save_electrons(dirname: str, phis: Sequence[OrbitalSet], occupations: Sequence, spin_density) -> None:
+    """systems::electrons::save (electrons.hpp:323-343): per k-point/spin set kpin<%010d>/states and
+    kpin<%010d>/occupations/array, and spin_density/<component %010d> ([npoint][nspin] float64)."""
+    import os
+    for i, (phi, occ) in enumerate(zip(phis, occupations)):
+        base = os.path.join(dirname, f"kpin{i:010d}")
+        phi.save(os.path.join(base, "states"))
+        o = np.ascontiguousarray(np.asarray(occ, dtype=np.float64))
+        _lib.check(_lib.load().inqb_array_save(os.path.join(base, "occupations").encode(), dptr(o), o.size))
+    d = np.ascontiguousarray(np.asarray(spin_density, dtype=np.float64).reshape(phis[0].basis.size(), -1))
+    _lib.check(_lib.load().inqb_field_save(os.path.join(dirname, "spin_density").encode(), dptr(d), d.shape[0],
+                                           d.shape[1]))
+
+
+def load_electrons(dirname: str, phis: Sequence[OrbitalSet], nspin: int = 1):
+    """systems::electrons::try_load (electrons.hpp:346-376): fills the sets; returns (occupations,
+    spin density [npoint][nspin]).  Raises InqbError when a file is missing."""
+    import os
+    occs = []
+    for i, phi in enumerate(phis):
+        base = os.path.join(dirname, f"kpin{i:010d}")
+        phi.load(os.path.join(base, "states"))
+        o = np.zeros(phi.nst)
+        _lib.check(_lib.load().inqb_array_load(os.path.join(base, "occupations").encode(), dptr(o), o.size))
+        occs.append(o)
+    d = np.zeros((phis[0].basis.size(), nspin))
+    _lib.check(_lib.load().inqb_field_load(os.path.join(dirname, "spin_density").encode(), dptr(d), d.shape[0],
+                                           nspin))
+    return occs, d
 
 
 def density(phis: Sequence[OrbitalSet], occupations: Sequence) -> np.ndarray:

@@ -9,7 +9,10 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdio>
 #include <cstring>
+#include <filesystem>
+#include <fstream>
 #include <memory>
 #include <numeric>
 
@@ -612,6 +615,66 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
 }
 
 }  // namespace
+
+// ------------------------------------------------------------------ restart files (operations/io.hpp)
+
+// utils::num_to_str (utils/num_str.hpp:16-20): ten digits, zero padded
+std::string num10(long n) {
+  char b[16];
+  std::snprintf(b, sizeof(b), "%010ld", n);
+  return std::string(b);
+}
+
+void write_file(const std::string &name, const void *data, size_t bytes) {
+  std::ofstream f(name, std::ios::binary | std::ios::trunc);
+  INQB_REQUIRE(f.good(), INQB_ERR_ARG, "cannot create restart file '" + name + "'");
+  f.write(static_cast<const char *>(data), std::streamsize(bytes));
+  INQB_REQUIRE(f.good(), INQB_ERR_ARG, "cannot write restart file '" + name + "'");
+}
+
+void read_file(const std::string &name, void *data, size_t bytes) {
+  std::ifstream f(name, std::ios::binary);
+  INQB_REQUIRE(f.good(), INQB_ERR_ARG, "cannot open restart file '" + name + "'");
+  f.read(static_cast<char *>(data), std::streamsize(bytes));
+  INQB_REQUIRE(size_t(f.gcount()) == bytes, INQB_ERR_ARG, "restart file '" + name + "' is too short");
+}
+
+// states of a set through contiguous complex128 rows, a block of states at a time (about 256 MB)
+template <typename R> void save_states(const Orbitals &phi, const std::string &dir) {
+  Ctx &ctx = *phi.ctx;
+  const long long np = phi.basis->npoints;
+  const int S = phi.nst;
+  const int blk = int(std::max<long long>(1, std::min<long long>(S, (256LL << 20) / (np * 16))));
+  double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * size_t(np) * blk));
+  std::vector<double2> h(size_t(np) * blk);
+  for (int s0 = 0; s0 < S; s0 += blk) {
+    const int ns = std::min(blk, S - s0);
+    launch_extract_states<R>(ctx, static_cast<const C2<R> *>(phi.data), S, np, s0, ns, d);
+    INQB_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(double2) * size_t(np) * ns, cudaMemcpyDeviceToHost, ctx.stream));
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+    for (int k = 0; k < ns; k++)
+      write_file(dir + "/" + num10(s0 + k) + "_" + num10(0), h.data() + size_t(k) * np, sizeof(double2) * size_t(np));
+  }
+  dev_free(ctx, d);
+}
+
+template <typename R> void load_states(Orbitals &phi, const std::string &dir) {
+  Ctx &ctx = *phi.ctx;
+  const long long np = phi.basis->npoints;
+  const int S = phi.nst;
+  const int blk = int(std::max<long long>(1, std::min<long long>(S, (256LL << 20) / (np * 16))));
+  double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * size_t(np) * blk));
+  std::vector<double2> h(size_t(np) * blk);
+  for (int s0 = 0; s0 < S; s0 += blk) {
+    const int ns = std::min(blk, S - s0);
+    for (int k = 0; k < ns; k++)
+      read_file(dir + "/" + num10(s0 + k) + "_" + num10(0), h.data() + size_t(k) * np, sizeof(double2) * size_t(np));
+    INQB_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(double2) * size_t(np) * ns, cudaMemcpyHostToDevice, ctx.stream));
+    launch_insert_states<R>(ctx, d, S, np, s0, ns, static_cast<C2<R> *>(phi.data));
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));  // the host block is refilled next
+  }
+  dev_free(ctx, d);
+}
 
 // ============================================================================ C ABI
 
@@ -1757,6 +1820,71 @@ int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int n
     dev_free(ctx, delta_dev);
     save.clear();
     INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+  });
+}
+
+int inqb_orbitals_save(const inqb_orbitals *phi, const char *dirname) {
+  return guarded(phi ? phi->ctx : nullptr, [&] {
+    INQB_REQUIRE(phi && dirname, INQB_ERR_ARG, "null argument");
+    set_device(*phi->ctx);
+    std::error_code ec;
+    std::filesystem::create_directories(dirname, ec);
+    INQB_REQUIRE(!ec, INQB_ERR_ARG, std::string("cannot create directory '") + dirname + "'");
+    if (phi->precision == INQB_F64) save_states<double>(*phi, dirname);
+    else save_states<float>(*phi, dirname);
+  });
+}
+
+int inqb_orbitals_load(inqb_orbitals *phi, const char *dirname) {
+  return guarded(phi ? phi->ctx : nullptr, [&] {
+    INQB_REQUIRE(phi && dirname, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(std::filesystem::is_directory(dirname), INQB_ERR_ARG,
+                 std::string("no restart directory '") + dirname + "'");
+    set_device(*phi->ctx);
+    if (phi->precision == INQB_F64) load_states<double>(*phi, dirname);
+    else load_states<float>(*phi, dirname);
+  });
+}
+
+int inqb_field_save(const char *dirname, const double *data, long long npoint, int ncomp) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(dirname && data && npoint > 0 && ncomp > 0, INQB_ERR_ARG, "bad argument");
+    std::error_code ec;
+    std::filesystem::create_directories(dirname, ec);
+    INQB_REQUIRE(!ec, INQB_ERR_ARG, std::string("cannot create directory '") + dirname + "'");
+    std::vector<double> col(static_cast<size_t>(npoint));
+    for (int c = 0; c < ncomp; c++) {
+      for (long long p = 0; p < npoint; p++) col[size_t(p)] = data[size_t(p) * ncomp + c];
+      write_file(std::string(dirname) + "/" + num10(c), col.data(), sizeof(double) * size_t(npoint));
+    }
+  });
+}
+
+int inqb_field_load(const char *dirname, double *data, long long npoint, int ncomp) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(dirname && data && npoint > 0 && ncomp > 0, INQB_ERR_ARG, "bad argument");
+    std::vector<double> col(static_cast<size_t>(npoint));
+    for (int c = 0; c < ncomp; c++) {
+      read_file(std::string(dirname) + "/" + num10(c), col.data(), sizeof(double) * size_t(npoint));
+      for (long long p = 0; p < npoint; p++) data[size_t(p) * ncomp + c] = col[size_t(p)];
+    }
+  });
+}
+
+int inqb_array_save(const char *dirname, const double *data, long long n) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(dirname && data && n >= 0, INQB_ERR_ARG, "bad argument");
+    std::error_code ec;
+    std::filesystem::create_directories(dirname, ec);
+    INQB_REQUIRE(!ec, INQB_ERR_ARG, std::string("cannot create directory '") + dirname + "'");
+    write_file(std::string(dirname) + "/array", data, sizeof(double) * size_t(n));
+  });
+}
+
+int inqb_array_load(const char *dirname, double *data, long long n) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(dirname && data && n >= 0, INQB_ERR_ARG, "bad argument");
+    read_file(std::string(dirname) + "/array", data, sizeof(double) * size_t(n));
   });
 }
 

@@ -217,6 +217,11 @@ template <typename R>
 void launch_shift_cvec(Ctx &ctx, C2<R> *y, const C2<R> *x, int S, long long npoints, const double2 *coef_dev,
                        double scale);
 template <typename R> void launch_tpa_precondition(Ctx &ctx, const Basis &b, C2<R> *x, int S, const double *kin_dev);
+// states [s0, s0 + ns) of a [np][S] set to / from contiguous complex128 rows [ns][np]
+template <typename R>
+void launch_extract_states(Ctx &ctx, const C2<R> *in, int S, long long np, int s0, int ns, double2 *out);
+template <typename R>
+void launch_insert_states(Ctx &ctx, const double2 *in, int S, long long np, int s0, int ns, C2<R> *out);
 template <typename R>
 void launch_shift_vec(Ctx &ctx, C2<R> *y, const C2<R> *x, int S, long long npoints, const double *coef_dev,
                       double scale);

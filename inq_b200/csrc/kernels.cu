@@ -699,6 +699,40 @@ template <typename R> void launch_tpa_precondition(Ctx &ctx, const Basis &b, C2<
   LAUNCHED(ctx);
 }
 
+// ------------------------------------------------------------------ restart files
+// out[k][pt] = (complex<double>) in[pt][s0 + k], k < ns: states [s0, s0 + ns) as contiguous rows
+template <typename R>
+__global__ void extract_states_kernel(const C2<R> *__restrict__ in, int S, long long np, int s0, int ns,
+                                      double2 *__restrict__ out) {
+  const long long n = np * ns;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long k = i / np, pt = i % np;
+    const C2<R> v = in[pt * S + s0 + k];
+    out[i] = make_double2(double(v.x), double(v.y));
+  }
+}
+// the reverse: out[pt][s0 + k] = in[k][pt]
+template <typename R>
+__global__ void insert_states_kernel(const double2 *__restrict__ in, int S, long long np, int s0, int ns,
+                                     C2<R> *__restrict__ out) {
+  const long long n = np * ns;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long k = i / np, pt = i % np;
+    const double2 v = in[i];
+    out[pt * S + s0 + k] = mk<C2<R>>(R(v.x), R(v.y));
+  }
+}
+template <typename R>
+void launch_extract_states(Ctx &ctx, const C2<R> *in, int S, long long np, int s0, int ns, double2 *out) {
+  extract_states_kernel<R><<<grid_for(np * ns, 256), 256, 0, ctx.stream>>>(in, S, np, s0, ns, out);
+  LAUNCHED(ctx);
+}
+template <typename R>
+void launch_insert_states(Ctx &ctx, const double2 *in, int S, long long np, int s0, int ns, C2<R> *out) {
+  insert_states_kernel<R><<<grid_for(np * ns, 256), 256, 0, ctx.stream>>>(in, S, np, s0, ns, out);
+  LAUNCHED(ctx);
+}
+
 // ------------------------------------------------------------------ interacting potential
 // (solvers/poisson.hpp, hamiltonian/xc_term.hpp, hamiltonian/self_consistency.hpp)
 
@@ -807,6 +841,8 @@ void launch_ks_potential(Ctx &ctx, const double *n, const double *vion, const do
   template void launch_axpy<R>(Ctx &, C2<R> *, const C2<R> *, long long, double, double);                          \
   template void launch_shift_vec<R>(Ctx &, C2<R> *, const C2<R> *, int, long long, const double *, double);        \
   template void launch_shift_cvec<R>(Ctx &, C2<R> *, const C2<R> *, int, long long, const double2 *, double);      \
+  template void launch_extract_states<R>(Ctx &, const C2<R> *, int, long long, int, int, double2 *);               \
+  template void launch_insert_states<R>(Ctx &, const double2 *, int, long long, int, int, C2<R> *);                \
   template void launch_tpa_precondition<R>(Ctx &, const Basis &, C2<R> *, int, const double *);                    \
   template void launch_laplacian<R>(Ctx &, const Basis &, const C2<R> *, C2<R> *, int, double, const double *);    \
   template void launch_overlap_diag<R>(Ctx &, const C2<R> *, const C2<R> *, int, long long, double, double2 *);    \
