@@ -7,6 +7,8 @@
 //   inq::operations::transform::to_fourier / to_real (src/operations/transform.hpp:186-249)
 //   inq::operations::overlap_diagonal, orthogonalize, exponential (operations/*.hpp)
 //   inq::real_time::etrs            (src/real_time/etrs.hpp:22-79)
+//   inq::operations::io::save/load  (src/operations/io.hpp:172-215)
+//   inq::eigensolvers::steepest_descent (src/eigensolvers/steepest_descent.hpp:23-86)
 //
 // Handles are RAII and move-only; failures throw inq::b200::error with the library's message.
 // Orbital data cross the boundary as [npoint][nst] std::complex<double> (field_set::matrix()).
@@ -222,12 +224,29 @@ inline std::vector<std::complex<double>> overlap_diagonal(states::orbital_set co
 inline void orthogonalize(states::orbital_set &phi) {
   b200::check(inqb_orthogonalize(phi.get()), phi.basis().ctx().get());
 }
+namespace io {
+// operations::io::save / load (io.hpp:172-215): one complex128 file per state in dirname
+inline void save(std::string const &dirname, states::orbital_set const &phi) {
+  b200::check(inqb_orbitals_save(phi.get(), dirname.c_str()), phi.basis().ctx().get());
+}
+inline void load(std::string const &dirname, states::orbital_set &phi) {
+  b200::check(inqb_orbitals_load(phi.get(), dirname.c_str()), phi.basis().ctx().get());
+}
+}  // namespace io
 inline void exponential_in_place(hamiltonian::ks_hamiltonian const &ham, std::complex<double> factor,
                                  states::orbital_set &phi, int order = 4) {
   b200::check(inqb_exponential_in_place(ham.get(), factor.real(), factor.imag(), phi.get(), order),
               phi.basis().ctx().get());
 }
 }  // namespace operations
+
+namespace eigensolvers {
+// eigensolvers::steepest_descent with the TPA preconditioner, then orthogonalize (steepest_descent.hpp:23-86);
+// fphi is a Fourier-space set
+inline void steepest_descent(hamiltonian::ks_hamiltonian const &ham, states::orbital_set &fphi) {
+  b200::check(inqb_steepest_descent(ham.get(), fphi.get()), fphi.basis().ctx().get());
+}
+}  // namespace eigensolvers
 
 namespace real_time {
 // one ETRS step of one orbital set with a fixed Hamiltonian; returns the electronic dipole
