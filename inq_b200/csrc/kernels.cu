@@ -85,63 +85,96 @@ void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[
 
 // ------------------------------------------------------------------ nonlocal projection
 // proj[p][l][s] = sum_i gcoef[p][i][l] * psi[pt_i][s]; projD = coeff[p] . proj
-// (projector_all.hpp:113-211).  CTA = (projector p, 32 states); each of 16 warps takes a
-// contiguous run of the sphere points, reads 32 point indices with one coalesced load and
-// hands them out by shuffles, keeping 8 row loads in flight; lanes are consecutive states
-// so each row load is one contiguous segment of the state-fastest layout.  The 16 warp
-// partials are summed in order.
-template <typename R, typename A>
-__global__ void __launch_bounds__(512, 2) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
-                                                         const int *__restrict__ pt, const C2<A> *__restrict__ gcoef,
-                                                         const int *__restrict__ npts, const A *__restrict__ coeff,
-                                                         int maxsph, C2<R> *projraw, C2<R> *projD) {
+// (projector_all.hpp:113-211).  Stage 1: CTA = (projector p, range rg of its sphere points, chunk of
+// 32 K states); each of its 8 warps takes a contiguous run of the range, reads 32 point indices with
+// one coalesced load and hands them out by shuffles, and keeps NP points in flight; a lane holds K
+// states 32 apart, so each point costs K contiguous 256-byte segments of the state-fastest row.  The
+// warp partials are summed in order into partial[p][rg][l][s].  Stage 2 sums the ranges in order and
+// applies the KB coefficients.
+constexpr int NLP_WARPS = 8, NLP_RANGES = 8;
+
+template <typename R, typename A, int K>
+__global__ void __launch_bounds__(NLP_WARPS * 32) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
+                                                                    const int *__restrict__ pt,
+                                                                    const C2<A> *__restrict__ gcoef,
+                                                                    const int *__restrict__ npts, int maxsph,
+                                                                    C2<A> *__restrict__ partial) {
   using T = C2<R>;
   using TA = C2<A>;
-  constexpr int NW = 16;  // warps per CTA, each over a contiguous run of the sphere points
-  constexpr int UN = 8;   // independent row loads in flight per warp
-  __shared__ TA part[NW][4][32];
-  const int p = blockIdx.x;
+  constexpr int NP = 4;  // points in flight per warp
+  __shared__ TA part[NLP_WARPS][4][32 * K];
+  const int p = blockIdx.x, rg = blockIdx.y;
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-  const int s = blockIdx.y * 32 + lane;
-  const bool active = s < S;
+  const int sbase = blockIdx.z * 32 * K;
   const int np = npts[p];
-  const int per = (np + NW - 1) / NW;
-  const int i0 = wp * per, i1 = min(np, i0 + per);
-  TA acc[4];
+  const int rper = (np + NLP_RANGES - 1) / NLP_RANGES;
+  const int r0 = rg * rper, r1 = min(np, r0 + rper);
+  const int per = (max(r1 - r0, 0) + NLP_WARPS - 1) / NLP_WARPS;
+  const int i0 = r0 + wp * per, i1 = min(r1, i0 + per);
+  TA acc[K][4];
 #pragma unroll
-  for (int l = 0; l < 4; l++) acc[l] = mk<TA>(A(0), A(0));
+  for (int k = 0; k < K; k++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) acc[k][l] = mk<TA>(A(0), A(0));
   const long long rowbase = (long long)p * maxsph;
   for (int base = i0; base < i1; base += 32) {
-    // 32 point indices with one coalesced load, handed out by shuffles
     const int cnt = min(32, i1 - base);
     const int qv = lane < cnt ? __ldg(&pt[rowbase + base + lane]) : 0;
-    for (int j = 0; j < cnt; j += UN) {
-      T x[UN];
+    for (int j = 0; j < cnt; j += NP) {
+      T x[NP][K];
 #pragma unroll
-      for (int u = 0; u < UN; u++) {
-        const int q = __shfl_sync(0xffffffffu, qv, (j + u) & 31);
-        x[u] = (active && j + u < cnt) ? psi[(long long)q * S + s] : mk<T>(R(0), R(0));
+      for (int u = 0; u < NP; u++) {
+        const long long q = __shfl_sync(0xffffffffu, qv, (j + u) & 31);
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const int s = sbase + k * 32 + lane;
+          x[u][k] = (j + u < cnt && s < S) ? psi[q * S + s] : mk<T>(R(0), R(0));
+        }
       }
 #pragma unroll
-      for (int u = 0; u < UN; u++) {
+      for (int u = 0; u < NP; u++) {
         if (j + u < cnt) {
-          const TA v = mk<TA>(A(x[u].x), A(x[u].y));
           const TA *g = gcoef + (rowbase + base + j + u) * 4;
+          TA gl[4];
 #pragma unroll
-          for (int l = 0; l < 4; l++) acc[l] = cadd(acc[l], cmul(g[l], v));
+          for (int l = 0; l < 4; l++) gl[l] = g[l];
+#pragma unroll
+          for (int k = 0; k < K; k++) {
+            const TA v = mk<TA>(A(x[u][k].x), A(x[u][k].y));
+#pragma unroll
+            for (int l = 0; l < 4; l++) acc[k][l] = cadd(acc[k][l], cmul(gl[l], v));
+          }
         }
       }
     }
   }
 #pragma unroll
-  for (int l = 0; l < 4; l++) part[wp][l][lane] = acc[l];
+  for (int k = 0; k < K; k++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) part[wp][l][k * 32 + lane] = acc[k][l];
   __syncthreads();
-  if (wp == 0 && active) {
+  for (int e = threadIdx.x; e < 4 * 32 * K; e += blockDim.x) {
+    const int l = e / (32 * K), sl = e % (32 * K);
+    const int s = sbase + sl;
+    TA t = part[0][l][sl];
+    for (int w = 1; w < NLP_WARPS; w++) t = cadd(t, part[w][l][sl]);
+    if (s < S) partial[(((long long)p * NLP_RANGES + rg) * 4 + l) * S + s] = t;
+  }
+}
+
+template <typename R, typename A>
+__global__ void nl_project_finish_kernel(const C2<A> *__restrict__ partial, int nproj, int S,
+                                         const A *__restrict__ coeff, C2<R> *projraw, C2<R> *projD) {
+  using T = C2<R>;
+  using TA = C2<A>;
+  const long long n = (long long)nproj * S;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int p = int(e / S), s = int(e % S);
     TA pr[4];
 #pragma unroll
     for (int l = 0; l < 4; l++) {
-      TA t = part[0][l][lane];
-      for (int k = 1; k < NW; k++) t = cadd(t, part[k][l][lane]);
+      TA t = partial[(((long long)p * NLP_RANGES) * 4 + l) * S + s];
+      for (int rg = 1; rg < NLP_RANGES; rg++) t = cadd(t, partial[(((long long)p * NLP_RANGES + rg) * 4 + l) * S + s]);
       pr[l] = t;
       projraw[((long long)p * 4 + l) * S + s] = mk<T>(R(t.x), R(t.y));
     }
@@ -160,16 +193,29 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
                        C2<R> *projD) {
   const Projectors &P = h.proj;
   if (P.nproj == 0) return;
-  dim3 grid(P.nproj, (S + 31) / 32);
-  if (sizeof(R) == 8 || ctx.mixed_compute != 0) {
-    // double-precision coefficients and accumulation
-    nl_project_kernel<R, double><<<grid, 512, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef, P.d_npts, P.d_coeff,
-                                                                P.maxsph, projraw, projD);
+  const bool dbl = sizeof(R) == 8 || ctx.mixed_compute != 0;  // double-precision coefficients and sums
+  const size_t pbytes = size_t(P.nproj) * NLP_RANGES * 4 * S * (dbl ? sizeof(double2) : sizeof(float2));
+  void *partial = dev_alloc(ctx, pbytes);
+  const long long fin = (long long)P.nproj * S;
+  if (dbl) {
+    constexpr int K = 2;
+    dim3 grid(P.nproj, NLP_RANGES, (S + 32 * K - 1) / (32 * K));
+    nl_project_kernel<R, double, K><<<grid, NLP_WARPS * 32, 0, ctx.stream>>>(
+        psi, S, P.d_pt, P.d_gcoef, P.d_npts, P.maxsph, static_cast<double2 *>(partial));
+    LAUNCHED(ctx);
+    nl_project_finish_kernel<R, double><<<grid_for(fin, 256), 256, 0, ctx.stream>>>(
+        static_cast<const double2 *>(partial), P.nproj, S, P.d_coeff, projraw, projD);
   } else {
-    nl_project_kernel<R, float><<<grid, 512, 0, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef32, P.d_npts, P.d_coeff32,
-                                                               P.maxsph, projraw, projD);
+    constexpr int K = 4;
+    dim3 grid(P.nproj, NLP_RANGES, (S + 32 * K - 1) / (32 * K));
+    nl_project_kernel<R, float, K><<<grid, NLP_WARPS * 32, 0, ctx.stream>>>(
+        psi, S, P.d_pt, P.d_gcoef32, P.d_npts, P.maxsph, static_cast<float2 *>(partial));
+    LAUNCHED(ctx);
+    nl_project_finish_kernel<R, float><<<grid_for(fin, 256), 256, 0, ctx.stream>>>(
+        static_cast<const float2 *>(partial), P.nproj, S, P.d_coeff32, projraw, projD);
   }
   LAUNCHED(ctx);
+  dev_free(ctx, partial);
 }
 
 // out[pt][s] = nonlocal term (ks_hamiltonian::non_local, ks_hamiltonian.hpp:106-120)
