@@ -71,7 +71,6 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void 
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 using ptx::fence_proxy_async;
 
@@ -534,21 +533,9 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
       coords(t, c0, c1, c2, c3);
       tma_store_4d(&map_out, buf, c0, c1, c2, c3);
       bulk_commit();
-      // A stage is refilled once its store has read it.  With three or more stages the refill waits
-      // for the previous tile's store instead of this one's, so the elected thread does not hold the
-      // next tile's barrier for a store drain (prefetch distance NS - 1); with two stages it waits for
-      // this tile's store (distance 2).
-      if (NS >= 3) {
-        if (i >= 1) {
-          bulk_wait_read1();
-          const long long tn = (t - gridDim.x) + (long long)NS * gridDim.x;
-          if (tn < gg.ntiles) issue((i - 1) % NS, tn);
-        }
-      } else {
-        bulk_wait_read0();
-        const long long tn = t + (long long)NS * gridDim.x;
-        if (tn < gg.ntiles) issue(st, tn);
-      }
+      bulk_wait_read0();  // the stage may be refilled once the store has read it
+      const long long tn = t + (long long)NS * gridDim.x;
+      if (tn < gg.ntiles) issue(st, tn);
     }
   }
   if (threadIdx.x == 0) bulk_wait0();
