@@ -765,6 +765,11 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, Geo
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;
   gg.stages = ggb.stages = ns;
+  // state blocks of this kernel's tile width (128-byte rows when the butterflies are wider than the data)
+  for (Geom2 *G : {&gg, &ggb}) {
+    G->nsb = (a.S + W - 1) / W;
+    G->ntiles = (b.npoints / b.n[G->axis]) * G->nsb;
+  }
   const size_t smem = TILE_BYTES * nbuf * ns + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
   auto kern = fft2_kernel<R, CR, N, VAR, VARB>;
