@@ -65,10 +65,7 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * inqb_orthogonalize and inqb_subspace_diagonalization -- on the tensor cores as split-BF16
  * products with FP32 accumulation and an FP64 sum of the per-SM partials; 16 significant bits
  * per value, so |error of S_ij| stays near 2^-16 |a_i| |b_j| / sqrt(npoint)) or 0 (FP64 SIMT
- * products, as for double-precision sets); "fft_pair" = 1 (default: where the y and z lines have
- * the same length, the forward z and y passes of H run as one launch, and so do the inverse y and z
- * passes, the second pass of each x plane reading the first one's output from L2; the arithmetic
- * per tile is that of one launch per pass) or 0. */
+ * products, as for double-precision sets). */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Free and total device memory in bytes (admission control for serving). */
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);

@@ -141,18 +141,14 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   PassArgs<R> a;
   a.S = S;
   a.dir = +1;
-  // forward z, y: one fused launch where covered (y reads the z output of each x plane from L2)
-  if (!launch_fft2_pair<R>(ctx, b, a, 2, 1, false, psi, hpsi, hpsi, hpsi)) {
-    a.axis = 2;
-    a.in = psi;
-    a.out = hpsi;
-    launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
-    a.axis = 1;
-    a.in = hpsi;
-    launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
-  }
-  a.in = hpsi;
+  // forward z, y
+  a.axis = 2;
+  a.in = psi;
   a.out = hpsi;
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
+  a.axis = 1;
+  a.in = hpsi;
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   // x: forward, kinetic factor -0.5*(-|G|^2 + gc.G), gc = -2 (k+A)^contra, backward; the 1/N of the
   // inverse transform is folded into the per-point factor (formed in double, rounded once)
   a.axis = 0;
@@ -161,8 +157,10 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   for (int i = 0; i < 3; i++) a.gc[i] = -2.0 * kc[i];
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   a.mid_kinetic = 0;
-  // backward y, then z with the real-space epilogue (fused where covered, as the forward pair)
+  // backward y, then z with the real-space epilogue
   a.dir = -1;
+  a.axis = 1;
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   a.axis = 2;
   a.psi = psi;
   if constexpr (sizeof(R) == 8) a.V = h.d_V;
@@ -174,15 +172,7 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   a.acc2 = static_cast<C2<R> *>(acc.acc2);
   a.c1 = mk<C2<R>>(R(acc.c1[0]), R(acc.c1[1]));
   a.c2 = mk<C2<R>>(R(acc.c2[0]), R(acc.c2[1]));
-  if (!launch_fft2_pair<R>(ctx, b, a, 1, 2, true, hpsi, hpsi, hpsi, hpsi)) {
-    PassArgs<R> y = a;
-    y.axis = 1;
-    y.psi = nullptr;
-    y.V = nullptr;
-    y.acc1 = y.acc2 = nullptr;
-    launch_fft_pass<R>(ctx, b, y, PRO_NONE, EPI_STORE);
-    launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_FINAL_REAL);
-  }
+  launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_FINAL_REAL);
   // nonlocal term added at the sphere points (and to the Taylor accumulators) by its own kernel: as a
   // fully occupied kernel of its own it hides the latency of the hit-table and projection reads, which
   // stall the FFT epilogue
@@ -838,9 +828,6 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     } else if (k == "mixed_compute") {
       INQB_REQUIRE(value >= 0 && value <= 3, INQB_ERR_ARG, "mixed_compute is 0, 1, 2 or 3");
       ctx->mixed_compute = int(value);
-    } else if (k == "fft_pair") {
-      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_pair is 0 (one launch per pass) or 1 (fused pairs)");
-      ctx->fft_pair = int(value);
     } else if (k == "overlap_tc") {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "overlap_tc is 0 (FP64 SIMT) or 1 (tensor cores)");
       ctx->overlap_tc = int(value);

@@ -17,8 +17,6 @@
 
 #include <cuda.h>
 
-#include <type_traits>
-
 #include "fft_common.cuh"
 #include "ptx.cuh"
 
@@ -74,9 +72,6 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait1() { asm volatile("cp.async.bulk.wait_group 1;" ::: "memory"); }
-// orders this thread's completed async-proxy global accesses with its following generic ones and back
-__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 using ptx::fence_proxy_async;
 
 // ------------------------------------------------------------------ register codelets (compile-time size)
@@ -374,72 +369,19 @@ template <typename R, typename CR, int N, int VAR> constexpr int min_ctas_of() {
   return (VAR == MID_KIN && sizeof(R) == 4 && sizeof(CR) == 4 && N <= 96) ? 4 : 0;
 }
 
-// Schedule of one launch.  Single pass: tile u is tile u of the pass.  Fused pair of passes over two
-// axes of the same line length (z then y, or y then z): the tiles of both passes are ordered by x
-// plane, pass A's tiles of plane j preceding pass B's tiles of plane j by `lag` planes, so B reads A's
-// output while it is still in L2 instead of from HBM.  A B tile starts only after every A tile of its
-// plane has been stored: the CTA that stored an A tile counts it in done[plane] once the store has
-// completed, and the load of a B tile waits (bounded) for the count.
-struct PairSched {
-  int pair = 0;
-  long long pa = 0, pb = 0;  // tiles per x plane of pass A and of pass B
-  int nplanes = 0, lag = 0;
-  long long total = 0;       // tiles of the launch
-  unsigned *done = nullptr;  // [nplanes] completed pass-A tiles per plane
-};
-
-__device__ __forceinline__ void sched_decode(const PairSched &ps, long long u, int &pass, long long &t) {
-  if (!ps.pair) {
-    pass = 0;
-    t = u;
-    return;
-  }
-  const int lag = ps.lag < ps.nplanes ? ps.lag : ps.nplanes;
-  const long long headA = (long long)lag * ps.pa;  // steps 0 .. lag - 1: A planes only
-  if (u < headA) {
-    pass = 0;
-    t = u;
-    return;
-  }
-  u -= headA;
-  const int nboth = ps.nplanes - lag;               // steps with an A plane and a B plane
-  const long long per = ps.pa + ps.pb;
-  if (u < (long long)nboth * per) {
-    const long long k = u / per, r = u % per;
-    if (r < ps.pa) {
-      pass = 0;
-      t = (lag + k) * ps.pa + r;
-    } else {
-      pass = 1;
-      t = k * ps.pb + (r - ps.pa);
-    }
-    return;
-  }
-  u -= (long long)nboth * per;
-  pass = 1;                                          // the last lag B planes
-  t = (long long)nboth * ps.pb + u;
-}
-
-template <int V> using vtag = std::integral_constant<int, V>;
-
-// VARB < 0: one pass of variant VAR over gg.  VARB >= 0: the fused pair (VAR over gg, then VARB over
-// ggb) scheduled by ps; the scale and the Taylor accumulators belong to the second pass.
-template <typename R, typename CR, int N, int VAR, int VARB>
-__global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR, N, VAR>())
-    fft2_kernel(const __grid_constant__ CUtensorMap map_in, const __grid_constant__ CUtensorMap map_out,
-                const __grid_constant__ CUtensorMap map_aux, const __grid_constant__ CUtensorMap map_in_b,
-                const __grid_constant__ CUtensorMap map_out_b, PassArgs<R> a, Geom2 gg, Geom2 ggb, PairSched ps,
-                const C2<CR> *__restrict__ twg, int *err) {
+template <typename R, typename CR, int N, int VAR>
+__global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR, N, VAR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
+                                                   const __grid_constant__ CUtensorMap map_out,
+                                                   const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
+                                                   const C2<CR> *__restrict__ twg, int *err) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr bool PAIR = VARB >= 0;
   constexpr int NT = threads_of<R, CR, N, VAR>();
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);    // exchange buffer in the arithmetic type
   constexpr int W = tile_w<R, CR>();
   constexpr int TILE = N * W;                       // complex elements per tile
   constexpr uint32_t TILE_BYTES = TILE * sizeof(T);
-  constexpr bool AUXA = has_aux(VAR), AUXB = PAIR && has_aux(VARB >= 0 ? VARB : 0);
-  constexpr bool AUX = AUXA || AUXB;
+  constexpr bool AUX = has_aux(VAR);
   const int NS = gg.stages;
 
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -452,6 +394,7 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
   uint64_t *bar = reinterpret_cast<uint64_t *>(tw + TWN + N);        // NS barriers (8-byte aligned)
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar + NS);
 
+  const Geom &g = gg.g;
   for (int i = threadIdx.x; i < TWN; i += NT) tw[i] = twg[i];
   if (threadIdx.x == 0) {
     *abort_flag = 0;
@@ -460,103 +403,70 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
   }
   __syncthreads();
 
-  auto coords = [&](const Geom2 &G, long long t, int &c0, int &c1, int &c2, int &c3) {
-    const long long L = t / G.nsb;
-    const int s0 = int(t % G.nsb) * W;
-    const int la = int(L / G.g.nb), lb = int(L % G.g.nb);
-    c0 = s0 * G.cwords;
-    if (G.axis == 2) { c1 = 0; c2 = lb; c3 = la; }        // z-lines: (x, y) fixed
-    else if (G.axis == 1) { c1 = lb; c2 = 0; c3 = la; }   // y-lines: (x, z) fixed
+  auto coords = [&](long long t, int &c0, int &c1, int &c2, int &c3) {
+    const long long L = t / gg.nsb;
+    const int s0 = int(t % gg.nsb) * W;
+    const int la = int(L / g.nb), lb = int(L % g.nb);
+    c0 = s0 * gg.cwords;
+    if (gg.axis == 2) { c1 = 0; c2 = lb; c3 = la; }        // z-lines: (x, y) fixed
+    else if (gg.axis == 1) { c1 = lb; c2 = 0; c3 = la; }   // y-lines: (x, z) fixed
     else { c1 = lb; c2 = la; c3 = 0; }                     // x-lines: (y, z) fixed
   };
-  // loads tile u into stage st (thread 0); a pass-B tile whose plane is not complete yet is left
-  // pending when `block` is false, and waited for (bounded) when it is true
-  long long pend[8];
-#pragma unroll
-  for (int k = 0; k < 8; k++) pend[k] = -1;
-  int sig_plane = -1;  // plane of the last pass-A tile whose store is not yet known to be complete
-  auto signal_done = [&]() {
-    if (sig_plane >= 0) {
-      fence_proxy_async_global();
-      __threadfence();
-      atomicAdd(&ps.done[sig_plane], 1u);
-      sig_plane = -1;
-    }
-  };
-  auto issue = [&](int st, long long u, bool block) {
-    int pass;
-    long long t;
-    sched_decode(ps, u, pass, t);
-    if constexpr (PAIR) {
-      if (pass == 1) {
-        const int plane = int(t / ps.pb);
-        volatile unsigned *cnt = ps.done + plane;
-        if (*cnt < unsigned(ps.pa)) {
-          if (!block) {
-            pend[st] = u;
-            return;
-          }
-          bulk_wait0();  // this CTA's own stored A tiles count too
-          signal_done();
-          const uint64_t t0 = global_ns();
-          while (*cnt < unsigned(ps.pa)) {
-            if (global_ns() - t0 > 2000000000ull) {
-              *abort_flag = 1;
-              atomicExch(err, 1);
-              return;
-            }
-          }
-        }
-        __threadfence();
-        fence_proxy_async_global();
-      }
-    }
+  auto issue = [&](int st, long long t) {
     int c0, c1, c2, c3;
-    const bool aux_here = PAIR ? (pass == 0 ? AUXA : AUXB) : AUXA;
-    mbar_expect_tx(&bar[st], aux_here ? 2 * TILE_BYTES : TILE_BYTES);
-    if (pass == 0) {
-      coords(gg, t, c0, c1, c2, c3);
-      tma_load_4d(stage_in + size_t(st) * TILE, &map_in, &bar[st], c0, c1, c2, c3);
-    } else {
-      coords(ggb, t, c0, c1, c2, c3);
-      tma_load_4d(stage_in + size_t(st) * TILE, &map_in_b, &bar[st], c0, c1, c2, c3);
-    }
-    if (aux_here) tma_load_4d(stage_aux + size_t(st) * TILE, &map_aux, &bar[st], c0, c1, c2, c3);
+    coords(t, c0, c1, c2, c3);
+    mbar_expect_tx(&bar[st], AUX ? 2 * TILE_BYTES : TILE_BYTES);
+    tma_load_4d(stage_in + size_t(st) * TILE, &map_in, &bar[st], c0, c1, c2, c3);
+    if constexpr (AUX) tma_load_4d(stage_aux + size_t(st) * TILE, &map_aux, &bar[st], c0, c1, c2, c3);
   };
 
-  const long long ntot = PAIR ? ps.total : gg.ntiles;
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; s++) {
-      const long long u = blockIdx.x + (long long)s * gridDim.x;
-      if (u < ntot) issue(s, u, false);
+      const long long t = blockIdx.x + (long long)s * gridDim.x;
+      if (t < gg.ntiles) issue(s, t);
     }
   }
 
   const bool scaled = a.scale != 1.0;
   const bool accum = (a.acc1 != nullptr) || (a.acc2 != nullptr);
+  int i = 0;
+  for (long long t = blockIdx.x; t < gg.ntiles; t += gridDim.x, i++) {
+    const int st = i % NS;
+    const uint32_t par = uint32_t(i / NS) & 1u;
+    // bounded wait for this stage's TMA load
+    {
+      const uint64_t t0 = global_ns();
+      while (!mbar_try_wait(&bar[st], par)) {
+        if (*abort_flag) break;
+        if (global_ns() - t0 > 2000000000ull) {
+          *abort_flag = 1;
+          atomicExch(err, 1);
+          break;
+        }
+      }
+    }
+    __syncthreads();
+    if (*abort_flag) break;
 
-  // one tile of variant V over geometry G; `last`: the pass that owns the scale and the accumulators
-  auto body = [&](auto vt, const Geom2 &G, long long t, T *buf, const T *aux, bool last) {
-    constexpr int V = decltype(vt)::value;
-    const Geom &g = G.g;
-    const long long L = t / G.nsb;
-    const int s0 = int(t % G.nsb) * W;
+    T *buf = stage_in + size_t(st) * TILE;
+    const T *aux = stage_aux + size_t(st) * TILE;
+    const long long L = t / gg.nsb;
+    const int s0 = int(t % gg.nsb) * W;
     const int la = int(L / g.nb), lb = int(L % g.nb);
     const long long pbase = la * g.sa + lb * g.sb;
-    const bool sc = scaled && last, acc = accum && last;
 
     // per-point factors of this line (consumed after the first barrier of the transform)
-    if constexpr (V == MID_KIN || V == FWD_LAPLADD) {
+    if constexpr (VAR == MID_KIN || VAR == FWD_LAPLADD) {
       for (int m = threadIdx.x; m < N; m += NT) {
         int ix, iy, iz;
-        line_coords(G.axis, la, lb, m, ix, iy, iz);
+        line_coords(gg.axis, la, lb, m, ix, iy, iz);
         linev[m] = CR(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc));
       }
-    } else if constexpr (V == INV_FINAL || V == FWD_VPSI) {
+    } else if constexpr (VAR == INV_FINAL || VAR == FWD_VPSI) {
       for (int m = threadIdx.x; m < N; m += NT)
         linev[m] = CR(a.V[(pbase + m * g.sp) * a.nspin + a.spin]) + CR(a.vshift);
     }
-    if constexpr (V == FWD_VPSI) {
+    if constexpr (VAR == FWD_VPSI) {
       __syncthreads();
       if (a.nl_offs) {
         // Fourier-form operator: (V + shift) psi + nonlocal(psi) formed in shared memory before the transform
@@ -575,22 +485,21 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
     // final store of one output value: epilogue terms, Taylor accumulators, write into the stage
     auto put_out = [&](int m, int w, TC v) {
       const int s = s0 + w;
-      if (sc) v = kscale(v, a.scale);
-      if constexpr (V == INV_FINAL || V == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
+      if (scaled) v = kscale(v, a.scale);
+      if constexpr (VAR == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
       const T o = conv<T>(v);
-      if (acc && s < a.S) {
+      if (accum && s < a.S) {
         const long long ge = (pbase + m * g.sp) * a.S + s;
         if (a.acc1) a.acc1[ge] = cadd(a.acc1[ge], cmul(a.c1, o));
         if (a.acc2) a.acc2[ge] = cadd(a.acc2[ge], cmul(a.c2, o));
       }
       buf[m * W + w] = o;
     };
-    const CR *pre = (V == FWD_VPSI && !a.nl_offs) ? linev : nullptr;
-    constexpr int D = dir_first<V>();
-    constexpr bool AUXV = has_aux(V);
+    const CR *pre = (VAR == FWD_VPSI && !a.nl_offs) ? linev : nullptr;
+    constexpr int D = dir_first<VAR>();
 
     if constexpr (SPLIT) {
-      if constexpr (V == MID_KIN) {
+      if constexpr (VAR == MID_KIN) {
         // forward, multiply by the kinetic factor, backward
         tile_dft<N, +1, W, NT, true, TC>(buf, exch, tw, (const CR *)nullptr,
                                          [&](int m, int w, TC v) { exch[m * W + w] = cscale(v, linev[m]); });
@@ -599,89 +508,37 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
         tile_dft<N, D, W, NT, false, TC>(buf, exch, tw, pre, put_out);
       }
     } else {
-      if constexpr (V == FWD_VPSI) {
+      if constexpr (VAR == FWD_VPSI) {
         if (!a.nl_offs) {
           for (int e = threadIdx.x; e < TILE; e += NT) buf[e] = cscale(buf[e], linev[e / W]);
           __syncthreads();
         }
       }
       tile_dft_inplace<N, D, W, NT, T>(buf, reinterpret_cast<const T *>(tw));
-      if constexpr (V == MID_KIN) {
+      if constexpr (VAR == MID_KIN) {
         for (int e = threadIdx.x; e < TILE; e += NT) buf[e] = cscale(buf[e], linev[e / W]);
         __syncthreads();
         tile_dft_inplace<N, -1, W, NT, T>(buf, reinterpret_cast<const T *>(tw));
       }
-      if (sc || AUXV || acc) {
+      if (scaled || AUX || accum) {
         for (int e = threadIdx.x; e < TILE; e += NT) put_out(e / W, e % W, buf[e]);
         __syncthreads();
       }
-    }
-  };
-
-  int i = 0;
-  for (long long u = blockIdx.x; u < ntot; u += gridDim.x, i++) {
-    const int st = i % NS;
-    const uint32_t par = uint32_t(i / NS) & 1u;
-    if constexpr (PAIR) {
-      if (threadIdx.x == 0 && pend[st] >= 0) {
-        const long long up = pend[st];
-        pend[st] = -1;
-        issue(st, up, true);
-      }
-    }
-    // bounded wait for this stage's TMA load
-    {
-      const uint64_t t0 = global_ns();
-      while (!mbar_try_wait(&bar[st], par)) {
-        if (*abort_flag) break;
-        if (global_ns() - t0 > 2000000000ull) {
-          *abort_flag = 1;
-          atomicExch(err, 1);
-          break;
-        }
-      }
-    }
-    __syncthreads();
-    if (*abort_flag) break;
-
-    T *buf = stage_in + size_t(st) * TILE;
-    const T *aux = stage_aux + size_t(st) * TILE;
-    int pass;
-    long long t;
-    sched_decode(ps, u, pass, t);
-    if constexpr (PAIR) {
-      if (pass == 0) body(vtag<VAR>{}, gg, t, buf, aux, false);
-      else body(vtag<(VARB >= 0 ? VARB : 0)>{}, ggb, t, buf, aux, true);
-    } else {
-      body(vtag<VAR>{}, gg, t, buf, aux, true);
     }
 
     fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0) {
       int c0, c1, c2, c3;
-      if (pass == 0) {
-        coords(gg, t, c0, c1, c2, c3);
-        tma_store_4d(&map_out, buf, c0, c1, c2, c3);
-      } else {
-        coords(ggb, t, c0, c1, c2, c3);
-        tma_store_4d(&map_out_b, buf, c0, c1, c2, c3);
-      }
+      coords(t, c0, c1, c2, c3);
+      tma_store_4d(&map_out, buf, c0, c1, c2, c3);
       bulk_commit();
-      if constexpr (PAIR) {
-        bulk_wait1();    // the previous tile's store has completed: count it if it was a pass-A tile
-        signal_done();
-        if (pass == 0) sig_plane = int(t / ps.pa);
-      }
       bulk_wait_read0();  // the stage may be refilled once the store has read it
-      const long long un = u + (long long)NS * gridDim.x;
-      if (un < ntot) issue(st, un, false);
+      const long long tn = t + (long long)NS * gridDim.x;
+      if (tn < gg.ntiles) issue(st, tn);
     }
   }
-  if (threadIdx.x == 0) {
-    bulk_wait0();
-    if constexpr (PAIR) signal_done();
-  }
+  if (threadIdx.x == 0) bulk_wait0();
 }
 
 }  // namespace v2
@@ -725,36 +582,13 @@ inline CUtensorMap orbital_map(const void *base, const Basis &b, int S, int cwor
   return m;
 }
 
-// Geometry of one pass over `axis`: line decomposition, state blocks of W, tile count.
-inline Geom2 pass_geom(const Basis &b, int axis, int S, int W, int cwords) {
-  Geom2 gg;
-  for (int i = 0; i < 3; i++) gg.g.n[i] = b.n[i];
-  for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++) gg.g.rlat[i][j] = b.rlat[i][j];
-  const long long ny = b.n[1], nz = b.n[2];
-  if (axis == 2) { gg.g.nb = int(ny); gg.g.sa = ny * nz; gg.g.sb = nz; gg.g.sp = 1; }
-  else if (axis == 1) { gg.g.nb = int(nz); gg.g.sa = ny * nz; gg.g.sb = 1; gg.g.sp = nz; }
-  else { gg.g.nb = int(nz); gg.g.sa = nz; gg.g.sb = 1; gg.g.sp = ny * nz; }
-  gg.axis = axis;
-  gg.nsb = (S + W - 1) / W;
-  gg.ntiles = (b.npoints / b.n[axis]) * gg.nsb;
-  gg.cwords = cwords;
-  gg.stages = 2;
-  return gg;
-}
-
-// One launch: a single pass (VARB < 0; inB / outB unused) or a fused pair of passes (axis gg.axis then
-// axis ggb.axis) over the x planes.
-template <typename R, typename CR, int N, int VAR, int VARB>
-void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, Geom2 ggb, const void *inA,
-                   void *outA, const void *inB, void *outB) {
+template <typename R, typename CR, int N, int VAR>
+void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr bool PAIR = VARB >= 0;
   constexpr int W = tile_w<R, CR>();
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
-  constexpr bool AUXA = has_aux(VAR), AUXB = PAIR && has_aux(VARB >= 0 ? VARB : 0);
-  const int nbuf = (AUXA || AUXB) ? 2 : 1;
+  const int nbuf = has_aux(VAR) ? 2 : 1;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
   constexpr int NT = threads_of<R, CR, N, VAR>();
   const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + size_t(tw_entries<CR>(N) + N) * sizeof(TC) + 64 + 16 * 8;
@@ -764,15 +598,12 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, Geo
   int ns = int((budget - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;
-  gg.stages = ggb.stages = ns;
-  // state blocks of this kernel's tile width (128-byte rows when the butterflies are wider than the data)
-  for (Geom2 *G : {&gg, &ggb}) {
-    G->nsb = (a.S + W - 1) / W;
-    G->ntiles = (b.npoints / b.n[G->axis]) * G->nsb;
-  }
+  gg.stages = ns;
+  gg.nsb = (a.S + W - 1) / W;
+  gg.ntiles = (b.npoints / b.n[gg.axis]) * gg.nsb;
   const size_t smem = TILE_BYTES * nbuf * ns + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
-  auto kern = fft2_kernel<R, CR, N, VAR, VARB>;
+  auto kern = fft2_kernel<R, CR, N, VAR>;
   // per instantiation: shared-memory attribute and occupancy, computed under a lock (several host
   // threads may drive contexts at once); the attribute only ever grows
   static std::mutex mtx;
@@ -787,55 +618,27 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, Geo
     }
     per_sm = occ_per_sm;
   }
-  PairSched ps;
-  const long long ntot = PAIR ? gg.ntiles + ggb.ntiles : gg.ntiles;
   long long grid = (long long)(per_sm < 1 ? 1 : per_sm) * ctx.num_sms;
-  if (grid > ntot) grid = ntot;
-  unsigned *done = nullptr;
-  if constexpr (PAIR) {
-    const int np = b.n[0];
-    ps.pair = 1;
-    ps.nplanes = np;
-    ps.pa = gg.ntiles / np;
-    ps.pb = ggb.ntiles / np;
-    ps.total = ntot;
-    // B tiles of a plane lag its A tiles by enough planes that their loads, issued NS tiles ahead,
-    // rarely wait; the A output of the planes in flight (lag + 1 of them) stays within ~60 MB of L2
-    const long long need = ((long long)(ns + 1) * grid + (ps.pa + ps.pb) - 1) / (ps.pa + ps.pb) + 1;
-    const size_t plane_bytes = size_t(b.npoints / np) * size_t(a.S) * sizeof(T);
-    long long cap = (long long)((60ull << 20) / (plane_bytes ? plane_bytes : 1)) - 1;
-    if (cap < 1) cap = 1;
-    long long lag = need < cap ? need : cap;
-    if (lag > np) lag = np;
-    ps.lag = int(lag);
-    done = static_cast<unsigned *>(dev_alloc(ctx, sizeof(unsigned) * np));
-    INQB_CUDA(cudaMemsetAsync(done, 0, sizeof(unsigned) * np, ctx.stream));
-    ps.done = done;
-  }
+  if (grid > gg.ntiles) grid = gg.ntiles;
   const int cwords = int(sizeof(T) / 4);
-  CUtensorMap mi = orbital_map(inA, b, a.S, cwords, gg.axis, W);
-  CUtensorMap mo = orbital_map(outA, b, a.S, cwords, gg.axis, W);
-  CUtensorMap mib = PAIR ? orbital_map(inB, b, a.S, cwords, ggb.axis, W) : mi;
-  CUtensorMap mob = PAIR ? orbital_map(outB, b, a.S, cwords, ggb.axis, W) : mo;
-  CUtensorMap mx = AUXA ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W)
-                        : (AUXB ? orbital_map(a.psi, b, a.S, cwords, ggb.axis, W) : mi);
+  CUtensorMap mi = orbital_map(a.in, b, a.S, cwords, gg.axis, W);
+  CUtensorMap mo = orbital_map(a.out, b, a.S, cwords, gg.axis, W);
+  CUtensorMap mx = has_aux(VAR) ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W) : mi;
   const TC *tw = reinterpret_cast<const TC *>(sizeof(CR) == 8 ? b.tw64[gg.axis] : b.tw32[gg.axis]);
-  kern<<<unsigned(grid), NT, smem, ctx.stream>>>(mi, mo, mx, mib, mob, a, gg, ggb, ps, tw, ctx.d_err);
+  kern<<<unsigned(grid), NT, smem, ctx.stream>>>(mi, mo, mx, a, gg, tw, ctx.d_err);
   INQB_CUDA(cudaGetLastError());
   ctx.launches++;
-  if (done) dev_free(ctx, done);
 }
 
 template <typename R, typename CR, int N>
 void launch_nc(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var) {
-  void *out = a.out;
   switch (var) {
-    case FWD_STORE: launch_kernel<R, CR, N, FWD_STORE, -1>(ctx, b, a, gg, gg, a.in, out, nullptr, nullptr); break;
-    case INV_STORE: launch_kernel<R, CR, N, INV_STORE, -1>(ctx, b, a, gg, gg, a.in, out, nullptr, nullptr); break;
-    case MID_KIN: launch_kernel<R, CR, N, MID_KIN, -1>(ctx, b, a, gg, gg, a.in, out, nullptr, nullptr); break;
-    case INV_FINAL: launch_kernel<R, CR, N, INV_FINAL, -1>(ctx, b, a, gg, gg, a.in, out, nullptr, nullptr); break;
-    case FWD_VPSI: launch_kernel<R, CR, N, FWD_VPSI, -1>(ctx, b, a, gg, gg, a.in, out, nullptr, nullptr); break;
-    default: launch_kernel<R, CR, N, FWD_LAPLADD, -1>(ctx, b, a, gg, gg, a.in, out, nullptr, nullptr); break;
+    case FWD_STORE: launch_kernel<R, CR, N, FWD_STORE>(ctx, b, a, gg); break;
+    case INV_STORE: launch_kernel<R, CR, N, INV_STORE>(ctx, b, a, gg); break;
+    case MID_KIN: launch_kernel<R, CR, N, MID_KIN>(ctx, b, a, gg); break;
+    case INV_FINAL: launch_kernel<R, CR, N, INV_FINAL>(ctx, b, a, gg); break;
+    case FWD_VPSI: launch_kernel<R, CR, N, FWD_VPSI>(ctx, b, a, gg); break;
+    default: launch_kernel<R, CR, N, FWD_LAPLADD>(ctx, b, a, gg); break;
   }
 }
 
@@ -857,16 +660,12 @@ void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var)
   launch_nc<R, double, N>(ctx, b, a, gg, var);
 }
 
-inline bool v2_length(int n) {
-  return n == 24 || n == 32 || n == 40 || n == 48 || n == 64 || n == 72 || n == 96 || n == 120 || n == 128;
-}
-
 // Returns false (and does nothing) when the pass is not covered by a specialised kernel.
 template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue) {
   using T = C2<R>;
   if (ctx.fft_impl == 1) return false;
   const int n = b.n[a.axis];
-  if (!v2_length(n)) return false;
+  if (n != 24 && n != 32 && n != 40 && n != 48 && n != 64 && n != 72 && n != 96 && n != 120 && n != 128) return false;
   if ((size_t(a.S) * sizeof(T)) % 16 != 0) return false;
   if (a.S < 256 / int(sizeof(T))) return false;  // fewer states than one 256-byte row: generic kernel
   int var;
@@ -878,7 +677,19 @@ template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a
   if ((var == INV_FINAL && a.dir > 0) || ((var == FWD_VPSI || var == FWD_LAPLADD) && a.dir < 0)) return false;
 
   constexpr int W = 256 / int(sizeof(T));
-  Geom2 gg = pass_geom(b, a.axis, a.S, W, int(sizeof(T) / 4));
+  Geom2 gg;
+  for (int i = 0; i < 3; i++) gg.g.n[i] = b.n[i];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) gg.g.rlat[i][j] = b.rlat[i][j];
+  const long long ny = b.n[1], nz = b.n[2];
+  if (a.axis == 2) { gg.g.nb = int(ny); gg.g.sa = ny * nz; gg.g.sb = nz; gg.g.sp = 1; }
+  else if (a.axis == 1) { gg.g.nb = int(nz); gg.g.sa = ny * nz; gg.g.sb = 1; gg.g.sp = nz; }
+  else { gg.g.nb = int(nz); gg.g.sa = nz; gg.g.sb = 1; gg.g.sp = ny * nz; }
+  gg.axis = a.axis;
+  gg.nsb = (a.S + W - 1) / W;
+  gg.ntiles = (b.npoints / n) * gg.nsb;
+  gg.cwords = int(sizeof(T) / 4);
+  gg.stages = 2;
   switch (n) {
     case 24: launch_n<R, 24>(ctx, b, a, gg, var); break;
     case 32: launch_n<R, 32>(ctx, b, a, gg, var); break;
@@ -889,45 +700,6 @@ template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a
     case 96: launch_n<R, 96>(ctx, b, a, gg, var); break;
     case 120: launch_n<R, 120>(ctx, b, a, gg, var); break;
     default: launch_n<R, 128>(ctx, b, a, gg, var); break;
-  }
-  return true;
-}
-
-template <typename R, int N>
-void launch_pair_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 ga, Geom2 gb, bool inverse,
-                   const void *inA, void *outA, const void *inB, void *outB) {
-  // same storage and arithmetic type in both passes (single-precision sets: mixed_compute 0)
-  if (inverse) launch_kernel<R, R, N, INV_STORE, INV_FINAL>(ctx, b, a, ga, gb, inA, outA, inB, outB);
-  else launch_kernel<R, R, N, FWD_STORE, FWD_STORE>(ctx, b, a, ga, gb, inA, outA, inB, outB);
-}
-
-// The fused pair of passes of the real-space operator: forward (FWD_STORE over axisA then axisB) or
-// inverse (INV_STORE over axisA, then INV_FINAL over axisB with the arguments of a).  Returns false
-// (and does nothing) when the pair is not covered: the two lines differ in length, the generic kernel
-// is selected, the states do not fill a 256-byte row, single-precision sets use FP64 butterflies in
-// either pass, or the context option fft_pair is 0.
-template <typename R>
-bool launch_pair(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int axisA, int axisB, bool inverse,
-                 const void *inA, void *outA, const void *inB, void *outB) {
-  using T = C2<R>;
-  if (ctx.fft_impl == 1 || !ctx.fft_pair) return false;
-  const int n = b.n[axisA];
-  if (n != b.n[axisB] || !v2_length(n)) return false;
-  if ((size_t(a.S) * sizeof(T)) % 16 != 0 || a.S < 256 / int(sizeof(T))) return false;
-  if (sizeof(R) == 4 && ctx.mixed_compute != 0) return false;
-  constexpr int W = 256 / int(sizeof(T));
-  Geom2 ga = pass_geom(b, axisA, a.S, W, int(sizeof(T) / 4));
-  Geom2 gb = pass_geom(b, axisB, a.S, W, int(sizeof(T) / 4));
-  switch (n) {
-    case 24: launch_pair_n<R, 24>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
-    case 32: launch_pair_n<R, 32>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
-    case 40: launch_pair_n<R, 40>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
-    case 48: launch_pair_n<R, 48>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
-    case 64: launch_pair_n<R, 64>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
-    case 72: launch_pair_n<R, 72>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
-    case 96: launch_pair_n<R, 96>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
-    case 120: launch_pair_n<R, 120>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
-    default: launch_pair_n<R, 128>(ctx, b, a, ga, gb, inverse, inA, outA, inB, outB); break;
   }
   return true;
 }

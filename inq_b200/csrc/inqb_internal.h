@@ -73,7 +73,6 @@ struct Ctx {
   int fft_stages = 0;        // shared-memory ring depth of the TMA FFT kernels (0: from the memory budget)
   int mixed_compute = 0;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
   int overlap_tc = 1;        // overlaps of single-precision sets on the tensor cores (split BF16)
-  int fft_pair = 1;          // fused z/y pass pairs in the real-space operator (L2-resident intermediate)
 };
 
 struct Basis {
@@ -185,17 +184,6 @@ void launch_fft_pass(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologu
 template <typename R> bool launch_fft2(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue);
 template <> bool launch_fft2<float>(Ctx &ctx, const Basis &b, const PassArgs<float> &a, int prologue, int epilogue);
 template <> bool launch_fft2<double>(Ctx &ctx, const Basis &b, const PassArgs<double> &a, int prologue, int epilogue);
-// fused pair of passes over two axes of equal length (fft2.cuh): forward (FWD_STORE, FWD_STORE) or
-// inverse (INV_STORE, then INV_FINAL with the arguments of a); false when not covered
-template <typename R>
-bool launch_fft2_pair(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int axisA, int axisB, bool inverse,
-                      const void *inA, void *outA, const void *inB, void *outB);
-template <>
-bool launch_fft2_pair<float>(Ctx &ctx, const Basis &b, const PassArgs<float> &a, int axisA, int axisB, bool inverse,
-                             const void *inA, void *outA, const void *inB, void *outB);
-template <>
-bool launch_fft2_pair<double>(Ctx &ctx, const Basis &b, const PassArgs<double> &a, int axisA, int axisB, bool inverse,
-                              const void *inA, void *outA, const void *inB, void *outB);
 
 template <typename R>
 void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<R> *psi, int S, C2<R> *projraw,

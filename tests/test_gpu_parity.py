@@ -264,30 +264,6 @@ def test_nonlocal_pieces(ib, c1):
     assert np.max(np.abs(res - ores)) < 1e-9
 
 
-@pytest.mark.parametrize("precision_name", ["F64", "F32"])
-def test_fused_pass_pairs_bitwise(ib, c1big, precision_name):
-    """The fused z/y pass pairs (option fft_pair) give the results of one launch per pass, with and
-    without Taylor accumulators (exponential): the same arithmetic per tile, up to the compiler's
-    different fused multiply-add choices in the two kernels (1e-14 relative in double, 1e-6 single)."""
-    sysm, basis, ham, phi, oh, ors = c1big
-    p = phi if precision_name == "F64" else phi.converted(getattr(ib, precision_name))
-    def exp_of(x):
-        y = x.copy()
-        ib.exponential_in_place(ham, complex(0.0, -0.01), y)
-        return y.matrix()
-    fused = ham(p).matrix()
-    e_fused = exp_of(p)
-    basis.ctx.set_option("fft_pair", 0)
-    try:
-        single = ham(p).matrix()
-        e_single = exp_of(p)
-    finally:
-        basis.ctx.set_option("fft_pair", 1)
-    tol = 1e-14 if precision_name == "F64" else 1e-6
-    assert rel(fused, single) < tol
-    assert rel(e_fused, e_single) < tol
-
-
 @pytest.mark.parametrize("mixed_compute", [1, 0])
 def test_hamiltonian_mixed_precision(ib, c1big, mixed_compute):
     """Mixed form (FP32 orbitals; FP64 or compensated FP32 butterflies): H|psi> within 2e-6 relative and
