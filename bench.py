@@ -227,15 +227,19 @@ def batch_leg(ctx, nsys=64, reps=5):
             "autotuned_shapes": len(tuning.table), "setup_s": setup_s}
 
 
-def serving_leg(ctx, rates=(10.0, 50.0, 200.0, 1000.0, 2000.0), nreq=120):
+def serving_leg(ctx, rates=(10.0, 50.0, 200.0, 1000.0, 2000.0), nreq=120, slots=4, bulk_slots=0,
+                bulk_grid_sms=0):
     """C5: Poisson stream of H|psi> and 10-step ETRS requests over C4-like systems plus 10% at 96^3 / 256
-    states, admitted by free device memory, four slots (streams); p50 / p99 latency and throughput."""
+    states, admitted by free device memory; ``slots`` slots (streams), of which ``bulk_slots`` take the
+    96^3 requests with their persistent kernels sized for ``bulk_grid_sms`` SMs; p50 / p99 latency
+    and throughput."""
     import inq_b200 as ib
     from inq_b200 import serving, synthetic
     pool = [serving.make_payload(s, ib.F32, ctx) for s in synthetic.batch_systems(12, seed=99)]
     large = serving.make_payload(synthetic.config("c2"), ib.F32, ctx)
-    out = {}
-    srv = serving.Server(slots=4, precision=ib.F32, keep_results=False)
+    out = {"slots": slots, "bulk_slots": bulk_slots, "bulk_grid_sms": bulk_grid_sms}
+    srv = serving.Server(slots=slots, precision=ib.F32, keep_results=False, bulk_slots=bulk_slots,
+                         bulk_min_bytes=1 << 30, bulk_grid_sms=bulk_grid_sms)
     for rate in rates:
         reqs = serving.poisson_requests(pool, nreq, rate, seed=int(rate), large=large)
         st = srv.run(reqs)

@@ -65,7 +65,12 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * inqb_orthogonalize and inqb_subspace_diagonalization -- on the tensor cores as split-BF16
  * products with FP32 accumulation and an FP64 sum of the per-SM partials; 16 significant bits
  * per value, so |error of S_ij| stays near 2^-16 |a_i| |b_j| / sqrt(npoint)) or 0 (FP64 SIMT
- * products, as for double-precision sets). */
+ * products, as for double-precision sets); "grid_sms" = 0 (default: the persistent kernels size
+ * their grids for every SM) or 1..#SMs (grids sized for that many SMs, leaving room on the device
+ * for the kernels of other contexts, e.g. small requests next to a large one in a serving loop);
+ * "stream_priority" = 0 (default, the device's lowest stream priority) or 1 (its highest: the
+ * block scheduler starts this context's pending blocks first).  Changing the priority replaces
+ * the context's stream (after the work queued on it), so callers query inqb_ctx_stream again. */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Free and total device memory in bytes (admission control for serving). */
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);

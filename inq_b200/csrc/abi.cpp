@@ -770,7 +770,7 @@ int inqb_ctx_create(int device, inqb_ctx **out) {
                      std::to_string(prop.minor));
     auto *c = new inqb_ctx();
     c->device = device;
-    c->num_sms = prop.multiProcessorCount;
+    c->num_sms = c->device_sms = prop.multiProcessorCount;
     c->max_smem_optin = prop.sharedMemPerBlockOptin;
     INQB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     INQB_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
@@ -831,6 +831,29 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     } else if (k == "overlap_tc") {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "overlap_tc is 0 (FP64 SIMT) or 1 (tensor cores)");
       ctx->overlap_tc = int(value);
+    } else if (k == "grid_sms") {
+      INQB_REQUIRE(value >= 0 && value <= ctx->device_sms, INQB_ERR_ARG,
+                   "grid_sms is 0 (every SM) or 1.." + std::to_string(ctx->device_sms));
+      ctx->num_sms = value == 0 ? ctx->device_sms : int(value);
+    } else if (k == "stream_priority") {
+      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "stream_priority is 0 (low) or 1 (high)");
+      if (int(value) != ctx->stream_priority) {
+        set_device(*ctx);
+        int least = 0, greatest = 0;
+        INQB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        cudaStream_t st = nullptr;
+        INQB_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, value ? greatest : least));
+        // work queued on the old stream finishes before anything queued on the new one
+        cudaEvent_t ev = nullptr;
+        INQB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        INQB_CUDA(cudaEventRecord(ev, ctx->stream));
+        INQB_CUDA(cudaStreamWaitEvent(st, ev, 0));
+        INQB_CUDA(cudaEventDestroy(ev));
+        INQB_CUDA(cudaStreamSynchronize(ctx->stream));
+        INQB_CUDA(cudaStreamDestroy(ctx->stream));
+        ctx->stream = st;
+        ctx->stream_priority = int(value);
+      }
     } else {
       throw Error(INQB_ERR_ARG, "unknown option " + k);
     }

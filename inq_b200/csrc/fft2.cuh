@@ -333,6 +333,59 @@ __device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *_
   __syncthreads();
 }
 
+// Forward transform, per-frequency factor fac[m], inverse transform of one [N][W] tile (the x pass of
+// the real-space operator).  The inverse runs the forward's two steps transposed (step B first, with
+// conjugate twiddles, then step A), so it starts from the forward's k1-major output and every step
+// writes the addresses it read: three shared-memory sweeps and two barriers, no transposition.
+//   forward A: N1-point DFTs down the columns j2, twiddle W_N^{j2 k1}           (asrc -> work)
+//   forward B, factor, inverse B: N2-point DFT along row k1, times fac[k1 + N1 k2], inverse
+//     N2-point DFT, twiddle W_N^{-j2 k1}                                      (work, in place)
+//   inverse A: inverse N1-point DFTs down the columns j2; x[j2 + N2 j1] goes to put(m, w, value)
+// `asrc` may be `work` itself.  No barrier follows the last step.
+template <int N, int W, int NT, typename TC, typename SA, typename Put>
+__device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC *__restrict__ tw,
+                                             const decltype(TC::x) *fac, Put put) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  for (int it = threadIdx.x; it < W * N2; it += NT) {
+    const int w = it % W, j2 = it / W;
+    TC s[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) s[j1] = conv<TC>(asrc[(j2 + N2 * j1) * W + w]);
+    dft<N1, +1, N>(s, tw);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; k1++) s[k1] = twmul<+1, N>(s[k1], tw, j2 * k1);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) work[(j2 + N2 * k1) * W + w] = s[k1];
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < W * N1; it += NT) {
+    const int w = it % W, k1 = it / W;
+    TC r[N2];
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++) r[j2] = work[(j2 + N2 * k1) * W + w];
+    dft<N2, +1, N>(r, tw);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) r[k2] = cscale(r[k2], fac[k1 + N1 * k2]);
+    dft<N2, -1, N>(r, tw);
+    if (k1 > 0) {
+#pragma unroll
+      for (int j2 = 1; j2 < N2; j2++) r[j2] = twmul<-1, N>(r[j2], tw, j2 * k1);
+    }
+#pragma unroll
+    for (int j2 = 0; j2 < N2; j2++) work[(j2 + N2 * k1) * W + w] = r[j2];
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < W * N2; it += NT) {
+    const int w = it % W, j2 = it / W;
+    TC s[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) s[k1] = work[(j2 + N2 * k1) * W + w];
+    dft<N1, -1, N>(s, tw);
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) put(j2 + N2 * j1, w, s[j1]);
+  }
+}
+
 struct Geom2 {
   Geom g;           // grid and line decomposition (point strides)
   int axis;
@@ -504,9 +557,7 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
     if constexpr (SPLIT) {
       if constexpr (VAR == MID_KIN) {
         // forward, multiply by the kinetic factor, backward
-        tile_dft<N, +1, W, NT, true, TC>(buf, exch, tw, (const CR *)nullptr,
-                                         [&](int m, int w, TC v) { exch[m * W + w] = cscale(v, linev[m]); });
-        tile_dft<N, -1, W, NT, false, TC>(exch, exch, tw, (const CR *)nullptr, put_out);
+        tile_dft_kin<N, W, NT, TC>(buf, exch, tw, linev, put_out);
       } else {
         tile_dft<N, D, W, NT, false, TC>(buf, exch, tw, pre, put_out);
       }
@@ -517,13 +568,17 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
           __syncthreads();
         }
       }
-      tile_dft_inplace<N, D, W, NT, T>(buf, reinterpret_cast<const T *>(tw));
       if constexpr (VAR == MID_KIN) {
-        for (int e = threadIdx.x; e < TILE; e += NT) buf[e] = cscale(buf[e], linev[e / W]);
-        __syncthreads();
-        tile_dft_inplace<N, -1, W, NT, T>(buf, reinterpret_cast<const T *>(tw));
+        if (scaled || accum) {
+          tile_dft_kin<N, W, NT, T>(buf, buf, reinterpret_cast<const T *>(tw), linev, put_out);
+        } else {
+          tile_dft_kin<N, W, NT, T>(buf, buf, reinterpret_cast<const T *>(tw), linev,
+                                    [&](int m, int w, T v) { buf[m * W + w] = v; });
+        }
+      } else {
+        tile_dft_inplace<N, D, W, NT, T>(buf, reinterpret_cast<const T *>(tw));
       }
-      if (scaled || AUX || accum) {
+      if (VAR != MID_KIN && (scaled || AUX || accum)) {
         for (int e = threadIdx.x; e < TILE; e += NT) put_out(e / W, e % W, buf[e]);
         __syncthreads();
       }

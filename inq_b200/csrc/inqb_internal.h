@@ -64,7 +64,8 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   long long launches = 0;
-  int num_sms = 0;
+  int num_sms = 0;           // SMs the persistent kernels size their grids for (option "grid_sms")
+  int device_sms = 0;        // SMs of the device
   size_t max_smem_optin = 0;
   int *d_err = nullptr;      // device flag raised by a kernel whose bounded wait expired
   std::vector<cudaStream_t> aux;        // fork streams of batched calls
@@ -73,6 +74,7 @@ struct Ctx {
   int fft_stages = 0;        // shared-memory ring depth of the TMA FFT kernels (0: from the memory budget)
   int mixed_compute = 0;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
   int overlap_tc = 1;        // overlaps of single-precision sets on the tensor cores (split BF16)
+  int stream_priority = 0;   // 0: the device's lowest stream priority, 1: its highest
 };
 
 struct Basis {

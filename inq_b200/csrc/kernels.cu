@@ -560,7 +560,7 @@ template <typename R>
 void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, long long npoints, double dv,
                     double2 *out) {
   const int gi = (Sa + 63) / 64, gj = (Sb + 63) / 64;
-  int nz = int((2LL * ctx.num_sms + gi * gj - 1) / (gi * gj));
+  int nz = int((2LL * ctx.device_sms + gi * gj - 1) / (gi * gj));  // independent of grid_sms
   if (nz < 1) nz = 1;
   if (nz > 256) nz = 256;
   long long chunk = (npoints + nz - 1) / nz;

@@ -265,7 +265,7 @@ void launch_overlap_tc(Ctx &ctx, const float2 *a, int Sa, const float2 *b, int S
   const int N = Sb < TC_N ? (Sb + 15) / 16 * 16 : TC_N;
   const int ntiles = (Sb + N - 1) / N;
   const int tiles = mtiles * ntiles;
-  int nsplit = ctx.num_sms / tiles;
+  int nsplit = ctx.device_sms / tiles;  // the split (and so the rounding) does not follow grid_sms
   if (nsplit < 1) nsplit = 1;
   long long kper = ((npoints + nsplit - 1) / nsplit + TC_KC - 1) / TC_KC * TC_KC;
   nsplit = int((npoints + kper - 1) / kper);  // every split holds at least one point

@@ -11,6 +11,12 @@ one H application or ``steps`` ETRS steps.  The server:
   different requests overlaps on the device, and keeps a request's orbitals and potential
   resident on the device across all its steps; a slot keeps the Hamiltonians (potential and
   projector tables) of the systems it served last, so a returning system skips its setup;
+* optionally splits the slots into two classes: "bulk" slots for requests whose footprint is at
+  least ``bulk_min_bytes`` and "interactive" slots for the rest.  Each class admits its own
+  requests in arrival order (a large request waiting for memory does not hold up small ones);
+  interactive contexts run at the device's highest stream priority and bulk contexts size their
+  persistent kernels for ``bulk_grid_sms`` SMs, so the kernels of small requests find room on the
+  device while a large request runs instead of waiting for each of its passes to drain;
 * records every request's latency (completion minus arrival) and result, and reports
   p50 / p99 latency beside throughput.
 
@@ -92,7 +98,10 @@ class Server:
 
     def __init__(self, device: int = 0, slots: int = 4, precision=F32, reserve_bytes: int = 8 << 30,
                  mixed_compute: int = 0, budget_bytes: int | None = None, contexts=None, execute=None,
-                 keep_results: bool = True, cache_per_slot: int = 8):
+                 keep_results: bool = True, cache_per_slot: int = 8, bulk_slots: int = 0,
+                 bulk_min_bytes: int = 1 << 30, bulk_grid_sms: int = 0):
+        if not 0 <= bulk_slots < slots:
+            raise ValueError("bulk_slots must leave at least one interactive slot")
         self.device = device
         self.cache = {}     # slot context -> payload -> (payload, basis, Hamiltonian), least recently used first
         self.cache_per_slot = cache_per_slot
@@ -101,9 +110,18 @@ class Server:
         self.staging = {}   # slot -> pinned host buffer for results
         if contexts is None:
             contexts = [core.Context(device) for _ in range(slots)]
-            for c in contexts:
+            for i, c in enumerate(contexts):
                 c.set_option("mixed_compute", mixed_compute)
+                if bulk_slots and i < bulk_slots:
+                    c.set_option("grid_sms", bulk_grid_sms)
+                elif bulk_slots:
+                    c.set_option("stream_priority", 1)
         self.contexts = list(contexts)
+        self.bulk_min_bytes = bulk_min_bytes
+        n = len(self.contexts)
+        self.free = ({"bulk": list(range(bulk_slots)), "interactive": list(range(bulk_slots, n))}
+                     if bulk_slots else {"all": list(range(n))})
+        self.slot_class = {i: c for c, idx in self.free.items() for i in idx}
         if budget_bytes is None:
             free, _ = self.contexts[0].mem_info()
             budget_bytes = max(0, free - reserve_bytes)
@@ -112,7 +130,6 @@ class Server:
         self.committed = 0
         self.peak_committed = 0
         self.lock = threading.Condition()
-        self.free_slots = list(range(len(self.contexts)))
 
     def _fetch(self, ctx, phi: core.OrbitalSet):
         """Copy a set to the host through the slot's pinned staging buffer."""
@@ -185,14 +202,38 @@ class Server:
             req.finished = time.perf_counter() - t0
             with self.lock:
                 self.committed -= fp
-                self.free_slots.append(slot)
+                self.free[self.slot_class[slot]].append(slot)
                 self.lock.notify_all()
+
+    def request_class(self, fp: int) -> str:
+        if "all" in self.free:
+            return "all"
+        return "bulk" if fp >= self.bulk_min_bytes else "interactive"
+
+    def _dispatch(self, queue, cls, t0, realtime, threads):
+        """Admit one class's requests in arrival order: wait for the arrival time, then for a free slot
+        of the class and room in the shared memory budget; run each on its own host thread."""
+        for req, fp in queue:
+            if realtime:
+                wait = req.arrival - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+            with self.lock:
+                while not self.free[cls] or self.committed + fp > self.budget:
+                    self.lock.wait()
+                slot = self.free[cls].pop(0)
+                self.committed += fp
+                self.peak_committed = max(self.peak_committed, self.committed)
+            req.admitted = time.perf_counter() - t0
+            th = threading.Thread(target=self._worker, args=(slot, req, t0, fp), daemon=True)
+            th.start()
+            threads.append(th)
 
     # ------------------------------------------------------------------ the loop
     def run(self, requests: list[Request], realtime: bool = True) -> dict:
         """Serve ``requests`` (sorted by arrival); returns latency / throughput statistics."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        threads = []
+        queues = {c: [] for c in self.free}
         t0 = time.perf_counter()
         for req in reqs:
             fp = req.footprint(self.precision)
@@ -200,22 +241,17 @@ class Server:
                 req.error = f"rejected: needs {fp} bytes, the budget is {self.budget}"
                 req.finished = req.admitted = time.perf_counter() - t0
                 continue
-            if realtime:
-                wait = req.arrival - (time.perf_counter() - t0)
-                if wait > 0:
-                    time.sleep(wait)
-            with self.lock:
-                while not self.free_slots or self.committed + fp > self.budget:
-                    self.lock.wait()
-                slot = self.free_slots.pop(0)
-                self.committed += fp
-                self.peak_committed = max(self.peak_committed, self.committed)
-            req.admitted = time.perf_counter() - t0
-            th = threading.Thread(target=self._worker, args=(slot, req, t0, fp), daemon=True)
-            th.start()
-            threads.append(th)
-        for th in threads:
-            th.join()
+            queues[self.request_class(fp)].append((req, fp))
+        threads = {c: [] for c in queues}
+        dispatchers = [threading.Thread(target=self._dispatch, args=(q, c, t0, realtime, threads[c]), daemon=True)
+                       for c, q in queues.items()]
+        for d in dispatchers:
+            d.start()
+        for d in dispatchers:
+            d.join()
+        for ths in threads.values():
+            for th in ths:
+                th.join()
         wall = time.perf_counter() - t0
         done = [r for r in reqs if not r.error]
         lat = np.array([r.latency for r in done]) if done else np.zeros(1)

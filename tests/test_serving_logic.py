@@ -83,3 +83,33 @@ def test_poisson_stream():
     frac = np.mean([r.payload is large for r in reqs])
     assert 0.05 < frac < 0.15
     assert any(r.kind == "etrs" for r in reqs) and any(r.kind == "apply" for r in reqs)
+
+
+def test_size_classes_do_not_block_each_other():
+    """With a bulk slot, large requests run only there and a large request waiting for it does not
+    hold up the small ones behind it in arrival order."""
+    started = {}
+    lock = threading.Lock()
+
+    def execute(req, ctx):
+        with lock:
+            started[req.rid] = ctx
+        time.sleep(0.3 if req.payload.system.npoints > 40 ** 3 else 0.01)
+        req.result = {"happs": 1}
+
+    ctxs = [object() for _ in range(3)]
+    big = [_req(i, 96, 256, 0.0) for i in range(2)]
+    small = [_req(10 + i, 16, 8, 0.01 * (i + 1)) for i in range(6)]
+    srv = serving.Server(slots=3, budget_bytes=1 << 40, contexts=ctxs, execute=execute, bulk_slots=1,
+                         bulk_min_bytes=big[0].footprint(serving.F32))
+    stats = srv.run(big + small)
+    assert stats["completed"] == 8
+    assert all(started[r.rid] is ctxs[0] for r in big)
+    assert all(started[r.rid] is not ctxs[0] for r in small)
+    assert max(r.finished for r in small) < big[1].admitted
+
+
+def test_bulk_slots_leave_an_interactive_slot():
+    import pytest
+    with pytest.raises(ValueError):
+        serving.Server(slots=2, budget_bytes=1 << 30, contexts=[object()] * 2, bulk_slots=2)
