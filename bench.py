@@ -227,7 +227,7 @@ def batch_leg(ctx, nsys=64, reps=5):
             "autotuned_shapes": len(tuning.table), "setup_s": setup_s}
 
 
-def serving_leg(ctx, rates=(10.0, 50.0, 200.0, 1000.0, 2000.0), nreq=120, slots=4, bulk_slots=0,
+def serving_leg(ctx, rates=(10.0, 50.0, 200.0, 1000.0, 2000.0), nreq=120, slots=5, bulk_slots=1,
                 bulk_grid_sms=0):
     """C5: Poisson stream of H|psi> and 10-step ETRS requests over C4-like systems plus 10% at 96^3 / 256
     states, admitted by free device memory; ``slots`` slots (streams), of which ``bulk_slots`` take the
@@ -245,8 +245,42 @@ def serving_leg(ctx, rates=(10.0, 50.0, 200.0, 1000.0, 2000.0), nreq=120, slots=
         st = srv.run(reqs)
         out[f"{int(rate)}_req_s"] = {k: st[k] for k in ("completed", "rejected", "throughput_req_s",
                                                         "state_applications_per_s", "p50_ms", "p99_ms", "max_ms",
-                                                        "by_size", "mean_phase_ms")}
+                                                        "by_size", "mean_phase_ms", "slowest_5pct_phase_ms")}
     srv.close()
+    return out
+
+
+def setup_leg(ctx, reps=3):
+    """Projector setup (ks_hamiltonian::update_projectors) of the 64-atom 96^3 and 128-atom 120^3
+    systems: the host construction against the device kernels, and moving every atom by ~0.1 bohr
+    (milliseconds per build, wall clock around a synchronised call)."""
+    import numpy as np
+    import inq_b200 as ib
+    from inq_b200 import synthetic
+    out = {}
+    for name in ("c2", "c3"):
+        sysm = synthetic.config(name, nst=1)
+        rs = ib.RealSpace(ib.Cell(sysm.lattice), sizes=sysm.sizes, ctx=ctx)
+        ham = ib.KSHamiltonian(rs)
+        res = {"atoms": len(sysm.positions), "grid": list(sysm.sizes)}
+        for key, dev in (("host_ms", False), ("device_ms", True)):
+            ham.update_projectors_gaussian(sysm.positions, sysm.radius, sysm.rc, sysm.kb, device=dev)
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                ham.update_projectors_gaussian(sysm.positions, sysm.radius, sysm.rc, sysm.kb, device=dev)
+            ctx.synchronize()
+            res[key] = (time.perf_counter() - t0) * 1e3 / reps
+        rng = np.random.default_rng(5)
+        moves = [sysm.positions + rng.normal(0.0, 0.1, sysm.positions.shape) for _ in range(reps)]
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for p in moves:
+            ham.move_atoms(p)
+        ctx.synchronize()
+        res["move_ms"] = (time.perf_counter() - t0) * 1e3 / reps
+        res["points"] = ham.projectors_info()[2]
+        out[name] = res
     return out
 
 
@@ -488,6 +522,7 @@ def run_ours(args):
     if world == 1 and not args.skip_legs:
         legs["overlap"] = overlap_leg(ctx, phi32, phi64, time_loop)
         legs["batch"] = batch_leg(ctx)
+        legs["setup"] = setup_leg(ctx)
         legs["serving"] = serving_leg(ctx)
         if args.etrs_steps > 0:
             legs["etrs"] = etrs_leg(ctx, args.etrs_steps, args.etrs_dt)

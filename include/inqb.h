@@ -157,6 +157,17 @@ int inqb_projectors_set(inqb_hamiltonian *ham, int nproj, int maxsph, int maxnlm
  * KB coefficients kb [natoms][4][4]. positions are cartesian [natoms][3]. */
 int inqb_projectors_build_gaussian(inqb_hamiltonian *ham, int natoms, const double *positions, double radius,
                                    double rc, const double *kb);
+/* The same tables built on the device (spherical_grid.hpp:59-160, projector.hpp:38-66 and the
+ * per-grid-point hit lists): the host only lists each atom's periodic images and their containing
+ * cubes; sphere membership (with the host construction's arithmetic, so the same points), the
+ * compaction in cube order, the projector values and the hit lists run as kernels.  Points, offsets,
+ * sphere sizes and hit lists equal the host build's; projector values agree to the last bits of exp. */
+int inqb_projectors_build_gaussian_device(inqb_hamiltonian *ham, int natoms, const double *positions, double radius,
+                                          double rc, const double *kb);
+/* ks_hamiltonian::update_projectors for atoms that moved (etrs.hpp:45-48): rebuilds the tables on
+ * the device for new cartesian positions [natoms][3], with the atom count, radius, rc and KB
+ * coefficients of the last inqb_projectors_build_gaussian(_device) call on this Hamiltonian. */
+int inqb_projectors_move(inqb_hamiltonian *ham, const double *positions);
 int inqb_projectors_info(const inqb_hamiltonian *ham, int *nproj, int *maxsph, long long *total_points);
 /* Host-only (no device, no context): basis::spherical_grid(basis, center, radius)
  * (src/basis/spherical_grid.hpp:59-160).  Writes up to `capacity` points: grid indices

@@ -69,6 +69,8 @@ SIGNATURES = {
     "inqb_update_hamiltonian": (I, [P, DP, DP]),
     "inqb_projectors_set": (I, [P, I, I, I, P, P, P, P, P, P]),
     "inqb_projectors_build_gaussian": (I, [P, I, DP, D, D, DP]),
+    "inqb_projectors_build_gaussian_device": (I, [P, I, DP, D, D, DP]),
+    "inqb_projectors_move": (I, [P, DP]),
     "inqb_projectors_info": (I, [P, C.POINTER(I), C.POINTER(I), C.POINTER(LL)]),
     "inqb_spherical_grid": (I, [DP, I, I, I, DP, D, LL, P, P, P, C.POINTER(LL)]),
     "inqb_projectors_get": (I, [P, P, P, P, P]),

@@ -420,12 +420,25 @@ class KSHamiltonian:
         self.ctx.check(self.ctx.lib.inqb_projectors_set(self.handle, nproj, maxsph, maxnlm, vp(points), vp(positions),
                                                         vp(matrices), vp(coeff), vp(npts), vp(nlm)))
 
-    def update_projectors_gaussian(self, positions, radius, rc, kb):
-        """Synthetic KB projectors (l = 0, 1; radial exp(-r^2/rc^2)) at cartesian atom positions."""
+    def update_projectors_gaussian(self, positions, radius, rc, kb, device: bool = False):
+        """Synthetic KB projectors (l = 0, 1; radial exp(-r^2/rc^2)) at cartesian atom positions.
+        ``device=True`` builds the spheres, values and hit lists with kernels (the host lists only the
+        periodic images and their containing cubes); the tables are the same."""
         pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
         kbv = np.ascontiguousarray(kb, dtype=np.float64).reshape(len(pos), 4, 4)
-        self.ctx.check(self.ctx.lib.inqb_projectors_build_gaussian(self.handle, len(pos), dptr(pos), float(radius),
-                                                                   float(rc), dptr(kbv)))
+        fn = (self.ctx.lib.inqb_projectors_build_gaussian_device if device
+              else self.ctx.lib.inqb_projectors_build_gaussian)
+        self.ctx.check(fn(self.handle, len(pos), dptr(pos), float(radius), float(rc), dptr(kbv)))
+
+    def move_atoms(self, positions):
+        """ks_hamiltonian::update_projectors after the atoms moved (etrs.hpp:45-48): the projector
+        tables rebuilt on the device for new cartesian positions, with the species parameters of the
+        last Gaussian build."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        nproj, _, _ = self.projectors_info()
+        if len(pos) != nproj:
+            raise ValueError(f"{len(pos)} positions for {nproj} atoms")
+        self.ctx.check(self.ctx.lib.inqb_projectors_move(self.handle, dptr(pos)))
 
     def projectors_info(self):
         n, m, t = C.c_int(), C.c_int(), C.c_longlong()

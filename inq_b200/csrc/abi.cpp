@@ -506,16 +506,20 @@ template <typename T> std::vector<T> download(Ctx &ctx, const void *dev, size_t 
   return h;
 }
 
+}  // namespace
+
 // all device memory of the library is stream-ordered (cudaMallocAsync / cudaFreeAsync on the owning
 // context's stream): releasing an object never synchronises the device, so contexts driven by
 // different host threads (the serving slots) do not stall one another
-void free_projectors(Projectors &P, cudaStream_t st) {
+void inqb::free_projectors(Projectors &P, cudaStream_t st) {
   void *ptrs[] = {P.d_pt, P.d_pos, P.d_mat, P.d_coeff, P.d_coeff32, P.d_npts, P.d_offs, P.d_hit, P.d_hitpts, P.d_hitp,
                   P.d_hrec, P.d_gcoef, P.d_hcoef, P.d_gcoef32, P.d_hcoef32};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, st);
   P = Projectors();
 }
+
+namespace {
 
 // the caller synchronises the stream before the host vector goes away
 template <typename T> T *upload_vec(const std::vector<T> &v, cudaStream_t st) {
@@ -1214,6 +1218,37 @@ int inqb_projectors_set(inqb_hamiltonian *h, int nproj, int maxsph, int maxnlm, 
     INQB_REQUIRE(nproj == 0 || (points && pos && matrices && coeff && npts && nlm), INQB_ERR_ARG, "null table");
     set_device(*h->ctx);
     set_projectors(*h, nproj, maxsph, maxnlm, points, pos, matrices, coeff, npts, nlm);
+    h->g_natoms = 0;  // explicit tables: nothing to move
+  });
+}
+
+// the species parameters of the last Gaussian build, for inqb_projectors_move
+static void remember_gaussian(Hamiltonian &h, int natoms, double radius, double rc, const double *kb) {
+  h.g_natoms = natoms;
+  h.g_radius = radius;
+  h.g_rc = rc;
+  h.g_kb.assign(kb, kb + size_t(natoms) * 16);
+}
+
+int inqb_projectors_build_gaussian_device(inqb_hamiltonian *h, int natoms, const double *positions, double radius,
+                                          double rc, const double *kb) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && (natoms == 0 || (positions && kb)), INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(natoms >= 0, INQB_ERR_ARG, "negative atom count");
+    INQB_REQUIRE(radius > 0.0 && rc > 0.0, INQB_ERR_ARG, "radius and rc must be positive");
+    set_device(*h->ctx);
+    build_projectors_gaussian_device(*h, natoms, positions, radius, rc, kb);
+    if (natoms > 0) remember_gaussian(*h, natoms, radius, rc, kb);
+  });
+}
+
+int inqb_projectors_move(inqb_hamiltonian *h, const double *positions) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && positions, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(h->g_natoms > 0, INQB_ERR_ARG, "no Gaussian projectors were built on this Hamiltonian");
+    set_device(*h->ctx);
+    const std::vector<double> kb = h->g_kb;
+    build_projectors_gaussian_device(*h, h->g_natoms, positions, h->g_radius, h->g_rc, kb.data());
   });
 }
 
@@ -1223,6 +1258,7 @@ int inqb_projectors_build_gaussian(inqb_hamiltonian *h, int natoms, const double
     INQB_REQUIRE(h && (natoms == 0 || (positions && kb)), INQB_ERR_ARG, "null argument");
     INQB_REQUIRE(radius > 0.0 && rc > 0.0, INQB_ERR_ARG, "radius and rc must be positive");
     set_device(*h->ctx);
+    if (natoms > 0) remember_gaussian(*h, natoms, radius, rc, kb);
     std::vector<SphereList> sph(natoms);
     int maxsph = 0;
     for (int a = 0; a < natoms; a++) {
@@ -1288,9 +1324,34 @@ int inqb_projectors_get(const inqb_hamiltonian *h, int32_t *points, float *pos, 
   return guarded(h ? h->ctx : nullptr, [&] {
     INQB_REQUIRE(h, INQB_ERR_ARG, "null argument");
     const Projectors &P = h->proj;
-    if (points) std::copy(P.h_points.begin(), P.h_points.end(), points);
-    if (pos) std::copy(P.h_pos.begin(), P.h_pos.end(), pos);
-    if (matrices) std::copy(P.h_mat.begin(), P.h_mat.end(), matrices);
+    if (P.device_built && P.nproj > 0) {
+      // tables built on the device: read them back in the packed host layout
+      set_device(*h->ctx);
+      Ctx &ctx = *h->ctx;
+      const size_t slots = size_t(P.nproj) * P.maxsph;
+      if (points) {
+        std::vector<int> flat = download<int>(ctx, P.d_pt, slots);
+        const int ny = h->basis->n[1], nz = h->basis->n[2];
+        for (size_t e = 0; e < slots; e++) {
+          const int f = flat[e];
+          points[3 * e] = f < 0 ? -1 : f / (ny * nz);
+          points[3 * e + 1] = f < 0 ? -1 : (f / nz) % ny;
+          points[3 * e + 2] = f < 0 ? -1 : f % nz;
+        }
+      }
+      if (pos) {
+        std::vector<float> v = download<float>(ctx, P.d_pos, 3 * slots);
+        std::copy(v.begin(), v.end(), pos);
+      }
+      if (matrices) {
+        std::vector<double> v = download<double>(ctx, P.d_mat, 4 * slots);
+        std::copy(v.begin(), v.end(), matrices);
+      }
+    } else {
+      if (points) std::copy(P.h_points.begin(), P.h_points.end(), points);
+      if (pos) std::copy(P.h_pos.begin(), P.h_pos.end(), pos);
+      if (matrices) std::copy(P.h_mat.begin(), P.h_mat.end(), matrices);
+    }
     if (npts) std::copy(P.h_npts.begin(), P.h_npts.end(), npts);
   });
 }
@@ -1316,8 +1377,9 @@ struct HostApplyRes {
     if (down) cudaStreamSynchronize(down);
     if (ctx) cudaStreamSynchronize(ctx->stream);
     for (int i = 0; i < 2; i++) {
-      if (bin[i]) cudaFree(bin[i]);
-      if (bout[i]) cudaFree(bout[i]);
+      // stream-ordered frees back to the pool: the next call reuses the blocks without cudaMalloc
+      if (bin[i]) cudaFreeAsync(bin[i], ctx->stream);
+      if (bout[i]) cudaFreeAsync(bout[i], ctx->stream);
       for (cudaEvent_t e : {ev_in[i], ev_comp[i], ev_out[i]})
         if (e) cudaEventDestroy(e);
     }
@@ -1353,7 +1415,7 @@ int inqb_apply_host(const inqb_hamiltonian *hc, int nst, const double kpoint_cov
       INQB_CUDA(cudaEventCreateWithFlags(&r.ev_out[i], cudaEventDisableTiming));
       for (void **p : {&r.bin[i], &r.bout[i]}) {
         if (i == 1 && nblocks == 1) continue;
-        cudaError_t e = cudaMalloc(p, npts * B * cs);
+        cudaError_t e = cudaMallocAsync(p, npts * B * cs, ctx.stream);
         if (e != cudaSuccess) {
           (void)cudaGetLastError();
           throw Error(INQB_ERR_MEMORY, "device allocation of a state block failed: " + std::string(cudaGetErrorString(e)));

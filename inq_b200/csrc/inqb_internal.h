@@ -126,6 +126,7 @@ struct Projectors {
   int *d_hitp = nullptr;                 // [total] projector index of each hit
   int4 *d_hrec = nullptr;                // [nhitpts] (point, first hit, hit count, first hit's projector)
   long long nhitpts = 0;
+  bool device_built = false;             // tables built on the device (no host copies of points / values)
   // (k+A)-dependent coefficient tables
   double kA[3] = {1e300, 1e300, 1e300};
   double2 *d_gcoef = nullptr;            // [nproj][maxsph][4]  dV e^{+ik.r} M
@@ -148,7 +149,16 @@ struct Hamiltonian {
   // interaction (self_consistency::update_hamiltonian): ionic potential, Hartree and LDA terms
   double *d_vion = nullptr;              // [npoints]
   int hartree = 0, xc = 0;
+  // species parameters of the last Gaussian projector build (for moving the atoms)
+  int g_natoms = 0;
+  double g_radius = 0.0, g_rc = 0.0;
+  std::vector<double> g_kb;              // [natoms][4][4]
 };
+
+void free_projectors(Projectors &P, cudaStream_t st);
+// spheres, projector values and per-point hit lists of Gaussian projectors, built on the device (setup.cu)
+void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *positions, double radius, double rc,
+                                      const double *kb);
 
 // ------------------------------------------------------------------ launchers (kernels.cu)
 

@@ -27,10 +27,8 @@ static inline void cart_to_contra(const double rlat[3][3], const double v[3], do
   for (int k = 0; k < 3; k++) out[k] = rlat[k][0] * v[0] + rlat[k][1] * v[1] + rlat[k][2] * v[2];
 }
 
-void spherical_grid_build(const Basis &b, const double center[3], double radius, SphereList &out) {
-  out.points.clear();
-  out.distance.clear();
-  out.relpos.clear();
+void sphere_cubes(const Basis &b, const double center[3], double radius, std::vector<SphereCube> &cubes) {
+  cubes.clear();
   const double(*lat)[3] = b.lat;
   const double(*rlat)[3] = b.rlat;
   double rlen[3];
@@ -82,6 +80,29 @@ void spherical_grid_build(const Basis &b, const double center[3], double radius,
       hi[d] = std::min(std::max(hi[d], rb), rend);
     }
     if ((hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]) <= 0) continue;
+    SphereCube c;
+    for (int d = 0; d < 3; d++) {
+      c.re[d] = re[d];
+      c.lo[d] = lo[d];
+      c.dim[d] = hi[d] - lo[d];
+    }
+    cubes.push_back(c);
+  }
+}
+
+void spherical_grid_build(const Basis &b, const double center[3], double radius, SphereList &out) {
+  out.points.clear();
+  out.distance.clear();
+  out.relpos.clear();
+  const double(*lat)[3] = b.lat;
+  const double(*rlat)[3] = b.rlat;
+  const double conspacing[3] = {1.0 / b.n[0], 1.0 / b.n[1], 1.0 / b.n[2]};
+  std::vector<SphereCube> cubes;
+  sphere_cubes(b, center, radius, cubes);
+  for (const SphereCube &cb : cubes) {
+    const double *re = cb.re;
+    const int lo[3] = {cb.lo[0], cb.lo[1], cb.lo[2]};
+    const int hi[3] = {cb.lo[0] + cb.dim[0], cb.lo[1] + cb.dim[1], cb.lo[2] + cb.dim[2]};
     for (int ix = lo[0]; ix < hi[0]; ix++)
       for (int iy = lo[1]; iy < hi[1]; iy++)
         for (int iz = lo[2]; iz < hi[2]; iz++) {

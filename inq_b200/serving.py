@@ -256,9 +256,15 @@ class Server:
         done = [r for r in reqs if not r.error]
         lat = np.array([r.latency for r in done]) if done else np.zeros(1)
         happs = sum(r.result.get("happs", 0) for r in done)
-        ph = np.array([r.result["phases_ms"] for r in done if "phases_ms" in r.result]).reshape(-1, 3)
-        phases = {k: float(ph[:, i].mean()) if len(ph) else 0.0
-                  for i, k in enumerate(("setup_ms", "compute_ms", "fetch_ms"))}
+        def phase_means(rs):
+            # queue: arrival to admission; setup, compute and fetch as the executor measured them
+            ph = np.array([[(r.admitted - r.arrival) * 1e3] + list(r.result["phases_ms"]) for r in rs
+                           if "phases_ms" in r.result]).reshape(-1, 4)
+            return {k: float(ph[:, i].mean()) if len(ph) else 0.0
+                    for i, k in enumerate(("queue_ms", "setup_ms", "compute_ms", "fetch_ms"))}
+        phases = phase_means(done)
+        tail_cut = np.percentile(lat, 95) if done else 0.0
+        tail = phase_means([r for r in done if r.latency >= tail_cut])
         def pct(rs, q):
             return float(np.percentile([r.latency for r in rs], q) * 1000) if rs else 0.0
         big = max((r.payload.system.npoints * r.payload.system.nst for r in done), default=0)
@@ -270,7 +276,7 @@ class Server:
                 "wall_s": wall, "throughput_req_s": len(done) / wall,
                 "state_applications_per_s": happs / wall,
                 "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000),
-                "max_ms": float(lat.max() * 1000), "mean_phase_ms": phases,
+                "max_ms": float(lat.max() * 1000), "mean_phase_ms": phases, "slowest_5pct_phase_ms": tail,
                 "peak_committed_bytes": self.peak_committed,
                 "budget_bytes": self.budget}
 
