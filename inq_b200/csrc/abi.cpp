@@ -138,6 +138,17 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   cov_to_cart(b, kA, ktmp);
   cart_to_contra(b, ktmp, kc);
 
+  // The z frequencies stay in digit-reversed order between the forward z pass and the final inverse z
+  // pass (the intermediate never leaves this function): the final pass, which also reads psi for the
+  // V psi epilogue, then needs no transposition barrier and runs its epilogue in the last step
+  // (96^3 x 256 single: 0.93 ms against 0.98 ms; 120^3: 3.6 ms against 5.1 ms).  The y passes keep
+  // natural order, which measured as fast or faster.  Kept only when the specialised kernels run every
+  // pass involved and every pass computes in the storage type (plain FP64, or single throughout).
+  const int es = int(sizeof(C2<R>));
+  const int py = 0;
+  int pz = fft2_perm_n2(ctx, b, S, es, 2);
+  if (!fft2_perm_n2(ctx, b, S, es, 0) || (sizeof(R) == 4 && ctx.mixed_compute != 0)) pz = 0;
+
   PassArgs<R> a;
   a.S = S;
   a.dir = +1;
@@ -145,23 +156,31 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   a.axis = 2;
   a.in = psi;
   a.out = hpsi;
+  a.perm = pz ? 1 : 0;
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   a.axis = 1;
   a.in = hpsi;
+  a.perm = py ? 1 : 0;
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   // x: forward, kinetic factor -0.5*(-|G|^2 + gc.G), gc = -2 (k+A)^contra, backward; the 1/N of the
   // inverse transform is folded into the per-point factor (formed in double, rounded once)
   a.axis = 0;
+  a.perm = 0;
+  a.perm_n2[1] = py;
+  a.perm_n2[2] = pz;
   a.mid_kinetic = 1;
   a.lap_factor = -0.5 / double(b.npoints);
   for (int i = 0; i < 3; i++) a.gc[i] = -2.0 * kc[i];
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   a.mid_kinetic = 0;
+  a.perm_n2[1] = a.perm_n2[2] = 0;
   // backward y, then z with the real-space epilogue
   a.dir = -1;
   a.axis = 1;
+  a.perm = py ? 1 : 0;
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_STORE);
   a.axis = 2;
+  a.perm = pz ? 1 : 0;
   a.psi = psi;
   if constexpr (sizeof(R) == 8) a.V = h.d_V;
   else a.V = h.d_V32;

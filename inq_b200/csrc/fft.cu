@@ -103,6 +103,8 @@ template <typename R>
 void launch_fft_pass(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue) {
   using T = C2<R>;
   if (launch_fft2<R>(ctx, b, a, prologue, epilogue)) return;
+  INQB_REQUIRE(!a.perm && !a.perm_n2[1] && !a.perm_n2[2], INQB_ERR_UNSUPPORTED,
+               "digit-reversed frequency order needs the specialised FFT kernel");
   const int axis = a.axis;
   Geom g;
   for (int i = 0; i < 3; i++) g.n[i] = b.n[i];
@@ -145,6 +147,17 @@ void launch_fft_pass(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologu
   else if (prologue == PRO_NONE && epilogue == EPI_LAPL_ADD) go(fft_pass_kernel<R, PRO_NONE, EPI_LAPL_ADD>);
   else if (prologue == PRO_VPSI && epilogue == EPI_STORE) go(fft_pass_kernel<R, PRO_VPSI, EPI_STORE>);
   else throw Error(INQB_ERR_UNSUPPORTED, "unsupported FFT pass fusion");
+}
+
+// N2 of the two-level split when the specialised TMA kernels (fft2.cuh) run every pass along `axis` for
+// S states of elem_bytes each (the conditions of v2::launch), else 0.
+int fft2_perm_n2(const Ctx &ctx, const Basis &b, int S, int elem_bytes, int axis) {
+  if (ctx.fft_impl == 1) return 0;
+  const int n = b.n[axis];
+  if (n != 24 && n != 32 && n != 40 && n != 48 && n != 64 && n != 72 && n != 96 && n != 120 && n != 128) return 0;
+  if ((size_t(S) * elem_bytes) % 16 != 0) return 0;
+  if (S < 256 / elem_bytes) return 0;
+  return n / 8;
 }
 
 template void launch_fft_pass<double>(Ctx &, const Basis &, const PassArgs<double> &, int, int);

@@ -23,9 +23,16 @@
 namespace inqb {
 namespace v2 {
 
-enum Variant { FWD_STORE = 0, INV_STORE = 1, MID_KIN = 2, INV_FINAL = 3, FWD_VPSI = 4, FWD_LAPLADD = 5 };
+enum Variant {
+  FWD_STORE = 0, INV_STORE = 1, MID_KIN = 2, INV_FINAL = 3, FWD_VPSI = 4, FWD_LAPLADD = 5,
+  // the same passes with the frequencies along the pass axis in digit-reversed order (position
+  // k2 + N2 k1 holds frequency k1 + N1 k2): forward output, inverse input
+  FWD_PERM = 6, INV_PERM = 7, INV_FINAL_PERM = 8
+};
 
-constexpr bool has_aux(int v) { return v == INV_FINAL || v == FWD_LAPLADD; }
+constexpr int base_var(int v) { return v == FWD_PERM ? FWD_STORE : (v == INV_PERM ? INV_STORE : (v == INV_FINAL_PERM ? INV_FINAL : v)); }
+constexpr bool is_perm(int v) { return v >= FWD_PERM; }
+constexpr bool has_aux(int v) { return base_var(v) == INV_FINAL || v == FWD_LAPLADD; }
 
 template <int N> struct Split { static constexpr int N1 = 0, N2 = 0; };
 template <> struct Split<24> { static constexpr int N1 = 8, N2 = 3; };
@@ -229,6 +236,10 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
 // Two-level in-place transform of a [N][W] tile (rows = points, natural order in and out).
 template <typename TO, typename TI> __device__ __forceinline__ TO conv(TI x) { return mk<TO>(decltype(TO::x)(x.x), decltype(TO::x)(x.y)); }
 
+// The tile transforms below end without a barrier: their last step writes only addresses the
+// writing thread owns in that step, and the kernel's fence + barrier before the TMA store (or an
+// explicit barrier before another sweep) orders those writes for the other threads.
+
 // Two-level transform of one [N][W] tile.
 //   step A: N1-point DFTs down the columns j2 (points j2 + N2 j1), twiddle W_N^{j2 k1};
 //   step B: N2-point DFTs along the rows k1, outputs in natural order m = k1 + N1 k2.
@@ -289,12 +300,23 @@ __device__ __forceinline__ void tile_dft(const SA *asrc, DA *adst, const TC *__r
       for (int k2 = 0; k2 < N2; k2++) put(k1 + N1 * k2, w, r[k2]);
     }
   }
-  __syncthreads();
 }
 
-// In-place two-level transform of a [N][W] tile when storage and arithmetic types agree.
-template <int N, int DIR, int W, int NT, typename T>
-__device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *__restrict__ tw) {
+// The in-place transforms below take the tile through one restrict-qualified pointer, so the compiler
+// may overlap one item's shared-memory loads with the previous item's stores, and hand every output
+// value to epi(m, w, value), which returns what is stored at row m (scaling, epilogue terms, Taylor
+// accumulators; the identity for a plain pass).  None ends with a barrier: the last step writes only
+// rows its thread read in that step, and the kernel's fence + barrier before the TMA store orders them.
+
+struct Identity {
+  template <typename T> __device__ __forceinline__ T operator()(int, int, T v) const { return v; }
+};
+
+// Natural order in and out: step A (N1-point DFTs down the columns j2, twiddle W_N^{j2 k1}), step B
+// (N2-point DFTs along the rows k1, outputs m = k1 + N1 k2).  Step B reads all its inputs before a
+// barrier and stores after it (it writes other rows than it reads).
+template <int N, int DIR, int W, int NT, typename T, typename Epi>
+__device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *__restrict__ tw, Epi epi) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   for (int it = threadIdx.x; it < W * N2; it += NT) {
     const int w = it % W, j2 = it / W;
@@ -327,24 +349,163 @@ __device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *_
     if (it < W * N1) {
       const int w = it % W, k1 = it / W;
 #pragma unroll
-      for (int k2 = 0; k2 < N2; k2++) buf[(k1 + N1 * k2) * W + w] = r[b][k2];
+      for (int k2 = 0; k2 < N2; k2++) buf[(k1 + N1 * k2) * W + w] = epi(k1 + N1 * k2, w, r[b][k2]);
+    }
+  }
+}
+
+// forward column step in place: N1-point DFT down column j2, twiddle W_N^{j2 k1}
+template <int N, int W, int NT, typename T>
+__device__ __forceinline__ void col_forward_inplace(T *__restrict__ buf, const T *__restrict__ tw) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  for (int it = threadIdx.x; it < W * N2; it += NT) {
+    const int w = it % W, j2 = it / W;
+    T s[N1];
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) s[j1] = buf[(j2 + N2 * j1) * W + w];
+    dft<N1, +1, N>(s, tw);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; k1++) s[k1] = twmul<+1, N>(s[k1], tw, j2 * k1);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) buf[(j2 + N2 * k1) * W + w] = s[k1];
+  }
+}
+
+// inverse column step in place: inverse N1-point DFT down column j2, x[j2 + N2 j1] in natural order
+template <int N, int W, int NT, typename T, typename Epi>
+__device__ __forceinline__ void col_inverse_inplace(T *__restrict__ buf, const T *__restrict__ tw, Epi epi) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  for (int it = threadIdx.x; it < W * N2; it += NT) {
+    const int w = it % W, j2 = it / W;
+    T s[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) s[k1] = buf[(j2 + N2 * k1) * W + w];
+    dft<N1, -1, N>(s, tw);
+#pragma unroll
+    for (int j1 = 0; j1 < N1; j1++) buf[(j2 + N2 * j1) * W + w] = epi(j2 + N2 * j1, w, s[j1]);
+  }
+}
+
+// The x pass of the real-space operator in place: forward transform, per-frequency factor fac[m],
+// inverse transform.  The inverse runs the forward's two steps transposed (step B first, with
+// conjugate twiddles, then step A), so it starts from the forward's k1-major output and every step
+// writes the rows it read: three shared-memory sweeps and two barriers, no transposition.
+//   forward A: N1-point DFTs down the columns j2, twiddle W_N^{j2 k1}
+//   forward B, factor, inverse B: N2-point DFT along row k1, times fac[k1 + N1 k2], inverse
+//     N2-point DFT, twiddle W_N^{-j2 k1} (rows of up to 12 points batched two items at a time)
+//   inverse A: inverse N1-point DFTs down the columns j2, natural order
+template <int N, int W, int NT, typename T, typename Epi>
+__device__ __forceinline__ void tile_kin_inplace(T *__restrict__ buf, const T *__restrict__ tw,
+                                                 const decltype(T::x) *__restrict__ fac, Epi epi) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  constexpr int IB = N2 <= 12 ? (W * N1 + NT - 1) / NT : 1;
+  col_forward_inplace<N, W, NT, T>(buf, tw);
+  __syncthreads();
+  for (int it0 = threadIdx.x; it0 < W * N1; it0 += IB * NT) {
+    T r[IB][N2];
+#pragma unroll
+    for (int b = 0; b < IB; b++) {
+      const int it = it0 + b * NT;
+      if (it < W * N1) {
+        const int w = it % W, k1 = it / W;
+#pragma unroll
+        for (int j2 = 0; j2 < N2; j2++) r[b][j2] = buf[(j2 + N2 * k1) * W + w];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < IB; b++) {
+      const int it = it0 + b * NT;
+      if (it < W * N1) {
+        const int w = it % W, k1 = it / W;
+        dft<N2, +1, N>(r[b], tw);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) r[b][k2] = cscale(r[b][k2], fac[k1 + N1 * k2]);
+        dft<N2, -1, N>(r[b], tw);
+        if (k1 > 0) {
+#pragma unroll
+          for (int j2 = 1; j2 < N2; j2++) r[b][j2] = twmul<-1, N>(r[b][j2], tw, j2 * k1);
+        }
+#pragma unroll
+        for (int j2 = 0; j2 < N2; j2++) buf[(j2 + N2 * k1) * W + w] = r[b][j2];
+      }
     }
   }
   __syncthreads();
+  col_inverse_inplace<N, W, NT, T>(buf, tw, epi);
 }
 
-// Forward transform, per-frequency factor fac[m], inverse transform of one [N][W] tile (the x pass of
-// the real-space operator).  The inverse runs the forward's two steps transposed (step B first, with
-// conjugate twiddles, then step A), so it starts from the forward's k1-major output and every step
-// writes the addresses it read: three shared-memory sweeps and two barriers, no transposition.
-//   forward A: N1-point DFTs down the columns j2, twiddle W_N^{j2 k1}           (asrc -> work)
-//   forward B, factor, inverse B: N2-point DFT along row k1, times fac[k1 + N1 k2], inverse
-//     N2-point DFT, twiddle W_N^{-j2 k1}                                      (work, in place)
-//   inverse A: inverse N1-point DFTs down the columns j2; x[j2 + N2 j1] goes to put(m, w, value)
-// `asrc` may be `work` itself.  No barrier follows the last step.
-template <int N, int W, int NT, typename TC, typename SA, typename Put>
-__device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC *__restrict__ tw,
-                                             const decltype(TC::x) *fac, Put put) {
+// Forward transform in place with the output in digit-reversed order: row k2 + N2 k1 receives
+// frequency k1 + N1 k2.  Step B writes the rows it read, so no second barrier is needed.
+template <int N, int W, int NT, typename T, typename Epi>
+__device__ __forceinline__ void tile_fwd_perm_inplace(T *__restrict__ buf, const T *__restrict__ tw, Epi epi) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, IB = (W * N1 + NT - 1) / NT;
+  col_forward_inplace<N, W, NT, T>(buf, tw);
+  __syncthreads();
+  T r[IB][N2];
+#pragma unroll
+  for (int b = 0; b < IB; b++) {
+    const int it = threadIdx.x + b * NT;
+    if (it < W * N1) {
+      const int w = it % W, k1 = it / W;
+#pragma unroll
+      for (int j2 = 0; j2 < N2; j2++) r[b][j2] = buf[(j2 + N2 * k1) * W + w];
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < IB; b++) {
+    const int it = threadIdx.x + b * NT;
+    if (it < W * N1) {
+      const int w = it % W, k1 = it / W;
+      dft<N2, +1, N>(r[b], tw);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) buf[(k2 + N2 * k1) * W + w] = epi(k2 + N2 * k1, w, r[b][k2]);
+    }
+  }
+}
+
+// Inverse transform in place of a tile whose rows are in digit-reversed order (row k2 + N2 k1 holds
+// frequency k1 + N1 k2): the forward's steps transposed, conjugate twiddles; natural order out.
+template <int N, int W, int NT, typename T, typename Epi>
+__device__ __forceinline__ void tile_inv_perm_inplace(T *__restrict__ buf, const T *__restrict__ tw, Epi epi) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, IB = (W * N1 + NT - 1) / NT;
+  T r[IB][N2];
+#pragma unroll
+  for (int b = 0; b < IB; b++) {
+    const int it = threadIdx.x + b * NT;
+    if (it < W * N1) {
+      const int w = it % W, k1 = it / W;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) r[b][k2] = buf[(k2 + N2 * k1) * W + w];
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < IB; b++) {
+    const int it = threadIdx.x + b * NT;
+    if (it < W * N1) {
+      const int w = it % W, k1 = it / W;
+      dft<N2, -1, N>(r[b], tw);
+      if (k1 > 0) {
+#pragma unroll
+        for (int j2 = 1; j2 < N2; j2++) r[b][j2] = twmul<-1, N>(r[b][j2], tw, j2 * k1);
+      }
+#pragma unroll
+      for (int j2 = 0; j2 < N2; j2++) buf[(j2 + N2 * k1) * W + w] = r[b][j2];
+    }
+  }
+  __syncthreads();
+  col_inverse_inplace<N, W, NT, T>(buf, tw, epi);
+}
+
+// Column and row steps of the two-level transforms below.
+//   column step: item (j2, w), N1 values at rows j2 + N2 j1; a runtime loop over the thread's items
+//   row step:    item (k1, w), N2 values at rows j2 + N2 k1; the thread's IB items are batched (all
+//                loads first, then the arithmetic, then the stores) so their loads are in flight
+//                together and their arithmetic interleaves
+// Both write only the rows they read, so no barrier separates a step's loads from its stores.
+
+// forward column step: N1-point DFT down column j2, twiddle W_N^{j2 k1}  (asrc -> work)
+template <int N, int W, int NT, typename TC, typename SA>
+__device__ __forceinline__ void col_forward(const SA *asrc, TC *work, const TC *__restrict__ tw) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   for (int it = threadIdx.x; it < W * N2; it += NT) {
     const int w = it % W, j2 = it / W;
@@ -357,24 +518,12 @@ __device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC 
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) work[(j2 + N2 * k1) * W + w] = s[k1];
   }
-  __syncthreads();
-  for (int it = threadIdx.x; it < W * N1; it += NT) {
-    const int w = it % W, k1 = it / W;
-    TC r[N2];
-#pragma unroll
-    for (int j2 = 0; j2 < N2; j2++) r[j2] = work[(j2 + N2 * k1) * W + w];
-    dft<N2, +1, N>(r, tw);
-#pragma unroll
-    for (int k2 = 0; k2 < N2; k2++) r[k2] = cscale(r[k2], fac[k1 + N1 * k2]);
-    dft<N2, -1, N>(r, tw);
-    if (k1 > 0) {
-#pragma unroll
-      for (int j2 = 1; j2 < N2; j2++) r[j2] = twmul<-1, N>(r[j2], tw, j2 * k1);
-    }
-#pragma unroll
-    for (int j2 = 0; j2 < N2; j2++) work[(j2 + N2 * k1) * W + w] = r[j2];
-  }
-  __syncthreads();
+}
+
+// inverse column step: inverse N1-point DFT down column j2; x[j2 + N2 j1] to put (natural order)
+template <int N, int W, int NT, typename TC, typename Put>
+__device__ __forceinline__ void col_inverse(const TC *work, const TC *__restrict__ tw, Put put) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   for (int it = threadIdx.x; it < W * N2; it += NT) {
     const int w = it % W, j2 = it / W;
     TC s[N1];
@@ -386,6 +535,57 @@ __device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC 
   }
 }
 
+// Forward transform, per-frequency factor fac[m], inverse transform of one [N][W] tile (the x pass of
+// the real-space operator), with the arithmetic in a separate buffer `work` (wider type than the
+// tile); the in-place form for equal types is tile_kin_inplace.  The inverse runs the forward's two steps transposed (step B first, with
+// conjugate twiddles, then step A), so it starts from the forward's k1-major output and every step
+// writes the addresses it read: three shared-memory sweeps and two barriers, no transposition.
+//   forward A: N1-point DFTs down the columns j2, twiddle W_N^{j2 k1}           (asrc -> work)
+//   forward B, factor, inverse B: N2-point DFT along row k1, times fac[k1 + N1 k2], inverse
+//     N2-point DFT, twiddle W_N^{-j2 k1}                                      (work, in place)
+//   inverse A: inverse N1-point DFTs down the columns j2; x[j2 + N2 j1] goes to put(m, w, value)
+// `asrc` may be `work` itself.  No barrier follows the last step.
+template <int N, int W, int NT, typename TC, typename SA, typename Put>
+__device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC *__restrict__ tw,
+                                             const decltype(TC::x) *fac, Put put) {
+  constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  // rows of up to 12 points are batched (two transforms per row keep longer rows one at a time)
+  constexpr int IB = N2 <= 12 ? (W * N1 + NT - 1) / NT : 1;
+  col_forward<N, W, NT, TC>(asrc, work, tw);
+  __syncthreads();
+  for (int it0 = threadIdx.x; it0 < W * N1; it0 += IB * NT) {
+    TC r[IB][N2];
+#pragma unroll
+    for (int b = 0; b < IB; b++) {
+      const int it = it0 + b * NT;
+      if (it < W * N1) {
+        const int w = it % W, k1 = it / W;
+#pragma unroll
+        for (int j2 = 0; j2 < N2; j2++) r[b][j2] = work[(j2 + N2 * k1) * W + w];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < IB; b++) {
+      const int it = it0 + b * NT;
+      if (it < W * N1) {
+        const int w = it % W, k1 = it / W;
+        dft<N2, +1, N>(r[b], tw);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) r[b][k2] = cscale(r[b][k2], fac[k1 + N1 * k2]);
+        dft<N2, -1, N>(r[b], tw);
+        if (k1 > 0) {
+#pragma unroll
+          for (int j2 = 1; j2 < N2; j2++) r[b][j2] = twmul<-1, N>(r[b][j2], tw, j2 * k1);
+        }
+#pragma unroll
+        for (int j2 = 0; j2 < N2; j2++) work[(j2 + N2 * k1) * W + w] = r[b][j2];
+      }
+    }
+  }
+  __syncthreads();
+  col_inverse<N, W, NT, TC>(work, tw, put);
+}
+
 struct Geom2 {
   Geom g;           // grid and line decomposition (point strides)
   int axis;
@@ -395,7 +595,7 @@ struct Geom2 {
   int cwords;       // 32-bit words per complex element
 };
 
-template <int VAR> constexpr int dir_first() { return (VAR == INV_STORE || VAR == INV_FINAL) ? -1 : +1; }
+template <int VAR> constexpr int dir_first() { return (base_var(VAR) == INV_STORE || base_var(VAR) == INV_FINAL) ? -1 : +1; }
 
 // Tiles of 256-byte rows, or 128-byte rows when the butterflies run in a wider type than the storage
 // (the tile then also needs an exchange buffer of that type, and smaller tiles let several CTAs share
@@ -407,14 +607,15 @@ template <typename R, typename CR> constexpr int tile_w() {
 // 128 threads and 16-state tiles (N1 = 8) the first step of N = 72, 96, 120, 128 takes two rounds in
 // which part of the CTA idles at the next barrier, so those tiles get one thread per first-step piece.
 // The kinetic pass (two transforms, the second with two idle thirds in its second step either way)
-// keeps 128 threads and more CTAs per SM.  The single-precision final pass of 96-point lines (two
-// tiles per stage, so two stages and 8 warps per SM at 128 threads) runs one thread per first-step
-// piece, 384 (measured: 1.06 ms against 1.15 ms at 96^3 x 256).
+// keeps 128 threads and more CTAs per SM.  The single-precision final passes of 96- to 128-point
+// lines (two tiles per stage: two stages, and 8 warps per SM at 128 threads for 96 points, 4 for
+// 120) run one thread per column item: 384 threads for 96 points (measured: 1.06 ms against 1.15 ms
+// at 96^3 x 256), 480 for 120.
 template <typename R, typename CR, int N, int VAR> constexpr int threads_of() {
   constexpr int W = tile_w<R, CR>();
   constexpr int A = W * Split<N>::N2, B = W * Split<N>::N1;
   constexpr int M = A > B ? A : B;
-  if constexpr (VAR == INV_FINAL && W == 32 && N == 96 && sizeof(CR) == 4) return 384;
+  if constexpr (base_var(VAR) == INV_FINAL && W == 32 && N >= 96 && sizeof(CR) == 4) return (A + 31) / 32 * 32;
   return (VAR != MID_KIN && W == 16 && M > 128 && M <= 256) ? (M + 31) / 32 * 32 : 128;
 }
 
@@ -516,9 +717,12 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
       for (int m = threadIdx.x; m < N; m += NT) {
         int ix, iy, iz;
         line_coords(gg.axis, la, lb, m, ix, iy, iz);
+        // axes held in digit-reversed frequency order: position k2 + N2 k1 is frequency k1 + N1 k2
+        if (a.perm_n2[1]) iy = iy / a.perm_n2[1] + (g.n[1] / a.perm_n2[1]) * (iy % a.perm_n2[1]);
+        if (a.perm_n2[2]) iz = iz / a.perm_n2[2] + (g.n[2] / a.perm_n2[2]) * (iz % a.perm_n2[2]);
         linev[m] = CR(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc));
       }
-    } else if constexpr (VAR == INV_FINAL || VAR == FWD_VPSI) {
+    } else if constexpr (base_var(VAR) == INV_FINAL || VAR == FWD_VPSI) {
       for (int m = threadIdx.x; m < N; m += NT)
         linev[m] = CR(a.V[(pbase + m * g.sp) * a.nspin + a.spin]) + CR(a.vshift);
     }
@@ -538,23 +742,26 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
       }
     }
 
-    // final store of one output value: epilogue terms, Taylor accumulators, write into the stage
-    auto put_out = [&](int m, int w, TC v) {
+    // final value of one output element: scaling, epilogue term, Taylor accumulators
+    auto epi_out = [&](int m, int w, TC v) -> T {
       const int s = s0 + w;
       if (scaled) v = kscale(v, a.scale);
-      if constexpr (VAR == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
+      if constexpr (base_var(VAR) == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
       const T o = conv<T>(v);
       if (accum && s < a.S) {
         const long long ge = (pbase + m * g.sp) * a.S + s;
         if (a.acc1) a.acc1[ge] = cadd(a.acc1[ge], cmul(a.c1, o));
         if (a.acc2) a.acc2[ge] = cadd(a.acc2[ge], cmul(a.c2, o));
       }
-      buf[m * W + w] = o;
+      return o;
     };
+    auto put_out = [&](int m, int w, TC v) { buf[m * W + w] = epi_out(m, w, v); };
     const CR *pre = (VAR == FWD_VPSI && !a.nl_offs) ? linev : nullptr;
     constexpr int D = dir_first<VAR>();
+    const T *twt = reinterpret_cast<const T *>(tw);
 
     if constexpr (SPLIT) {
+      static_assert(!is_perm(VAR), "digit-reversed passes run with equal storage and arithmetic types");
       if constexpr (VAR == MID_KIN) {
         // forward, multiply by the kinetic factor, backward
         tile_dft_kin<N, W, NT, TC>(buf, exch, tw, linev, put_out);
@@ -568,19 +775,29 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
           __syncthreads();
         }
       }
+      // plain passes (no scaling, no accumulators) store the transform's values as they are
+      const bool plain = !AUX && !scaled && !accum;
       if constexpr (VAR == MID_KIN) {
-        if (scaled || accum) {
-          tile_dft_kin<N, W, NT, T>(buf, buf, reinterpret_cast<const T *>(tw), linev, put_out);
-        } else {
-          tile_dft_kin<N, W, NT, T>(buf, buf, reinterpret_cast<const T *>(tw), linev,
-                                    [&](int m, int w, T v) { buf[m * W + w] = v; });
+        if (plain) tile_kin_inplace<N, W, NT, T>(buf, twt, linev, Identity());
+        else tile_kin_inplace<N, W, NT, T>(buf, twt, linev, epi_out);
+      } else if constexpr (VAR == INV_FINAL_PERM) {
+        tile_inv_perm_inplace<N, W, NT, T>(buf, twt, epi_out);
+      } else if constexpr (VAR == FWD_PERM || VAR == INV_PERM) {
+        if constexpr (VAR == FWD_PERM) tile_fwd_perm_inplace<N, W, NT, T>(buf, twt, Identity());
+        else tile_inv_perm_inplace<N, W, NT, T>(buf, twt, Identity());
+        if (!plain) {
+          __syncthreads();
+          for (int e = threadIdx.x; e < TILE; e += NT) put_out(e / W, e % W, buf[e]);
         }
+      } else if constexpr (AUX) {
+        // the epilogue (V psi or the Laplacian term, Taylor accumulators) in the transform's last step
+        tile_dft_inplace<N, D, W, NT, T>(buf, twt, epi_out);
       } else {
-        tile_dft_inplace<N, D, W, NT, T>(buf, reinterpret_cast<const T *>(tw));
-      }
-      if (VAR != MID_KIN && (scaled || AUX || accum)) {
-        for (int e = threadIdx.x; e < TILE; e += NT) put_out(e / W, e % W, buf[e]);
-        __syncthreads();
+        tile_dft_inplace<N, D, W, NT, T>(buf, twt, Identity());
+        if (!plain) {
+          __syncthreads();
+          for (int e = threadIdx.x; e < TILE; e += NT) put_out(e / W, e % W, buf[e]);
+        }
       }
     }
 
@@ -696,6 +913,18 @@ void launch_nc(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var
     case MID_KIN: launch_kernel<R, CR, N, MID_KIN>(ctx, b, a, gg); break;
     case INV_FINAL: launch_kernel<R, CR, N, INV_FINAL>(ctx, b, a, gg); break;
     case FWD_VPSI: launch_kernel<R, CR, N, FWD_VPSI>(ctx, b, a, gg); break;
+    case FWD_PERM:
+    case INV_PERM:
+    case INV_FINAL_PERM:
+      // digit-reversed passes exist for equal storage and arithmetic types only
+      if constexpr (sizeof(CR) == sizeof(R)) {
+        if (var == FWD_PERM) launch_kernel<R, CR, N, FWD_PERM>(ctx, b, a, gg);
+        else if (var == INV_PERM) launch_kernel<R, CR, N, INV_PERM>(ctx, b, a, gg);
+        else launch_kernel<R, CR, N, INV_FINAL_PERM>(ctx, b, a, gg);
+      } else {
+        throw Error(INQB_ERR_UNSUPPORTED, "digit-reversed FFT passes need equal storage and arithmetic types");
+      }
+      break;
     default: launch_kernel<R, CR, N, FWD_LAPLADD>(ctx, b, a, gg); break;
   }
 }
@@ -708,8 +937,9 @@ template <typename R, int N>
 void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var) {
   if constexpr (sizeof(R) == 4) {
     const int mode = ctx.mixed_compute;
-    const bool single = mode == 0 || (mode >= 2 && var == INV_FINAL) ||
-                        (mode == 3 && a.axis == 2 && (var == FWD_STORE || var == FWD_VPSI));
+    const int bv = base_var(var);
+    const bool single = mode == 0 || (mode >= 2 && bv == INV_FINAL) ||
+                        (mode == 3 && a.axis == 2 && (bv == FWD_STORE || var == FWD_VPSI));
     if (single) {
       launch_nc<R, float, N>(ctx, b, a, gg, var);
       return;
@@ -733,6 +963,11 @@ template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a
   else if (epilogue == EPI_LAPL_ADD) var = FWD_LAPLADD;
   else var = a.dir > 0 ? FWD_STORE : INV_STORE;
   if ((var == INV_FINAL && a.dir > 0) || ((var == FWD_VPSI || var == FWD_LAPLADD) && a.dir < 0)) return false;
+  if (a.perm) {
+    INQB_REQUIRE(var == FWD_STORE || var == INV_STORE || var == INV_FINAL, INQB_ERR_UNSUPPORTED,
+                 "digit-reversed frequency order is only kept by the plain forward and inverse passes");
+    var = var == FWD_STORE ? FWD_PERM : (var == INV_STORE ? INV_PERM : INV_FINAL_PERM);
+  }
 
   constexpr int W = 256 / int(sizeof(T));
   Geom2 gg;

@@ -173,6 +173,8 @@ template <typename R> struct PassArgs {
   int axis = 0;
   int dir = +1;                 // +1 forward (e^{-i}), -1 backward
   int mid_kinetic = 0;          // forward, multiply by lapl factor, backward (same axis)
+  int perm = 0;                 // forward: output, inverse: input in digit-reversed frequency order along the axis
+  int perm_n2[3] = {0, 0, 0};   // kinetic pass: axes held in digit-reversed order (their N2), 0 = natural
   double scale = 1.0;           // applied at the store
   // lapl factor data: factor*(-|G|^2 + gc.G)
   double lap_factor = 0.0, gc[3] = {0, 0, 0};
@@ -194,6 +196,7 @@ template <typename R>
 void launch_fft_pass(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue);
 // specialised persistent TMA kernels (fft2.cuh); false when the pass is not covered
 template <typename R> bool launch_fft2(Ctx &ctx, const Basis &b, const PassArgs<R> &a, int prologue, int epilogue);
+int fft2_perm_n2(const Ctx &ctx, const Basis &b, int S, int elem_bytes, int axis);
 template <> bool launch_fft2<float>(Ctx &ctx, const Basis &b, const PassArgs<float> &a, int prologue, int epilogue);
 template <> bool launch_fft2<double>(Ctx &ctx, const Basis &b, const PassArgs<double> &a, int prologue, int epilogue);
 

@@ -269,10 +269,12 @@ __global__ void __launch_bounds__(128) nl_apply_kernel(long long nitems, int nch
   const int lane = threadIdx.x & 31;
   const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  // the record of the warp's next item is requested while the current one is processed
+  int4 next = warp < nitems ? hrec[warp / nchunks] : make_int4(0, 0, 0, 0);
   for (long long it = warp; it < nitems; it += nwarps) {
-    const long long r = it / nchunks;
     const int s0 = int(it % nchunks) * (32 * U);
-    const int4 rec = hrec[r];
+    const int4 rec = next;
+    if (it + nwarps < nitems) next = hrec[(it + nwarps) / nchunks];
     const long long pt = rec.x;
     const int h0 = rec.y, nh = rec.z, p0 = rec.w;
     T hc[4], o[U], pd[4][U];
