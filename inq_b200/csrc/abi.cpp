@@ -915,14 +915,14 @@ int inqb_basis_create(inqb_ctx *ctx, const double lattice[9], int nx, int ny, in
         const int n = b->n[ax];
         b->radices[ax] = fft_radices(n);
         std::vector<double2> t64(n);
-        std::vector<float2> t32(2 * n);  // float parts, then the remainders (cos - float(cos), ...)
+        std::vector<float2> t32(2 * n);  // per twiddle: float part, then remainder (cos - float(cos), ...)
         const long double two_pi = 6.283185307179586476925286766559005768L;
         for (int t = 0; t < n; t++) {
           const long double ang = two_pi * (long double)t / (long double)n;
           t64[t] = make_double2(double(cosl(ang)), double(-sinl(ang)));
           const long double c = cosl(ang), sn = -sinl(ang);
-          t32[t] = make_float2(float(c), float(sn));
-          t32[n + t] = make_float2(float(c - (long double)t32[t].x), float(sn - (long double)t32[t].y));
+          t32[2 * t] = make_float2(float(c), float(sn));
+          t32[2 * t + 1] = make_float2(float(c - (long double)t32[2 * t].x), float(sn - (long double)t32[2 * t].y));
         }
         INQB_CUDA(cudaMallocAsync(&b->tw64[ax], sizeof(double2) * n, ctx->stream));
         INQB_CUDA(cudaMallocAsync(&b->tw32[ax], sizeof(float2) * 2 * n, ctx->stream));

@@ -108,11 +108,13 @@ template <typename T> __device__ __forceinline__ T kscale(T a, double c) {
     return mk<T>(a.x * R(c), a.y * R(c));
   }
 }
-// a times twiddle `idx` of the line table; single-precision tables hold N high parts then N low parts.
+// a times twiddle `idx` of the line table; single-precision tables interleave each twiddle's float
+// part and float remainder (one 16-byte load).
 template <int DIR, int N, typename T> __device__ __forceinline__ T twmul(T a, const T *__restrict__ tw, int idx) {
   using R = decltype(T::x);
   if constexpr (sizeof(R) == 4) {
-    const T h = twid<DIR>(tw[idx]), l = twid<DIR>(tw[idx + N]);
+    const float4 q = reinterpret_cast<const float4 *>(tw)[idx];
+    const T h = twid<DIR>(mk<T>(q.x, q.y)), l = twid<DIR>(mk<T>(q.z, q.w));
     const R lr = __fmaf_rn(-a.y, l.y, a.x * l.x), li = __fmaf_rn(a.y, l.x, a.x * l.y);
     return mk<T>(__fmaf_rn(a.x, h.x, __fmaf_rn(-a.y, h.y, lr)), __fmaf_rn(a.x, h.y, __fmaf_rn(a.y, h.x, li)));
   } else {
@@ -135,7 +137,92 @@ template <int RR> __host__ __device__ constexpr double odd_sin(int m) {
                 : (m == 2 ? 0.97492791218182360701813168299393121723 : 0.43388373911755812047576833284835875461);
 }
 
-template <int M, int DIR, int N, typename T>
+// cos and sin of 2 pi p / q, evaluated at compile time: the angle is folded into [0, pi/4] by exact
+// integer reflections, multiples of 30 and 45 degrees take exact values, the rest a Taylor series
+// (x <= pi/4, terms to x^27).
+struct CosSin {
+  double c, s;
+};
+__host__ __device__ constexpr double taylor_sin(double x) {
+  double term = x, sum = x;
+  for (int n = 1; n < 14; n++) {
+    term = -term * x * x / double((2 * n) * (2 * n + 1));
+    sum += term;
+  }
+  return sum;
+}
+__host__ __device__ constexpr double taylor_cos(double x) {
+  double term = 1.0, sum = 1.0;
+  for (int n = 1; n < 14; n++) {
+    term = -term * x * x / double((2 * n - 1) * (2 * n));
+    sum += term;
+  }
+  return sum;
+}
+__host__ __device__ constexpr CosSin cos_sin_turn(long long p, long long q) {
+  p %= q;
+  if (p < 0) p += q;
+  bool neg_s = false, neg_c = false, swap = false;
+  if (2 * p > q) { p = q - p; neg_s = true; }              // 2 pi - theta
+  if (4 * p > q) { p = q - 2 * p; q = 2 * q; neg_c = true; }  // pi - theta
+  if (8 * p > q) { p = q - 4 * p; q = 4 * q; swap = true; }   // pi / 2 - theta
+  double c = taylor_cos(6.283185307179586476925286766559 * double(p) / double(q));
+  double s = taylor_sin(6.283185307179586476925286766559 * double(p) / double(q));
+  if (p == 0) { c = 1.0; s = 0.0; }
+  if (8 * p == q) c = s = 0.70710678118654752440084436210484903928;
+  if (12 * p == q) { c = 0.86602540378443864676372317075293618347; s = 0.5; }
+  if (swap) { const double t = c; c = s; s = t; }
+  if (neg_c) c = -c;
+  if (neg_s) s = -s;
+  return CosSin{c, s};
+}
+
+// a times the compile-time twiddle W_M^TT = exp(-2 pi i TT DIR / M).  Single precision: the same
+// compensated product as twmul (twiddle = float part + float remainder), with the terms of exact
+// parts dropped; unit twiddles are sign changes and swaps.
+template <int DIR, int M, int TT, typename T> __device__ __forceinline__ T tw_const(T a) {
+  using R = decltype(T::x);
+  constexpr CosSin cs = cos_sin_turn(TT, M);
+  constexpr double tx = cs.c, ty = -double(DIR) * cs.s;
+  if constexpr (ty == 0.0) {
+    if constexpr (tx > 0.0) return a;
+    else return mk<T>(-a.x, -a.y);
+  } else if constexpr (tx == 0.0) {
+    if constexpr (ty > 0.0) return mk<T>(-a.y, a.x);
+    else return mk<T>(a.y, -a.x);
+  } else if constexpr (sizeof(R) == 4) {
+    constexpr float hx = float(tx), hy = float(ty);
+    constexpr float lx = float(tx - double(hx)), ly = float(ty - double(hy));
+    R lr, li;
+    if constexpr (lx == 0.0f && ly == 0.0f) {
+      lr = R(0);
+      li = R(0);
+      return mk<T>(__fmaf_rn(a.x, hx, -a.y * hy), __fmaf_rn(a.x, hy, a.y * hx));
+    } else if constexpr (ly == 0.0f) {
+      lr = a.x * lx;
+      li = a.y * lx;
+    } else if constexpr (lx == 0.0f) {
+      lr = -a.y * ly;
+      li = a.x * ly;
+    } else {
+      lr = __fmaf_rn(-a.y, ly, a.x * lx);
+      li = __fmaf_rn(a.y, lx, a.x * ly);
+    }
+    return mk<T>(__fmaf_rn(a.x, hx, __fmaf_rn(-a.y, hy, lr)), __fmaf_rn(a.x, hy, __fmaf_rn(a.y, hx, li)));
+  } else {
+    return mk<T>(a.x * R(tx) - a.y * R(ty), a.x * R(ty) + a.y * R(tx));
+  }
+}
+// tw_const with the exponent known only after unrolling (folds to one product once t is constant)
+template <int DIR, int M, int TT = 1, typename T> __device__ __forceinline__ T tw_const_at(T a, int t) {
+  if constexpr (TT >= M) return a;
+  else return t == TT ? tw_const<DIR, M, TT>(a) : tw_const_at<DIR, M, TT + 1>(a, t);
+}
+
+// M-point DFT in registers.  Composite sizes take their inner twiddles as compile-time constants, or
+// from the line's table when TABLE is set (the faster choice measured for the single-precision
+// forward streaming passes; the constants win everywhere else).
+template <int M, int DIR, int N, bool TABLE = false, typename T>
 __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
   using R = decltype(T::x);
   if constexpr (M == 1) {
@@ -205,7 +292,7 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
 #pragma unroll
     for (int k = 0; k < M; k++) v[k] = y[k];
   } else {
-    // composite: Cooley-Tukey M = A * B, twiddles W_M^t = tw[t * N / M]
+    // composite: Cooley-Tukey M = A * B, twiddles W_M^t = constants or tw[t * N / M]
     constexpr int A = first_factor(M);
     constexpr int B = M / A;
     T tmp[M];
@@ -214,11 +301,12 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
       T s[A];
 #pragma unroll
       for (int j1 = 0; j1 < A; j1++) s[j1] = v[j2 + B * j1];
-      dft<A, DIR, N>(s, tw);
+      dft<A, DIR, N, TABLE>(s, tw);
 #pragma unroll
       for (int k1 = 0; k1 < A; k1++) {
         if (j2 * k1 == 0) tmp[k1 * B + j2] = s[k1];
-        else tmp[k1 * B + j2] = twmul<DIR, N>(s[k1], tw, (j2 * k1) * (N / M));
+        else if constexpr (TABLE) tmp[k1 * B + j2] = twmul<DIR, N>(s[k1], tw, (j2 * k1) * (N / M));
+        else tmp[k1 * B + j2] = tw_const_at<DIR, M>(s[k1], j2 * k1);
       }
     }
 #pragma unroll
@@ -226,7 +314,7 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
       T s[B];
 #pragma unroll
       for (int j2 = 0; j2 < B; j2++) s[j2] = tmp[k1 * B + j2];
-      dft<B, DIR, N>(s, tw);
+      dft<B, DIR, N, TABLE>(s, tw);
 #pragma unroll
       for (int k2 = 0; k2 < B; k2++) v[k1 + A * k2] = s[k2];
     }
@@ -339,7 +427,7 @@ __device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *_
       const int w = it % W, k1 = it / W;
 #pragma unroll
       for (int j2 = 0; j2 < N2; j2++) r[b][j2] = buf[(j2 + N2 * k1) * W + w];
-      dft<N2, DIR, N>(r[b], tw);
+      dft<N2, DIR, N, (sizeof(decltype(T::x)) == 4 && DIR > 0)>(r[b], tw);
     }
   }
   __syncthreads();
@@ -456,7 +544,7 @@ __device__ __forceinline__ void tile_fwd_perm_inplace(T *__restrict__ buf, const
     const int it = threadIdx.x + b * NT;
     if (it < W * N1) {
       const int w = it % W, k1 = it / W;
-      dft<N2, +1, N>(r[b], tw);
+      dft<N2, +1, N, (sizeof(decltype(T::x)) == 4)>(r[b], tw);
 #pragma unroll
       for (int k2 = 0; k2 < N2; k2++) buf[(k2 + N2 * k1) * W + w] = epi(k2 + N2 * k1, w, r[b][k2]);
     }

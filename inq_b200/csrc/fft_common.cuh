@@ -120,7 +120,8 @@ __device__ __forceinline__ void stockham_pass(const T *__restrict__ src, T *__re
     if (Ns > 1) {
 #pragma unroll
       for (int q = 1; q < RR; q++) {
-        T t = __ldg(&tw[k * q * tstep]);
+        // single-precision tables interleave each twiddle's float part and remainder
+        T t = __ldg(&tw[(sizeof(decltype(T::x)) == 4 ? 2 : 1) * (k * q * tstep)]);
         if (sgn < 0) t.y = -t.y;
         v[q] = cmul(v[q], t);
       }
