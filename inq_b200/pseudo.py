@@ -322,3 +322,80 @@ def projector_tables(cell, sizes, atoms):
         nlm[p] = len(v)
         owner[p] = ia
     return points, positions, matrices, coeff, npts, nlm, owner
+
+
+# ---------------------------------------------------------------- local potential
+
+def _erf(x):
+    from scipy.special import erf
+    return erf(x)
+
+
+def local_potential(cell, sizes, atoms, sigma: float | None = None, tolerance: float = 1e-10) -> np.ndarray:
+    """The ions' local potential on the grid (Hartree), [nx, ny, nz].
+
+    Each atom's V_loc(r), whose tail is -Z/r, is split as in hamiltonian/atomic_potential.hpp:117-200
+    into a short-range part V_sr(r) = V_loc(r) + Z erf(r / sigma) / r, summed on the atom's sphere
+    (spline through the mesh, out to where |V_sr| falls below ``tolerance``), and the potential of a
+    Gaussian charge Z of width sigma, -Z erf(r / sigma) / r, summed over all periodic images in Fourier
+    space: V(G) = -4 pi Z exp(-G^2 sigma^2 / 4) / (Omega G^2) e^{-i G.R}, G = 0 dropped (the neutralising
+    background of a periodic cell, as the Poisson solver of the Hartree term drops it); the constant
+    that leaves is set so the grid average is sum_atoms alpha_Z / Omega, alpha_Z = int (V_loc + Z/r)
+    d^3 r, whatever sigma is.  The default
+    sigma, 3.1 grid spacings, keeps exp(-G^2 sigma^2 / 4) below 1e-10 at the grid's largest G, so the
+    Fourier sum of the Gaussian part is not truncated."""
+    from scipy.interpolate import CubicSpline
+    from .core import spherical_grid
+    lat = np.asarray(cell.lattice, dtype=np.float64)
+    n = tuple(int(v) for v in sizes)
+    if sigma is None:
+        sigma = 3.1 * max(np.linalg.norm(lat[i]) / n[i] for i in range(3))
+    npoint = int(np.prod(n))
+    V = np.zeros(npoint)
+    rec = 2.0 * np.pi * np.linalg.inv(lat).T              # rows b_i, a_i . b_j = 2 pi delta_ij
+    omega = abs(np.linalg.det(lat))
+    # long range: Gaussian charges in Fourier space
+    m = [np.fft.fftfreq(k, 1.0 / k) for k in n]
+    M = np.stack(np.meshgrid(*m, indexing="ij"), axis=-1)   # integer frequencies
+    G = M @ rec
+    g2 = np.sum(G * G, axis=-1)
+    rho = np.zeros(n, dtype=np.complex128)
+    for ps, R in atoms:
+        rho += ps.z_valence * np.exp(-1j * (G @ np.asarray(R, dtype=np.float64)))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        vg = np.where(g2 > 0, -4.0 * np.pi * rho * np.exp(-g2 * sigma * sigma / 4.0) / (omega * np.where(g2 > 0, g2, 1.0)), 0.0)
+    V += np.real(np.fft.ifftn(vg) * npoint).reshape(-1)
+    # the sphere sums below carry the mean of V_sr, (alpha_Z - pi Z sigma^2) / Omega per atom with
+    # alpha_Z = int (V_loc + Z / r) d^3 r; adding pi Z sigma^2 / Omega leaves the G = 0 term at the
+    # pseudopotential's own alpha_Z, independent of the split
+    V += sum(np.pi * ps.z_valence * sigma * sigma for ps, _ in atoms) / omega
+    # short range: spheres
+    for ps, R in atoms:
+        r = ps.r
+        with np.errstate(divide="ignore", invalid="ignore"):
+            tail = np.where(r > 0, ps.z_valence * _erf(r / sigma) / np.where(r > 0, r, 1.0),
+                            ps.z_valence * 2.0 / (np.sqrt(np.pi) * sigma))
+        vsr = ps.vlocal + tail
+        big = np.nonzero(np.abs(vsr) > tolerance)[0]
+        if not len(big):
+            continue
+        last = min(int(big[-1]) + 2, len(r) - 1)
+        keep = np.concatenate([[True], np.diff(r[: last + 1]) > 0])
+        sp = CubicSpline(r[: last + 1][keep], vsr[: last + 1][keep], extrapolate=False)
+        pts, dist, _ = spherical_grid(cell, sizes, np.asarray(R, dtype=np.float64), float(r[last]))
+        vals = np.nan_to_num(sp(dist.astype(np.float64)), nan=0.0)
+        flat = (pts[:, 0].astype(np.int64) * n[1] + pts[:, 1]) * n[2] + pts[:, 2]
+        np.add.at(V, flat, vals)
+    return V.reshape(n)
+
+
+def set_ions(ham, atoms, sigma: float | None = None):
+    """The local potential and the nonlocal projectors of ``atoms`` = [(Pseudopotential, cartesian
+    position)] on a KSHamiltonian (its basis's cell and grid); returns the local potential."""
+    basis = ham.basis
+    cell, sizes = basis.cell, tuple(basis.sizes)
+    V = local_potential(cell, sizes, atoms, sigma)
+    ham.set_scalar_potential(V)
+    points, pos, mats, coeff, npts, nlm, _ = projector_tables(cell, sizes, atoms)
+    ham.set_projectors(points, pos, mats, coeff, npts, nlm)
+    return V
