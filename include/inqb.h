@@ -164,9 +164,23 @@ int inqb_projectors_build_gaussian(inqb_hamiltonian *ham, int natoms, const doub
  * sphere sizes and hit lists equal the host build's; projector values agree to the last bits of exp. */
 int inqb_projectors_build_gaussian_device(inqb_hamiltonian *ham, int natoms, const double *positions, double radius,
                                           double rc, const double *kb);
+/* Projectors of pseudopotentials built on the device (projector.hpp:38-101 with tabulated radial
+ * functions): atom a has species species[a]; species s has a sphere of radius radius[s] and
+ * ngroups[s] projectors of up to four functions each.  The groups of species 0, then 1, ... are
+ *   functions [group][4][3] = (table index, l <= 3, m index 0..2l), table index -1 = unused slot
+ *   kb        [group][4][4] KB block of the group
+ * and a function's value at distance d and cartesian offset x is table(d) * Y_lm(x): cubic
+ * convolution on the uniform grid r_k = k dr of tables [ntables][nr], real harmonics (l = 1 as
+ * (y, z, x) sqrt(3/4pi)/r, l = 2, 3 tesseral).  Projector p of the result is group g of atom a,
+ * atom-major. */
+int inqb_projectors_build_radial(inqb_hamiltonian *ham, int natoms, const double *positions, const int32_t *species,
+                                 int nspecies, const double *radius, int nr, double dr, int ntables,
+                                 const double *tables, const int32_t *ngroups, const int32_t *functions,
+                                 const double *kb);
 /* ks_hamiltonian::update_projectors for atoms that moved (etrs.hpp:45-48): rebuilds the tables on
- * the device for new cartesian positions [natoms][3], with the atom count, radius, rc and KB
- * coefficients of the last inqb_projectors_build_gaussian(_device) call on this Hamiltonian. */
+ * the device for new cartesian positions [natoms][3], with everything else (atom count, species,
+ * radii, radial functions or Gaussian parameters, KB coefficients) of the last Gaussian or radial
+ * build on this Hamiltonian. */
 int inqb_projectors_move(inqb_hamiltonian *ham, const double *positions);
 int inqb_projectors_info(const inqb_hamiltonian *ham, int *nproj, int *maxsph, long long *total_points);
 /* Host-only (no device, no context): basis::spherical_grid(basis, center, radius)

@@ -71,6 +71,7 @@ SIGNATURES = {
     "inqb_projectors_build_gaussian": (I, [P, I, DP, D, D, DP]),
     "inqb_projectors_build_gaussian_device": (I, [P, I, DP, D, D, DP]),
     "inqb_projectors_move": (I, [P, DP]),
+    "inqb_projectors_build_radial": (I, [P, I, DP, P, I, DP, I, D, I, DP, P, P, DP]),
     "inqb_projectors_info": (I, [P, C.POINTER(I), C.POINTER(I), C.POINTER(LL)]),
     "inqb_spherical_grid": (I, [DP, I, I, I, DP, D, LL, P, P, P, C.POINTER(LL)]),
     "inqb_projectors_get": (I, [P, P, P, P, P]),

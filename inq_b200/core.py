@@ -408,6 +408,7 @@ class KSHamiltonian:
 
     def set_projectors(self, points, positions, matrices, coeff, npts, nlm):
         """Packed projector_all tables (see include/inqb.h inqb_projectors_set)."""
+        self._moving_atoms = 0
         points = np.ascontiguousarray(points, dtype=np.int32)
         positions = np.ascontiguousarray(positions, dtype=np.float32)
         matrices = np.ascontiguousarray(matrices, dtype=np.float64)
@@ -429,15 +430,18 @@ class KSHamiltonian:
         fn = (self.ctx.lib.inqb_projectors_build_gaussian_device if device
               else self.ctx.lib.inqb_projectors_build_gaussian)
         self.ctx.check(fn(self.handle, len(pos), dptr(pos), float(radius), float(rc), dptr(kbv)))
+        self._moving_atoms = len(pos)
 
     def move_atoms(self, positions):
         """ks_hamiltonian::update_projectors after the atoms moved (etrs.hpp:45-48): the projector
         tables rebuilt on the device for new cartesian positions, with the species parameters of the
         last Gaussian build."""
         pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
-        nproj, _, _ = self.projectors_info()
-        if len(pos) != nproj:
-            raise ValueError(f"{len(pos)} positions for {nproj} atoms")
+        natoms = getattr(self, "_moving_atoms", 0)
+        if natoms == 0:
+            raise ValueError("no Gaussian or pseudopotential projectors were built on this Hamiltonian")
+        if len(pos) != natoms:
+            raise ValueError(f"{len(pos)} positions for {natoms} atoms")
         self.ctx.check(self.ctx.lib.inqb_projectors_move(self.handle, dptr(pos)))
 
     def projectors_info(self):

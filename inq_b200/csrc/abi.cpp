@@ -1237,16 +1237,18 @@ int inqb_projectors_set(inqb_hamiltonian *h, int nproj, int maxsph, int maxnlm, 
     INQB_REQUIRE(nproj == 0 || (points && pos && matrices && coeff && npts && nlm), INQB_ERR_ARG, "null table");
     set_device(*h->ctx);
     set_projectors(*h, nproj, maxsph, maxnlm, points, pos, matrices, coeff, npts, nlm);
-    h->g_natoms = 0;  // explicit tables: nothing to move
+    h->dev_natoms = 0;  // explicit tables: nothing to move
   });
 }
 
-// the species parameters of the last Gaussian build, for inqb_projectors_move
-static void remember_gaussian(Hamiltonian &h, int natoms, double radius, double rc, const double *kb) {
-  h.g_natoms = natoms;
-  h.g_radius = radius;
-  h.g_rc = rc;
-  h.g_kb.assign(kb, kb + size_t(natoms) * 16);
+// what the last Gaussian build was made of, for inqb_projectors_move
+static DeviceProjectorSpec gaussian_spec(int natoms, double radius, double rc, const double *kb) {
+  DeviceProjectorSpec sp;
+  sp.gaussian = 1;
+  sp.radius = radius;
+  sp.rc = rc;
+  sp.kb.assign(kb, kb + size_t(natoms) * 16);
+  return sp;
 }
 
 int inqb_projectors_build_gaussian_device(inqb_hamiltonian *h, int natoms, const double *positions, double radius,
@@ -1256,18 +1258,51 @@ int inqb_projectors_build_gaussian_device(inqb_hamiltonian *h, int natoms, const
     INQB_REQUIRE(natoms >= 0, INQB_ERR_ARG, "negative atom count");
     INQB_REQUIRE(radius > 0.0 && rc > 0.0, INQB_ERR_ARG, "radius and rc must be positive");
     set_device(*h->ctx);
-    build_projectors_gaussian_device(*h, natoms, positions, radius, rc, kb);
-    if (natoms > 0) remember_gaussian(*h, natoms, radius, rc, kb);
+    DeviceProjectorSpec sp = gaussian_spec(natoms, radius, rc, natoms ? kb : nullptr);
+    build_projectors_device(*h, natoms, positions, sp);
+    h->dev_natoms = natoms;
+    h->dev_spec = std::move(sp);
+  });
+}
+
+int inqb_projectors_build_radial(inqb_hamiltonian *h, int natoms, const double *positions, const int32_t *species,
+                                 int nspecies, const double *radius, int nr, double dr, int ntables,
+                                 const double *tables, const int32_t *ngroups, const int32_t *functions,
+                                 const double *kb) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && natoms >= 0 && nspecies >= 0 && ntables >= 0, INQB_ERR_ARG, "bad argument");
+    INQB_REQUIRE(natoms == 0 || (positions && species && radius && ngroups), INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(nr > 0 && dr > 0.0, INQB_ERR_ARG, "radial tables need nr > 0 points and dr > 0");
+    DeviceProjectorSpec sp;
+    sp.gaussian = 0;
+    sp.species.assign(species, species + natoms);
+    sp.sradius.assign(radius, radius + nspecies);
+    sp.ngroups.assign(ngroups, ngroups + nspecies);
+    int groups = 0;
+    for (int s = 0; s < nspecies; s++) {
+      INQB_REQUIRE(ngroups[s] >= 0 && radius[s] >= 0.0, INQB_ERR_ARG, "bad species description");
+      groups += ngroups[s];
+    }
+    INQB_REQUIRE(groups == 0 || (functions && kb && (ntables == 0 || tables)), INQB_ERR_ARG, "null table");
+    sp.fn.assign(functions, functions + size_t(groups) * 12);
+    sp.gkb.assign(kb, kb + size_t(groups) * 16);
+    sp.tables.assign(tables, tables + size_t(ntables) * nr);
+    sp.nr = nr;
+    sp.dr = dr;
+    set_device(*h->ctx);
+    build_projectors_device(*h, natoms, positions, sp);
+    h->dev_natoms = natoms;
+    h->dev_spec = std::move(sp);
   });
 }
 
 int inqb_projectors_move(inqb_hamiltonian *h, const double *positions) {
   return guarded(h ? h->ctx : nullptr, [&] {
     INQB_REQUIRE(h && positions, INQB_ERR_ARG, "null argument");
-    INQB_REQUIRE(h->g_natoms > 0, INQB_ERR_ARG, "no Gaussian projectors were built on this Hamiltonian");
+    INQB_REQUIRE(h->dev_natoms > 0, INQB_ERR_ARG, "no Gaussian or radial projectors were built on this Hamiltonian");
     set_device(*h->ctx);
-    const std::vector<double> kb = h->g_kb;
-    build_projectors_gaussian_device(*h, h->g_natoms, positions, h->g_radius, h->g_rc, kb.data());
+    const DeviceProjectorSpec sp = h->dev_spec;
+    build_projectors_device(*h, h->dev_natoms, positions, sp);
   });
 }
 
@@ -1277,7 +1312,10 @@ int inqb_projectors_build_gaussian(inqb_hamiltonian *h, int natoms, const double
     INQB_REQUIRE(h && (natoms == 0 || (positions && kb)), INQB_ERR_ARG, "null argument");
     INQB_REQUIRE(radius > 0.0 && rc > 0.0, INQB_ERR_ARG, "radius and rc must be positive");
     set_device(*h->ctx);
-    if (natoms > 0) remember_gaussian(*h, natoms, radius, rc, kb);
+    if (natoms > 0) {
+      h->dev_natoms = natoms;
+      h->dev_spec = gaussian_spec(natoms, radius, rc, kb);
+    }
     std::vector<SphereList> sph(natoms);
     int maxsph = 0;
     for (int a = 0; a < natoms; a++) {

@@ -135,6 +135,23 @@ struct Projectors {
   float2 *d_hcoef32 = nullptr;
 };
 
+// What device-built projectors are made of.  Gaussian: one projector per atom, radial exp(-d^2/rc^2)
+// times Y_00 and Y_1m, KB blocks kb[atom][4][4].  Radial: per species a sphere radius and ngroups
+// projectors, each with up to four functions (table, l, m index) of uniform radial tables r_k = k dr.
+struct DeviceProjectorSpec {
+  int gaussian = 1;
+  double radius = 0.0, rc = 0.0;
+  std::vector<double> kb;          // Gaussian: [natoms][16]
+  std::vector<int> species;        // radial: [natoms]
+  std::vector<double> sradius;     // [nspecies]
+  std::vector<int> ngroups;        // [nspecies]
+  std::vector<int> fn;             // [groups][4][3]
+  std::vector<double> gkb;         // [groups][16]
+  std::vector<double> tables;      // [ntables][nr]
+  int nr = 0;
+  double dr = 0.0;
+};
+
 struct Hamiltonian {
   Ctx *ctx = nullptr;
   const Basis *basis = nullptr;
@@ -149,16 +166,14 @@ struct Hamiltonian {
   // interaction (self_consistency::update_hamiltonian): ionic potential, Hartree and LDA terms
   double *d_vion = nullptr;              // [npoints]
   int hartree = 0, xc = 0;
-  // species parameters of the last Gaussian projector build (for moving the atoms)
-  int g_natoms = 0;
-  double g_radius = 0.0, g_rc = 0.0;
-  std::vector<double> g_kb;              // [natoms][4][4]
+  // what the last device-side projector build was made of (for moving the atoms); natoms 0: none
+  int dev_natoms = 0;
+  DeviceProjectorSpec dev_spec;
 };
 
 void free_projectors(Projectors &P, cudaStream_t st);
-// spheres, projector values and per-point hit lists of Gaussian projectors, built on the device (setup.cu)
-void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *positions, double radius, double rc,
-                                      const double *kb);
+// spheres, projector values and per-point hit lists built on the device (setup.cu)
+void build_projectors_device(Hamiltonian &h, int natoms, const double *positions, const DeviceProjectorSpec &spec);
 
 // ------------------------------------------------------------------ launchers (kernels.cu)
 

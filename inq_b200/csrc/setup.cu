@@ -31,6 +31,7 @@ namespace {
 
 struct CubeJob {
   double re[3];      // image of the atom (cartesian)
+  double r2;         // squared sphere radius of the atom
   int lo[3];         // first symmetric-range index of the cube per axis
   int dim[3];        // cube extent per axis
   long long off;     // first cell of this cube in the concatenated cell range
@@ -41,7 +42,6 @@ struct SetupGeom {
   double lat[3][3], rlat[3][3];
   double cons[3];    // 1 / n per axis
   int n[3];
-  double r2;         // radius^2
 };
 
 __device__ __forceinline__ int find_job(const CubeJob *jobs, int njobs, long long c) {
@@ -86,7 +86,7 @@ __global__ void sphere_flag_kernel(SetupGeom G, const CubeJob *__restrict__ jobs
     int g[3];
     double df[3];
     const double n2 = eval_cell(G, J, c, g, df);
-    flag[c] = (n2 > G.r2) ? 0 : 1;
+    flag[c] = (n2 > J.r2) ? 0 : 1;
   }
 }
 
@@ -135,9 +135,81 @@ __global__ void sphere_rank_kernel(const long long *__restrict__ aoff, const uns
   if (threadIdx.x == 0) count[a] = carry;
 }
 
+// Real spherical harmonics Y_l^m (m index mm = m + l) at a cartesian offset, zero at the origin for
+// l > 0: l = 1 is (y, z, x) sqrt(3 / 4 pi) / r, l = 2 and 3 the tesseral harmonics without the
+// Condon-Shortley phase (the same table as the host construction).
+__device__ __forceinline__ double ylm(int l, int mm, const double c[3]) {
+  const double x = c[0], y = c[1], z = c[2];
+  if (l == 0) return 0.5 / sqrt(M_PI);
+  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+  if (!(r2 > 0.0)) return 0.0;
+  const double r = sqrt(r2);
+  if (l == 1) {
+    const double k1 = sqrt(3.0 / (4.0 * M_PI));
+    const double v = mm == 0 ? y : (mm == 1 ? z : x);
+    return __dmul_rn(k1, v) / r;
+  }
+  if (l == 2) {
+    const double c1 = 0.5 * sqrt(15.0 / M_PI);
+    switch (mm) {
+      case 0: return c1 * x * y / r2;
+      case 1: return c1 * y * z / r2;
+      case 2: return 0.25 * sqrt(5.0 / M_PI) * (3.0 * z * z - r2) / r2;
+      case 3: return c1 * x * z / r2;
+      default: return 0.25 * sqrt(15.0 / M_PI) * (x * x - y * y) / r2;
+    }
+  }
+  const double r3 = r2 * r;
+  const double a = 0.25 * sqrt(35.0 / (2.0 * M_PI)), b = 0.5 * sqrt(105.0 / M_PI);
+  const double cc = 0.25 * sqrt(21.0 / (2.0 * M_PI)), d = 0.25 * sqrt(7.0 / M_PI);
+  switch (mm) {
+    case 0: return a * y * (3.0 * x * x - y * y) / r3;
+    case 1: return b * x * y * z / r3;
+    case 2: return cc * y * (5.0 * z * z - r2) / r3;
+    case 3: return d * z * (5.0 * z * z - 3.0 * r2) / r3;
+    case 4: return cc * x * (5.0 * z * z - r2) / r3;
+    case 5: return 0.5 * b * z * (x * x - y * y) / r3;
+    default: return a * x * (x * x - 3.0 * y * y) / r3;
+  }
+}
+
+// Cubic convolution (Catmull-Rom) of a uniform radial table at distance d: the point before r = 0
+// mirrors the table with the parity of r^l, points past the end are zero.
+__device__ __forceinline__ double radial_value(const double *__restrict__ tab, int nr, double dr, int l, double d) {
+  const double xx = d / dr;
+  const double fk = floor(xx);
+  const int k = int(fk);
+  const double t = xx - fk;
+  if (k >= nr) return 0.0;
+  const double sg = (l & 1) ? -1.0 : 1.0;
+  auto f = [&](int i) -> double {
+    if (i < 0) return sg * tab[min(-i, nr - 1)];
+    return i < nr ? tab[i] : 0.0;
+  };
+  const double fm = f(k - 1), f0 = f(k), f1 = f(k + 1), f2 = f(k + 2);
+  return 0.5 * (2.0 * f0 + (f1 - fm) * t + (2.0 * fm - 5.0 * f0 + 4.0 * f1 - f2) * t * t +
+                (3.0 * f0 - fm - 3.0 * f1 + f2) * t * t * t);
+}
+
+// What the projector values of a species are made of.  Gaussian mode: one projector per atom with
+// exp(-d^2 / rc^2) Y_00, Y_1m.  Radial mode: ngroups projectors per atom, each with up to four
+// functions (radial table index, l, m index) taken from the uniform tables.
+struct FillSpec {
+  int gaussian;
+  double rc2;                        // Gaussian: rc^2
+  const int *first_proj;             // [natoms] index of the atom's first projector
+  const int *species;                // [natoms]
+  const int *ngroups;                // [nspecies] projectors per atom
+  const int *group_base;             // [nspecies] first group of the species in fn
+  const int *fn;                     // [groups][4][3] (table, l, mm), table -1 = unused
+  const double *tables;              // [ntables][nr]
+  int nr;
+  double dr;
+};
+
 __global__ void sphere_fill_kernel(SetupGeom G, const CubeJob *__restrict__ jobs, int njobs, long long ncells,
                                    const unsigned char *__restrict__ flag, const int *__restrict__ rank, int maxsph,
-                                   double rc2, int *__restrict__ pt, float *__restrict__ pos, double *__restrict__ mat) {
+                                   FillSpec F, int *__restrict__ pt, float *__restrict__ pos, double *__restrict__ mat) {
   const double y00 = 0.5 / sqrt(M_PI);
   const double k1 = sqrt(3.0 / (4.0 * M_PI));
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells; c += (long long)gridDim.x * blockDim.x) {
@@ -146,32 +218,48 @@ __global__ void sphere_fill_kernel(SetupGeom G, const CubeJob *__restrict__ jobs
     int g[3];
     double df[3];
     const double n2 = eval_cell(G, J, c, g, df);
-    const size_t slot = size_t(J.atom) * maxsph + rank[c];
-    pt[slot] = int((static_cast<long long>(g[0]) * G.n[1] + g[1]) * G.n[2] + g[2]);
+    const int a = J.atom, i = rank[c];
+    const int gpt = int((static_cast<long long>(g[0]) * G.n[1] + g[1]) * G.n[2] + g[2]);
     float rel[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const double cp = __dadd_rn(__dadd_rn(__dmul_rn(G.rlat[k][0], df[0]), __dmul_rn(G.rlat[k][1], df[1])),
                                   __dmul_rn(G.rlat[k][2], df[2]));
       rel[k] = float(cp);
-      pos[slot * 3 + k] = rel[k];
     }
     // projector values from the stored float32 distance and offset, as the host construction does
     const double d = double(float(sqrt(n2)));
-    const double rad = exp(-__dmul_rn(d, d) / rc2);
     double cc[3];
 #pragma unroll
     for (int j = 0; j < 3; j++)
       cc[j] = __dadd_rn(__dadd_rn(__dmul_rn(G.lat[0][j], double(rel[0])), __dmul_rn(G.lat[1][j], double(rel[1]))),
                         __dmul_rn(G.lat[2][j], double(rel[2])));
-    const double r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(cc[0], cc[0]), __dmul_rn(cc[1], cc[1])), __dmul_rn(cc[2], cc[2])));
-    const bool on = r > 0.0;
-    // ilm order of projector.hpp:48-66: l = 0, then l = 1 with m = -1, 0, 1 (components y, z, x)
-    const size_t mb = size_t(J.atom) * 4 * maxsph + rank[c];
-    mat[mb] = __dmul_rn(rad, y00);
-    mat[mb + maxsph] = __dmul_rn(rad, on ? __dmul_rn(k1, cc[1]) / r : 0.0);
-    mat[mb + 2 * size_t(maxsph)] = __dmul_rn(rad, on ? __dmul_rn(k1, cc[2]) / r : 0.0);
-    mat[mb + 3 * size_t(maxsph)] = __dmul_rn(rad, on ? __dmul_rn(k1, cc[0]) / r : 0.0);
+    const int p0 = F.first_proj[a];
+    const int ng = F.gaussian ? 1 : F.ngroups[F.species[a]];
+    for (int gi = 0; gi < ng; gi++) {
+      const size_t slot = size_t(p0 + gi) * maxsph + i;
+      pt[slot] = gpt;
+#pragma unroll
+      for (int k = 0; k < 3; k++) pos[slot * 3 + k] = rel[k];
+      const size_t mb = size_t(p0 + gi) * 4 * maxsph + i;
+      if (F.gaussian) {
+        const double rad = exp(-__dmul_rn(d, d) / F.rc2);
+        const double r = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(cc[0], cc[0]), __dmul_rn(cc[1], cc[1])), __dmul_rn(cc[2], cc[2])));
+        const bool on = r > 0.0;
+        // ilm order of projector.hpp:48-66: l = 0, then l = 1 with m = -1, 0, 1 (components y, z, x)
+        mat[mb] = __dmul_rn(rad, y00);
+        mat[mb + maxsph] = __dmul_rn(rad, on ? __dmul_rn(k1, cc[1]) / r : 0.0);
+        mat[mb + 2 * size_t(maxsph)] = __dmul_rn(rad, on ? __dmul_rn(k1, cc[2]) / r : 0.0);
+        mat[mb + 3 * size_t(maxsph)] = __dmul_rn(rad, on ? __dmul_rn(k1, cc[0]) / r : 0.0);
+      } else {
+        const int *fg = F.fn + size_t(F.group_base[F.species[a]] + gi) * 12;
+        for (int f = 0; f < 4; f++) {
+          const int ti = fg[3 * f], l = fg[3 * f + 1], mm = fg[3 * f + 2];
+          mat[mb + size_t(f) * maxsph] =
+              ti < 0 ? 0.0 : radial_value(F.tables + size_t(ti) * F.nr, F.nr, F.dr, l, d) * ylm(l, mm, cc);
+        }
+      }
+    }
   }
 }
 
@@ -299,8 +387,7 @@ unsigned blocks_for(long long n, int threads) {
 
 }  // namespace
 
-void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *positions, double radius, double rc,
-                                      const double *kb) {
+void build_projectors_device(Hamiltonian &h, int natoms, const double *positions, const DeviceProjectorSpec &spec) {
   Ctx &ctx = *h.ctx;
   const Basis &b = *h.basis;
   cudaStream_t st = ctx.stream;
@@ -308,14 +395,25 @@ void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *
   Projectors &P = h.proj;
   P.device_built = true;
   if (natoms == 0) return;
+  const bool gauss = spec.gaussian != 0;
+  const int nspecies = gauss ? 0 : int(spec.ngroups.size());
+  if (!gauss) {
+    INQB_REQUIRE(int(spec.species.size()) == natoms, INQB_ERR_ARG, "one species index per atom expected");
+    for (int a = 0; a < natoms; a++)
+      INQB_REQUIRE(spec.species[a] >= 0 && spec.species[a] < nspecies, INQB_ERR_ARG, "species index out of range");
+  }
+  auto radius_of = [&](int a) { return gauss ? spec.radius : spec.sradius[spec.species[a]]; };
+  auto groups_of = [&](int a) { return gauss ? 1 : spec.ngroups[spec.species[a]]; };
 
-  // host: images and containing cubes of every atom
+  // host: images and containing cubes of every atom; projectors (atom-major, group-minor)
   std::vector<CubeJob> jobs;
   std::vector<long long> aoff(size_t(natoms) + 1, 0);
+  std::vector<int> first_proj(natoms), proj_atom;
   std::vector<SphereCube> cubes;
   long long ncells = 0;
   for (int a = 0; a < natoms; a++) {
-    sphere_cubes(b, positions + 3 * a, radius, cubes);
+    const double rad = radius_of(a);
+    sphere_cubes(b, positions + 3 * a, rad, cubes);
     for (const SphereCube &c : cubes) {
       CubeJob j;
       for (int d = 0; d < 3; d++) {
@@ -323,13 +421,17 @@ void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *
         j.lo[d] = c.lo[d];
         j.dim[d] = c.dim[d];
       }
+      j.r2 = rad * rad;
       j.off = ncells;
       j.atom = a;
       jobs.push_back(j);
       ncells += (long long)c.dim[0] * c.dim[1] * c.dim[2];
     }
     aoff[size_t(a) + 1] = ncells;
+    first_proj[a] = int(proj_atom.size());
+    for (int g = 0; g < groups_of(a); g++) proj_atom.push_back(a);
   }
+  const int nproj = int(proj_atom.size());
   SetupGeom G;
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) {
@@ -340,7 +442,6 @@ void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *
     G.n[d] = b.n[d];
     G.cons[d] = 1.0 / b.n[d];
   }
-  G.r2 = radius * radius;
 
   const int njobs = int(jobs.size());
   CubeJob *d_jobs = static_cast<CubeJob *>(dev_alloc(ctx, sizeof(CubeJob) * std::max(1, njobs)));
@@ -363,37 +464,80 @@ void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *
   INQB_CUDA(cudaStreamSynchronize(st));
   int maxsph = 0;
   long long total = 0;
-  for (int c : counts) {
-    maxsph = std::max(maxsph, c);
-    total += c;
+  std::vector<int> npts(nproj);
+  for (int p = 0; p < nproj; p++) {
+    npts[p] = counts[proj_atom[p]];
+    maxsph = std::max(maxsph, npts[p]);
+    total += npts[p];
   }
   INQB_REQUIRE(total < (1LL << 31), INQB_ERR_UNSUPPORTED, "too many sphere points");
 
-  P.nproj = natoms;
+  // KB blocks per projector
+  std::vector<double> coeff(size_t(nproj) * 16, 0.0);
+  std::vector<int> group_base(std::max(1, nspecies), 0);
+  for (int s = 1; s < nspecies; s++) group_base[s] = group_base[s - 1] + spec.ngroups[s - 1];
+  for (int p = 0; p < nproj; p++) {
+    const int a = proj_atom[p];
+    const double *src = gauss ? spec.kb.data() + size_t(a) * 16
+                              : spec.gkb.data() + size_t(group_base[spec.species[a]] + (p - first_proj[a])) * 16;
+    std::copy(src, src + 16, coeff.begin() + size_t(p) * 16);
+  }
+  P.nproj = nproj;
   P.maxsph = maxsph;
   P.maxnlm = 4;
   P.total = total;
-  P.h_npts = counts;
-  P.h_nlm.assign(natoms, 4);
-  P.h_coeff.assign(kb, kb + size_t(natoms) * 16);
-  std::vector<float> coeff32(size_t(natoms) * 16);
-  for (size_t i = 0; i < coeff32.size(); i++) coeff32[i] = float(kb[i]);
-  const size_t slots = std::max<size_t>(1, size_t(natoms) * maxsph);
+  P.h_npts = npts;
+  P.h_nlm.assign(nproj, 4);
+  P.h_coeff = coeff;
+  std::vector<float> coeff32(coeff.size());
+  for (size_t i = 0; i < coeff.size(); i++) coeff32[i] = float(coeff[i]);
+  const size_t slots = std::max<size_t>(1, size_t(nproj) * maxsph);
   INQB_CUDA(cudaMallocAsync(&P.d_pt, sizeof(int) * slots, st));
   INQB_CUDA(cudaMallocAsync(&P.d_pos, sizeof(float) * 3 * slots, st));
   INQB_CUDA(cudaMallocAsync(&P.d_mat, sizeof(double) * 4 * slots, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_coeff, sizeof(double) * 16 * natoms, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_coeff32, sizeof(float) * 16 * natoms, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_npts, sizeof(int) * natoms, st));
+  INQB_CUDA(cudaMallocAsync(&P.d_coeff, sizeof(double) * 16 * nproj, st));
+  INQB_CUDA(cudaMallocAsync(&P.d_coeff32, sizeof(float) * 16 * nproj, st));
+  INQB_CUDA(cudaMallocAsync(&P.d_npts, sizeof(int) * nproj, st));
   INQB_CUDA(cudaMemsetAsync(P.d_pt, 0xff, sizeof(int) * slots, st));  // -1 padding
   INQB_CUDA(cudaMemsetAsync(P.d_pos, 0, sizeof(float) * 3 * slots, st));
   INQB_CUDA(cudaMemsetAsync(P.d_mat, 0, sizeof(double) * 4 * slots, st));
-  INQB_CUDA(cudaMemcpyAsync(P.d_coeff, kb, sizeof(double) * 16 * natoms, cudaMemcpyHostToDevice, st));
-  INQB_CUDA(cudaMemcpyAsync(P.d_coeff32, coeff32.data(), sizeof(float) * 16 * natoms, cudaMemcpyHostToDevice, st));
-  INQB_CUDA(cudaMemcpyAsync(P.d_npts, counts.data(), sizeof(int) * natoms, cudaMemcpyHostToDevice, st));
+  INQB_CUDA(cudaMemcpyAsync(P.d_coeff, coeff.data(), sizeof(double) * 16 * nproj, cudaMemcpyHostToDevice, st));
+  INQB_CUDA(cudaMemcpyAsync(P.d_coeff32, coeff32.data(), sizeof(float) * 16 * nproj, cudaMemcpyHostToDevice, st));
+  INQB_CUDA(cudaMemcpyAsync(P.d_npts, npts.data(), sizeof(int) * nproj, cudaMemcpyHostToDevice, st));
+
+  // what the values are made of
+  int *d_first = static_cast<int *>(dev_alloc(ctx, sizeof(int) * natoms));
+  INQB_CUDA(cudaMemcpyAsync(d_first, first_proj.data(), sizeof(int) * natoms, cudaMemcpyHostToDevice, st));
+  FillSpec F{};
+  F.gaussian = gauss ? 1 : 0;
+  F.rc2 = spec.rc * spec.rc;
+  F.first_proj = d_first;
+  std::vector<void *> spec_dev;
+  auto upload = [&](const void *src, size_t bytes) {
+    void *d = dev_alloc(ctx, std::max<size_t>(bytes, 16));
+    if (bytes) INQB_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st));
+    spec_dev.push_back(d);
+    return d;
+  };
+  if (!gauss) {
+    INQB_REQUIRE(spec.nr > 0 && spec.dr > 0.0 && spec.tables.size() % size_t(spec.nr) == 0, INQB_ERR_ARG,
+                 "radial tables must hold whole rows of nr points");
+    const int ntab = int(spec.tables.size() / size_t(spec.nr));
+    for (size_t k = 0; k < spec.fn.size(); k += 3)
+      INQB_REQUIRE(spec.fn[k] < ntab && spec.fn[k + 1] >= 0 && spec.fn[k + 1] <= 3 && spec.fn[k + 2] >= 0 &&
+                       spec.fn[k + 2] <= 2 * spec.fn[k + 1],
+                   INQB_ERR_ARG, "projector function (table, l, m) out of range");
+    F.species = static_cast<const int *>(upload(spec.species.data(), sizeof(int) * spec.species.size()));
+    F.ngroups = static_cast<const int *>(upload(spec.ngroups.data(), sizeof(int) * spec.ngroups.size()));
+    F.group_base = static_cast<const int *>(upload(group_base.data(), sizeof(int) * group_base.size()));
+    F.fn = static_cast<const int *>(upload(spec.fn.data(), sizeof(int) * spec.fn.size()));
+    F.tables = static_cast<const double *>(upload(spec.tables.data(), sizeof(double) * spec.tables.size()));
+    F.nr = spec.nr;
+    F.dr = spec.dr;
+  }
   if (ncells > 0) {
-    sphere_fill_kernel<<<blocks_for(ncells, 256), 256, 0, st>>>(G, d_jobs, njobs, ncells, d_flag, d_rank, maxsph,
-                                                                 rc * rc, P.d_pt, P.d_pos, P.d_mat);
+    sphere_fill_kernel<<<blocks_for(ncells, 256), 256, 0, st>>>(G, d_jobs, njobs, ncells, d_flag, d_rank, maxsph, F,
+                                                                 P.d_pt, P.d_pos, P.d_mat);
     INQB_CUDA(cudaGetLastError());
     ctx.launches++;
   }
@@ -407,12 +551,12 @@ void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *
   INQB_CUDA(cudaMallocAsync(&P.d_hit, sizeof(int) * std::max<long long>(1, total), st));
   INQB_CUDA(cudaMallocAsync(&P.d_hitp, sizeof(int) * std::max<long long>(1, total), st));
   INQB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int) * np, st));
-  const long long nslots = (long long)natoms * maxsph;
-  hit_count_kernel<<<blocks_for(nslots, 256), 256, 0, st>>>(natoms, maxsph, P.d_npts, P.d_pt, d_cnt);
+  const long long nslots = (long long)nproj * maxsph;
+  hit_count_kernel<<<blocks_for(nslots, 256), 256, 0, st>>>(nproj, maxsph, P.d_npts, P.d_pt, d_cnt);
   INQB_CUDA(cudaGetLastError());
   exclusive_scan(ctx, d_cnt, np, P.d_offs);
   INQB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int) * np, st));
-  hit_place_kernel<<<blocks_for(nslots, 256), 256, 0, st>>>(natoms, maxsph, P.d_npts, P.d_pt, P.d_offs, d_cnt, P.d_hit);
+  hit_place_kernel<<<blocks_for(nslots, 256), 256, 0, st>>>(nproj, maxsph, P.d_npts, P.d_pt, P.d_offs, d_cnt, P.d_hit);
   INQB_CUDA(cudaGetLastError());
   hit_sort_kernel<<<blocks_for(np, 256), 256, 0, st>>>(np, P.d_offs, maxsph, P.d_hit, P.d_hitp, d_nonempty);
   INQB_CUDA(cudaGetLastError());
@@ -433,8 +577,9 @@ void build_projectors_gaussian_device(Hamiltonian &h, int natoms, const double *
   INQB_CUDA(cudaMallocAsync(&P.d_hcoef32, sizeof(float2) * std::max<long long>(1, total) * 4, st));
   for (void *p : {static_cast<void *>(d_jobs), static_cast<void *>(d_aoff), static_cast<void *>(d_flag),
                   static_cast<void *>(d_rank), static_cast<void *>(d_count), static_cast<void *>(d_cnt),
-                  static_cast<void *>(d_nonempty), static_cast<void *>(d_slot)})
+                  static_cast<void *>(d_nonempty), static_cast<void *>(d_slot), static_cast<void *>(d_first)})
     dev_free(ctx, p);
+  for (void *p : spec_dev) dev_free(ctx, p);
   P.kA[0] = P.kA[1] = P.kA[2] = 1e300;  // (k + A) tables are built on first use
 }
 

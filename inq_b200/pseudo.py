@@ -245,15 +245,54 @@ def real_ylm(l: int, xyz: np.ndarray) -> np.ndarray:
     raise ValueError("projectors up to l = 3 are supported")
 
 
-def _radial(ps: Pseudopotential, i: int, d: np.ndarray) -> np.ndarray:
-    """beta_i at distances d: a cubic spline through the mesh points up to the cutoff (zero beyond)."""
+RADIAL_DR = 0.002   # spacing (bohr) of the uniform radial tables
+
+
+def radial_tables(ps: Pseudopotential, dr: float = RADIAL_DR) -> np.ndarray:
+    """Every beta_i resampled on the uniform grid r_k = k dr up to the projector radius (a cubic spline
+    through the file's mesh points up to each projector's end, zero beyond): [nbeta, nr].  The host
+    and the device evaluate projectors from these tables with the same cubic convolution."""
     from scipy.interpolate import CubicSpline
-    c = min(ps.beta_cutoff[i] + 2, len(ps.r))
-    rr, bb = ps.r[:c], ps.beta[i][:c]
-    keep = np.concatenate([[True], np.diff(rr) > 0])
-    sp = CubicSpline(rr[keep], bb[keep], extrapolate=False)
-    out = sp(np.asarray(d, dtype=np.float64))
-    return np.nan_to_num(out, nan=0.0)
+    cache = getattr(ps, "_tables", None)
+    if cache is not None and cache[0] == dr:
+        return cache[1]
+    nr = int(np.ceil(ps.projector_radius() / dr)) + 3
+    rk = np.arange(nr) * dr
+    out = np.zeros((len(ps.beta_l), nr))
+    for i in range(len(ps.beta_l)):
+        c = min(ps.beta_cutoff[i] + 2, len(ps.r))
+        rr, bb = ps.r[:c], ps.beta[i][:c]
+        keep = np.concatenate([[True], np.diff(rr) > 0])
+        sp = CubicSpline(rr[keep], bb[keep], extrapolate=False)
+        out[i] = np.nan_to_num(sp(rk), nan=0.0)
+        out[i][rk > rr[-1]] = 0.0
+    ps._tables = (dr, out)
+    return out
+
+
+def radial_eval(table: np.ndarray, dr: float, l: int, d: np.ndarray) -> np.ndarray:
+    """Cubic convolution (Catmull-Rom) on the uniform table at distances d; the point before r = 0
+    mirrors the table with the parity of r^l, points past the end are zero."""
+    d = np.asarray(d, dtype=np.float64)
+    nr = len(table)
+    x = d / dr
+    k = np.floor(x).astype(np.int64)
+    t = x - k
+    sgn = -1.0 if l % 2 else 1.0
+
+    def f(i):
+        v = np.where((i >= 0) & (i < nr), table[np.clip(i, 0, nr - 1)], 0.0)
+        return np.where(i < 0, sgn * table[np.clip(-i, 0, nr - 1)], v)
+
+    fm, f0, f1, f2 = f(k - 1), f(k), f(k + 1), f(k + 2)
+    val = 0.5 * (2.0 * f0 + (f1 - fm) * t + (2.0 * fm - 5.0 * f0 + 4.0 * f1 - f2) * t * t
+                 + (3.0 * f0 - fm - 3.0 * f1 + f2) * t * t * t)
+    return np.where(k < nr, val, 0.0)
+
+
+def _radial(ps: Pseudopotential, i: int, d: np.ndarray) -> np.ndarray:
+    """beta_i at distances d (the uniform table and its cubic convolution)."""
+    return radial_eval(radial_tables(ps)[i], RADIAL_DR, ps.beta_l[i], d)
 
 
 def group_functions(ps: Pseudopotential, width: int = 4):
@@ -389,13 +428,65 @@ def local_potential(cell, sizes, atoms, sigma: float | None = None, tolerance: f
     return V.reshape(n)
 
 
-def set_ions(ham, atoms, sigma: float | None = None):
+def set_ions(ham, atoms, sigma: float | None = None, device: bool = False):
     """The local potential and the nonlocal projectors of ``atoms`` = [(Pseudopotential, cartesian
-    position)] on a KSHamiltonian (its basis's cell and grid); returns the local potential."""
+    position)] on a KSHamiltonian (its basis's cell and grid); returns the local potential.  With
+    ``device`` the projector tables are built by the device kernels from the same uniform radial
+    tables and groups (the same projectors, in the same order, as ``projector_tables``), and
+    ``ham.move_atoms`` later rebuilds them on the device for new positions."""
     basis = ham.basis
     cell, sizes = basis.cell, tuple(basis.sizes)
     V = local_potential(cell, sizes, atoms, sigma)
     ham.set_scalar_potential(V)
-    points, pos, mats, coeff, npts, nlm, _ = projector_tables(cell, sizes, atoms)
-    ham.set_projectors(points, pos, mats, coeff, npts, nlm)
+    if device:
+        build_radial_device(ham, atoms)
+    else:
+        points, pos, mats, coeff, npts, nlm, _ = projector_tables(cell, sizes, atoms)
+        ham.set_projectors(points, pos, mats, coeff, npts, nlm)
     return V
+
+
+def build_radial_device(ham, atoms):
+    """The projectors of ``atoms`` built on the device (``inqb_projectors_build_radial``)."""
+    import ctypes as C
+    from . import _lib
+    species, index = [], {}
+    for ps, _ in atoms:
+        if id(ps) not in index:
+            index[id(ps)] = len(species)
+            species.append(ps)
+    tabs = [radial_tables(ps) for ps in species]
+    nr = max([t.shape[1] for t in tabs] + [1])
+    rows, fn, kb, ngroups, radius = [], [], [], [], []
+    for ps, t in zip(species, tabs):
+        base = len(rows)
+        for row in t:
+            rows.append(np.pad(row, (0, nr - len(row))))
+        groups = group_functions(ps) if ps.num_projectors_lm() else []
+        kbf = ps.kb_coefficients()
+        lmf = ps.lm_functions()
+        for g in groups:
+            f = np.full((4, 3), -1, np.int32)
+            f[:, 1:] = 0
+            blk = np.zeros((4, 4))
+            for j, k in enumerate(g):
+                i, l, mm = lmf[k]
+                f[j] = (base + i, l, mm)
+            blk[: len(g), : len(g)] = kbf[np.ix_(g, g)]
+            fn.append(f)
+            kb.append(blk)
+        ngroups.append(len(groups))
+        radius.append(ps.projector_radius())
+    pos = np.ascontiguousarray(np.array([R for _, R in atoms], dtype=np.float64).reshape(-1, 3))
+    spc = np.ascontiguousarray([index[id(ps)] for ps, _ in atoms], dtype=np.int32)
+    tables = np.ascontiguousarray(np.array(rows, dtype=np.float64).reshape(-1))
+    fn_a = np.ascontiguousarray(np.array(fn, dtype=np.int32).reshape(-1))
+    kb_a = np.ascontiguousarray(np.array(kb, dtype=np.float64).reshape(-1))
+    ng = np.ascontiguousarray(ngroups, dtype=np.int32)
+    rad = np.ascontiguousarray(radius, dtype=np.float64)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    dp = lambda a: a.ctypes.data_as(_lib.DP)
+    ham.ctx.check(ham.ctx.lib.inqb_projectors_build_radial(
+        ham.handle, len(atoms), dp(pos), vp(spc), len(species), dp(rad), int(nr), float(RADIAL_DR), len(rows),
+        dp(tables) if len(rows) else None, vp(ng), vp(fn_a) if len(fn) else None, dp(kb_a) if len(kb) else None))
+    ham._moving_atoms = len(atoms)

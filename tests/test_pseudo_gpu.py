@@ -83,3 +83,42 @@ def test_hamiltonian_with_upf_projectors_matches_oracle(rng):
     e = ham.non_local_energy(ib.OrbitalSet.from_array(rs, x, kpoint=kp), occ)
     e_ref = oh.non_local_energy(x, occ, kp)
     assert abs(e - e_ref) < 1e-10 * max(1.0, abs(e_ref)), (e, e_ref)
+
+
+def test_device_built_pseudopotential_projectors(rng):
+    """The device kernels build the same projectors as ``projector_tables`` on the host: equal sphere
+    points, offsets and sizes, values to 1e-13 relative (the harmonics' last bits), and an H|psi>
+    within 1e-13; ``move_atoms`` rebuilds them for new positions like a fresh host build.  Two species
+    (18 and 4 functions), a skewed cell."""
+    import inq_b200 as ib
+    from inq_b200 import pseudo
+    ps = _synthetic()
+    small = pseudo.Pseudopotential("Yy", 1.0, ps.r, ps.rab, ps.vlocal, [0, 1], [ps.beta[0], ps.beta[2]],
+                                   [ps.beta_cutoff[0], ps.beta_cutoff[2]], np.diag([1.5, -0.7]))
+    lat = np.array([[8.0, 0.0, 0.0], [1.5, 7.5, 0.0], [0.5, 1.0, 8.5]])
+    sizes = (24, 20, 24)
+    cell = ib.Cell(lat)
+    rs = ib.RealSpace(cell, sizes=sizes)
+    atoms = [(ps, np.array([1.0, 2.0, -1.5])), (small, np.array([-3.0, 0.5, 2.5])), (ps, np.array([3.5, -2.0, 1.0]))]
+    hh = ib.KSHamiltonian(rs)
+    pseudo.set_ions(hh, atoms)
+    hd = ib.KSHamiltonian(rs)
+    pseudo.set_ions(hd, atoms, device=True)
+    assert hh.projectors_info() == hd.projectors_info()
+    p_h, x_h, m_h, n_h = hh.projector_tables()
+    p_d, x_d, m_d, n_d = hd.projector_tables()
+    assert np.array_equal(n_h, n_d) and np.array_equal(p_h, p_d) and np.array_equal(x_h, x_d)
+    assert np.max(np.abs(m_h - m_d)) <= 1e-13 * np.max(np.abs(m_h))
+    x = rng.standard_normal(tuple(sizes) + (4,)) + 1j * rng.standard_normal(tuple(sizes) + (4,))
+    phi = ib.OrbitalSet.from_array(rs, x, kpoint=(0.05, 0.0, -0.1))
+    a, b = hd(phi).matrix(), hh(phi).matrix()
+    assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(b)
+    # moving the atoms
+    moved = [(p_, R + rng.normal(0.0, 0.2, 3)) for p_, R in atoms]
+    hd.move_atoms(np.array([R for _, R in moved]))
+    hr = ib.KSHamiltonian(rs)
+    pseudo.set_ions(hr, moved)
+    p_m, x_m, m_m, n_m = hd.projector_tables()
+    p_r, x_r, m_r, n_r = hr.projector_tables()
+    assert np.array_equal(n_m, n_r) and np.array_equal(p_m, p_r) and np.array_equal(x_m, x_r)
+    assert np.max(np.abs(m_m - m_r)) <= 1e-13 * np.max(np.abs(m_r))
