@@ -324,6 +324,23 @@ __device__ __forceinline__ void dft(T (&v)[M], const T *__restrict__ tw) {
 // Two-level in-place transform of a [N][W] tile (rows = points, natural order in and out).
 template <typename TO, typename TI> __device__ __forceinline__ TO conv(TI x) { return mk<TO>(decltype(TO::x)(x.x), decltype(TO::x)(x.y)); }
 
+// Barrier of the CTA's NT compute threads (named barrier 1).  A kernel with a producer warp runs it
+// after the NT compute threads; that warp never joins, so the compute threads synchronise among
+// themselves.  Without a producer warp NT is the whole CTA.
+template <int NT> __device__ __forceinline__ void csync() { asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); }
+// the same barrier, returning whether any compute thread passed a nonzero value (uniform result)
+template <int NT> __device__ __forceinline__ bool csync_or(int v) {
+  uint32_t r;
+  asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+               : "=r"(r)
+               : "r"(v), "n"(NT)
+               : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // The tile transforms below end without a barrier: their last step writes only addresses the
 // writing thread owns in that step, and the kernel's fence + barrier before the TMA store (or an
 // explicit barrier before another sweep) orders those writes for the other threads.
@@ -353,7 +370,7 @@ __device__ __forceinline__ void tile_dft(const SA *asrc, DA *adst, const TC *__r
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) adst[(j2 + N2 * k1) * W + w] = conv<DA>(s[k1]);
   }
-  __syncthreads();
+  csync<NT>();
   if constexpr (HOLD) {
     constexpr int IB = (W * N1 + NT - 1) / NT;
     TC r[IB][N2];
@@ -367,7 +384,7 @@ __device__ __forceinline__ void tile_dft(const SA *asrc, DA *adst, const TC *__r
         dft<N2, DIR, N>(r[b], tw);
       }
     }
-    __syncthreads();
+    csync<NT>();
 #pragma unroll
     for (int b = 0; b < IB; b++) {
       const int it = threadIdx.x + b * NT;
@@ -417,7 +434,7 @@ __device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *_
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) buf[(j2 + N2 * k1) * W + w] = s[k1];
   }
-  __syncthreads();
+  csync<NT>();
   constexpr int IB = (W * N1 + NT - 1) / NT;
   T r[IB][N2];
 #pragma unroll
@@ -430,7 +447,7 @@ __device__ __forceinline__ void tile_dft_inplace(T *__restrict__ buf, const T *_
       dft<N2, DIR, N, (sizeof(decltype(T::x)) == 4 && DIR > 0)>(r[b], tw);
     }
   }
-  __syncthreads();
+  csync<NT>();
 #pragma unroll
   for (int b = 0; b < IB; b++) {
     const int it = threadIdx.x + b * NT;
@@ -488,7 +505,7 @@ __device__ __forceinline__ void tile_kin_inplace(T *__restrict__ buf, const T *_
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   constexpr int IB = N2 <= 12 ? (W * N1 + NT - 1) / NT : 1;
   col_forward_inplace<N, W, NT, T>(buf, tw);
-  __syncthreads();
+  csync<NT>();
   for (int it0 = threadIdx.x; it0 < W * N1; it0 += IB * NT) {
     T r[IB][N2];
 #pragma unroll
@@ -518,7 +535,7 @@ __device__ __forceinline__ void tile_kin_inplace(T *__restrict__ buf, const T *_
       }
     }
   }
-  __syncthreads();
+  csync<NT>();
   col_inverse_inplace<N, W, NT, T>(buf, tw, epi);
 }
 
@@ -528,7 +545,7 @@ template <int N, int W, int NT, typename T, typename Epi>
 __device__ __forceinline__ void tile_fwd_perm_inplace(T *__restrict__ buf, const T *__restrict__ tw, Epi epi) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, IB = (W * N1 + NT - 1) / NT;
   col_forward_inplace<N, W, NT, T>(buf, tw);
-  __syncthreads();
+  csync<NT>();
   T r[IB][N2];
 #pragma unroll
   for (int b = 0; b < IB; b++) {
@@ -580,7 +597,7 @@ __device__ __forceinline__ void tile_inv_perm_inplace(T *__restrict__ buf, const
       for (int j2 = 0; j2 < N2; j2++) buf[(j2 + N2 * k1) * W + w] = r[b][j2];
     }
   }
-  __syncthreads();
+  csync<NT>();
   col_inverse_inplace<N, W, NT, T>(buf, tw, epi);
 }
 
@@ -640,7 +657,7 @@ __device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC 
   // rows of up to 12 points are batched (two transforms per row keep longer rows one at a time)
   constexpr int IB = N2 <= 12 ? (W * N1 + NT - 1) / NT : 1;
   col_forward<N, W, NT, TC>(asrc, work, tw);
-  __syncthreads();
+  csync<NT>();
   for (int it0 = threadIdx.x; it0 < W * N1; it0 += IB * NT) {
     TC r[IB][N2];
 #pragma unroll
@@ -670,7 +687,7 @@ __device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC 
       }
     }
   }
-  __syncthreads();
+  csync<NT>();
   col_inverse<N, W, NT, TC>(work, tw, put);
 }
 
@@ -707,6 +724,15 @@ template <typename R, typename CR, int N, int VAR> constexpr int threads_of() {
   return (VAR != MID_KIN && W == 16 && M > 128 && M <= 256) ? (M + 31) / 32 * 32 : 128;
 }
 
+// Whether the kernel runs a producer warp: one extra warp whose lane 0 issues every TMA load and
+// store and waits for the stores to drain, so no compute thread stalls on the copies.
+template <typename R, typename CR, int N, int VAR> constexpr bool ws_of() {
+  return sizeof(R) == 4 && sizeof(CR) == 4 && VAR != MID_KIN;
+}
+template <typename R, typename CR, int N, int VAR> constexpr int block_threads_of() {
+  return threads_of<R, CR, N, VAR>() + (ws_of<R, CR, N, VAR>() ? 32 : 0);
+}
+
 // CTAs per SM the register allocation must allow: four for the single-precision kinetic pass of lines
 // up to 96 points (two transforms per tile, latency-bound with fewer warps; longer lines would spill);
 // 0 (no constraint: the compiler's own register choice) otherwise.
@@ -715,13 +741,15 @@ template <typename R, typename CR, int N, int VAR> constexpr int min_ctas_of() {
 }
 
 template <typename R, typename CR, int N, int VAR>
-__global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR, N, VAR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
+__global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR, N, VAR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
                                                    const __grid_constant__ CUtensorMap map_out,
                                                    const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
                                                    const C2<CR> *__restrict__ twg, int *err) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr int NT = threads_of<R, CR, N, VAR>();
+  constexpr int NT = threads_of<R, CR, N, VAR>();   // compute threads
+  constexpr bool WS = ws_of<R, CR, N, VAR>();       // plus a producer warp
+  constexpr int NTT = block_threads_of<R, CR, N, VAR>();
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);    // exchange buffer in the arithmetic type
   constexpr int W = tile_w<R, CR>();
   constexpr int TILE = N * W;                       // complex elements per tile
@@ -736,14 +764,18 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
   constexpr int TWN = tw_entries<CR>(N);
   TC *tw = exch + (SPLIT ? TILE : 0);                                // twiddles (high, then low parts)
   CR *linev = reinterpret_cast<CR *>(tw + TWN);                      // N per-point factors of the current line
-  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + TWN + N);        // NS barriers (8-byte aligned)
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(bar + NS);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tw + TWN + N);        // NS "tile loaded" barriers (8-byte aligned)
+  uint64_t *done = bar + NS;                                         // NS "tile computed" barriers (producer warp)
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(done + NS);
 
   const Geom &g = gg.g;
-  for (int i = threadIdx.x; i < TWN; i += NT) tw[i] = twg[i];
+  for (int i = threadIdx.x; i < TWN; i += NTT) tw[i] = twg[i];
   if (threadIdx.x == 0) {
     *abort_flag = 0;
-    for (int s = 0; s < NS; s++) mbar_init(&bar[s], 1);
+    for (int s = 0; s < NS; s++) {
+      mbar_init(&bar[s], 1);
+      if constexpr (WS) mbar_init(&done[s], NT);
+    }
     mbar_init_fence();
   }
   __syncthreads();
@@ -765,10 +797,46 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
     if constexpr (AUX) tma_load_4d(stage_aux + size_t(st) * TILE, &map_aux, &bar[st], c0, c1, c2, c3);
   };
 
-  if (threadIdx.x == 0) {
+  // bounded wait on an mbarrier phase; false (and the error flag raised) on expiry or abort
+  auto wait_bar = [&](uint64_t *b, uint32_t parity) -> bool {
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(b, parity)) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > 2000000000ull) {
+        *abort_flag = 1;
+        atomicExch(err, 1);
+        return false;
+      }
+    }
+    return true;
+  };
+
+  if (threadIdx.x == (WS ? NT : 0)) {
     for (int s = 0; s < NS; s++) {
       const long long t = blockIdx.x + (long long)s * gridDim.x;
       if (t < gg.ntiles) issue(s, t);
+    }
+  }
+  if constexpr (WS) {
+    if (threadIdx.x >= NT) {
+      // producer warp: lane 0 stores every computed tile, waits for the store to read the stage and
+      // refills it with the tile NS steps ahead
+      if (threadIdx.x == NT) {
+        int k = 0;
+        for (long long t = blockIdx.x; t < gg.ntiles; t += gridDim.x, k++) {
+          const int st = k % NS;
+          if (!wait_bar(&done[st], uint32_t(k / NS) & 1u)) break;
+          int c0, c1, c2, c3;
+          coords(t, c0, c1, c2, c3);
+          tma_store_4d(&map_out, stage_in + size_t(st) * TILE, c0, c1, c2, c3);
+          bulk_commit();
+          bulk_wait_read0();
+          const long long tn = t + (long long)NS * gridDim.x;
+          if (tn < gg.ntiles) issue(st, tn);
+        }
+        bulk_wait0();
+      }
+      return;
     }
   }
 
@@ -778,20 +846,9 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
   for (long long t = blockIdx.x; t < gg.ntiles; t += gridDim.x, i++) {
     const int st = i % NS;
     const uint32_t par = uint32_t(i / NS) & 1u;
-    // bounded wait for this stage's TMA load
-    {
-      const uint64_t t0 = global_ns();
-      while (!mbar_try_wait(&bar[st], par)) {
-        if (*abort_flag) break;
-        if (global_ns() - t0 > 2000000000ull) {
-          *abort_flag = 1;
-          atomicExch(err, 1);
-          break;
-        }
-      }
-    }
-    __syncthreads();
-    if (*abort_flag) break;
+    // bounded wait for this stage's TMA load; every compute thread takes the same decision
+    const bool ok = wait_bar(&bar[st], par);
+    if (csync_or<NT>(!ok || *abort_flag)) break;
 
     T *buf = stage_in + size_t(st) * TILE;
     const T *aux = stage_aux + size_t(st) * TILE;
@@ -815,7 +872,7 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
         linev[m] = CR(a.V[(pbase + m * g.sp) * a.nspin + a.spin]) + CR(a.vshift);
     }
     if constexpr (VAR == FWD_VPSI) {
-      __syncthreads();
+      csync<NT>();
       if (a.nl_offs) {
         // Fourier-form operator: (V + shift) psi + nonlocal(psi) formed in shared memory before the transform
         for (int e = threadIdx.x; e < TILE; e += NT) {
@@ -826,7 +883,7 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
             buf[e] = cadd(v, nl_term<R>(a, pt, s));
           }
         }
-        __syncthreads();
+        csync<NT>();
       }
     }
 
@@ -860,7 +917,7 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
       if constexpr (VAR == FWD_VPSI) {
         if (!a.nl_offs) {
           for (int e = threadIdx.x; e < TILE; e += NT) buf[e] = cscale(buf[e], linev[e / W]);
-          __syncthreads();
+          csync<NT>();
         }
       }
       // plain passes (no scaling, no accumulators) store the transform's values as they are
@@ -874,7 +931,7 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
         if constexpr (VAR == FWD_PERM) tile_fwd_perm_inplace<N, W, NT, T>(buf, twt, Identity());
         else tile_inv_perm_inplace<N, W, NT, T>(buf, twt, Identity());
         if (!plain) {
-          __syncthreads();
+          csync<NT>();
           for (int e = threadIdx.x; e < TILE; e += NT) put_out(e / W, e % W, buf[e]);
         }
       } else if constexpr (AUX) {
@@ -883,25 +940,29 @@ __global__ void __launch_bounds__(threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR
       } else {
         tile_dft_inplace<N, D, W, NT, T>(buf, twt, Identity());
         if (!plain) {
-          __syncthreads();
+          csync<NT>();
           for (int e = threadIdx.x; e < TILE; e += NT) put_out(e / W, e % W, buf[e]);
         }
       }
     }
 
     fence_proxy_async();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int c0, c1, c2, c3;
-      coords(t, c0, c1, c2, c3);
-      tma_store_4d(&map_out, buf, c0, c1, c2, c3);
-      bulk_commit();
-      bulk_wait_read0();  // the stage may be refilled once the store has read it
-      const long long tn = t + (long long)NS * gridDim.x;
-      if (tn < gg.ntiles) issue(st, tn);
+    if constexpr (WS) {
+      mbar_arrive(&done[st]);  // the producer warp stores the tile and refills the stage
+    } else {
+      csync<NT>();
+      if (threadIdx.x == 0) {
+        int c0, c1, c2, c3;
+        coords(t, c0, c1, c2, c3);
+        tma_store_4d(&map_out, buf, c0, c1, c2, c3);
+        bulk_commit();
+        bulk_wait_read0();  // the stage may be refilled once the store has read it
+        const long long tn = t + (long long)NS * gridDim.x;
+        if (tn < gg.ntiles) issue(st, tn);
+      }
     }
   }
-  if (threadIdx.x == 0) bulk_wait0();
+  if (!WS && threadIdx.x == 0) bulk_wait0();
 }
 
 }  // namespace v2
@@ -953,7 +1014,7 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
   const int nbuf = has_aux(VAR) ? 2 : 1;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
-  constexpr int NT = threads_of<R, CR, N, VAR>();
+  constexpr int NT = block_threads_of<R, CR, N, VAR>();
   const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + size_t(tw_entries<CR>(N) + N) * sizeof(TC) + 64 + 16 * 8;
   // shared memory per CTA: ~113 KB (two CTAs per SM) for the streaming passes; ~56 KB (four per SM)
   // for the wide-arithmetic and the kinetic passes, whose arithmetic needs more warps to hide latency
