@@ -1018,9 +1018,11 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
   constexpr int NT = block_threads_of<R, CR, N, VAR>();
   const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + size_t(tw_entries<CR>(N) + N) * sizeof(TC) + 64 + 16 * 8;
-  // shared memory per CTA: ~113 KB (two CTAs per SM) for the streaming passes; ~56 KB (four per SM)
-  // for the wide-arithmetic and the kinetic passes, whose arithmetic needs more warps to hide latency
-  const size_t budget = (SPLIT || VAR == MID_KIN) ? 56 * 1024 : 113 * 1024;
+  // shared memory per CTA: ~113 KB (two CTAs per SM) for the FP64 streaming passes; ~56 KB (four per SM)
+  // for the wide-arithmetic, the kinetic and the producer-warp (single-precision) passes, whose
+  // arithmetic needs more warps to hide latency (96^3 x 256 single: 3.81 ms per H against 3.89 with
+  // four stages of 113 KB)
+  const size_t budget = (SPLIT || VAR == MID_KIN || ws_of<R, CR, N, VAR>()) ? 56 * 1024 : 113 * 1024;
   int ns = int((budget - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;
