@@ -110,12 +110,13 @@ SIGNATURES = {
 
 
 def load(path: str | None = None):
-    """Load (once) and return the CDLL with argtypes set.  Raises if the library is absent."""
+    """Load (once) and return the CDLL with argtypes set: ``path``, else the INQB_LIBRARY environment
+    variable, else the in-tree build.  Raises if the library is absent."""
     global _lib
     with _lock:
         if _lib is not None:
             return _lib
-        p = path or LIB_PATH
+        p = path or os.environ.get("INQB_LIBRARY") or LIB_PATH
         if not os.path.exists(p):
             raise InqbError(-1, f"{p} is missing: build it with `python -m inq_b200.build`")
         lib = C.CDLL(p)

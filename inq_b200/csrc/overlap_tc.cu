@@ -15,7 +15,8 @@
 // accumulator that is restarted every WIN chunks, its window sum read out (tcgen05.ld) and added with
 // round-to-nearest into an FP32 running sum in shared memory; the small correction products (2^-8 of
 // the main ones, random in sign) go into a "corr" accumulator kept over the whole range.  Remaining
-// bias: ~2 MMAs per chunk x WIN chunks x 2^-25.
+// bias: ~2 MMAs per chunk x WIN chunks x 2^-25.  Measured at 96^3 x 256: WIN = 2, 4, 8 give diagonal
+// biases of -1.0e-7, -1.9e-7, -4.0e-7 and 4.1, 3.5, 3.2 ms per overlap; 4 keeps a 5x margin to 1e-6.
 //
 // Tiles.  One CTA per SM holds 128 states of a (tensor-memory lanes) against 128 states of b: the
 // main and corr accumulators of the real and imaginary parts take the 4 x 128 tensor-memory columns;
@@ -24,8 +25,9 @@
 // per thread and eight consecutive points, coalesced across the warp), split them and store the BF16
 // planes in the canonical K-major layout (core matrices of 8 rows x 16 bytes), and one thread issues
 // the chunk's 16 MMAs (128 x N x 16, kind::f16, BF16 in, FP32 accumulate) and commits them to the
-// buffer's mbarrier.  Two operand buffers alternate; the next chunk's loads are in flight while the
-// current chunk is converted.  The per-CTA FP32 partial sums go to global memory and a second kernel
+// buffer's mbarrier.  Two operand buffers alternate; the loads of the chunk two ahead are in flight
+// while the current chunk is converted (one ahead: 3.5 ms per overlap at 96^3 x 256; two: 3.0; more
+// gains nothing).  The per-CTA FP32 partial sums go to global memory and a second kernel
 // adds them in a fixed order in FP64, so the result does not depend on scheduling.
 //
 // Every mbarrier wait is bounded (2 s by %globaltimer); on expiry the kernel raises the context's
@@ -43,7 +45,8 @@ constexpr int TC_M = 128;         // states of a per CTA = tensor-memory lanes =
 constexpr int TC_N = 128;         // states of b per CTA at most = MMA N
 constexpr int TC_KC = 16;         // points per chunk = MMA K
 constexpr int TC_THREADS = 256;
-constexpr int WIN = 2;            // chunks per window of the main accumulators
+constexpr int WIN = 4;            // chunks per window of the main accumulators
+constexpr int LOOK = 3;           // chunks whose values are held in registers (current + 2 in flight)
 constexpr uint32_t PLANE = TC_M * TC_KC * 2;            // bytes of one BF16 plane (4 KB; a and b alike)
 constexpr uint32_t BUF_BYTES = 8 * PLANE;               // re_hi, re_lo, im_hi, im_lo of a, then of b
 constexpr uint32_t SUM_BYTES = 2 * TC_N * TC_M * 4;     // FP32 running sums of the main products
@@ -125,21 +128,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   // flush and epilogue roles: lane quarter (rows) and real / imaginary part of this warp
   const int q = warp & 3, h = warp >> 2;
   const int myrow = q * 32 + lane;
-  float2 ca[8], cb[8], na[8], nb[8];
-  if (nchunks > 0) {
-    load_unit(a, Sa, acol, aok, kbeg + kh * 8, kend, ca);
-    load_unit(b, Sb, bcol, bok, kbeg + kh * 8, kend, cb);
-  }
+  // values of the current chunk and of the next LOOK - 1: the loads of chunk c + LOOK - 1 are issued
+  // while chunk c is converted, LOOK - 1 chunk times ahead of their use
+  float2 pa[LOOK][8], pb[LOOK][8];
+#pragma unroll
+  for (int d = 0; d < LOOK - 1; d++)
+    if (d < nchunks) {
+      load_unit(a, Sa, acol, aok, kbeg + (long long)d * TC_KC + kh * 8, kend, pa[d]);
+      load_unit(b, Sb, bcol, bok, kbeg + (long long)d * TC_KC + kh * 8, kend, pb[d]);
+    }
 
   int issued = 0;
   for (int c = 0; c < nchunks; c++) {
     const int bsel = c & 1;
     unsigned char *bufA = smem + bsel * BUF_BYTES;
     unsigned char *bufB = bufA + 4 * PLANE;
-    if (c + 1 < nchunks) {
-      const long long k1 = kbeg + (long long)(c + 1) * TC_KC + kh * 8;
-      load_unit(a, Sa, acol, aok, k1, kend, na);
-      load_unit(b, Sb, bcol, bok, k1, kend, nb);
+    if (c + LOOK - 1 < nchunks) {
+      const long long kn = kbeg + (long long)(c + LOOK - 1) * TC_KC + kh * 8;
+      load_unit(a, Sa, acol, aok, kn, kend, pa[LOOK - 1]);
+      load_unit(b, Sb, bcol, bok, kn, kend, pb[LOOK - 1]);
     }
     // the MMAs of chunk c - 2 read this buffer
     if (c >= 2 && !ptx::mbar_wait_bounded(&done[bsel], uint32_t((c - 2) >> 1) & 1u, WAIT_NS)) {
@@ -148,8 +155,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     __syncthreads();
     if (*abort_flag) break;
-    store_unit(bufA, row, kh, ca);
-    store_unit(bufB, row, kh, cb);
+    store_unit(bufA, row, kh, pa[0]);
+    store_unit(bufB, row, kh, pb[0]);
     ptx::fence_proxy_async();
     __syncthreads();
     if (t == 0) {
@@ -204,10 +211,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       __syncthreads();
     }
 #pragma unroll
-    for (int u = 0; u < 8; u++) {
-      ca[u] = na[u];
-      cb[u] = nb[u];
-    }
+    for (int d = 0; d < LOOK - 1; d++)
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        pa[d][u] = pa[d + 1][u];
+        pb[d][u] = pb[d + 1][u];
+      }
   }
 
   // on an abort, the last commit covers every MMA issued before it
