@@ -337,9 +337,7 @@ template <int NT> __device__ __forceinline__ bool csync_or(int v) {
                : "memory");
   return r != 0;
 }
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
+using ptx::mbar_arrive;
 
 // The tile transforms below end without a barrier: their last step writes only addresses the
 // writing thread owns in that step, and the kernel's fence + barrier before the TMA store (or an

@@ -50,7 +50,8 @@ constexpr int LOOK = 3;           // chunks whose values are held in registers (
 constexpr uint32_t PLANE = TC_M * TC_KC * 2;            // bytes of one BF16 plane (4 KB; a and b alike)
 constexpr uint32_t BUF_BYTES = 8 * PLANE;               // re_hi, re_lo, im_hi, im_lo of a, then of b
 constexpr uint32_t SUM_BYTES = 2 * TC_N * TC_M * 4;     // FP32 running sums of the main products
-constexpr size_t TC_SMEM = 2 * BUF_BYTES + SUM_BYTES + 64;
+constexpr int NB = 3;             // operand buffers (converted chunks in flight to the tensor cores)
+constexpr size_t TC_SMEM = NB * BUF_BYTES + SUM_BYTES + 128;
 constexpr uint64_t WAIT_NS = 2000000000ull;
 // tensor-memory columns of the four accumulators
 constexpr uint32_t COL_MAIN_RE = 0, COL_MAIN_IM = 128, COL_CORR_RE = 256, COL_CORR_IM = 384;
@@ -89,15 +90,20 @@ __device__ __forceinline__ void load_unit(const float2 *__restrict__ src, int S,
     x[u] = (colok && k + u < kend) ? __ldg(&src[(k + u) * S + col]) : make_float2(0.f, 0.f);
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TC_THREADS + 32, 1)
     overlap_tc_kernel(const float2 *__restrict__ a, int Sa, const float2 *__restrict__ b, int Sb,
                       long long npoints, int mtiles, int ntiles, int N, long long kper, float *__restrict__ partial,
                       int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  float *sums = reinterpret_cast<float *>(smem + 2 * BUF_BYTES);                    // [2][TC_N][TC_M]
-  uint64_t *done = reinterpret_cast<uint64_t *>(smem + 2 * BUF_BYTES + SUM_BYTES);  // one per operand buffer
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 2);
+  float *sums = reinterpret_cast<float *>(smem + NB * BUF_BYTES);                    // [2][TC_N][TC_M]
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + NB * BUF_BYTES + SUM_BYTES);  // chunk converted, per buffer
+  uint64_t *empty = full + NB;                                                      // chunk's MMAs done, per buffer
+  uint64_t *win_done = empty + NB;                                                  // a window's MMAs done
+  uint64_t *flushed = win_done + 1;                                                 // its main sums flushed
+  uint64_t *fin = flushed + 1;                                                      // every issued MMA done
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(fin + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tslot + 1);
+  volatile int *issued_any = abort_flag + 1;
 
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int tiles = mtiles * ntiles;
@@ -107,11 +113,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const long long kend = kbeg + kper < npoints ? kbeg + kper : npoints;
   const int nchunks = kend > kbeg ? int((kend - kbeg + TC_KC - 1) / TC_KC) : 0;
 
-  for (int i = t; i < 2 * TC_N * TC_M; i += TC_THREADS) sums[i] = 0.f;
+  for (int i = t; i < 2 * TC_N * TC_M; i += TC_THREADS + 32) sums[i] = 0.f;
   if (t == 0) {
-    ptx::mbar_init(&done[0], 1);
-    ptx::mbar_init(&done[1], 1);
+    for (int i = 0; i < NB; i++) {
+      ptx::mbar_init(&full[i], TC_THREADS);
+      ptx::mbar_init(&empty[i], 1);
+    }
+    ptx::mbar_init(win_done, 1);
+    ptx::mbar_init(flushed, TC_THREADS);
+    ptx::mbar_init(fin, 1);
     *abort_flag = 0;
+    *issued_any = 0;
     ptx::mbar_init_fence();
   }
   if (warp == 0) ptx::tmem_alloc(tslot, 512);
@@ -120,135 +132,146 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   ptx::tc_fence_after();
   const uint32_t tmem = *tslot;
   const uint32_t id = ptx::idesc_bf16_f32(TC_M, N, false), idn = ptx::idesc_bf16_f32(TC_M, N, true);
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicExch(err, 1);
+  };
+  auto wait = [&](uint64_t *bar, uint32_t parity) -> bool {
+    const uint64_t t0 = ptx::global_ns();
+    while (!ptx::mbar_try_wait(bar, parity)) {
+      if (*abort_flag) return false;
+      if (ptx::global_ns() - t0 > WAIT_NS) {
+        fail();
+        return false;
+      }
+    }
+    return true;
+  };
 
-  // conversion units: each chunk of a and of b has 128 rows x 2 K halves, one unit of each per thread
-  const int row = t & (TC_M - 1), kh = t >> 7;
-  const int acol = m0 + row, bcol = n0 + row;
-  const bool aok = acol < Sa, bok = row < N && bcol < Sb;
-  // flush and epilogue roles: lane quarter (rows) and real / imaginary part of this warp
-  const int q = warp & 3, h = warp >> 2;
-  const int myrow = q * 32 + lane;
-  // values of the current chunk and of the next LOOK - 1: the loads of chunk c + LOOK - 1 are issued
-  // while chunk c is converted, LOOK - 1 chunk times ahead of their use
-  float2 pa[LOOK][8], pb[LOOK][8];
+  if (warp == TC_THREADS / 32) {
+    // issuer warp: lane 0 issues every chunk's 16 MMAs once its planes are in shared memory
+    if (lane == 0) {
+      int issued = 0;
+      for (int c = 0; c < nchunks; c++) {
+        const int bsel = c % NB;
+        if (!wait(&full[bsel], uint32_t(c / NB) & 1u)) break;
+        if (c % WIN == 0 && c > 0 && !wait(flushed, uint32_t(c / WIN - 1) & 1u)) break;  // main restarts
+        ptx::tc_fence_after();
+        const uint32_t ab = ptx::smem_u32(smem + bsel * BUF_BYTES), bb = ab + 4 * PLANE;
+        uint64_t da[4], db[4];
 #pragma unroll
-  for (int d = 0; d < LOOK - 1; d++)
-    if (d < nchunks) {
-      load_unit(a, Sa, acol, aok, kbeg + (long long)d * TC_KC + kh * 8, kend, pa[d]);
-      load_unit(b, Sb, bcol, bok, kbeg + (long long)d * TC_KC + kh * 8, kend, pb[d]);
-    }
-
-  int issued = 0;
-  for (int c = 0; c < nchunks; c++) {
-    const int bsel = c & 1;
-    unsigned char *bufA = smem + bsel * BUF_BYTES;
-    unsigned char *bufB = bufA + 4 * PLANE;
-    if (c + LOOK - 1 < nchunks) {
-      const long long kn = kbeg + (long long)(c + LOOK - 1) * TC_KC + kh * 8;
-      load_unit(a, Sa, acol, aok, kn, kend, pa[LOOK - 1]);
-      load_unit(b, Sb, bcol, bok, kn, kend, pb[LOOK - 1]);
-    }
-    // the MMAs of chunk c - 2 read this buffer
-    if (c >= 2 && !ptx::mbar_wait_bounded(&done[bsel], uint32_t((c - 2) >> 1) & 1u, WAIT_NS)) {
-      *abort_flag = 1;
-      atomicExch(err, 1);
-    }
-    __syncthreads();
-    if (*abort_flag) break;
-    store_unit(bufA, row, kh, pa[0]);
-    store_unit(bufB, row, kh, pb[0]);
-    ptx::fence_proxy_async();
-    __syncthreads();
-    if (t == 0) {
-      ptx::tc_fence_after();
-      const uint32_t ab = ptx::smem_u32(bufA), bb = ptx::smem_u32(bufB);
-      uint64_t da[4], db[4];
-#pragma unroll
-      for (int p = 0; p < 4; p++) {
-        da[p] = ptx::smem_desc_kmajor(ab + p * PLANE, 128, 256);
-        db[p] = ptx::smem_desc_kmajor(bb + p * PLANE, 128, 256);
+        for (int p = 0; p < 4; p++) {
+          da[p] = ptx::smem_desc_kmajor(ab + p * PLANE, 128, 256);
+          db[p] = ptx::smem_desc_kmajor(bb + p * PLANE, 128, 256);
+        }
+        const bool fresh_main = (c % WIN) == 0, fresh_corr = c == 0;
+        const uint32_t mre = tmem + COL_MAIN_RE, mim = tmem + COL_MAIN_IM;
+        const uint32_t cre = tmem + COL_CORR_RE, cim = tmem + COL_CORR_IM;
+        // planes: 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo
+        ptx::mma_bf16(mre, da[0], db[0], id, !fresh_main);
+        ptx::mma_bf16(mre, da[2], db[2], id, true);
+        ptx::mma_bf16(mim, da[0], db[2], id, !fresh_main);
+        ptx::mma_bf16(mim, da[2], db[0], idn, true);
+        ptx::mma_bf16(cre, da[0], db[1], id, !fresh_corr);
+        ptx::mma_bf16(cre, da[1], db[0], id, true);
+        ptx::mma_bf16(cre, da[1], db[1], id, true);
+        ptx::mma_bf16(cre, da[2], db[3], id, true);
+        ptx::mma_bf16(cre, da[3], db[2], id, true);
+        ptx::mma_bf16(cre, da[3], db[3], id, true);
+        ptx::mma_bf16(cim, da[0], db[3], id, !fresh_corr);
+        ptx::mma_bf16(cim, da[1], db[2], id, true);
+        ptx::mma_bf16(cim, da[1], db[3], id, true);
+        ptx::mma_bf16(cim, da[2], db[1], idn, true);
+        ptx::mma_bf16(cim, da[3], db[0], idn, true);
+        ptx::mma_bf16(cim, da[3], db[1], idn, true);
+        ptx::mma_commit(&empty[bsel]);
+        if ((c % WIN) == WIN - 1 || c == nchunks - 1) ptx::mma_commit(win_done);
+        issued = c + 1;
+        *issued_any = 1;
       }
-      const bool fresh_main = (c % WIN) == 0, fresh_corr = c == 0;
-      const uint32_t mre = tmem + COL_MAIN_RE, mim = tmem + COL_MAIN_IM;
-      const uint32_t cre = tmem + COL_CORR_RE, cim = tmem + COL_CORR_IM;
-      // planes: 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo
-      ptx::mma_bf16(mre, da[0], db[0], id, !fresh_main);
-      ptx::mma_bf16(mre, da[2], db[2], id, true);
-      ptx::mma_bf16(mim, da[0], db[2], id, !fresh_main);
-      ptx::mma_bf16(mim, da[2], db[0], idn, true);
-      ptx::mma_bf16(cre, da[0], db[1], id, !fresh_corr);
-      ptx::mma_bf16(cre, da[1], db[0], id, true);
-      ptx::mma_bf16(cre, da[1], db[1], id, true);
-      ptx::mma_bf16(cre, da[2], db[3], id, true);
-      ptx::mma_bf16(cre, da[3], db[2], id, true);
-      ptx::mma_bf16(cre, da[3], db[3], id, true);
-      ptx::mma_bf16(cim, da[0], db[3], id, !fresh_corr);
-      ptx::mma_bf16(cim, da[1], db[2], id, true);
-      ptx::mma_bf16(cim, da[1], db[3], id, true);
-      ptx::mma_bf16(cim, da[2], db[1], idn, true);
-      ptx::mma_bf16(cim, da[3], db[0], idn, true);
-      ptx::mma_bf16(cim, da[3], db[1], idn, true);
-      ptx::mma_commit(&done[bsel]);
+      if (issued > 0) ptx::mma_commit(fin);
     }
-    issued = c + 1;
-    if ((c % WIN) == WIN - 1 || c == nchunks - 1) {
-      // end of a window: add the main accumulators into the shared-memory running sums
-      if (!ptx::mbar_wait_bounded(&done[bsel], uint32_t(c >> 1) & 1u, WAIT_NS)) {
-        *abort_flag = 1;
-        atomicExch(err, 1);
-      }
-      __syncthreads();
-      if (*abort_flag) break;
-      ptx::tc_fence_after();
-      float *sum = sums + size_t(h) * TC_N * TC_M;
-      for (int j0 = 0; j0 < N; j0 += 16) {
-        float v[16];
-        ptx::tmem_ld16(tmem + (uint32_t(q * 32) << 16) + (h ? COL_MAIN_IM : COL_MAIN_RE) + uint32_t(j0), v);
-#pragma unroll
-        for (int u = 0; u < 16; u++) sum[(j0 + u) * TC_M + myrow] += v[u];
-      }
-      ptx::tc_fence_before();
-      __syncthreads();
-    }
+  } else {
+    // converter warps: load, split and store the chunks; flush the main sums at each window's end
+    const int row = t & (TC_M - 1), kh = t >> 7;
+    const int acol = m0 + row, bcol = n0 + row;
+    const bool aok = acol < Sa, bok = row < N && bcol < Sb;
+    const int q = warp & 3, h = warp >> 2;
+    const int myrow = q * 32 + lane;
+    float2 pa[LOOK][8], pb[LOOK][8];
 #pragma unroll
     for (int d = 0; d < LOOK - 1; d++)
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        pa[d][u] = pa[d + 1][u];
-        pb[d][u] = pb[d + 1][u];
+      if (d < nchunks) {
+        load_unit(a, Sa, acol, aok, kbeg + (long long)d * TC_KC + kh * 8, kend, pa[d]);
+        load_unit(b, Sb, bcol, bok, kbeg + (long long)d * TC_KC + kh * 8, kend, pb[d]);
       }
-  }
-
-  // on an abort, the last commit covers every MMA issued before it
-  if (*abort_flag && issued > 0) {
-    const int last = issued - 1;
-    (void)ptx::mbar_wait_bounded(&done[last & 1], uint32_t(last >> 1) & 1u, WAIT_NS);
-  }
-  ptx::tc_fence_before();
-  __syncthreads();
-  ptx::tc_fence_after();
-  if (!*abort_flag) {
-    const int ia = m0 + myrow;
-    const float *sum = sums + size_t(h) * TC_N * TC_M;
-    float *dst = partial + ((size_t(ks) * 2 + h) * size_t(Sa) + size_t(ia)) * size_t(Sb) + n0;
-    for (int j0 = 0; j0 < N; j0 += 16) {
-      float v[16];
-      if (issued > 0) {
-        ptx::tmem_ld16(tmem + (uint32_t(q * 32) << 16) + (h ? COL_CORR_IM : COL_CORR_RE) + uint32_t(j0), v);
-      } else {
-#pragma unroll
-        for (int u = 0; u < 16; u++) v[u] = 0.f;
+    bool ok = true;
+    for (int c = 0; c < nchunks && ok; c++) {
+      const int bsel = c % NB;
+      if (c + LOOK - 1 < nchunks) {
+        const long long kn = kbeg + (long long)(c + LOOK - 1) * TC_KC + kh * 8;
+        load_unit(a, Sa, acol, aok, kn, kend, pa[LOOK - 1]);
+        load_unit(b, Sb, bcol, bok, kn, kend, pb[LOOK - 1]);
       }
-      if (ia < Sa) {
+      // the MMAs of chunk c - NB read this buffer
+      if (c >= NB && !wait(&empty[bsel], uint32_t(c / NB - 1) & 1u)) break;
+      unsigned char *bufA = smem + bsel * BUF_BYTES;
+      store_unit(bufA, row, kh, pa[0]);
+      store_unit(bufA + 4 * PLANE, row, kh, pb[0]);
+      ptx::fence_proxy_async();
+      ptx::mbar_arrive(&full[bsel]);
 #pragma unroll
-        for (int u = 0; u < 16; u++)
-          if (n0 + j0 + u < Sb) dst[j0 + u] = sum[(j0 + u) * TC_M + myrow] + v[u];
+      for (int d = 0; d < LOOK - 1; d++)
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          pa[d][u] = pa[d + 1][u];
+          pb[d][u] = pb[d + 1][u];
+        }
+      if ((c % WIN) == WIN - 1 || c == nchunks - 1) {
+        // end of a window: add the main accumulators into the shared-memory running sums
+        if (!wait(win_done, uint32_t(c / WIN) & 1u)) break;
+        ptx::tc_fence_after();
+        float *sum = sums + size_t(h) * TC_N * TC_M;
+        for (int j0 = 0; j0 < N; j0 += 16) {
+          float v[16];
+          ptx::tmem_ld16(tmem + (uint32_t(q * 32) << 16) + (h ? COL_MAIN_IM : COL_MAIN_RE) + uint32_t(j0), v);
+#pragma unroll
+          for (int u = 0; u < 16; u++) sum[(j0 + u) * TC_M + myrow] += v[u];
+        }
+        ptx::tc_fence_before();
+        ptx::mbar_arrive(flushed);
+      }
+    }
+    // epilogue: running sums plus the correction accumulators (complete once the last window is done)
+    if (!*abort_flag) {
+      ptx::tc_fence_after();
+      const int ia = m0 + myrow;
+      const float *sum = sums + size_t(h) * TC_N * TC_M;
+      float *dst = partial + ((size_t(ks) * 2 + h) * size_t(Sa) + size_t(ia)) * size_t(Sb) + n0;
+      for (int j0 = 0; j0 < N; j0 += 16) {
+        float v[16];
+        if (nchunks > 0) {
+          ptx::tmem_ld16(tmem + (uint32_t(q * 32) << 16) + (h ? COL_CORR_IM : COL_CORR_RE) + uint32_t(j0), v);
+        } else {
+#pragma unroll
+          for (int u = 0; u < 16; u++) v[u] = 0.f;
+        }
+        if (ia < Sa) {
+#pragma unroll
+          for (int u = 0; u < 16; u++)
+            if (n0 + j0 + u < Sb) dst[j0 + u] = sum[(j0 + u) * TC_M + myrow] + v[u];
+        }
       }
     }
   }
+  // tensor memory is freed only after every issued MMA has completed (also after an abort)
   ptx::tc_fence_before();
   __syncthreads();
-  if (warp == 0) ptx::tmem_dealloc(tmem, 512);
+  if (warp == 0) {
+    if (*issued_any) (void)ptx::mbar_wait_bounded(fin, 0u, WAIT_NS);
+    ptx::tc_fence_after();
+    ptx::tmem_dealloc(tmem, 512);
+  }
 }
 
 // out[i][j] = dv * sum over the point splits, in split order, in FP64
@@ -280,7 +303,7 @@ void launch_overlap_tc(Ctx &ctx, const float2 *a, int Sa, const float2 *b, int S
   nsplit = int((npoints + kper - 1) / kper);  // every split holds at least one point
   float *partial = static_cast<float *>(dev_alloc(ctx, sizeof(float) * size_t(nsplit) * 2 * Sa * Sb));
   ensure_smem_attr(reinterpret_cast<const void *>(overlap_tc_kernel), TC_SMEM);
-  overlap_tc_kernel<<<unsigned(tiles * nsplit), TC_THREADS, TC_SMEM, ctx.stream>>>(
+  overlap_tc_kernel<<<unsigned(tiles * nsplit), TC_THREADS + 32, TC_SMEM, ctx.stream>>>(
       a, Sa, b, Sb, npoints, mtiles, ntiles, N, kper, partial, ctx.d_err);
   INQB_CUDA(cudaGetLastError());
   ctx.launches++;
