@@ -21,13 +21,16 @@
 // Tiles.  One CTA per SM holds 128 states of a (tensor-memory lanes) against 128 states of b: the
 // main and corr accumulators of the real and imaginary parts take the 4 x 128 tensor-memory columns;
 // the running sums take 2 x 64 KB of shared memory.  The points are split over the CTAs; each CTA
-// streams its range in 16-point chunks: all 256 threads read the FP32 values (8-byte loads, one state
-// per thread and eight consecutive points, coalesced across the warp), split them and store the BF16
-// planes in the canonical K-major layout (core matrices of 8 rows x 16 bytes), and one thread issues
-// the chunk's 16 MMAs (128 x N x 16, kind::f16, BF16 in, FP32 accumulate) and commits them to the
-// buffer's mbarrier.  Two operand buffers alternate; the loads of the chunk two ahead are in flight
-// while the current chunk is converted (one ahead: 3.5 ms per overlap at 96^3 x 256; two: 3.0; more
-// gains nothing).  The per-CTA FP32 partial sums go to global memory and a second kernel
+// streams its range in 16-point chunks.  Eight converter warps read the FP32 values (8-byte loads, one
+// state per thread and eight consecutive points, coalesced across the warp), split them, store the
+// BF16 planes in the canonical K-major layout (core matrices of 8 rows x 16 bytes) into one of three
+// operand buffers and arrive on its "full" mbarrier; lane 0 of a ninth, issuer warp waits for it,
+// issues the chunk's 16 MMAs (128 x N x 16, kind::f16, BF16 in, FP32 accumulate) and commits them to
+// the buffer's "empty" mbarrier (and, at a window's end, to the window's).  The converters flush a
+// finished window and arrive on "flushed" before the issuer restarts the main accumulators.  The loads
+// of the chunk two ahead are in flight while the current chunk is converted (one ahead: 3.5 ms per
+// overlap at 96^3 x 256 before the issuer warp; two: 3.0; more gains nothing; with the issuer warp
+// 2.7).  The per-CTA FP32 partial sums go to global memory and a second kernel
 // adds them in a fixed order in FP64, so the result does not depend on scheduling.
 //
 // Every mbarrier wait is bounded (2 s by %globaltimer); on expiry the kernel raises the context's
