@@ -42,7 +42,8 @@ typedef struct inqb_hamiltonian inqb_hamiltonian;
 
 /* ---- context ------------------------------------------------------------- */
 /* Replaces the process-wide runtime of the reference (input/environment.hpp:27-92,
- * gpurun host.hpp:40-145): one device, one stream, explicit device memory. */
+ * and the reference's GPU runtime header gpu/host.hpp:40-145): one device, one stream, explicit
+ * device memory. */
 int inqb_ctx_create(int device, inqb_ctx **out);
 int inqb_ctx_destroy(inqb_ctx *ctx);
 const char *inqb_last_error(const inqb_ctx *ctx);
