@@ -95,8 +95,8 @@ __device__ __forceinline__ void load_unit(const float2 *__restrict__ src, int S,
 
 __global__ void __launch_bounds__(TC_THREADS + 32, 1)
     overlap_tc_kernel(const float2 *__restrict__ a, int Sa, const float2 *__restrict__ b, int Sb,
-                      long long npoints, int mtiles, int ntiles, int N, long long kper, float *__restrict__ partial,
-                      int *err) {
+                      long long npoints, int mtiles, int ntiles, int N, long long kper, int sym,
+                      float *__restrict__ partial, int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   float *sums = reinterpret_cast<float *>(smem + NB * BUF_BYTES);                    // [2][TC_N][TC_M]
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + NB * BUF_BYTES + SUM_BYTES);  // chunk converted, per buffer
@@ -109,8 +109,19 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1)
   volatile int *issued_any = abort_flag + 1;
 
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int tiles = mtiles * ntiles;
-  const int mt = blockIdx.x % mtiles, nt = (blockIdx.x / mtiles) % ntiles, ks = blockIdx.x / tiles;
+  // tiles of the result: all mtiles x ntiles, or for a set with itself (sym) only those with nt >= mt
+  const int tiles = sym ? mtiles * (mtiles + 1) / 2 : mtiles * ntiles;
+  const int ti = blockIdx.x % tiles, ks = blockIdx.x / tiles;
+  int mt = ti % mtiles, nt = ti / mtiles;
+  if (sym) {
+    mt = 0;
+    int r = ti;
+    while (r >= mtiles - mt) {
+      r -= mtiles - mt;
+      mt++;
+    }
+    nt = mt + r;
+  }
   const int m0 = mt * TC_M, n0 = nt * N;
   const long long kbeg = (long long)ks * kper;
   const long long kend = kbeg + kper < npoints ? kbeg + kper : npoints;
@@ -277,17 +288,21 @@ __global__ void __launch_bounds__(TC_THREADS + 32, 1)
   }
 }
 
-// out[i][j] = dv * sum over the point splits, in split order, in FP64
-__global__ void overlap_tc_reduce(const float *__restrict__ partial, int nsplit, int Sa, int Sb, double dv,
+// out[i][j] = dv * sum over the point splits, in split order, in FP64; for a set with itself (sym) the
+// tiles below the diagonal were not computed and take the conjugate of their mirror
+__global__ void overlap_tc_reduce(const float *__restrict__ partial, int nsplit, int Sa, int Sb, int sym, double dv,
                                   double2 *__restrict__ out) {
   const long long n = (long long)Sa * Sb;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int i = int(e / Sb), j = int(e % Sb);
+    const bool mirror = sym && (i / TC_M) > (j / TC_M);
+    const long long f = mirror ? (long long)j * Sb + i : e;
     double re = 0.0, im = 0.0;
     for (int z = 0; z < nsplit; z++) {
-      re += double(partial[(2LL * z) * n + e]);
-      im += double(partial[(2LL * z + 1) * n + e]);
+      re += double(partial[(2LL * z) * n + f]);
+      im += double(partial[(2LL * z + 1) * n + f]);
     }
-    out[e] = make_double2(dv * re, dv * im);
+    out[e] = make_double2(dv * re, mirror ? -dv * im : dv * im);
   }
 }
 
@@ -299,7 +314,9 @@ void launch_overlap_tc(Ctx &ctx, const float2 *a, int Sa, const float2 *b, int S
   const int mtiles = (Sa + TC_M - 1) / TC_M;
   const int N = Sb < TC_N ? (Sb + 15) / 16 * 16 : TC_N;
   const int ntiles = (Sb + N - 1) / N;
-  const int tiles = mtiles * ntiles;
+  // a set with itself: S is Hermitian, so only the tiles on and above the diagonal are computed
+  const int sym = (a == b && Sa == Sb && N == TC_M) ? 1 : 0;
+  const int tiles = sym ? mtiles * (mtiles + 1) / 2 : mtiles * ntiles;
   int nsplit = ctx.device_sms / tiles;  // the split (and so the rounding) does not follow grid_sms
   if (nsplit < 1) nsplit = 1;
   long long kper = ((npoints + nsplit - 1) / nsplit + TC_KC - 1) / TC_KC * TC_KC;
@@ -307,13 +324,13 @@ void launch_overlap_tc(Ctx &ctx, const float2 *a, int Sa, const float2 *b, int S
   float *partial = static_cast<float *>(dev_alloc(ctx, sizeof(float) * size_t(nsplit) * 2 * Sa * Sb));
   ensure_smem_attr(reinterpret_cast<const void *>(overlap_tc_kernel), TC_SMEM);
   overlap_tc_kernel<<<unsigned(tiles * nsplit), TC_THREADS + 32, TC_SMEM, ctx.stream>>>(
-      a, Sa, b, Sb, npoints, mtiles, ntiles, N, kper, partial, ctx.d_err);
+      a, Sa, b, Sb, npoints, mtiles, ntiles, N, kper, sym, partial, ctx.d_err);
   INQB_CUDA(cudaGetLastError());
   ctx.launches++;
   const long long n = (long long)Sa * Sb;
   long long blocks = (n + 255) / 256;
   if (blocks > 4L * ctx.num_sms) blocks = 4L * ctx.num_sms;
-  overlap_tc_reduce<<<unsigned(blocks), 256, 0, ctx.stream>>>(partial, nsplit, Sa, Sb, dv, out);
+  overlap_tc_reduce<<<unsigned(blocks), 256, 0, ctx.stream>>>(partial, nsplit, Sa, Sb, sym, dv, out);
   INQB_CUDA(cudaGetLastError());
   ctx.launches++;
   dev_free(ctx, partial);
