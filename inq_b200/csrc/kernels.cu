@@ -490,11 +490,19 @@ void launch_kinetic_ev(Ctx &ctx, const Basis &b, const C2<R> *fphi, int S, doubl
 // 256 threads with a 4x4 register tile each; partial tiles summed in chunk order.
 template <typename R>
 __global__ void __launch_bounds__(256) overlap_kernel(const C2<R> *__restrict__ a, int Sa, const C2<R> *__restrict__ b,
-                                                      int Sb, long long npoints, long long chunk, double2 *partial) {
+                                                      int Sb, long long npoints, long long chunk, int sym,
+                                                      double2 *partial) {
   constexpr int TB = 64, KT = 16;
   __shared__ double2 As[KT][TB];
   __shared__ double2 Bs[KT][TB];
-  const int ti = blockIdx.x * TB, tj = blockIdx.y * TB;
+  // sym: blockIdx.x enumerates the tiles on and above the diagonal, column by column
+  int bi = blockIdx.x, bj = blockIdx.y;
+  if (sym) {
+    bj = 0;
+    while ((bj + 1) * (bj + 2) / 2 <= bi) bj++;
+    bi -= bj * (bj + 1) / 2;
+  }
+  const int ti = bi * TB, tj = bj * TB;
   const long long p0 = blockIdx.z * chunk;
   const long long p1 = min(npoints, p0 + chunk);
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -549,14 +557,26 @@ __global__ void __launch_bounds__(256) overlap_kernel(const C2<R> *__restrict__ 
     }
 }
 
-__global__ void sum_tiles_kernel(const double2 *partial, int nz, long long n, double scale, double2 *out) {
+// With sym (a set against itself, S x S) only tiles with i/64 <= j/64 were computed: an element below
+// them is the conjugate of its mirror, since <a_j|a_i> = conj(<a_i|a_j>).
+__global__ void sum_tiles_kernel(const double2 *partial, int nz, long long n, int S, int sym, double scale,
+                                 double2 *out) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    long long src = e;
+    bool mirror = false;
+    if (sym) {
+      const int i = int(e / S), j = int(e % S);
+      if (i / 64 > j / 64) {
+        src = (long long)j * S + i;
+        mirror = true;
+      }
+    }
     double re = 0.0, im = 0.0;
     for (int z = 0; z < nz; z++) {
-      re += partial[z * n + e].x;
-      im += partial[z * n + e].y;
+      re += partial[z * n + src].x;
+      im += partial[z * n + src].y;
     }
-    out[e] = make_double2(scale * re, scale * im);
+    out[e] = make_double2(scale * re, mirror ? -scale * im : scale * im);
   }
 }
 
@@ -564,17 +584,20 @@ template <typename R>
 void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, long long npoints, double dv,
                     double2 *out) {
   const int gi = (Sa + 63) / 64, gj = (Sb + 63) / 64;
-  int nz = int((2LL * ctx.device_sms + gi * gj - 1) / (gi * gj));  // independent of grid_sms
+  const int sym = (a == b && Sa == Sb) ? 1 : 0;
+  const int tiles = sym ? gi * (gi + 1) / 2 : gi * gj;
+  int nz = int((2LL * ctx.device_sms + tiles - 1) / tiles);  // independent of grid_sms
   if (nz < 1) nz = 1;
   if (nz > 256) nz = 256;
   long long chunk = (npoints + nz - 1) / nz;
   chunk = ((chunk + 15) / 16) * 16;
   nz = int((npoints + chunk - 1) / chunk);
   double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * (size_t)nz * Sa * Sb));
-  overlap_kernel<R><<<dim3(gi, gj, nz), 256, 0, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, partial);
+  const dim3 grid = sym ? dim3(tiles, 1, nz) : dim3(gi, gj, nz);
+  overlap_kernel<R><<<grid, 256, 0, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, sym, partial);
   LAUNCHED(ctx);
   const long long n = (long long)Sa * Sb;
-  sum_tiles_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(partial, nz, n, dv, out);
+  sum_tiles_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(partial, nz, n, Sb, sym, dv, out);
   LAUNCHED(ctx);
   dev_free(ctx, partial);
 }
