@@ -249,6 +249,18 @@ int inqb_steepest_descent(const inqb_hamiltonian *ham, inqb_orbitals *fphi);
 int inqb_shift(double re, double im, const inqb_orbitals *chi, inqb_orbitals *phi);
 /* operations::rotate (rotate.hpp:27-62): phi <- phi R, R host [nst][nst] complex128 row-major. */
 int inqb_rotate(inqb_orbitals *phi, const double *R);
+/* operations::rotate with alpha and beta (rotate.hpp:83-142): rotphi <- alpha phi R + beta rotphi, R host
+ * [phi.nst][rotphi.nst] complex128 row-major, alpha and beta complex (re, im).  phi and rotphi are distinct
+ * sets on one basis, of one precision and space.  The state-parallel rotation multiplies the local block
+ * of states by its rows of R for each destination block (rotate.hpp:38-58). */
+int inqb_rotate_to(const inqb_orbitals *phi, inqb_orbitals *rotphi, const double *R, const double alpha[2],
+                   const double beta[2]);
+/* matrix::cholesky (matrix/cholesky.hpp:28-99) then matrix::invert_triangular (invert_triangular.hpp:20-60)
+ * on the host in FP64: S [n][n] complex128 Hermitian positive definite = U^H U, X = U^-1 (upper).  The
+ * matrix inqb_orthogonalize applies; a state-partitioned orthogonalize forms it from the all-reduced
+ * overlap on every rank.  INQB_ERR_NUMERIC if S is not positive definite (message via
+ * inqb_last_error(NULL)). */
+int inqb_cholesky_inverse(int n, const double *S, double *X);
 /* energy::calculate eigenvalue part (energy.hpp:83-89): eig[s] = Re<phi|H phi>/<phi|phi>,
  * normres[s] = <r|r> with r = H phi - eig phi.  Host outputs [nst]. */
 int inqb_eigenvalues(const inqb_hamiltonian *ham, const inqb_orbitals *phi, double *eig, double *normres);

@@ -577,6 +577,28 @@ def rotate(phi: OrbitalSet, R):
     return phi
 
 
+def rotate_to(phi: OrbitalSet, rotphi: OrbitalSet, R, alpha=1.0, beta=0.0):
+    """rotphi <- alpha phi R + beta rotphi (operations::rotate with alpha and beta, rotate.hpp:83-142);
+    R is [phi.nst][rotphi.nst]."""
+    r = np.ascontiguousarray(R, dtype=np.complex128).reshape(phi.nst, rotphi.nst)
+    a = np.array([complex(alpha).real, complex(alpha).imag])
+    b = np.array([complex(beta).real, complex(beta).imag])
+    phi.ctx.check(phi.ctx.lib.inqb_rotate_to(phi.handle, rotphi.handle, r.view(np.float64).reshape(-1).ctypes.data_as(_lib.DP),
+                                             a.ctypes.data_as(_lib.DP), b.ctypes.data_as(_lib.DP)))
+    return rotphi
+
+
+def cholesky_inverse(S) -> np.ndarray:
+    """U^-1 for the upper Cholesky factor of S = U^H U (matrix::cholesky, then invert_triangular), in FP64
+    on the host: the matrix ``orthogonalize`` applies to a set whose overlap is S."""
+    s = np.ascontiguousarray(S, dtype=np.complex128)
+    n = s.shape[0]
+    x = np.zeros((n, n), np.complex128)
+    _lib.check(_lib.load().inqb_cholesky_inverse(n, s.view(np.float64).reshape(-1).ctypes.data_as(_lib.DP),
+                                                 x.view(np.float64).reshape(-1).ctypes.data_as(_lib.DP)))
+    return x
+
+
 def shift(factor, chi: OrbitalSet, phi: OrbitalSet):
     f = complex(factor)
     phi.ctx.check(phi.ctx.lib.inqb_shift(f.real, f.imag, chi.handle, phi.handle))

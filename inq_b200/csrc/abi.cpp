@@ -1707,6 +1707,39 @@ int inqb_rotate(inqb_orbitals *phi, const double *R) {
   });
 }
 
+int inqb_rotate_to(const inqb_orbitals *phi, inqb_orbitals *rotphi, const double *R, const double alpha[2],
+                   const double beta[2]) {
+  return guarded(phi ? phi->ctx : nullptr, [&] {
+    INQB_REQUIRE(phi && rotphi && R && alpha && beta, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(phi != rotphi, INQB_ERR_ARG, "rotate_to needs distinct sets (inqb_rotate rotates in place)");
+    INQB_REQUIRE(phi->ctx == rotphi->ctx && phi->basis == rotphi->basis, INQB_ERR_ARG, "sets on different contexts or bases");
+    INQB_REQUIRE(phi->precision == rotphi->precision && phi->space == rotphi->space, INQB_ERR_ARG,
+                 "sets of different precisions or spaces");
+    set_device(*phi->ctx);
+    Ctx &ctx = *phi->ctx;
+    const int Si = phi->nst, So = rotphi->nst;
+    double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * Si * So));
+    INQB_CUDA(cudaMemcpyAsync(d, R, sizeof(double2) * Si * So, cudaMemcpyHostToDevice, ctx.stream));
+    const double2 a = make_double2(alpha[0], alpha[1]), be = make_double2(beta[0], beta[1]);
+    const long long np = phi->basis->npoints;
+    if (phi->precision == INQB_F64)
+      launch_rotate_to<double>(ctx, static_cast<const double2 *>(phi->data), Si, static_cast<double2 *>(rotphi->data), So,
+                               np, d, a, be);
+    else
+      launch_rotate_to<float>(ctx, static_cast<const float2 *>(phi->data), Si, static_cast<float2 *>(rotphi->data), So,
+                              np, d, a, be);
+    dev_free(ctx, d);
+    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+  });
+}
+
+int inqb_cholesky_inverse(int n, const double *S, double *X) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(n > 0 && S && X, INQB_ERR_ARG, "bad argument");
+    cholesky_inverse(n, reinterpret_cast<const std::complex<double> *>(S), reinterpret_cast<std::complex<double> *>(X));
+  });
+}
+
 int inqb_eigenvalues(const inqb_hamiltonian *hc, const inqb_orbitals *phi, double *eig, double *normres) {
   auto *h = const_cast<inqb_hamiltonian *>(hc);
   return guarded(h ? h->ctx : nullptr, [&] {

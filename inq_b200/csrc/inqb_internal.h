@@ -240,6 +240,9 @@ void launch_overlap_diag(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long l
 template <typename R>
 void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev);
 template <typename R>
+void launch_rotate_to(Ctx &ctx, const C2<R> *in, int Sin, C2<R> *out, int Sout, long long npoints, const double2 *Rdev,
+                      double2 alpha, double2 beta);
+template <typename R>
 void launch_density(Ctx &ctx, const C2<R> *phi, int S, long long npoints, const double *occ_dev, double *dens,
                     int accumulate);
 template <typename R> void launch_kick(Ctx &ctx, const Basis &b, C2<R> *phi, int S, const double ecov[3]);

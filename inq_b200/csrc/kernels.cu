@@ -602,49 +602,71 @@ void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, lo
   dev_free(ctx, partial);
 }
 
-// ------------------------------------------------------------------ rotate: phi[p][:] <- phi[p][:] R
+// ------------------------------------------------------------------ rotate: out[p][:] <- alpha in[p][:] R + beta out[p][:]
 template <typename R>
-__global__ void __launch_bounds__(256) rotate_kernel(C2<R> *phi, int S, long long npoints, const double2 *__restrict__ Rm) {
+__global__ void __launch_bounds__(256) rotate_kernel(const C2<R> *in, int Sin, C2<R> *out, int Sout, long long npoints,
+                                                     const double2 *__restrict__ Rm, double2 alpha, double2 beta,
+                                                     int scaled, int use_beta) {
   constexpr int ROWS = 8;
   extern __shared__ __align__(16) unsigned char sm[];
-  double2 *rows = reinterpret_cast<double2 *>(sm);  // [ROWS][S]
+  double2 *rows = reinterpret_cast<double2 *>(sm);  // [ROWS][Sin]
   for (long long p0 = (long long)blockIdx.x * ROWS; p0 < npoints; p0 += (long long)gridDim.x * ROWS) {
     const int nr = int(min((long long)ROWS, npoints - p0));
-    for (int e = threadIdx.x; e < ROWS * S; e += blockDim.x) {
-      const int r = e / S, k = e % S;
+    for (int e = threadIdx.x; e < ROWS * Sin; e += blockDim.x) {
+      const int r = e / Sin, k = e % Sin;
       double2 v = make_double2(0.0, 0.0);
       if (r < nr) {
-        C2<R> x = phi[(p0 + r) * S + k];
+        C2<R> x = in[(p0 + r) * Sin + k];
         v = make_double2(double(x.x), double(x.y));
       }
       rows[e] = v;
     }
-    __syncthreads();
-    for (int j = threadIdx.x; j < S; j += blockDim.x) {
+    __syncthreads();  // in place (in == out): every row is staged before any is overwritten
+    for (int j = threadIdx.x; j < Sout; j += blockDim.x) {
       double2 acc[ROWS];
 #pragma unroll
       for (int r = 0; r < ROWS; r++) acc[r] = make_double2(0.0, 0.0);
-      for (int k = 0; k < S; k++) {
-        const double2 rk = Rm[(long long)k * S + j];
+      for (int k = 0; k < Sin; k++) {
+        const double2 rk = Rm[(long long)k * Sout + j];
 #pragma unroll
         for (int r = 0; r < ROWS; r++) {
-          const double2 x = rows[r * S + k];
+          const double2 x = rows[r * Sin + k];
           acc[r].x += x.x * rk.x - x.y * rk.y;
           acc[r].y += x.x * rk.y + x.y * rk.x;
         }
       }
-      for (int r = 0; r < nr; r++) phi[(p0 + r) * S + j] = mk<C2<R>>(R(acc[r].x), R(acc[r].y));
+      for (int r = 0; r < nr; r++) {
+        double2 v = acc[r];
+        if (scaled) v = make_double2(alpha.x * v.x - alpha.y * v.y, alpha.x * v.y + alpha.y * v.x);
+        C2<R> *o = out + (p0 + r) * Sout + j;
+        if (use_beta) {
+          const double2 y = make_double2(double(o->x), double(o->y));
+          v.x += beta.x * y.x - beta.y * y.y;
+          v.y += beta.x * y.y + beta.y * y.x;
+        }
+        *o = mk<C2<R>>(R(v.x), R(v.y));
+      }
     }
     __syncthreads();
   }
 }
 
-template <typename R> void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev) {
-  const size_t smem = sizeof(double2) * 8 * S;
+// out <- alpha (in Rm) + beta out, Rm [Sin][Sout]; in == out (Sin == Sout) rotates in place
+template <typename R>
+void launch_rotate_to(Ctx &ctx, const C2<R> *in, int Sin, C2<R> *out, int Sout, long long npoints, const double2 *Rdev,
+                      double2 alpha, double2 beta) {
+  const size_t smem = sizeof(double2) * 8 * Sin;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "too many states for rotate");
+  const int scaled = !(alpha.x == 1.0 && alpha.y == 0.0);
+  const int use_beta = !(beta.x == 0.0 && beta.y == 0.0);
   ensure_smem_attr(reinterpret_cast<const void *>(rotate_kernel<R>), smem);
-  rotate_kernel<R><<<grid_for(npoints, 8, 148LL * 16), 256, smem, ctx.stream>>>(phi, S, npoints, Rdev);
+  rotate_kernel<R><<<grid_for(npoints, 8, 148LL * 16), 256, smem, ctx.stream>>>(in, Sin, out, Sout, npoints, Rdev, alpha,
+                                                                              beta, scaled, use_beta);
   LAUNCHED(ctx);
+}
+
+template <typename R> void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev) {
+  launch_rotate_to<R>(ctx, phi, S, phi, S, npoints, Rdev, make_double2(1.0, 0.0), make_double2(0.0, 0.0));
 }
 
 // ------------------------------------------------------------------ density n[p] (+)= sum_s occ_s |phi[p][s]|^2
@@ -923,6 +945,8 @@ void launch_ks_potential(Ctx &ctx, const double *n, const double *vion, const do
                                      double *);                                                                   \
   template void launch_overlap<R>(Ctx &, const C2<R> *, int, const C2<R> *, int, long long, double, double2 *);   \
   template void launch_rotate<R>(Ctx &, C2<R> *, int, long long, const double2 *);                                 \
+  template void launch_rotate_to<R>(Ctx &, const C2<R> *, int, C2<R> *, int, long long, const double2 *, double2,     \
+                                    double2);                                                                      \
   template void launch_density<R>(Ctx &, const C2<R> *, int, long long, const double *, double *, int);            \
   template void launch_kick<R>(Ctx &, const Basis &, C2<R> *, int, const double *);
 
