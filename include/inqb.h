@@ -261,6 +261,10 @@ int inqb_rotate_to(const inqb_orbitals *phi, inqb_orbitals *rotphi, const double
  * overlap on every rank.  INQB_ERR_NUMERIC if S is not positive definite (message via
  * inqb_last_error(NULL)). */
 int inqb_cholesky_inverse(int n, const double *S, double *X);
+/* matrix::diagonalize (diagonalize.hpp:100-190) on the host in FP64 by cyclic Jacobi rotations: A [n][n]
+ * complex128 Hermitian, read from its upper triangle; w the eigenvalues ascending, column k of the
+ * row-major V [n][n] the eigenvector of w[k].  The decomposition inqb_subspace_diagonalization uses. */
+int inqb_hermitian_eigen(int n, const double *A, double *w, double *V);
 /* energy::calculate eigenvalue part (energy.hpp:83-89): eig[s] = Re<phi|H phi>/<phi|phi>,
  * normres[s] = <r|r> with r = H phi - eig phi.  Host outputs [nst]. */
 int inqb_eigenvalues(const inqb_hamiltonian *ham, const inqb_orbitals *phi, double *eig, double *normres);

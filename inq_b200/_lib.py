@@ -95,6 +95,7 @@ SIGNATURES = {
     "inqb_rotate": (I, [P, DP]),
     "inqb_rotate_to": (I, [P, P, DP, DP, DP]),
     "inqb_cholesky_inverse": (I, [I, DP, DP]),
+    "inqb_hermitian_eigen": (I, [I, DP, DP, DP]),
     "inqb_eigenvalues": (I, [P, P, DP, DP]),
     "inqb_subspace_diagonalization": (I, [P, P, DP]),
     "inqb_exponential_in_place": (I, [P, D, D, P, I]),

@@ -599,6 +599,20 @@ def cholesky_inverse(S) -> np.ndarray:
     return x
 
 
+def hermitian_eigen(A):
+    """(eigenvalues ascending, eigenvectors as columns) of a Hermitian matrix read from its upper
+    triangle (matrix::diagonalize), in FP64 on the host: the decomposition ``subspace_diagonalization``
+    uses."""
+    a = np.ascontiguousarray(A, dtype=np.complex128)
+    n = a.shape[0]
+    w = np.zeros(n)
+    v = np.zeros((n, n), np.complex128)
+    _lib.check(_lib.load().inqb_hermitian_eigen(n, a.view(np.float64).reshape(-1).ctypes.data_as(_lib.DP),
+                                                w.ctypes.data_as(_lib.DP),
+                                                v.view(np.float64).reshape(-1).ctypes.data_as(_lib.DP)))
+    return w, v
+
+
 def shift(factor, chi: OrbitalSet, phi: OrbitalSet):
     f = complex(factor)
     phi.ctx.check(phi.ctx.lib.inqb_shift(f.real, f.imag, chi.handle, phi.handle))

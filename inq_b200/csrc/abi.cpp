@@ -1733,6 +1733,13 @@ int inqb_rotate_to(const inqb_orbitals *phi, inqb_orbitals *rotphi, const double
   });
 }
 
+int inqb_hermitian_eigen(int n, const double *A, double *w, double *V) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(n > 0 && A && w && V, INQB_ERR_ARG, "bad argument");
+    hermitian_eigen(n, reinterpret_cast<const std::complex<double> *>(A), w, reinterpret_cast<std::complex<double> *>(V));
+  });
+}
+
 int inqb_cholesky_inverse(int n, const double *S, double *X) {
   return guarded(nullptr, [&] {
     INQB_REQUIRE(n > 0 && S && X, INQB_ERR_ARG, "bad argument");

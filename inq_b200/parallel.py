@@ -203,3 +203,15 @@ def sharded_orthogonalize(phi, part: Partition, group=None, blocks=None):
     ops = blocks or SetBlocks(phi, group)
     S = sharded_overlap(phi, part, None, group, ops)
     return sharded_rotate(phi, cholesky_inverse(S), part, group, ops)
+
+
+def sharded_subspace_diagonalization(ham, phi, part: Partition, group=None, blocks=None) -> np.ndarray:
+    """ground_state::subspace_diagonalization of a state-partitioned set (subspace_diagonalization.hpp:21-29):
+    H applied to the local states (it couples none), the all-reduced <phi_i|H phi_j>, its eigenvectors
+    formed in FP64 on every rank and the state-parallel rotation onto them.  Returns the eigenvalues."""
+    from .core import hermitian_eigen
+    ops = blocks or SetBlocks(phi, group)
+    hs = sharded_overlap(phi, part, ham(phi), group, ops)
+    w, V = hermitian_eigen(hs)
+    sharded_rotate(phi, V, part, group, ops)
+    return w

@@ -124,7 +124,10 @@ def _blocks_main(rank, world, port, nst, out):
         S = parallel.sharded_overlap(local, part, blocks=ops)
         rot = parallel.sharded_rotate(local.copy(), R, part, blocks=ops)
         orth = parallel.sharded_orthogonalize(local.copy(), part, blocks=ops)
-        out[rank] = (part.start, part.end, S, rot, orth)
+        V = 0.5 + np.cos(np.arange(int(np.prod(sizes))).reshape(sizes) / 7.0)
+        sub = orth.copy()
+        w = parallel.sharded_subspace_diagonalization(lambda x: V[..., None] * x, sub, part, blocks=ops)
+        out[rank] = (part.start, part.end, S, rot, orth, w, sub)
     finally:
         dist.destroy_process_group()
 
@@ -153,16 +156,28 @@ def test_state_parallel_overlap_rotate_orthogonalize_gloo(world, nst):
     S_ref = O.overlap(rs, psi)
     rot = np.zeros_like(psi)
     orth = np.zeros_like(psi)
+    sub = np.zeros_like(psi)
     for r in range(world):
-        a, b, S, rr, oo = out[r]
+        a, b, S, rr, oo, w, ss = out[r]
         assert np.max(np.abs(S - S_ref)) <= 1e-13 * np.max(np.abs(S_ref))
         rot[..., a:b] = rr
         orth[..., a:b] = oo
+        sub[..., a:b] = ss
+        if r == 0:
+            w0 = w
+        assert np.array_equal(w, w0)    # every rank forms the same eigenvalues
     rot_ref = (psi.reshape(-1, nst) @ R).reshape(psi.shape)
     assert np.max(np.abs(rot - rot_ref)) <= 1e-13 * np.max(np.abs(rot_ref))
     orth_ref = O.orthogonalize(rs, psi)
     assert np.max(np.abs(orth - orth_ref)) <= 1e-12 * np.max(np.abs(orth_ref))
     assert np.max(np.abs(O.overlap(rs, orth) - np.eye(nst))) < 1e-12
+    # subspace diagonalisation of the orthonormal set under a real potential: <sub_i|V|sub_j> diagonal
+    import inq_b200 as ib
+    V = 0.5 + np.cos(np.arange(int(np.prod(rs.sizes))).reshape(rs.sizes) / 7.0)
+    w_ref, U = ib.hermitian_eigen(O.overlap(rs, orth_ref, V[..., None] * orth_ref))
+    assert np.max(np.abs(w0 - w_ref)) < 1e-12 * np.max(np.abs(w_ref))
+    hs = O.overlap(rs, sub, V[..., None] * sub)
+    assert np.max(np.abs(hs - np.diag(w_ref))) < 1e-11 * np.max(np.abs(w_ref))
 
 
 def test_cholesky_inverse_host():

@@ -1,5 +1,6 @@
-"""GPU tests of the state-parallel overlap, rotation and orthogonalisation (overlap.hpp:42-56,
-rotate.hpp:27-142, orthogonalize.hpp:25-31) through the device kernels.
+"""GPU tests of the state-parallel overlap, rotation, orthogonalisation and subspace diagonalisation
+(overlap.hpp:42-56, rotate.hpp:27-142, orthogonalize.hpp:25-31, subspace_diagonalization.hpp:21-29)
+through the device kernels.
 
 One GPU is available per run, so: the rectangular rotation kernel against numpy; the NCCL path (device
 buffers viewed in place, collectives ordered on the context's stream) with one rank; and two ranks as
@@ -69,9 +70,23 @@ def test_state_parallel_nccl_one_rank():
         ref = ib.orthogonalize(phi.copy()).matrix()
         got = parallel.sharded_orthogonalize(phi, part).matrix()
         assert np.max(np.abs(got - ref)) <= 1e-13 * np.max(np.abs(ref))
+        ham = _hamiltonian(rs)
+        single = phi.copy()
+        w_ref = ham.subspace_diagonalization(single)
+        w = parallel.sharded_subspace_diagonalization(ham, phi, part)
+        assert np.max(np.abs(w - w_ref)) <= 1e-13 * np.max(np.abs(w_ref))
+        assert np.max(np.abs(phi.matrix() - single.matrix())) <= 1e-12 * np.max(np.abs(single.matrix()))
         torch.cuda.synchronize()
     finally:
         dist.destroy_process_group()
+
+
+def _hamiltonian(rs):
+    import inq_b200 as ib
+    ham = ib.KSHamiltonian(rs)
+    n = int(np.prod(rs.sizes))
+    ham.set_scalar_potential((0.4 + 0.3 * np.cos(np.arange(n) / 11.0)).reshape(rs.sizes))
+    return ham
 
 
 def _rank_main(rank, world, port, nst, out):
@@ -87,7 +102,9 @@ def _rank_main(rank, world, port, nst, out):
         phi = ib.OrbitalSet.from_array(rs, psi[..., part.start:part.end])
         S = parallel.sharded_overlap(phi, part)
         parallel.sharded_orthogonalize(phi, part)
-        out[rank] = (part.start, part.end, S, phi.hypercubic())
+        orth = phi.hypercubic()
+        w = parallel.sharded_subspace_diagonalization(_hamiltonian(rs), phi, part)
+        out[rank] = (part.start, part.end, S, orth, w, phi.hypercubic())
     finally:
         dist.destroy_process_group()
 
@@ -110,10 +127,20 @@ def test_state_parallel_two_ranks_one_gpu():
     phi = ib.OrbitalSet.from_array(rs, psi)
     S_ref = ib.overlap(phi)
     ref = ib.orthogonalize(phi).hypercubic()
+    ham = _hamiltonian(rs)
+    w_ref = ham.subspace_diagonalization(phi)
     got = np.zeros_like(ref)
+    sub = np.zeros_like(ref)
     for r in range(world):
-        a, b, S, blk = out[r]
+        a, b, S, blk, w, sb = out[r]
         assert np.max(np.abs(S - S_ref)) <= 1e-13 * np.max(np.abs(S_ref))
+        assert np.max(np.abs(w - w_ref)) <= 1e-12 * np.max(np.abs(w_ref))
         got[..., a:b] = blk
+        sub[..., a:b] = sb
     assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
     assert np.max(np.abs(ib.overlap(ib.OrbitalSet.from_array(rs, got)) - np.eye(nst))) < 1e-12
+    # the rotated states diagonalise the subspace Hamiltonian like the single-set call
+    sub_set = ib.OrbitalSet.from_array(rs, sub)
+    hs = ib.overlap(sub_set, ham(sub_set))
+    assert np.max(np.abs(hs - np.diag(w_ref))) <= 1e-11 * np.max(np.abs(w_ref))
+    assert np.max(np.abs(sub - phi.hypercubic())) <= 1e-10 * np.max(np.abs(sub))
