@@ -2,9 +2,10 @@
 
 * The reader is pinned to the reference's projector test (projector.hpp:160-240): for its N.upf and
   N_non_diagonal.upf.gz files, 8 projector functions and the KB coefficients it checks (D_ij / 2,
-  coupled only within equal m).  Those files are read from the reference's unit-test data directory
-  (INQ_REFERENCE_DATA) when it is present; without it these checks are skipped and the synthetic
-  files below still run.
+  coupled only within equal m).  ``golden/upf_reference_pins.json`` holds what the reader parsed from
+  those files (made by ``golden/make_upf_golden.py``); the KB coefficients are built from it on every
+  run.  With INQ_REFERENCE_DATA naming the reference's unit-test data directory the files themselves
+  are parsed again and compared with the pins.
 * A synthetic UPF (version 2, written by ``write_upf``) reads back unchanged; a version-1 text
   block parses to the same values.
 * Real spherical harmonics up to l = 3 are orthonormal on the sphere.
@@ -19,7 +20,18 @@ import pytest
 
 from inq_b200 import pseudo
 
-REF = os.environ.get("INQ_REFERENCE_DATA", "/root/reference/share/unit_tests_data")
+REF = os.environ.get("INQ_REFERENCE_DATA", "")
+PINS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "upf_reference_pins.json")
+
+
+def _pinned(name):
+    import json
+    with open(PINS) as f:
+        p = json.load(f)[name]
+    n = len(p["beta_l"])
+    mesh = np.linspace(0.0, 1.0, 2)
+    return pseudo.Pseudopotential(p["element"], p["z_valence"], mesh, mesh, mesh, list(p["beta_l"]),
+                                  [mesh] * n, [1] * n, np.array(p["dij"]))
 
 
 def _synthetic(lmax=2, nproj_per_l=2, seed=3):
@@ -45,16 +57,15 @@ def _synthetic(lmax=2, nproj_per_l=2, seed=3):
     return pseudo.Pseudopotential("Xx", 5.0, r, rab, vloc, beta_l, beta, cut, d)
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "N.upf")), reason="reference test data not present")
 def test_kb_coefficients_of_the_reference_projector_test():
-    ps = pseudo.read_upf(os.path.join(REF, "N.upf"))
+    ps = _pinned("N.upf")
     assert ps.num_projectors_lm() == 8 and ps.z_valence == 5.0
     kb = ps.kb_coefficients()
     expect = [7.494508815, 0.6363049519, -4.2939052122, -4.2939052122, -4.2939052122,
               -1.0069878791, -1.0069878791, -1.0069878791]
     assert np.allclose(np.diag(kb), expect, atol=5e-10)
     assert np.count_nonzero(kb - np.diag(np.diag(kb))) == 0
-    nd = pseudo.read_upf(os.path.join(REF, "N_non_diagonal.upf.gz")).kb_coefficients()
+    nd = _pinned("N_non_diagonal.upf.gz").kb_coefficients()
     assert nd[0, 0] == pytest.approx(4.0654068834, abs=5e-10) and nd[1, 1] == pytest.approx(4.0654068834, abs=5e-10)
     assert nd[0, 1] == pytest.approx(-3.4291019316, abs=5e-10) and nd[1, 0] == pytest.approx(-3.4291019316, abs=5e-10)
     for i in (2, 3, 4):
@@ -64,11 +75,21 @@ def test_kb_coefficients_of_the_reference_projector_test():
     assert nd[0, 2] == 0.0 and nd[2, 3] == 0.0
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "F.UPF")), reason="reference test data not present")
 def test_version_one_file_of_the_reference_data():
-    ps = pseudo.read_upf(os.path.join(REF, "F.UPF"))
+    ps = _pinned("F.UPF")
     assert ps.element == "F" and ps.z_valence == 7.0 and ps.beta_l == [0]
-    assert ps.projector_radius() > 0.0
+
+
+@pytest.mark.skipif(not (REF and os.path.exists(os.path.join(REF, "N.upf"))), reason="reference test data not given")
+def test_reader_reproduces_the_pins():
+    import json
+    with open(PINS) as f:
+        pins = json.load(f)
+    for name, p in pins.items():
+        ps = pseudo.read_upf(os.path.join(REF, name))
+        assert ps.element == p["element"] and ps.z_valence == p["z_valence"] and ps.beta_l == p["beta_l"]
+        assert np.array_equal(ps.dij, np.array(p["dij"])) and len(ps.r) == p["mesh_size"]
+        assert ps.projector_radius() == p["projector_radius"] and ps.projector_radius() > 0.0
 
 
 def test_write_and_read_back(tmp_path):
@@ -221,7 +242,7 @@ def test_local_potential_does_not_depend_on_the_range_split():
         assert np.mean(v_a) == pytest.approx(2 * np.pi * 3.0 * a * a / cell.volume, rel=1e-12)
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "N.upf")), reason="reference test data not present")
+@pytest.mark.skipif(not (REF and os.path.exists(os.path.join(REF, "N.upf"))), reason="reference test data not given")
 def test_local_potential_average_of_a_pseudopotential_file():
     """The grid average of the local potential of a real pseudopotential is its alpha_Z / Omega,
     alpha_Z = int (V_loc(r) + Z / r) 4 pi r^2 dr on the radial mesh."""
