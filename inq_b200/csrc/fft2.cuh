@@ -59,9 +59,7 @@ using ptx::mbar_init;
 using ptx::mbar_init_fence;
 using ptx::mbar_try_wait;
 using ptx::smem_u32;
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
+using ptx::mbar_expect_tx;
 __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
                                             int c3) {
   asm volatile(
@@ -76,9 +74,9 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void 
                "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
                : "memory");
 }
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+using ptx::bulk_commit;
+using ptx::bulk_wait0;
+using ptx::bulk_wait_read0;
 using ptx::fence_proxy_async;
 
 // ------------------------------------------------------------------ register codelets (compile-time size)

@@ -5,6 +5,9 @@
 // reproducible run to run; no floating-point atomics are used anywhere.
 
 #include "inqb_internal.h"
+#include "ptx.cuh"
+
+#include <mutex>
 
 namespace inqb {
 
@@ -313,6 +316,163 @@ __global__ void __launch_bounds__(128) nl_apply_kernel(long long nitems, int nch
   }
 }
 
+// Bulk-copy form of the apply.  A CTA takes batches of KB consecutive hit points: a producer warp
+// copies the points' output rows (S contiguous states each) into shared memory with bulk asynchronous
+// copies, the compute threads add the nonlocal term to them there, and the producer writes the rows
+// back with bulk copies.  Two stages overlap one batch's copies with the next batch's arithmetic, and
+// the copy engine keeps the bytes in flight that the register-held form could not.  The arithmetic and
+// its order are those of nl_apply_kernel, so the result is bitwise the same.
+constexpr int NLA_NT = 128;   // compute threads
+constexpr int NLA_NS = 2;     // stages
+constexpr int NLA_KMAX = 32;  // largest batch (one producer lane per row)
+
+__device__ __forceinline__ void nla_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NLA_NT) : "memory"); }
+__device__ __forceinline__ bool nla_sync_or(int v) {
+  uint32_t r;
+  asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+               : "=r"(r)
+               : "r"(v), "n"(NLA_NT)
+               : "memory");
+  return r != 0;
+}
+
+template <typename R, int J>
+__global__ void __launch_bounds__(NLA_NT + 32) nl_apply_bulk_kernel(long long nrec, int KB, int S,
+                                                                     const int4 *__restrict__ hrec,
+                                                                     const int *__restrict__ hitp,
+                                                                     const C2<R> *__restrict__ hcoef,
+                                                                     const C2<R> *__restrict__ projD, C2<R> *out,
+                                                                     C2<R> *acc1, C2<R> c1, C2<R> *acc2, C2<R> c2,
+                                                                     int *err) {
+  using T = C2<R>;
+  using namespace ptx;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T *rows = reinterpret_cast<T *>(smem);                                 // [NS][KB][S]
+  T *hcs = rows + size_t(NLA_NS) * KB * S;                               // [KB][4] first-hit coefficients
+  int4 *recs = reinterpret_cast<int4 *>(hcs + NLA_KMAX * 4);             // [NS][KMAX]
+  uint64_t *full = reinterpret_cast<uint64_t *>(recs + NLA_NS * NLA_KMAX);  // rows and records loaded
+  uint64_t *done = full + NLA_NS;                                        // rows computed
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(done + NLA_NS);
+  const long long nbatch = (nrec + KB - 1) / KB;
+  const uint32_t row_bytes = uint32_t(S) * uint32_t(sizeof(T));
+  if (threadIdx.x == 0) {
+    *abort_flag = 0;
+    for (int st = 0; st < NLA_NS; st++) {
+      mbar_init(&full[st], 1);
+      mbar_init(&done[st], NLA_NT);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  // bounded wait on an mbarrier phase; false (and the error flag raised) on expiry or abort
+  auto wait_bar = [&](uint64_t *b, uint32_t parity) -> bool {
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(b, parity)) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > 2000000000ull) {
+        *abort_flag = 1;
+        atomicExch(err, 1);
+        return false;
+      }
+    }
+    return true;
+  };
+
+  if (threadIdx.x >= NLA_NT) {
+    // producer warp: lane q copies row q of a batch in and out
+    const int lane = threadIdx.x - NLA_NT;
+    auto issue = [&](int st, long long b) {
+      const long long k0 = b * KB;
+      const int nb = int(min((long long)KB, nrec - k0));
+      int4 rec = make_int4(0, 0, 0, 0);
+      if (lane < nb) {
+        rec = hrec[k0 + lane];
+        recs[st * NLA_KMAX + lane] = rec;
+      }
+      __threadfence_block();
+      __syncwarp();
+      if (lane == 0) mbar_expect_tx(&full[st], uint32_t(nb) * row_bytes);
+      __syncwarp();
+      if (lane < nb) bulk_load(rows + (size_t(st) * KB + lane) * S, out + (long long)rec.x * S, row_bytes, &full[st]);
+    };
+    for (int st = 0; st < NLA_NS; st++) {
+      const long long b = blockIdx.x + (long long)st * gridDim.x;
+      if (b < nbatch) issue(st, b);
+    }
+    int k = 0;
+    for (long long b = blockIdx.x; b < nbatch; b += gridDim.x, k++) {
+      const int st = k % NLA_NS;
+      if (!wait_bar(&done[st], uint32_t(k / NLA_NS) & 1u)) break;
+      const int nb = int(min((long long)KB, nrec - b * KB));
+      if (lane < nb)
+        bulk_store(out + (long long)recs[st * NLA_KMAX + lane].x * S, rows + (size_t(st) * KB + lane) * S, row_bytes);
+      bulk_commit();
+      bulk_wait_read0();  // the stage may be refilled once its rows are read out
+      __syncwarp();
+      const long long bn = b + (long long)NLA_NS * gridDim.x;
+      if (bn < nbatch) issue(st, bn);
+    }
+    bulk_wait0();
+    return;
+  }
+
+  const int tid = threadIdx.x;
+  T pd[J][4];
+  int pprev = -1;
+  int i = 0;
+  for (long long b = blockIdx.x; b < nbatch; b += gridDim.x, i++) {
+    const int st = i % NLA_NS;
+    const bool ok = wait_bar(&full[st], uint32_t(i / NLA_NS) & 1u);
+    if (nla_sync_or(!ok || *abort_flag)) break;
+    const int nb = int(min((long long)KB, nrec - b * KB));
+    const int4 *rc = recs + st * NLA_KMAX;
+    T *rw = rows + size_t(st) * KB * S;
+    // the batch's first-hit coefficients, requested together
+    for (int t = tid; t < nb * 4; t += NLA_NT) hcs[t] = hcoef[(long long)rc[t >> 2].y * 4 + (t & 3)];
+    nla_sync();
+    for (int q = 0; q < nb; q++) {
+      const int4 rec = rc[q];
+      const int h0 = rec.y, nh = rec.z, p0 = rec.w;
+      if (p0 != pprev) {
+#pragma unroll
+        for (int j = 0; j < J; j++) {
+          const int s = tid + j * NLA_NT;
+          if (s < S) {
+#pragma unroll
+            for (int l = 0; l < 4; l++) pd[j][l] = projD[((long long)p0 * 4 + l) * S + s];
+          }
+        }
+        pprev = p0;
+      }
+      T hc[4];
+#pragma unroll
+      for (int l = 0; l < 4; l++) hc[l] = hcs[q * 4 + l];
+#pragma unroll
+      for (int j = 0; j < J; j++) {
+        const int s = tid + j * NLA_NT;
+        if (s >= S) continue;
+        T accv = mk<T>(R(0), R(0));
+#pragma unroll
+        for (int l = 0; l < 4; l++) accv = cadd(accv, cmul(hc[l], pd[j][l]));
+        for (int k = 1; k < nh; k++) {
+          const int h = h0 + k;
+          const int p = hitp[h];
+#pragma unroll
+          for (int l = 0; l < 4; l++)
+            accv = cadd(accv, cmul(hcoef[(long long)h * 4 + l], projD[((long long)p * 4 + l) * S + s]));
+        }
+        T *o = rw + (size_t)q * S + s;
+        *o = cadd(*o, accv);
+        const long long e = (long long)rec.x * S + s;
+        if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, accv));
+        if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, accv));
+      }
+    }
+    fence_proxy_async();
+    mbar_arrive(&done[st]);  // the producer writes the rows back and refills the stage
+  }
+}
+
 template <typename R>
 void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out, C2<R> *acc1, C2<R> c1,
                      C2<R> *acc2, C2<R> c2) {
@@ -321,6 +481,42 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
   const C2<R> *hc;
   if constexpr (sizeof(R) == 8) hc = P.d_hcoef;
   else hc = P.d_hcoef32;
+  // bulk form: rows of 16-byte multiples (and 16-byte aligned starts), up to 4 states per compute thread
+  const size_t row_bytes = size_t(S) * sizeof(C2<R>);
+  if (row_bytes % 16 == 0 && S <= 4 * NLA_NT && reinterpret_cast<uintptr_t>(out) % 16 == 0) {
+    // about 32 KB of rows per stage, 4..32 points per batch
+    int KB = int(32768 / row_bytes);
+    KB = KB < 4 ? 4 : (KB > NLA_KMAX ? NLA_KMAX : KB);
+    const size_t smem = size_t(NLA_NS) * KB * row_bytes + NLA_KMAX * 4 * sizeof(C2<R>) + NLA_NS * NLA_KMAX * sizeof(int4) +
+                        2 * NLA_NS * sizeof(uint64_t) + 16;
+    if (smem <= size_t(ctx.max_smem_optin)) {
+      auto kern = S <= 2 * NLA_NT ? nl_apply_bulk_kernel<R, 2> : nl_apply_bulk_kernel<R, 4>;
+      ensure_smem_attr(reinterpret_cast<const void *>(kern), smem);
+      // CTAs per SM for this kernel and shared-memory size, computed once under a lock
+      static std::mutex mtx;
+      static const void *occ_kern[2] = {nullptr, nullptr};
+      static size_t occ_smem[2] = {0, 0};
+      static int occ_per_sm[2] = {1, 1};
+      const int slot = S <= 2 * NLA_NT ? 0 : 1;
+      int per_sm;
+      {
+        std::lock_guard<std::mutex> lock(mtx);
+        if (occ_kern[slot] != reinterpret_cast<const void *>(kern) || occ_smem[slot] != smem) {
+          INQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_per_sm[slot], kern, NLA_NT + 32, smem));
+          occ_kern[slot] = reinterpret_cast<const void *>(kern);
+          occ_smem[slot] = smem;
+        }
+        per_sm = occ_per_sm[slot];
+      }
+      const long long nbatch = (P.nhitpts + KB - 1) / KB;
+      long long grid = (long long)(per_sm < 1 ? 1 : per_sm) * ctx.num_sms;
+      if (grid > nbatch) grid = nbatch;
+      kern<<<unsigned(grid), NLA_NT + 32, smem, ctx.stream>>>(P.nhitpts, KB, S, P.d_hrec, P.d_hitp, hc, projD, out, acc1,
+                                                             c1, acc2, c2, ctx.d_err);
+      LAUNCHED(ctx);
+      return;
+    }
+  }
   const int chunk = 32 * int(16 / sizeof(R));
   const int nchunks = (S + chunk - 1) / chunk;
   const long long nitems = P.nhitpts * nchunks;
