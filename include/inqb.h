@@ -70,7 +70,10 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * their grids for every SM) or 1..#SMs (grids sized for that many SMs, leaving room on the device
  * for the kernels of other contexts, e.g. small requests next to a large one in a serving loop);
  * "stream_priority" = 0 (default, the device's lowest stream priority) or 1 (its highest: the
- * block scheduler starts this context's pending blocks first).  Changing the priority replaces
+ * block scheduler starts this context's pending blocks first); "nl_bulk" = 0 (default: the
+ * nonlocal apply, and the projection when it has at least two CTAs per SM, move whole rows of
+ * states through shared memory with bulk asynchronous copies), 1 (those forms wherever a row is a
+ * multiple of 16 bytes) or -1 (never: register-held gathers).  Changing the priority replaces
  * the context's stream (after the work queued on it), so callers query inqb_ctx_stream again. */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Free and total device memory in bytes (admission control for serving). */

@@ -74,6 +74,7 @@ struct Ctx {
   int fft_stages = 0;        // shared-memory ring depth of the TMA FFT kernels (0: from the memory budget)
   int mixed_compute = 0;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
   int overlap_tc = 1;        // overlaps of single-precision sets on the tensor cores (split BF16)
+  int nl_bulk = 0;           // nonlocal kernels: 0 automatic, 1 bulk-copy forms wherever they apply, -1 never
   int stream_priority = 0;   // 0: the device's lowest stream priority, 1: its highest
 };
 

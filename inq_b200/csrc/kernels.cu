@@ -7,6 +7,7 @@
 #include "inqb_internal.h"
 #include "ptx.cuh"
 
+#include <algorithm>
 #include <mutex>
 
 namespace inqb {
@@ -84,6 +85,37 @@ void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[
     LAUNCHED(ctx);
   }
   for (int i = 0; i < 3; i++) P.kA[i] = kA[i];
+}
+
+// ------------------------------------------------------------------ bulk-copy kernels: shared pieces
+// The bulk-copy forms of the projection and the apply run NLA_NT compute threads beside one producer
+// warp that moves whole rows of states (contiguous in the state-fastest layout) with bulk
+// asynchronous copies.  The compute threads synchronise among themselves on named barrier 1.
+constexpr int NLA_NT = 128;
+
+__device__ __forceinline__ void nla_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NLA_NT) : "memory"); }
+// the same barrier, returning whether any compute thread passed a nonzero value (uniform result)
+__device__ __forceinline__ bool nla_sync_or(int v) {
+  uint32_t r;
+  asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+               : "=r"(r)
+               : "r"(v), "n"(NLA_NT)
+               : "memory");
+  return r != 0;
+}
+// bounded wait on an mbarrier phase (2 s); false, with the CTA's abort flag and the error flag raised,
+// on expiry, and false as soon as another thread of the CTA has raised the abort flag
+__device__ __forceinline__ bool nla_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag, int *err) {
+  const uint64_t t0 = ptx::global_ns();
+  while (!ptx::mbar_try_wait(b, parity)) {
+    if (*abort_flag) return false;
+    if (ptx::global_ns() - t0 > 2000000000ull) {
+      *abort_flag = 1;
+      atomicExch(err, 1);
+      return false;
+    }
+  }
+  return true;
 }
 
 // ------------------------------------------------------------------ nonlocal projection
@@ -165,6 +197,122 @@ __global__ void __launch_bounds__(NLP_WARPS * 32) nl_project_kernel(const C2<R> 
   }
 }
 
+// Bulk-copy form of the projection.  CTA = (projector p, range rg of its sphere points, chunk of up to
+// NLA_NT * J states).  The producer warp copies the range's points in batches of KB -- each point's
+// row of the chunk's states and the point's four gather coefficients -- into a ring of NLP_NS stages;
+// each compute thread owns J states and sums over the range's points in order (a batch's points first,
+// then the batch sums, so the chains stay as short as in nl_project_kernel).  No cross-warp reduction:
+// the thread writes its states of partial[p][rg][l][s] directly.
+constexpr int NLP_NS = 3;
+
+template <typename R, typename A, int J>
+__global__ void __launch_bounds__(NLA_NT + 32) nl_project_bulk_kernel(const C2<R> *psi, int S,
+                                                                       const int *__restrict__ pt,
+                                                                       const C2<A> *gcoef,
+                                                                       const int *__restrict__ npts, int maxsph,
+                                                                       int KB, C2<A> *__restrict__ partial, int *err) {
+  using T = C2<R>;
+  using TA = C2<A>;
+  using namespace ptx;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int p = blockIdx.x, rg = blockIdx.y;
+  const int s0 = blockIdx.z * NLA_NT * J;
+  const int SCmax = min(NLA_NT * J, S);  // row stride of the stages
+  const int SC = min(NLA_NT * J, S - s0);  // states of this chunk
+  T *rows = reinterpret_cast<T *>(smem);                                     // [NS][KB][SCmax]
+  TA *gs = reinterpret_cast<TA *>(rows + size_t(NLP_NS) * KB * SCmax);        // [NS][KB][4]
+  uint64_t *full = reinterpret_cast<uint64_t *>(gs + size_t(NLP_NS) * KB * 4);  // stage loaded
+  uint64_t *done = full + NLP_NS;                                            // stage consumed
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(done + NLP_NS);
+  const int np = npts[p];
+  const int rper = (np + NLP_RANGES - 1) / NLP_RANGES;
+  const int r0 = rg * rper, r1 = min(np, r0 + rper);
+  const int n = max(r1 - r0, 0);
+  const int nbatch = (n + KB - 1) / KB;
+  const long long rowbase = (long long)p * maxsph;
+  const uint32_t row_bytes = uint32_t(SC) * uint32_t(sizeof(T));
+  if (threadIdx.x == 0) {
+    *abort_flag = 0;
+    for (int st = 0; st < NLP_NS; st++) {
+      mbar_init(&full[st], 1);
+      mbar_init(&done[st], NLA_NT);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+
+  if (threadIdx.x >= NLA_NT) {
+    // producer warp: lane q copies point q of a batch, lane 0 also the batch's coefficients
+    const int lane = threadIdx.x - NLA_NT;
+    auto issue = [&](int st, int b) {
+      const int base = r0 + b * KB;
+      const int nb = min(KB, r1 - base);
+      const long long q = lane < nb ? (long long)pt[rowbase + base + lane] : 0;
+      if (lane == 0) mbar_expect_tx(&full[st], uint32_t(nb) * (row_bytes + 4 * uint32_t(sizeof(TA))));
+      __syncwarp();
+      if (lane < nb) bulk_load(rows + (size_t(st) * KB + lane) * SCmax, psi + q * S + s0, row_bytes, &full[st]);
+      if (lane == 0)
+        bulk_load(gs + size_t(st) * KB * 4, gcoef + (rowbase + base) * 4, uint32_t(nb) * 4 * uint32_t(sizeof(TA)),
+                  &full[st]);
+    };
+    for (int b = 0; b < NLP_NS && b < nbatch; b++) issue(b, b);
+    for (int b = 0; b + NLP_NS < nbatch; b++) {
+      const int st = b % NLP_NS;
+      if (!nla_wait(&done[st], uint32_t(b / NLP_NS) & 1u, abort_flag, err)) break;
+      issue(st, b + NLP_NS);
+    }
+    return;
+  }
+
+  const int tid = threadIdx.x;
+  TA acc[J][4];
+#pragma unroll
+  for (int j = 0; j < J; j++)
+#pragma unroll
+    for (int l = 0; l < 4; l++) acc[j][l] = mk<TA>(A(0), A(0));
+  for (int b = 0; b < nbatch; b++) {
+    const int st = b % NLP_NS;
+    const bool ok = nla_wait(&full[st], uint32_t(b / NLP_NS) & 1u, abort_flag, err);
+    if (nla_sync_or(!ok || *abort_flag)) break;
+    const int nb = min(KB, r1 - (r0 + b * KB));
+    const T *rw = rows + size_t(st) * KB * SCmax;
+    const TA *g = gs + size_t(st) * KB * 4;
+    TA bacc[J][4];
+#pragma unroll
+    for (int j = 0; j < J; j++)
+#pragma unroll
+      for (int l = 0; l < 4; l++) bacc[j][l] = mk<TA>(A(0), A(0));
+    for (int q = 0; q < nb; q++) {
+      TA gl[4];
+#pragma unroll
+      for (int l = 0; l < 4; l++) gl[l] = g[q * 4 + l];
+#pragma unroll
+      for (int j = 0; j < J; j++) {
+        const int sl = tid + j * NLA_NT;
+        if (sl < SC) {
+          const T x = rw[(size_t)q * SCmax + sl];
+          const TA v = mk<TA>(A(x.x), A(x.y));
+#pragma unroll
+          for (int l = 0; l < 4; l++) bacc[j][l] = cadd(bacc[j][l], cmul(gl[l], v));
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < J; j++)
+#pragma unroll
+      for (int l = 0; l < 4; l++) acc[j][l] = cadd(acc[j][l], bacc[j][l]);
+    mbar_arrive(&done[st]);  // the producer refills the stage
+  }
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    const int sl = tid + j * NLA_NT;
+    if (sl < SC) {
+#pragma unroll
+      for (int l = 0; l < 4; l++) partial[(((long long)p * NLP_RANGES + rg) * 4 + l) * S + s0 + sl] = acc[j][l];
+    }
+  }
+}
+
 template <typename R, typename A>
 __global__ void nl_project_finish_kernel(const C2<A> *__restrict__ partial, int nproj, int S,
                                          const A *__restrict__ coeff, C2<R> *projraw, C2<R> *projD) {
@@ -200,6 +348,42 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   const size_t pbytes = size_t(P.nproj) * NLP_RANGES * 4 * S * (dbl ? sizeof(double2) : sizeof(float2));
   void *partial = dev_alloc(ctx, pbytes);
   const long long fin = (long long)P.nproj * S;
+  // bulk form: rows of 16-byte multiples, and (automatic choice) enough CTAs to fill the device
+  constexpr int JB = 2;
+  const size_t row_bytes = size_t(S) * sizeof(C2<R>);
+  const int nchunks = (S + NLA_NT * JB - 1) / (NLA_NT * JB);
+  const bool bulk_ok = row_bytes % 16 == 0 && reinterpret_cast<uintptr_t>(psi) % 16 == 0;
+  const bool bulk = bulk_ok && (ctx.nl_bulk > 0 ||
+                                (ctx.nl_bulk == 0 && (long long)P.nproj * NLP_RANGES * nchunks >= 2LL * ctx.num_sms));
+  if (bulk) {
+    const int SCmax = std::min(NLA_NT * JB, S);
+    const size_t srow = size_t(SCmax) * sizeof(C2<R>);
+    int KB = int(16384 / srow);  // about 16 KB of rows per stage
+    KB = KB < 1 ? 1 : (KB > 32 ? 32 : KB);
+    const size_t abytes = dbl ? sizeof(double2) : sizeof(float2);
+    const size_t smem = size_t(NLP_NS) * KB * srow + size_t(NLP_NS) * KB * 4 * abytes + 2 * NLP_NS * sizeof(uint64_t) + 16;
+    const dim3 grid(P.nproj, NLP_RANGES, nchunks);
+    if (dbl) {
+      auto kern = nl_project_bulk_kernel<R, double, JB>;
+      ensure_smem_attr(reinterpret_cast<const void *>(kern), smem);
+      kern<<<grid, NLA_NT + 32, smem, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef, P.d_npts, P.maxsph, KB,
+                                                    static_cast<double2 *>(partial), ctx.d_err);
+      LAUNCHED(ctx);
+      nl_project_finish_kernel<R, double><<<grid_for(fin, 256), 256, 0, ctx.stream>>>(
+          static_cast<const double2 *>(partial), P.nproj, S, P.d_coeff, projraw, projD);
+    } else {
+      auto kern = nl_project_bulk_kernel<R, float, JB>;
+      ensure_smem_attr(reinterpret_cast<const void *>(kern), smem);
+      kern<<<grid, NLA_NT + 32, smem, ctx.stream>>>(psi, S, P.d_pt, P.d_gcoef32, P.d_npts, P.maxsph, KB,
+                                                    static_cast<float2 *>(partial), ctx.d_err);
+      LAUNCHED(ctx);
+      nl_project_finish_kernel<R, float><<<grid_for(fin, 256), 256, 0, ctx.stream>>>(
+          static_cast<const float2 *>(partial), P.nproj, S, P.d_coeff32, projraw, projD);
+    }
+    LAUNCHED(ctx);
+    dev_free(ctx, partial);
+    return;
+  }
   if (dbl) {
     constexpr int K = 2;
     dim3 grid(P.nproj, NLP_RANGES, (S + 32 * K - 1) / (32 * K));
@@ -322,19 +506,8 @@ __global__ void __launch_bounds__(128) nl_apply_kernel(long long nitems, int nch
 // back with bulk copies.  Two stages overlap one batch's copies with the next batch's arithmetic, and
 // the copy engine keeps the bytes in flight that the register-held form could not.  The arithmetic and
 // its order are those of nl_apply_kernel, so the result is bitwise the same.
-constexpr int NLA_NT = 128;   // compute threads
 constexpr int NLA_NS = 2;     // stages
 constexpr int NLA_KMAX = 32;  // largest batch (one producer lane per row)
-
-__device__ __forceinline__ void nla_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NLA_NT) : "memory"); }
-__device__ __forceinline__ bool nla_sync_or(int v) {
-  uint32_t r;
-  asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
-               : "=r"(r)
-               : "r"(v), "n"(NLA_NT)
-               : "memory");
-  return r != 0;
-}
 
 template <typename R, int J>
 __global__ void __launch_bounds__(NLA_NT + 32) nl_apply_bulk_kernel(long long nrec, int KB, int S,
@@ -364,19 +537,7 @@ __global__ void __launch_bounds__(NLA_NT + 32) nl_apply_bulk_kernel(long long nr
     mbar_init_fence();
   }
   __syncthreads();
-  // bounded wait on an mbarrier phase; false (and the error flag raised) on expiry or abort
-  auto wait_bar = [&](uint64_t *b, uint32_t parity) -> bool {
-    const uint64_t t0 = global_ns();
-    while (!mbar_try_wait(b, parity)) {
-      if (*abort_flag) return false;
-      if (global_ns() - t0 > 2000000000ull) {
-        *abort_flag = 1;
-        atomicExch(err, 1);
-        return false;
-      }
-    }
-    return true;
-  };
+  auto wait_bar = [&](uint64_t *b, uint32_t parity) { return nla_wait(b, parity, abort_flag, err); };
 
   if (threadIdx.x >= NLA_NT) {
     // producer warp: lane q copies row q of a batch in and out
@@ -483,10 +644,11 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
   else hc = P.d_hcoef32;
   // bulk form: rows of 16-byte multiples (and 16-byte aligned starts), up to 4 states per compute thread
   const size_t row_bytes = size_t(S) * sizeof(C2<R>);
-  if (row_bytes % 16 == 0 && S <= 4 * NLA_NT && reinterpret_cast<uintptr_t>(out) % 16 == 0) {
-    // about 32 KB of rows per stage, 4..32 points per batch
-    int KB = int(32768 / row_bytes);
-    KB = KB < 4 ? 4 : (KB > NLA_KMAX ? NLA_KMAX : KB);
+  if (ctx.nl_bulk >= 0 && row_bytes % 16 == 0 && S <= 4 * NLA_NT && reinterpret_cast<uintptr_t>(out) % 16 == 0) {
+    // 8 points per batch (measured at 96^3 x 256: 211 us FP32 / 318 us FP64, against 229 / 357 with
+    // 16 / 4 points and 466 / 562 with 32 / 16), fewer when a stage would pass 48 KB
+    int KB = int(49152 / row_bytes);
+    KB = KB < 1 ? 1 : (KB > 8 ? 8 : KB);
     const size_t smem = size_t(NLA_NS) * KB * row_bytes + NLA_KMAX * 4 * sizeof(C2<R>) + NLA_NS * NLA_KMAX * sizeof(int4) +
                         2 * NLA_NS * sizeof(uint64_t) + 16;
     if (smem <= size_t(ctx.max_smem_optin)) {
