@@ -126,7 +126,7 @@ __device__ __forceinline__ bool nla_wait(uint64_t *b, uint32_t parity, volatile 
 // states 32 apart, so each point costs K contiguous 256-byte segments of the state-fastest row.  The
 // warp partials are summed in order into partial[p][rg][l][s].  Stage 2 sums the ranges in order and
 // applies the KB coefficients.
-constexpr int NLP_WARPS = 8, NLP_RANGES = 8;
+constexpr int NLP_WARPS = 8, NLP_RANGES = 16;  // 16 ranges: the bulk projection 181 us against 218 with 8 (FP64, 96^3 x 256)
 
 template <typename R, typename A, int K>
 __global__ void __launch_bounds__(NLP_WARPS * 32) nl_project_kernel(const C2<R> *__restrict__ psi, int S,
@@ -348,13 +348,14 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   const size_t pbytes = size_t(P.nproj) * NLP_RANGES * 4 * S * (dbl ? sizeof(double2) : sizeof(float2));
   void *partial = dev_alloc(ctx, pbytes);
   const long long fin = (long long)P.nproj * S;
-  // bulk form: rows of 16-byte multiples, and (automatic choice) enough CTAs to fill the device
+  // bulk form: rows of 16-byte multiples, and (automatic choice) enough CTAs to fill the device; the
+  // choice (and so the summation order) follows the device's SM count, not the grid_sms option
   constexpr int JB = 2;
   const size_t row_bytes = size_t(S) * sizeof(C2<R>);
   const int nchunks = (S + NLA_NT * JB - 1) / (NLA_NT * JB);
   const bool bulk_ok = row_bytes % 16 == 0 && reinterpret_cast<uintptr_t>(psi) % 16 == 0;
   const bool bulk = bulk_ok && (ctx.nl_bulk > 0 ||
-                                (ctx.nl_bulk == 0 && (long long)P.nproj * NLP_RANGES * nchunks >= 2LL * ctx.num_sms));
+                                (ctx.nl_bulk == 0 && (long long)P.nproj * NLP_RANGES * nchunks >= 2LL * ctx.device_sms));
   if (bulk) {
     const int SCmax = std::min(NLA_NT * JB, S);
     const size_t srow = size_t(SCmax) * sizeof(C2<R>);
