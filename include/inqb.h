@@ -76,6 +76,11 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * multiple of 16 bytes) or -1 (never: register-held gathers).  Changing the priority replaces
  * the context's stream (after the work queued on it), so callers query inqb_ctx_stream again. */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
+/* Self-test of the bounded device-side waits: queues one kernel whose wait on an mbarrier phase that
+ * nothing completes runs out after limit_ns (1e6 .. 1e9) and raises the context's error flag, as an
+ * expired wait of the FFT, overlap or nonlocal kernels does.  The next inqb_ctx_synchronize returns
+ * INQB_ERR_TIMEOUT and clears the flag; the context stays usable.  No fault or hang is involved. */
+int inqb_ctx_check_wait_timeout(inqb_ctx *ctx, long long limit_ns);
 /* Free and total device memory in bytes (admission control for serving). */
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
 

@@ -94,6 +94,7 @@ SIGNATURES = {
     "inqb_shift": (I, [D, D, P, P]),
     "inqb_rotate": (I, [P, DP]),
     "inqb_rotate_to": (I, [P, P, DP, DP, DP]),
+    "inqb_ctx_check_wait_timeout": (I, [P, LL]),
     "inqb_cholesky_inverse": (I, [I, DP, DP]),
     "inqb_hermitian_eigen": (I, [I, DP, DP, DP]),
     "inqb_eigenvalues": (I, [P, P, DP, DP]),

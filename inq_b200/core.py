@@ -57,6 +57,10 @@ class Context:
     def synchronize(self):
         self.check(self.lib.inqb_ctx_synchronize(self.handle))
 
+    def check_wait_timeout(self, limit_s: float = 0.05):
+        """Queue the bounded-wait self-test: the next ``synchronize`` raises InqbError (INQB_ERR_TIMEOUT)."""
+        self.check(self.lib.inqb_ctx_check_wait_timeout(self.handle, int(limit_s * 1e9)))
+
     def stream(self) -> int:
         p = C.c_void_p()
         self.check(self.lib.inqb_ctx_stream(self.handle, C.byref(p)))

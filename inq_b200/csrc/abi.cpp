@@ -838,6 +838,16 @@ int inqb_ctx_synchronize(inqb_ctx *ctx) {
   });
 }
 
+int inqb_ctx_check_wait_timeout(inqb_ctx *ctx, long long limit_ns) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(limit_ns >= 1000000 && limit_ns <= 1000000000, INQB_ERR_ARG, "limit_ns is 1e6 .. 1e9");
+    set_device(*ctx);
+    launch_wait_timeout(*ctx, limit_ns);
+    INQB_CUDA(cudaGetLastError());
+  });
+}
+
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
   return guarded(ctx, [&] {
     INQB_REQUIRE(ctx && key, INQB_ERR_ARG, "null argument");

@@ -240,6 +240,7 @@ void launch_overlap_diag(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long l
                          double2 *out_dev /*[S]*/);
 template <typename R>
 void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev);
+void launch_wait_timeout(Ctx &ctx, long long limit_ns);
 template <typename R>
 void launch_rotate_to(Ctx &ctx, const C2<R> *in, int Sin, C2<R> *out, int Sout, long long npoints, const double2 *Rdev,
                       double2 alpha, double2 beta);

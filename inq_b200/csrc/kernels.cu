@@ -709,6 +709,25 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
   LAUNCHED(ctx);
 }
 
+// ------------------------------------------------------------------ bounded-wait self-test
+// One thread waits on an mbarrier phase that nothing completes; the wait is bounded by `limit_ns` of
+// %globaltimer, after which the context's error flag is raised exactly as by an expired wait of the
+// FFT ring, the tensor-core overlap or the bulk-copy nonlocal kernels.
+__global__ void wait_timeout_kernel(int *err, long long limit_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    ptx::mbar_init(&bar, 1);
+    ptx::mbar_init_fence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !ptx::mbar_wait_bounded(&bar, 0, uint64_t(limit_ns))) atomicExch(err, 1);
+}
+
+void launch_wait_timeout(Ctx &ctx, long long limit_ns) {
+  wait_timeout_kernel<<<1, 32, 0, ctx.stream>>>(ctx.d_err, limit_ns);
+  LAUNCHED(ctx);
+}
+
 // ------------------------------------------------------------------ elementwise
 template <typename R> __global__ void fill_kernel(C2<R> *p, long long n, R re, R im) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
