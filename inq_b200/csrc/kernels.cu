@@ -957,6 +957,79 @@ __global__ void __launch_bounds__(256, 2) overlap_kernel(const C2<R> *__restrict
 
 // With sym (a set against itself, S x S) only tiles with i/64 <= j/64 were computed: an element below
 // them is the conjugate of its mirror, since <a_j|a_i> = conj(<a_i|a_j>).
+// The FP64 form of overlap_kernel with its operand tiles double-buffered in shared memory: the next
+// 16 points of a and b are copied with cp.async while the current ones are multiplied, so the global
+// latency no longer stalls the tile.  Same tiles, order and arithmetic: bitwise the same result.
+__global__ void __launch_bounds__(256, 2) overlap64_kernel(const double2 *__restrict__ a, int Sa,
+                                                        const double2 *__restrict__ b, int Sb, long long npoints,
+                                                        long long chunk, int sym, double2 *partial) {
+  constexpr int TB = 64, KT = 16;
+  extern __shared__ __align__(16) double2 osm[];  // [2 buffers][a, b][KT][TB]
+  int bi = blockIdx.x, bj = blockIdx.y;
+  if (sym) {
+    bj = 0;
+    while ((bj + 1) * (bj + 2) / 2 <= bi) bj++;
+    bi -= bj * (bj + 1) / 2;
+  }
+  const int ti = bi * TB, tj = bj * TB;
+  const long long p0 = blockIdx.z * chunk;
+  const long long p1 = min(npoints, p0 + chunk);
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  auto tile = [&](int buf, int ab) { return osm + (size_t(buf) * 2 + ab) * KT * TB; };
+  auto issue = [&](int buf, long long k0) {
+    double2 *As = tile(buf, 0), *Bs = tile(buf, 1);
+    for (int e = threadIdx.x; e < KT * TB; e += 256) {
+      const int kk = e / TB, c = e % TB;
+      const long long p = k0 + kk;
+      const bool va = p < p1 && ti + c < Sa, vb = p < p1 && tj + c < Sb;
+      ptx::cp_async16(As + e, va ? a + p * Sa + ti + c : a, va ? 16u : 0u);
+      ptx::cp_async16(Bs + e, vb ? b + p * Sb + tj + c : b, vb ? 16u : 0u);
+    }
+    ptx::cp_async_commit();
+  };
+  double2 acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) acc[u][v] = make_double2(0.0, 0.0);
+  if (p0 < p1) issue(0, p0);
+  int cur = 0;
+  for (long long k0 = p0; k0 < p1; k0 += KT, cur ^= 1) {
+    if (k0 + KT < p1) {
+      issue(cur ^ 1, k0 + KT);  // the other buffer was released by the barrier closing the last step
+      ptx::cp_async_wait<1>();
+    } else {
+      ptx::cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double2 *As = tile(cur, 0), *Bs = tile(cur, 1);
+#pragma unroll 4
+    for (int kk = 0; kk < KT; kk++) {
+      double2 av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) av[u] = As[kk * TB + ty + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 4; v++) bv[v] = Bs[kk * TB + tx + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          acc[u][v].x += av[u].x * bv[v].x + av[u].y * bv[v].y;
+          acc[u][v].y += av[u].x * bv[v].y - av[u].y * bv[v].x;
+        }
+    }
+    __syncthreads();
+  }
+  const long long base = (long long)blockIdx.z * Sa * Sb;
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const int i = ti + ty + 16 * u, j = tj + tx + 16 * v;
+      if (i < Sa && j < Sb) partial[base + (long long)i * Sb + j] = acc[u][v];
+    }
+}
+
 __global__ void sum_tiles_kernel(const double2 *partial, int nz, long long n, int S, int sym, double scale,
                                  double2 *out) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
@@ -992,7 +1065,13 @@ void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, lo
   nz = int((npoints + chunk - 1) / chunk);
   double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * (size_t)nz * Sa * Sb));
   const dim3 grid = sym ? dim3(tiles, 1, nz) : dim3(gi, gj, nz);
-  overlap_kernel<R><<<grid, 256, 0, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, sym, partial);
+  if constexpr (sizeof(R) == 8) {
+    const size_t smem = 2 * 2 * 16 * 64 * sizeof(double2);
+    ensure_smem_attr(reinterpret_cast<const void *>(overlap64_kernel), smem);
+    overlap64_kernel<<<grid, 256, smem, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, sym, partial);
+  } else {
+    overlap_kernel<R><<<grid, 256, 0, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, sym, partial);
+  }
   LAUNCHED(ctx);
   const long long n = (long long)Sa * Sb;
   sum_tiles_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(partial, nz, n, Sb, sym, dv, out);
