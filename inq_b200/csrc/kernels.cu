@@ -1130,14 +1130,140 @@ __global__ void __launch_bounds__(256) rotate_kernel(const C2<R> *in, int Sin, C
   }
 }
 
+// Tiled form of the rotation for distinct in and out: CTA = 64 points x 64 output states, 4 x 4 per
+// thread, the states k in steps of 16 with both operand tiles (rows of in, rows of Rm) double-buffered
+// in shared memory by cp.async.  Each CTA reads Rm's 64 columns once for 64 points (the row form reads
+// all of Rm for every 8 points: 116 GB of cache traffic at 96^3 x 256).  Rows of in must be 16-byte
+// multiples (an even state count in single precision).
+template <typename R>
+__global__ void __launch_bounds__(256, 2) rotate_tiled_kernel(const C2<R> *__restrict__ in, int Sin,
+                                                           C2<R> *__restrict__ out, int Sout, long long npoints,
+                                                           const double2 *__restrict__ Rm, double2 alpha,
+                                                           double2 beta, int scaled, int use_beta) {
+  using T = C2<R>;
+  constexpr int TP = 64, TJ = 64, KT = 16;
+  constexpr int EPC = 16 / int(sizeof(T));  // elements of in per 16-byte copy
+  extern __shared__ __align__(16) unsigned char rsm[];
+  T *Abuf = reinterpret_cast<T *>(rsm);                                   // [2][TP][KT]
+  double2 *Bbuf = reinterpret_cast<double2 *>(Abuf + 2 * TP * KT);        // [2][KT][TJ]
+  // blockIdx.x enumerates (point tile, output tile) with the output tiles fastest, so the CTAs that
+  // read one tile of points run together
+  const int njt = (Sout + TJ - 1) / TJ;
+  const int j0 = int(blockIdx.x % njt) * TJ;
+  const long long p0 = (long long)(blockIdx.x / njt) * TP;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  auto issue = [&](int buf, int k0) {
+    T *As = Abuf + buf * TP * KT;
+    double2 *Bs = Bbuf + buf * KT * TJ;
+    for (int e = threadIdx.x; e < TP * KT / EPC; e += 256) {
+      const int r = e / (KT / EPC), kk = (e % (KT / EPC)) * EPC;
+      const long long p = p0 + r;
+      const bool v = p < npoints && k0 + kk < Sin;
+      ptx::cp_async16(As + r * KT + kk, v ? in + p * Sin + k0 + kk : in, v ? 16u : 0u);
+    }
+    for (int e = threadIdx.x; e < KT * TJ; e += 256) {
+      const int kk = e / TJ, c = e % TJ;
+      const bool v = k0 + kk < Sin && j0 + c < Sout;
+      ptx::cp_async16(Bs + e, v ? Rm + (long long)(k0 + kk) * Sout + j0 + c : Rm, v ? 16u : 0u);
+    }
+    ptx::cp_async_commit();
+  };
+  double2 acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) acc[u][v] = make_double2(0.0, 0.0);
+  issue(0, 0);
+  int cur = 0;
+  for (int k0 = 0; k0 < Sin; k0 += KT, cur ^= 1) {
+    if (k0 + KT < Sin) {
+      issue(cur ^ 1, k0 + KT);  // the other buffer was released by the barrier closing the last step
+      ptx::cp_async_wait<1>();
+    } else {
+      ptx::cp_async_wait<0>();
+    }
+    __syncthreads();
+    const T *As = Abuf + cur * TP * KT;
+    const double2 *Bs = Bbuf + cur * KT * TJ;
+#pragma unroll 4
+    for (int kk = 0; kk < KT; kk++) {
+      double2 av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const T x = As[(ty + 16 * u) * KT + kk];
+        av[u] = make_double2(double(x.x), double(x.y));
+      }
+#pragma unroll
+      for (int v = 0; v < 4; v++) bv[v] = Bs[kk * TJ + tx + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          acc[u][v].x += av[u].x * bv[v].x - av[u].y * bv[v].y;
+          acc[u][v].y += av[u].x * bv[v].y + av[u].y * bv[v].x;
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const long long p = p0 + ty + 16 * u;
+      const int j = j0 + tx + 16 * v;
+      if (p < npoints && j < Sout) {
+        double2 w = acc[u][v];
+        if (scaled) w = make_double2(alpha.x * w.x - alpha.y * w.y, alpha.x * w.y + alpha.y * w.x);
+        T *o = out + p * Sout + j;
+        if (use_beta) {
+          const double2 y = make_double2(double(o->x), double(o->y));
+          w.x += beta.x * y.x - beta.y * y.y;
+          w.y += beta.x * y.y + beta.y * y.x;
+        }
+        *o = mk<T>(R(w.x), R(w.y));
+      }
+    }
+}
+
 // out <- alpha (in Rm) + beta out, Rm [Sin][Sout]; in == out (Sin == Sout) rotates in place
 template <typename R>
 void launch_rotate_to(Ctx &ctx, const C2<R> *in, int Sin, C2<R> *out, int Sout, long long npoints, const double2 *Rdev,
                       double2 alpha, double2 beta) {
-  const size_t smem = sizeof(double2) * 8 * Sin;
-  INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "too many states for rotate");
   const int scaled = !(alpha.x == 1.0 && alpha.y == 0.0);
   const int use_beta = !(beta.x == 0.0 && beta.y == 0.0);
+  const bool aligned = (size_t(Sin) * sizeof(C2<R>)) % 16 == 0 && reinterpret_cast<uintptr_t>(in) % 16 == 0 &&
+                       reinterpret_cast<uintptr_t>(Rdev) % 16 == 0;
+  if (aligned) {
+    // tiled kernel, out of place; in place, chunks of 32768 points go through a scratch block and are
+    // copied back (the kernel's CTAs for one tile of points read all of its states)
+    const size_t tsmem = 2 * 64 * 16 * sizeof(C2<R>) + 2 * 16 * 64 * sizeof(double2);
+    ensure_smem_attr(reinterpret_cast<const void *>(rotate_tiled_kernel<R>), tsmem);
+    auto launch = [&](const C2<R> *src, C2<R> *dst, long long n) {
+      const long long nblk = (long long)((Sout + 63) / 64) * ((n + 63) / 64);
+      INQB_REQUIRE(nblk < (1LL << 31), INQB_ERR_UNSUPPORTED, "set too large for the rotation grid");
+      rotate_tiled_kernel<R><<<unsigned(nblk), 256, tsmem, ctx.stream>>>(src, Sin, dst, Sout, n, Rdev, alpha, beta,
+                                                                        scaled, use_beta);
+      LAUNCHED(ctx);
+    };
+    if (in != out) {
+      launch(in, out, npoints);
+      return;
+    }
+    INQB_REQUIRE(Sin == Sout && !use_beta, INQB_ERR_ARG, "an in-place rotation is square and has no beta term");
+    constexpr long long CH = 32768;
+    const long long ch = npoints < CH ? npoints : CH;
+    C2<R> *scratch = static_cast<C2<R> *>(dev_alloc(ctx, sizeof(C2<R>) * size_t(ch) * Sout));
+    for (long long c0 = 0; c0 < npoints; c0 += CH) {
+      const long long n = npoints - c0 < CH ? npoints - c0 : CH;
+      launch(in + c0 * Sin, scratch, n);
+      INQB_CUDA(cudaMemcpyAsync(out + c0 * Sout, scratch, sizeof(C2<R>) * size_t(n) * Sout, cudaMemcpyDeviceToDevice,
+                                ctx.stream));
+    }
+    dev_free(ctx, scratch);
+    return;
+  }
+  const size_t smem = sizeof(double2) * 8 * Sin;
+  INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "too many states for rotate");
   ensure_smem_attr(reinterpret_cast<const void *>(rotate_kernel<R>), smem);
   rotate_kernel<R><<<grid_for(npoints, 8, 148LL * 16), 256, smem, ctx.stream>>>(in, Sin, out, Sout, npoints, Rdev, alpha,
                                                                               beta, scaled, use_beta);
