@@ -266,12 +266,18 @@ __global__ void __launch_bounds__(NLA_NT + 32) nl_project_bulk_kernel(const C2<R
         bulk_load(gs + size_t(st) * KB * 4, gcoef + (rowbase + base) * 4, uint32_t(nb) * 4 * uint32_t(sizeof(TA)),
                   &full[st]);
     };
-    for (int b = 0; b < NLP_NS && b < nbatch; b++) issue(b, b);
+    int issued = 0;  // batches whose copies were issued
+    for (int b = 0; b < NLP_NS && b < nbatch; b++) issue(b, b), issued++;
     for (int b = 0; b + NLP_NS < nbatch; b++) {
       const int st = b % NLP_NS;
       if (!nla_wait(&done[st], uint32_t(b / NLP_NS) & 1u, abort_flag, err)) break;
       issue(st, b + NLP_NS);
+      issued++;
     }
+    // after an abort the compute threads may leave early: wait (bounded) for every issued copy to land
+    // before the CTA's shared memory is released (on the normal path these phases are already complete)
+    for (int b = issued - NLP_NS < 0 ? 0 : issued - NLP_NS; b < issued; b++)
+      mbar_wait_bounded(&full[b % NLP_NS], uint32_t(b / NLP_NS) & 1u, 2000000000ull);
     return;
   }
 
@@ -576,9 +582,10 @@ __global__ void __launch_bounds__(NLA_NT + 32, sizeof(R) == 4 ? 6 : 3) nl_apply_
       __syncwarp();
       if (lane < nb) bulk_load(rows + (size_t(st) * KB + lane) * S, out + (long long)rec.x * S, row_bytes, &full[st]);
     };
+    int issued = 0;  // batches whose loads were issued, in order
     for (int st = 0; st < NLA_NS; st++) {
       const long long b = blockIdx.x + (long long)st * gridDim.x;
-      if (b < nbatch) issue(st, b);
+      if (b < nbatch) issue(st, b), issued++;
     }
     int k = 0;
     for (long long b = blockIdx.x; b < nbatch; b += gridDim.x, k++) {
@@ -591,8 +598,12 @@ __global__ void __launch_bounds__(NLA_NT + 32, sizeof(R) == 4 ? 6 : 3) nl_apply_
       bulk_wait_read0();  // the stage may be refilled once its rows are read out
       __syncwarp();
       const long long bn = b + (long long)NLA_NS * gridDim.x;
-      if (bn < nbatch) issue(st, bn);
+      if (bn < nbatch) issue(st, bn), issued++;
     }
+    // after an abort the compute threads may leave early: wait (bounded) for every issued load to land
+    // before the CTA's shared memory is released (on the normal path these phases are already complete)
+    for (int i = issued - NLA_NS < 0 ? 0 : issued - NLA_NS; i < issued; i++)
+      mbar_wait_bounded(&full[i % NLA_NS], uint32_t(i / NLA_NS) & 1u, 2000000000ull);
     bulk_wait0();
     return;
   }
