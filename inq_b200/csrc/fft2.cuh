@@ -809,10 +809,18 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR>(), min_ctas_of
     return true;
   };
 
+  // tiles whose loads the issuing thread has started (the i-th goes to stage i % NS, phase i / NS);
+  // before the CTA ends, that thread waits (bounded) for the last NS of them, so that after an aborted
+  // wait no load still lands in shared memory (on the normal path those phases are complete already)
+  int nissued = 0;
+  auto drain = [&]() {
+    for (int i = nissued - NS < 0 ? 0 : nissued - NS; i < nissued; i++)
+      ptx::mbar_wait_bounded(&bar[i % NS], uint32_t(i / NS) & 1u, 2000000000ull);
+  };
   if (threadIdx.x == (WS ? NT : 0)) {
     for (int s = 0; s < NS; s++) {
       const long long t = blockIdx.x + (long long)s * gridDim.x;
-      if (t < gg.ntiles) issue(s, t);
+      if (t < gg.ntiles) issue(s, t), nissued++;
     }
   }
   if constexpr (WS) {
@@ -830,8 +838,9 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR>(), min_ctas_of
           bulk_commit();
           bulk_wait_read0();
           const long long tn = t + (long long)NS * gridDim.x;
-          if (tn < gg.ntiles) issue(st, tn);
+          if (tn < gg.ntiles) issue(st, tn), nissued++;
         }
+        drain();
         bulk_wait0();
       }
       return;
@@ -956,11 +965,14 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR>(), min_ctas_of
         bulk_commit();
         bulk_wait_read0();  // the stage may be refilled once the store has read it
         const long long tn = t + (long long)NS * gridDim.x;
-        if (tn < gg.ntiles) issue(st, tn);
+        if (tn < gg.ntiles) issue(st, tn), nissued++;
       }
     }
   }
-  if (!WS && threadIdx.x == 0) bulk_wait0();
+  if (!WS && threadIdx.x == 0) {
+    drain();
+    bulk_wait0();
+  }
 }
 
 }  // namespace v2
