@@ -105,6 +105,11 @@ class orbital_set {
   int spin_;
   int precision_;
 
+  orbital_set(basis::real_space const &basis, inqb_orbitals *p, int nst, std::array<double, 3> kpoint, int spin_index,
+              int precision)
+      : basis_(basis), o_(p, inqb_orbitals_destroy), nst_(nst), kpoint_(kpoint), spin_(spin_index),
+        precision_(precision) {}
+
  public:
   orbital_set(basis::real_space const &basis, int nst, std::array<double, 3> kpoint = {0, 0, 0}, int spin_index = 0,
               space sp = space::real, int precision = INQB_F64)
@@ -118,6 +123,19 @@ class orbital_set {
   }
   orbital_set(orbital_set &&) = default;
   orbital_set &operator=(orbital_set &&) = default;
+
+  // A set over caller-owned storage of nst complex numbers per point, [npoint][nst], already on the
+  // device (device memory of the context's device, or managed memory such as the reference's
+  // gpu::array): no copy, and the storage is not freed with the set (inqb_orbitals_wrap).
+  static orbital_set wrap(basis::real_space const &basis, void *device_data, int nst,
+                          std::array<double, 3> kpoint = {0, 0, 0}, int spin_index = 0, space sp = space::real,
+                          int precision = INQB_F64) {
+    inqb_orbitals *p = nullptr;
+    b200::check(inqb_orbitals_wrap(basis.ctx().get(), basis.get(), device_data, nst, 1, kpoint.data(), spin_index,
+                                   int(sp), precision, &p),
+                basis.ctx().get());
+    return orbital_set(basis, p, nst, kpoint, spin_index, precision);
+  }
 
   // a new set with the same basis, size, k-point, spin and space (orbital_set::skeleton)
   orbital_set skeleton() const { return orbital_set(basis_, nst_, kpoint_, spin_, current_space(), precision_); }
@@ -186,6 +204,10 @@ class ks_hamiltonian {
     states::orbital_set hphi = phi.skeleton();
     b200::check(inqb_apply(h_.get(), phi.get(), hphi.get()), basis_.ctx().get());
     return hphi;
+  }
+  // hphi = H phi into an existing set of the same shape (with wrapped sets: no allocation, no copy)
+  void apply(states::orbital_set const &phi, states::orbital_set &hphi) const {
+    b200::check(inqb_apply(h_.get(), phi.get(), hphi.get()), basis_.ctx().get());
   }
   double non_local_energy(states::orbital_set const &phi, std::vector<double> const &occupations) const {
     double e = 0;

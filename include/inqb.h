@@ -81,6 +81,9 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
  * expired wait of the FFT, overlap or nonlocal kernels does.  The next inqb_ctx_synchronize returns
  * INQB_ERR_TIMEOUT and clears the flag; the context stays usable.  No fault or hang is involved. */
 int inqb_ctx_check_wait_timeout(inqb_ctx *ctx, long long limit_ns);
+/* Number of device allocations (cudaMalloc / cudaMallocAsync) the library has made in this
+ * process so far, over all contexts; a diagnostic for callers that budget device memory. */
+int inqb_device_alloc_count(long long *count);
 /* Free and total device memory in bytes (admission control for serving). */
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
 
@@ -98,6 +101,18 @@ int inqb_basis_volume_element(const inqb_basis *basis, double *dv);
 int inqb_orbitals_create(inqb_ctx *ctx, const inqb_basis *basis, int nst, int spinor_dim,
                          const double kpoint_cov[3], int spin_index, int space, int precision,
                          inqb_orbitals **out);
+/* The same set over caller-owned storage, with no copy: the zero-copy form of the boundary, for
+ * orbitals that are already on the device, e.g. field_set::matrix().data_elements() of a
+ * reference orbital_set, whose gpu::array lives in CUDA managed memory prefetched to the device
+ * (external_libs/gpurun/include/gpu/array.hpp:66-110).  data holds npoint*nst complex numbers of
+ * `precision` in the layout [npoint][nst], 16-byte aligned, in device memory of the context's
+ * device or in managed memory (prefetched to the device on the context's stream here); anything
+ * else is refused with INQB_ERR_ARG.  The set borrows the storage: inqb_orbitals_destroy does not
+ * free it, and the caller keeps it alive, and leaves it alone while work queued on the context
+ * reads or writes it, until then. */
+int inqb_orbitals_wrap(inqb_ctx *ctx, const inqb_basis *basis, void *data, int nst, int spinor_dim,
+                       const double kpoint_cov[3], int spin_index, int space, int precision,
+                       inqb_orbitals **out);
 int inqb_orbitals_destroy(inqb_orbitals *orb);
 /* Host <-> device copies of the whole set, layout [npoint][nst] in the set's precision. */
 int inqb_orbitals_upload(inqb_orbitals *orb, const void *host);
@@ -238,12 +253,13 @@ int inqb_overlap_diagonal(const inqb_orbitals *a, const inqb_orbitals *b, double
  * library allocate device memory (a serving loop whose admission control has handed all
  * device memory to resident orbital sets; latency-sensitive code that must not risk the
  * implicit synchronisation of cudaMalloc/cudaFree).  Allocates nothing: out_dev is a
- * caller-owned device buffer of nst complex128 (2*nst doubles) on the sets' device, and the
- * reduction's partial sums use a fixed 2.3 MiB array inside the library (held by every GPU
- * that loads it).  At most 512 states; larger sets get INQB_ERR_ARG.  Asynchronous on the
- * context's stream.  The first call on a device looks up that array's device address; make
- * it before any stream capture.  All calls share the array: calls that overlap on the GPU
- * (different streams or contexts) race. */
+ * caller-owned buffer of nst complex128 (2*nst doubles, 8-byte aligned) in device memory of
+ * the sets' device or in managed memory; host memory and other devices' memory are refused
+ * with INQB_ERR_ARG.  The reduction's partial sums use a fixed 2.3 MiB array inside the
+ * library, placed on a device by the first inqb_ctx_create there and held until the process
+ * exits.  At most 512 states; larger sets get INQB_ERR_ARG.  Asynchronous on the context's
+ * stream.  All calls share the array: calls that overlap on the GPU (different streams or
+ * contexts) race.  A context, and so this entry point, does not survive cudaDeviceReset. */
 int inqb_overlap_diagonal_noalloc(const inqb_orbitals *a, const inqb_orbitals *b, double *out_dev);
 /* operations::orthogonalize (orthogonalize.hpp:25-31): FP64 overlap, FP64 Cholesky
  * (matrix/cholesky.hpp:28-99), phi <- phi U^-1 (rotate.hpp:147-156). */

@@ -43,11 +43,13 @@ SIGNATURES = {
     "inqb_ctx_stream": (I, [P, C.POINTER(P)]),
     "inqb_ctx_launch_count": (I, [P, C.POINTER(LL)]),
     "inqb_ctx_set_option": (I, [P, C.c_char_p, LL]),
+    "inqb_device_alloc_count": (I, [C.POINTER(LL)]),
     "inqb_ctx_mem_info": (I, [P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "inqb_basis_create": (I, [P, DP, I, I, I, C.POINTER(P)]),
     "inqb_basis_destroy": (I, [P]),
     "inqb_basis_volume_element": (I, [P, DP]),
     "inqb_orbitals_create": (I, [P, P, I, I, DP, I, I, I, C.POINTER(P)]),
+    "inqb_orbitals_wrap": (I, [P, P, P, I, I, DP, I, I, I, C.POINTER(P)]),
     "inqb_orbitals_destroy": (I, [P]),
     "inqb_orbitals_upload": (I, [P, P]),
     "inqb_orbitals_download": (I, [P, P]),

@@ -85,6 +85,13 @@ class Context:
             self.handle = None
 
 
+def device_alloc_count() -> int:
+    """Device allocations the library has made in this process so far (inqb_device_alloc_count)."""
+    n = C.c_longlong()
+    check(_lib.load().inqb_device_alloc_count(C.byref(n)))
+    return n.value
+
+
 # ---------------------------------------------------------------- cell and bases
 
 
@@ -338,6 +345,44 @@ class OrbitalSet:
 
     def nbytes(self) -> int:
         return self.basis.size() * self.nst * (16 if self.precision == F64 else 8)
+
+    @classmethod
+    def wrap(cls, basis, data_ptr: int, nst: int, kpoint=(0.0, 0.0, 0.0), spin_index: int = 0,
+             space: int = REAL_SPACE, precision: int = F64, owner=None) -> "OrbitalSet":
+        """A set over caller-owned device or managed storage [npoint][nst], with no copy (inqb_orbitals_wrap).
+        ``owner`` (e.g. the torch tensor holding the storage) is kept alive as long as the set."""
+        self = cls.__new__(cls)
+        self.basis = basis
+        self.ctx = basis.ctx
+        self.nst = int(nst)
+        self._kpoint = np.asarray(kpoint, dtype=np.float64).copy()
+        self._spin = int(spin_index)
+        self.precision = precision
+        self._owner = owner
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.inqb_orbitals_wrap(self.ctx.handle, basis.handle, C.c_void_p(int(data_ptr)),
+                                                       self.nst, 1, dptr(self._kpoint), self._spin, space, precision,
+                                                       C.byref(h)))
+        self.handle = h
+        return self
+
+    @classmethod
+    def from_tensor(cls, basis, tensor, kpoint=(0.0, 0.0, 0.0), spin_index: int = 0, space: int = REAL_SPACE):
+        """Borrow a contiguous CUDA torch tensor of complex128 or complex64 with basis.size() * nst
+        elements (shape [npoint, nst] or [nx, ny, nz, nst]) as an orbital set, with no copy."""
+        import torch
+        if not tensor.is_cuda or not tensor.is_contiguous():
+            raise ValueError("from_tensor takes a contiguous CUDA tensor")
+        if tensor.dtype == torch.complex128:
+            precision = F64
+        elif tensor.dtype == torch.complex64:
+            precision = F32
+        else:
+            raise ValueError("from_tensor takes complex128 or complex64")
+        nst = tensor.shape[-1]
+        if tensor.numel() != basis.size() * nst:
+            raise ValueError(f"tensor has {tensor.numel()} elements, the basis wants {basis.size()} x {nst}")
+        return cls.wrap(basis, tensor.data_ptr(), nst, kpoint, spin_index, space, precision, owner=tensor)
 
     @classmethod
     def from_array(cls, basis, arr, kpoint=(0.0, 0.0, 0.0), spin_index=0, space=REAL_SPACE, precision=F64):

@@ -100,8 +100,8 @@ template <typename R> C2<R> *proj_buf(Hamiltonian &h, int S, int which) {
     if (h.d_projD) INQB_CUDA(cudaFreeAsync(h.d_projD, h.ctx->stream));
     h.d_projraw = h.d_projD = nullptr;
     h.proj_bytes = 0;
-    INQB_CUDA(cudaMallocAsync(&h.d_projraw, need, h.ctx->stream));
-    INQB_CUDA(cudaMallocAsync(&h.d_projD, need, h.ctx->stream));
+    INQB_CUDA(counted_malloc_async(&h.d_projraw, need, h.ctx->stream));
+    INQB_CUDA(counted_malloc_async(&h.d_projD, need, h.ctx->stream));
     h.proj_bytes = need;
   }
   return static_cast<C2<R> *>(which == 0 ? h.d_projraw : h.d_projD);
@@ -544,7 +544,7 @@ namespace {
 template <typename T> T *upload_vec(const std::vector<T> &v, cudaStream_t st) {
   T *d = nullptr;
   const size_t bytes = std::max<size_t>(sizeof(T), v.size() * sizeof(T));
-  INQB_CUDA(cudaMallocAsync(&d, bytes, st));
+  INQB_CUDA(counted_malloc_async(&d, bytes, st));
   if (!v.empty()) INQB_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   return d;
 }
@@ -629,10 +629,10 @@ void set_projectors(Hamiltonian &h, int nproj, int maxsph, int maxnlm, const int
   P.d_hitpts = upload_vec(hitpts, st);
   P.d_hitp = upload_vec(hitp, st);
   P.d_hrec = upload_vec(hrec, st);
-  INQB_CUDA(cudaMallocAsync(&P.d_gcoef, sizeof(double2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4), st));
-  INQB_CUDA(cudaMallocAsync(&P.d_gcoef32, sizeof(float2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4), st));
-  INQB_CUDA(cudaMallocAsync(&P.d_hcoef, sizeof(double2) * std::max<size_t>(1, size_t(P.total) * 4), st));
-  INQB_CUDA(cudaMallocAsync(&P.d_hcoef32, sizeof(float2) * std::max<size_t>(1, size_t(P.total) * 4), st));
+  INQB_CUDA(counted_malloc_async(&P.d_gcoef, sizeof(double2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4), st));
+  INQB_CUDA(counted_malloc_async(&P.d_gcoef32, sizeof(float2) * std::max<size_t>(1, size_t(nproj) * maxsph * 4), st));
+  INQB_CUDA(counted_malloc_async(&P.d_hcoef, sizeof(double2) * std::max<size_t>(1, size_t(P.total) * 4), st));
+  INQB_CUDA(counted_malloc_async(&P.d_hcoef32, sizeof(float2) * std::max<size_t>(1, size_t(P.total) * 4), st));
   INQB_CUDA(cudaStreamSynchronize(st));  // the host tables above go out of scope
   P.kA[0] = P.kA[1] = P.kA[2] = 1e300;  // tables are built on first use for a given k + A
 }
@@ -795,9 +795,18 @@ int inqb_ctx_create(int device, inqb_ctx **out) {
     c->device = device;
     c->num_sms = c->device_sms = prop.multiProcessorCount;
     c->max_smem_optin = prop.sharedMemPerBlockOptin;
-    INQB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    INQB_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
-    INQB_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+    try {
+      INQB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      note_device_alloc();
+      INQB_CUDA(cudaMalloc(&c->d_err, sizeof(int)));
+      INQB_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+      noalloc_prepare(*c);
+    } catch (...) {
+      if (c->d_err) cudaFree(c->d_err);
+      if (c->stream) cudaStreamDestroy(c->stream);
+      delete c;
+      throw;
+    }
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
       uint64_t thr = UINT64_MAX;
@@ -904,6 +913,13 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count) {
   return guarded(ctx, [&] { *count = ctx->launches; });
 }
 
+int inqb_device_alloc_count(long long *count) {
+  return guarded(nullptr, [&] {
+    INQB_REQUIRE(count, INQB_ERR_ARG, "null argument");
+    *count = device_alloc_count();
+  });
+}
+
 int inqb_ctx_mem_info(inqb_ctx *ctx, size_t *free_bytes, size_t *total_bytes) {
   return guarded(ctx, [&] {
     set_device(*ctx);
@@ -937,8 +953,8 @@ int inqb_basis_create(inqb_ctx *ctx, const double lattice[9], int nx, int ny, in
           t32[2 * t] = make_float2(float(c), float(sn));
           t32[2 * t + 1] = make_float2(float(c - (long double)t32[2 * t].x), float(sn - (long double)t32[2 * t].y));
         }
-        INQB_CUDA(cudaMallocAsync(&b->tw64[ax], sizeof(double2) * n, ctx->stream));
-        INQB_CUDA(cudaMallocAsync(&b->tw32[ax], sizeof(float2) * 2 * n, ctx->stream));
+        INQB_CUDA(counted_malloc_async(&b->tw64[ax], sizeof(double2) * n, ctx->stream));
+        INQB_CUDA(counted_malloc_async(&b->tw32[ax], sizeof(float2) * 2 * n, ctx->stream));
         INQB_CUDA(cudaMemcpyAsync(b->tw64[ax], t64.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, ctx->stream));
         INQB_CUDA(cudaMemcpyAsync(b->tw32[ax], t32.data(), sizeof(float2) * 2 * n, cudaMemcpyHostToDevice, ctx->stream));
         INQB_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -991,7 +1007,7 @@ int inqb_orbitals_create(inqb_ctx *ctx, const inqb_basis *basis, int nst, int sp
     o->spin_index = spin_index;
     o->space = space;
     o->precision = precision;
-    cudaError_t e = cudaMallocAsync(&o->data, o->bytes(), ctx->stream);
+    cudaError_t e = counted_malloc_async(&o->data, o->bytes(), ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // usable from any stream on return
     if (e != cudaSuccess) {
       (void)cudaGetLastError();
@@ -1002,10 +1018,59 @@ int inqb_orbitals_create(inqb_ctx *ctx, const inqb_basis *basis, int nst, int sp
   });
 }
 
+int inqb_orbitals_wrap(inqb_ctx *ctx, const inqb_basis *basis, void *data, int nst, int spinor_dim,
+                       const double kpoint_cov[3], int spin_index, int space, int precision, inqb_orbitals **out) {
+  return guarded(ctx, [&] {
+    INQB_REQUIRE(ctx && basis && data && out, INQB_ERR_ARG, "null argument");
+    INQB_REQUIRE(basis->ctx == ctx, INQB_ERR_ARG, "the basis belongs to another context");
+    INQB_REQUIRE(nst > 0, INQB_ERR_ARG, "number of states must be positive");
+    INQB_REQUIRE(spinor_dim == 1, INQB_ERR_UNSUPPORTED, "spinor orbital sets are not implemented");
+    INQB_REQUIRE(space == INQB_REAL_SPACE || space == INQB_FOURIER_SPACE, INQB_ERR_ARG, "bad space tag");
+    INQB_REQUIRE(precision == INQB_F64 || precision == INQB_F32, INQB_ERR_ARG, "bad precision tag");
+    INQB_REQUIRE(spin_index >= 0, INQB_ERR_ARG, "bad spin index");
+    INQB_REQUIRE(reinterpret_cast<uintptr_t>(data) % 16 == 0, INQB_ERR_ARG,
+                 "wrapped orbital storage must be aligned to 16 bytes");
+    set_device(*ctx);
+    cudaPointerAttributes attr{};
+    const cudaError_t e = cudaPointerGetAttributes(&attr, data);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      throw Error(INQB_ERR_ARG, std::string("wrapped storage is not a CUDA pointer: ") + cudaGetErrorString(e));
+    }
+    INQB_REQUIRE(attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged, INQB_ERR_ARG,
+                 "wrapped storage must be device or managed memory (got host or unregistered memory)");
+    if (attr.type == cudaMemoryTypeDevice)
+      INQB_REQUIRE(attr.device == ctx->device, INQB_ERR_ARG,
+                   "wrapped storage is memory of device " + std::to_string(attr.device) + ", the context's is " +
+                       std::to_string(ctx->device));
+    auto *o = new inqb_orbitals();
+    o->ctx = ctx;
+    o->basis = basis;
+    o->nst = nst;
+    for (int i = 0; i < 3; i++) o->kpoint[i] = kpoint_cov ? kpoint_cov[i] : 0.0;
+    o->spin_index = spin_index;
+    o->space = space;
+    o->precision = precision;
+    o->data = data;
+    o->owned = false;
+    if (attr.type == cudaMemoryTypeManaged) {
+      // the reference's allocator prefetches its managed arrays to the device (gpu/array.hpp:84-88); the
+      // same here, ordered before every kernel the context queues on the set
+      const cudaError_t pe = cudaMemPrefetchAsync(data, o->bytes(), ctx->device, ctx->stream);
+      if (pe != cudaSuccess) {
+        (void)cudaGetLastError();
+        delete o;
+        throw Error(INQB_ERR_CUDA, std::string("prefetch of managed orbital storage failed: ") + cudaGetErrorString(pe));
+      }
+    }
+    *out = o;
+  });
+}
+
 int inqb_orbitals_destroy(inqb_orbitals *o) {
   if (!o) return INQB_OK;
   cudaSetDevice(o->ctx->device);
-  if (o->data) cudaFreeAsync(o->data, o->ctx->stream);
+  if (o->data && o->owned) cudaFreeAsync(o->data, o->ctx->stream);
   delete o;
   return INQB_OK;
 }
@@ -1162,8 +1227,8 @@ int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, i
     h->basis = basis;
     h->nspin = nspin;
     const size_t nv = size_t(basis->npoints) * nspin;
-    INQB_CUDA(cudaMallocAsync(&h->d_V, sizeof(double) * nv, ctx->stream));
-    INQB_CUDA(cudaMallocAsync(&h->d_V32, sizeof(float) * nv, ctx->stream));
+    INQB_CUDA(counted_malloc_async(&h->d_V, sizeof(double) * nv, ctx->stream));
+    INQB_CUDA(counted_malloc_async(&h->d_V32, sizeof(float) * nv, ctx->stream));
     INQB_CUDA(cudaMemsetAsync(h->d_V, 0, sizeof(double) * nv, ctx->stream));
     INQB_CUDA(cudaMemsetAsync(h->d_V32, 0, sizeof(float) * nv, ctx->stream));
     INQB_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1485,7 +1550,7 @@ int inqb_apply_host(const inqb_hamiltonian *hc, int nst, const double kpoint_cov
       INQB_CUDA(cudaEventCreateWithFlags(&r.ev_out[i], cudaEventDisableTiming));
       for (void **p : {&r.bin[i], &r.bout[i]}) {
         if (i == 1 && nblocks == 1) continue;
-        cudaError_t e = cudaMallocAsync(p, npts * B * cs, ctx.stream);
+        cudaError_t e = counted_malloc_async(p, npts * B * cs, ctx.stream);
         if (e != cudaSuccess) {
           (void)cudaGetLastError();
           throw Error(INQB_ERR_MEMORY, "device allocation of a state block failed: " + std::string(cudaGetErrorString(e)));

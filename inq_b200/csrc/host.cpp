@@ -4,6 +4,7 @@
 // reference's arithmetic (spherical_grid.hpp:96-135) bit for bit.
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -83,10 +84,17 @@ double set_volume_element(const Orbitals &o) {
 
 // ------------------------------------------------------------------ scratch memory
 
+namespace {
+std::atomic<long long> g_device_allocs{0};
+}
+
+void note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
+long long device_alloc_count() { return g_device_allocs.load(std::memory_order_relaxed); }
+
 void *dev_alloc(Ctx &ctx, size_t bytes) {
   void *p = nullptr;
   if (bytes == 0) bytes = 16;
-  cudaError_t e = cudaMallocAsync(&p, bytes, ctx.stream);
+  cudaError_t e = counted_malloc_async(&p, bytes, ctx.stream);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     throw Error(INQB_ERR_MEMORY, std::string("device allocation of ") + std::to_string(bytes) +

@@ -76,6 +76,7 @@ struct Ctx {
   int overlap_tc = 1;        // overlaps of single-precision sets on the tensor cores (split BF16)
   int nl_bulk = 0;           // nonlocal kernels: 0 automatic, 1 bulk-copy forms wherever they apply, -1 never
   int stream_priority = 0;   // 0: the device's lowest stream priority, 1: its highest
+  void *noalloc_partial = nullptr;  // device address of noalloc.cu's fixed partial-sum array on this device
 };
 
 struct Basis {
@@ -101,6 +102,7 @@ struct Orbitals {
   int space = INQB_REAL_SPACE;
   int precision = INQB_F64;
   void *data = nullptr;
+  bool owned = true;     // false: caller memory borrowed by inqb_orbitals_wrap, never freed here
   size_t bytes() const { return size_t(basis->npoints) * nst * (precision == INQB_F64 ? 16 : 8); }
 };
 
@@ -287,9 +289,23 @@ void launch_ks_potential(Ctx &ctx, const double *n, const double *vion, const do
 void launch_overlap_tc(Ctx &ctx, const float2 *a, int Sa, const float2 *b, int Sb, long long npoints, double dv,
                        double2 *out);
 
+// Looks up the device address of the fixed array of the allocation-free entry point (noalloc.cu) and
+// loads its kernels, with the context's device current; called when a context is created, so the
+// array and the kernels' code are resident before the entry point's first call.
+void noalloc_prepare(Ctx &ctx);
+
 // scratch allocation on the context stream (stream-ordered pool)
 void *dev_alloc(Ctx &ctx, size_t bytes);
 void dev_free(Ctx &ctx, void *p);
+
+// Every device allocation of the library goes through counted_malloc_async (or dev_alloc, which calls
+// it), so inqb_device_alloc_count can report how many the process has made.
+void note_device_alloc();
+long long device_alloc_count();
+template <typename T> cudaError_t counted_malloc_async(T **p, size_t bytes, cudaStream_t st) {
+  note_device_alloc();
+  return cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st);
+}
 
 }  // namespace inqb
 

@@ -5,10 +5,13 @@
 // byte, so a surprise allocation can fail or push out a request), and latency-sensitive callers
 // that must not risk the implicit device-wide synchronisation cudaMalloc/cudaFree can trigger.
 // inqb_overlap_diagonal_noalloc serves them: the caller passes the orbital sets and a device
-// buffer for the result, and the block partial sums live in the fixed array below, which is
-// part of the library image (every GPU that loads the library holds its 2.3 MiB until exit).
-
-#include <mutex>
+// buffer for the result, and the block partial sums live in the fixed array below.
+//
+// When the memory is taken: CUDA loads a library's device code lazily by default, so the array
+// would otherwise be placed on a device at the first use of this file's code there.  Every
+// inqb_ctx_create calls noalloc_prepare, which looks the array's address up (loading this file's
+// module, array included) and loads the two kernels; from then on the device holds the array's
+// 2.3 MiB until the process exits, and the entry point's calls on that context allocate nothing.
 
 #include "inqb_internal.h"
 
@@ -22,25 +25,6 @@ constexpr int NOALLOC_MAX_STATES = 512;   // largest orbital set accepted
 // stage 2 reads, so nothing has to be cleared between calls.  All calls share this array:
 // calls whose kernels overlap on the GPU (different streams or contexts) race on it.
 static __device__ __align__(256) double2 g_noalloc_partial[NOALLOC_BLOCKS * NOALLOC_MAX_STATES];
-
-constexpr int MAX_DEVICES = 64;
-std::mutex g_mutex;
-double2 *g_partial_addr[MAX_DEVICES] = {};
-
-// Device address of the array on the current device.  In host code the array's name is only a
-// host-side handle, so it must never be passed to a kernel; the address comes from the runtime,
-// looked up once per device with that device current.
-double2 *partial_address(int device) {
-  INQB_REQUIRE(device >= 0 && device < MAX_DEVICES, INQB_ERR_UNSUPPORTED, "device index too large");
-  std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_partial_addr[device]) {
-    void *p = nullptr;
-    INQB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partial));
-    INQB_REQUIRE(p != nullptr, INQB_ERR_CUDA, "cudaGetSymbolAddress returned no address");
-    g_partial_addr[device] = static_cast<double2 *>(p);
-  }
-  return g_partial_addr[device];
-}
 
 // stage 1: block b sums conj(a) b over its contiguous point range, one thread per state
 template <typename R>
@@ -60,19 +44,55 @@ __global__ void noalloc_partial_kernel(const C2<R> *__restrict__ a, const C2<R> 
   }
 }
 
-// stage 2: partials summed in block order, times the volume element
-__global__ void noalloc_sum_kernel(const double2 *partial, int nblk, int S, double scale, double2 *out) {
+// stage 2: partials summed in block order, times the volume element; the result is written as
+// two separate doubles, so out needs only the 8-byte alignment of a double
+__global__ void noalloc_sum_kernel(const double2 *partial, int nblk, int S, double scale, double *out) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
     double re = 0.0, im = 0.0;
     for (int k = 0; k < nblk; k++) {
       re += partial[(long long)k * S + s].x;
       im += partial[(long long)k * S + s].y;
     }
-    out[s] = make_double2(scale * re, scale * im);
+    out[2 * s] = scale * re;
+    out[2 * s + 1] = scale * im;
+  }
+}
+
+// A device buffer the kernels may store to: device memory or managed memory reachable from the
+// context's device.  Host memory (pageable or pinned) and other devices' memory are refused, as
+// the store would fault the GPU or silently write somewhere else.
+void check_output_buffer(const Ctx &ctx, const double *out_dev) {
+  INQB_REQUIRE(reinterpret_cast<uintptr_t>(out_dev) % alignof(double) == 0, INQB_ERR_ARG,
+               "out_dev is not aligned to 8 bytes");
+  cudaPointerAttributes attr{};
+  const cudaError_t e = cudaPointerGetAttributes(&attr, out_dev);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw Error(INQB_ERR_ARG, std::string("out_dev is not a CUDA pointer: ") + cudaGetErrorString(e));
+  }
+  if (attr.type == cudaMemoryTypeDevice) {
+    INQB_REQUIRE(attr.device == ctx.device, INQB_ERR_ARG,
+                 "out_dev is device memory of device " + std::to_string(attr.device) + ", the sets live on device " +
+                     std::to_string(ctx.device));
+  } else {
+    INQB_REQUIRE(attr.type == cudaMemoryTypeManaged, INQB_ERR_ARG,
+                 "out_dev must be device or managed memory (got host or unregistered memory)");
   }
 }
 
 }  // namespace
+
+void noalloc_prepare(Ctx &ctx) {
+  void *p = nullptr;
+  INQB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partial));
+  INQB_REQUIRE(p != nullptr, INQB_ERR_CUDA, "cudaGetSymbolAddress returned no address");
+  cudaFuncAttributes fa;
+  INQB_CUDA(cudaFuncGetAttributes(&fa, noalloc_partial_kernel<double>));
+  INQB_CUDA(cudaFuncGetAttributes(&fa, noalloc_partial_kernel<float>));
+  INQB_CUDA(cudaFuncGetAttributes(&fa, noalloc_sum_kernel));
+  ctx.noalloc_partial = p;
+}
+
 }  // namespace inqb
 
 using namespace inqb;
@@ -87,7 +107,9 @@ extern "C" int inqb_overlap_diagonal_noalloc(const inqb_orbitals *a, const inqb_
                  "inqb_overlap_diagonal_noalloc accepts at most " + std::to_string(NOALLOC_MAX_STATES) +
                      " states (got " + std::to_string(a->nst) + "); use inqb_overlap_diagonal");
     INQB_CUDA(cudaSetDevice(ctx->device));
-    double2 *partial = partial_address(ctx->device);
+    INQB_REQUIRE(ctx->noalloc_partial != nullptr, INQB_ERR_STATE, "context was not prepared for this entry point");
+    check_output_buffer(*ctx, out_dev);
+    double2 *partial = static_cast<double2 *>(ctx->noalloc_partial);
     const int S = a->nst;
     const long long np = a->basis->npoints;
     const double dv = set_volume_element(*a);
@@ -98,8 +120,7 @@ extern "C" int inqb_overlap_diagonal_noalloc(const inqb_orbitals *a, const inqb_
       noalloc_partial_kernel<float><<<NOALLOC_BLOCKS, 256, 0, ctx->stream>>>(
           static_cast<const float2 *>(a->data), static_cast<const float2 *>(b->data), S, np, partial);
     INQB_CUDA(cudaGetLastError());
-    noalloc_sum_kernel<<<(S + 255) / 256, 256, 0, ctx->stream>>>(partial, NOALLOC_BLOCKS, S, dv,
-                                                                 reinterpret_cast<double2 *>(out_dev));
+    noalloc_sum_kernel<<<(S + 255) / 256, 256, 0, ctx->stream>>>(partial, NOALLOC_BLOCKS, S, dv, out_dev);
     INQB_CUDA(cudaGetLastError());
     ctx->launches += 2;
     return INQB_OK;

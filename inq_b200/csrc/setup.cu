@@ -492,12 +492,12 @@ void build_projectors_device(Hamiltonian &h, int natoms, const double *positions
   std::vector<float> coeff32(coeff.size());
   for (size_t i = 0; i < coeff.size(); i++) coeff32[i] = float(coeff[i]);
   const size_t slots = std::max<size_t>(1, size_t(nproj) * maxsph);
-  INQB_CUDA(cudaMallocAsync(&P.d_pt, sizeof(int) * slots, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_pos, sizeof(float) * 3 * slots, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_mat, sizeof(double) * 4 * slots, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_coeff, sizeof(double) * 16 * nproj, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_coeff32, sizeof(float) * 16 * nproj, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_npts, sizeof(int) * nproj, st));
+  INQB_CUDA(counted_malloc_async(&P.d_pt, sizeof(int) * slots, st));
+  INQB_CUDA(counted_malloc_async(&P.d_pos, sizeof(float) * 3 * slots, st));
+  INQB_CUDA(counted_malloc_async(&P.d_mat, sizeof(double) * 4 * slots, st));
+  INQB_CUDA(counted_malloc_async(&P.d_coeff, sizeof(double) * 16 * nproj, st));
+  INQB_CUDA(counted_malloc_async(&P.d_coeff32, sizeof(float) * 16 * nproj, st));
+  INQB_CUDA(counted_malloc_async(&P.d_npts, sizeof(int) * nproj, st));
   INQB_CUDA(cudaMemsetAsync(P.d_pt, 0xff, sizeof(int) * slots, st));  // -1 padding
   INQB_CUDA(cudaMemsetAsync(P.d_pos, 0, sizeof(float) * 3 * slots, st));
   INQB_CUDA(cudaMemsetAsync(P.d_mat, 0, sizeof(double) * 4 * slots, st));
@@ -547,9 +547,9 @@ void build_projectors_device(Hamiltonian &h, int natoms, const double *positions
   int *d_cnt = static_cast<int *>(dev_alloc(ctx, sizeof(int) * np));
   int *d_nonempty = static_cast<int *>(dev_alloc(ctx, sizeof(int) * np));
   int *d_slot = static_cast<int *>(dev_alloc(ctx, sizeof(int) * (np + 1)));
-  INQB_CUDA(cudaMallocAsync(&P.d_offs, sizeof(int) * (np + 1), st));
-  INQB_CUDA(cudaMallocAsync(&P.d_hit, sizeof(int) * std::max<long long>(1, total), st));
-  INQB_CUDA(cudaMallocAsync(&P.d_hitp, sizeof(int) * std::max<long long>(1, total), st));
+  INQB_CUDA(counted_malloc_async(&P.d_offs, sizeof(int) * (np + 1), st));
+  INQB_CUDA(counted_malloc_async(&P.d_hit, sizeof(int) * std::max<long long>(1, total), st));
+  INQB_CUDA(counted_malloc_async(&P.d_hitp, sizeof(int) * std::max<long long>(1, total), st));
   INQB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int) * np, st));
   const long long nslots = (long long)nproj * maxsph;
   hit_count_kernel<<<blocks_for(nslots, 256), 256, 0, st>>>(nproj, maxsph, P.d_npts, P.d_pt, d_cnt);
@@ -565,16 +565,16 @@ void build_projectors_device(Hamiltonian &h, int natoms, const double *positions
   INQB_CUDA(cudaMemcpyAsync(&nhit, d_slot + np, sizeof(int), cudaMemcpyDeviceToHost, st));
   INQB_CUDA(cudaStreamSynchronize(st));
   P.nhitpts = nhit;
-  INQB_CUDA(cudaMallocAsync(&P.d_hitpts, sizeof(int) * std::max(1, nhit), st));
-  INQB_CUDA(cudaMallocAsync(&P.d_hrec, sizeof(int4) * std::max(1, nhit), st));
+  INQB_CUDA(counted_malloc_async(&P.d_hitpts, sizeof(int) * std::max(1, nhit), st));
+  INQB_CUDA(counted_malloc_async(&P.d_hrec, sizeof(int4) * std::max(1, nhit), st));
   hit_records_kernel<<<blocks_for(np, 256), 256, 0, st>>>(np, P.d_offs, P.d_hitp, d_nonempty, d_slot, P.d_hitpts,
                                                           P.d_hrec);
   INQB_CUDA(cudaGetLastError());
   ctx.launches += 4;
-  INQB_CUDA(cudaMallocAsync(&P.d_gcoef, sizeof(double2) * slots * 4, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_gcoef32, sizeof(float2) * slots * 4, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_hcoef, sizeof(double2) * std::max<long long>(1, total) * 4, st));
-  INQB_CUDA(cudaMallocAsync(&P.d_hcoef32, sizeof(float2) * std::max<long long>(1, total) * 4, st));
+  INQB_CUDA(counted_malloc_async(&P.d_gcoef, sizeof(double2) * slots * 4, st));
+  INQB_CUDA(counted_malloc_async(&P.d_gcoef32, sizeof(float2) * slots * 4, st));
+  INQB_CUDA(counted_malloc_async(&P.d_hcoef, sizeof(double2) * std::max<long long>(1, total) * 4, st));
+  INQB_CUDA(counted_malloc_async(&P.d_hcoef32, sizeof(float2) * std::max<long long>(1, total) * 4, st));
   for (void *p : {static_cast<void *>(d_jobs), static_cast<void *>(d_aoff), static_cast<void *>(d_flag),
                   static_cast<void *>(d_rank), static_cast<void *>(d_count), static_cast<void *>(d_cnt),
                   static_cast<void *>(d_nonempty), static_cast<void *>(d_slot), static_cast<void *>(d_first)})

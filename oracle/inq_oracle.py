@@ -582,6 +582,7 @@ def overlap(rs, phi1, phi2=None):
 
 
 def overlap_diagonal(rs, phi1, phi2=None):
+    """d[i] = dV sum_r conj(phi1[r,i]) phi2[r,i] (overlap_diagonal.hpp:25-55)."""
     if phi2 is None:
         phi2 = phi1
     return rs.volume_element() * np.sum(np.conj(phi1) * phi2, axis=(0, 1, 2))

@@ -1,6 +1,8 @@
 // The reference's ks_hamiltonian unit test (ks_hamiltonian.hpp:297-445) written against the C++
-// facade of libinqb200: 10 bohr cube, 20^3 grid, no atoms.  Prints the three checks and returns
-// non-zero when one fails.
+// facade of libinqb200: 10 bohr cube, 20^3 grid, no atoms.  Prints the checks (and that wrapped
+// caller-owned device buffers give the same H|psi>) and returns non-zero when one fails.
+#include <cuda_runtime.h>
+
 #include <cmath>
 #include <cstdio>
 
@@ -74,5 +76,29 @@ int main() {
   diff /= double(hf.size());
   std::printf("harmonic oscillator, fourier form: %.10f\n", diff);
   fail |= !(std::abs(diff - 0.0051420503) < 1.2e-5 * 0.0051420503);
+
+  // zero-copy boundary: the same operator on caller-owned device buffers wrapped as orbital sets
+  // gives bitwise the result of the owned sets
+  const size_t bytes = size_t(np) * nst * sizeof(std::complex<double>);
+  void *din = nullptr, *dout = nullptr;
+  if (cudaMalloc(&din, bytes) != cudaSuccess || cudaMalloc(&dout, bytes) != cudaSuccess) {
+    std::printf("cudaMalloc failed\n");
+    return 1;
+  }
+  cudaMemcpy(din, m.data(), bytes, cudaMemcpyHostToDevice);
+  {
+    auto win = states::orbital_set::wrap(rs, din, nst);
+    auto wout = states::orbital_set::wrap(rs, dout, nst);
+    ham.apply(win, wout);
+    ctx.synchronize();
+  }
+  std::vector<std::complex<double>> hw(size_t(np) * nst);
+  cudaMemcpy(hw.data(), dout, bytes, cudaMemcpyDeviceToHost);
+  size_t ndiff = 0;
+  for (size_t e = 0; e < hw.size(); e++) ndiff += (hw[e] != h[e]);
+  std::printf("wrapped device buffers: %zu values differ from the owned sets\n", ndiff);
+  fail |= ndiff != 0;
+  cudaFree(din);
+  cudaFree(dout);
   return fail;
 }

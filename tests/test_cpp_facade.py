@@ -12,8 +12,10 @@ LIBDIR = os.path.join(ROOT, "inq_b200")
 
 def _compile(out):
     src = os.path.join(ROOT, "tests", "cpp", "ks_hamiltonian_kat.cpp")
-    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), src, "-o", out, "-L", LIBDIR, "-linqb200",
-           f"-Wl,-rpath,{LIBDIR}"]
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"), src,
+           "-o", out, "-L", LIBDIR, "-linqb200", f"-Wl,-rpath,{LIBDIR}", "-L", os.path.join(cuda, "lib64"), "-lcudart",
+           f"-Wl,-rpath,{os.path.join(cuda, 'lib64')}"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     return out
@@ -32,3 +34,4 @@ def test_facade_known_answers(tmp_path):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "harmonic oscillator: 0.00514" in r.stdout
+    assert "wrapped device buffers: 0 values differ" in r.stdout
