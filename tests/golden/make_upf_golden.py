@@ -6,7 +6,8 @@ The CPU tests build the KB coefficients from these values and compare them with 
 reference's projector test asserts (projector.hpp:160-240), so the pin holds where the reference tree
 is absent; with INQ_REFERENCE_DATA pointing at the data directory they also re-parse the files.
 
-Run from the repository root:  python tests/golden/make_upf_golden.py [data_dir]
+Run from the repository root:  python tests/golden/make_upf_golden.py <data_dir>
+(data_dir: the reference's share/unit_tests_data; INQ_REFERENCE_DATA is used when no argument is given)
 """
 
 import json
@@ -18,14 +19,17 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from inq_b200 import pseudo  # noqa: E402
 
-DATA = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/share/unit_tests_data"
 FILES = ["N.upf", "N_non_diagonal.upf.gz", "F.UPF"]
 
 
 def main():
+    data = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("INQ_REFERENCE_DATA")
+    if not data:
+        sys.exit("usage: make_upf_golden.py <reference share/unit_tests_data directory> "
+                 "(or set INQ_REFERENCE_DATA)")
     out = {}
     for name in FILES:
-        ps = pseudo.read_upf(os.path.join(DATA, name))
+        ps = pseudo.read_upf(os.path.join(data, name))
         out[name] = {"element": ps.element, "z_valence": ps.z_valence, "beta_l": list(ps.beta_l),
                      "dij": ps.dij.tolist(), "projector_radius": ps.projector_radius(), "mesh_size": int(len(ps.r))}
     with open(os.path.join(HERE, "upf_reference_pins.json"), "w") as f:
