@@ -557,7 +557,7 @@ def run_ours(args):
     peak, peak_kind = measured_hbm_gbs()
     achieved = alg_bytes / (pass_ms[0] / 1000.0) / 1e9
     achieved_d = alg_bytes / (pass_ms[1] / 1000.0) / 1e9
-    traffic = profile_traffic("fft2_kernel_f32f32_c2")
+    traffic = profile_traffic("fft2_kernel_f32f32w_c2")
     # whole-operator algorithmic bytes s_c (5N + 3P) per state
     _, _, P = ham.projectors_info()
     b_alg = 8.0 * (5 * N + 3 * P) * S
@@ -619,8 +619,9 @@ def run_ours(args):
                                      "ms_per_step": mode_ms[m] / args.steps, "rel_err_hpsi_vs_fp64": acc[m][0],
                                      "max_eigenvalue_err_ha": acc[m][1]} for m in (0, 1, 2, 3)},
             "roofline": {"bound": "hbm",
-                         "kernel": "fft2_kernel<float,float,96,FWD_STORE>: one batched 1-D FFT pass over the set "
-                                   "(FP32 data and butterflies, the forward passes of the headline step)",
+                         "kernel": "fft2_kernel<float,float,96,FWD_STORE,1>: one batched 1-D FFT pass over the set "
+                                   "(FP32 data and butterflies, 512-byte rows; the forward passes of the headline "
+                                   "step)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes, "launch_ms": pass_ms[0],

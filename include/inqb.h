@@ -73,7 +73,9 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * block scheduler starts this context's pending blocks first); "nl_bulk" = 0 (default: the
  * nonlocal apply, and the projection when it has at least two CTAs per SM, move whole rows of
  * states through shared memory with bulk asynchronous copies), 1 (those forms wherever a row is a
- * multiple of 16 bytes) or -1 (never: register-held gathers).  Changing the priority replaces
+ * multiple of 16 bytes) or -1 (never: register-held gathers); "fft_wide" = 1 (default: the plain streaming
+ * FFT passes of single-precision sets of at least 64 states move 512-byte rows, 64 states, in three
+ * stages at one CTA per SM) or 0 (256-byte rows, 32 states, as the other passes).  Changing the priority replaces
  * the context's stream (after the work queued on it), so callers query inqb_ctx_stream again. */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Self-test of the bounded device-side waits: queues one kernel whose wait on an mbarrier phase that

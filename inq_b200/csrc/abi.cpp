@@ -876,6 +876,9 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     } else if (k == "nl_bulk") {
       INQB_REQUIRE(value >= -1 && value <= 1, INQB_ERR_ARG, "nl_bulk is 0 (automatic), 1 (always) or -1 (never)");
       ctx->nl_bulk = int(value);
+    } else if (k == "fft_wide") {
+      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_wide is 0 (256-byte rows) or 1 (512-byte rows)");
+      ctx->fft_wide = int(value);
     } else if (k == "grid_sms") {
       INQB_REQUIRE(value >= 0 && value <= ctx->device_sms, INQB_ERR_ARG,
                    "grid_sms is 0 (every SM) or 1.." + std::to_string(ctx->device_sms));

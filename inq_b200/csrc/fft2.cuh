@@ -701,8 +701,8 @@ template <int VAR> constexpr int dir_first() { return (base_var(VAR) == INV_STOR
 // Tiles of 256-byte rows, or 128-byte rows when the butterflies run in a wider type than the storage
 // (the tile then also needs an exchange buffer of that type, and smaller tiles let several CTAs share
 // an SM to cover the double-precision latency).
-template <typename R, typename CR> constexpr int tile_w() {
-  return (sizeof(CR) > sizeof(R) ? 128 : 256) / int(2 * sizeof(R));
+template <typename R, typename CR, int WIDE = 0> constexpr int tile_w() {
+  return WIDE ? 512 / int(2 * sizeof(R)) : (sizeof(CR) > sizeof(R) ? 128 : 256) / int(2 * sizeof(R));
 }
 // Threads per CTA.  The two steps of a tile transform have W*N2 and W*N1 independent line pieces; with
 // 128 threads and 16-state tiles (N1 = 8) the first step of N = 72, 96, 120, 128 takes two rounds in
@@ -712,10 +712,11 @@ template <typename R, typename CR> constexpr int tile_w() {
 // lines (two tiles per stage: two stages, and 8 warps per SM at 128 threads for 96 points, 4 for
 // 120) run one thread per column item: 384 threads for 96 points (measured: 1.06 ms against 1.15 ms
 // at 96^3 x 256), 480 for 120.
-template <typename R, typename CR, int N, int VAR> constexpr int threads_of() {
-  constexpr int W = tile_w<R, CR>();
+template <typename R, typename CR, int N, int VAR, int WIDE = 0> constexpr int threads_of() {
+  constexpr int W = tile_w<R, CR, WIDE>();
   constexpr int A = W * Split<N>::N2, B = W * Split<N>::N1;
   constexpr int M = A > B ? A : B;
+  if constexpr (WIDE) return 256;
   if constexpr (base_var(VAR) == INV_FINAL && W == 32 && N >= 96 && sizeof(CR) == 4) return (A + 31) / 32 * 32;
   return (VAR != MID_KIN && W == 16 && M > 128 && M <= 256) ? (M + 31) / 32 * 32 : 128;
 }
@@ -727,29 +728,30 @@ template <typename R, typename CR, int N, int VAR> constexpr int threads_of() {
 template <typename R, typename CR, int N, int VAR> constexpr bool ws_of() {
   return sizeof(R) == 4 && sizeof(CR) == 4;
 }
-template <typename R, typename CR, int N, int VAR> constexpr int block_threads_of() {
-  return threads_of<R, CR, N, VAR>() + (ws_of<R, CR, N, VAR>() ? 32 : 0);
+template <typename R, typename CR, int N, int VAR, int WIDE = 0> constexpr int block_threads_of() {
+  return threads_of<R, CR, N, VAR, WIDE>() + (ws_of<R, CR, N, VAR>() ? 32 : 0);
 }
 
 // CTAs per SM the register allocation must allow: four for the single-precision kinetic pass of lines
 // up to 96 points (two transforms per tile, latency-bound with fewer warps; longer lines would spill);
 // 0 (no constraint: the compiler's own register choice) otherwise.
-template <typename R, typename CR, int N, int VAR> constexpr int min_ctas_of() {
+template <typename R, typename CR, int N, int VAR, int WIDE = 0> constexpr int min_ctas_of() {
+  if constexpr (WIDE) return 0;
   return (VAR == MID_KIN && sizeof(R) == 4 && sizeof(CR) == 4 && N <= 96) ? 4 : 0;
 }
 
-template <typename R, typename CR, int N, int VAR>
-__global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR>(), min_ctas_of<R, CR, N, VAR>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
+template <typename R, typename CR, int N, int VAR, int WIDE>
+__global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_ctas_of<R, CR, N, VAR, WIDE>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
                                                    const __grid_constant__ CUtensorMap map_out,
                                                    const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
                                                    const C2<CR> *__restrict__ twg, int *err) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr int NT = threads_of<R, CR, N, VAR>();   // compute threads
-  constexpr bool WS = ws_of<R, CR, N, VAR>();       // plus a producer warp
-  constexpr int NTT = block_threads_of<R, CR, N, VAR>();
-  constexpr bool SPLIT = sizeof(CR) > sizeof(R);    // exchange buffer in the arithmetic type
-  constexpr int W = tile_w<R, CR>();
+  constexpr int NT = threads_of<R, CR, N, VAR, WIDE>();   // compute threads
+  constexpr bool WS = ws_of<R, CR, N, VAR>();             // plus a producer warp
+  constexpr int NTT = block_threads_of<R, CR, N, VAR, WIDE>();
+  constexpr bool SPLIT = sizeof(CR) > sizeof(R);          // exchange buffer in the arithmetic type
+  constexpr int W = tile_w<R, CR, WIDE>();
   constexpr int TILE = N * W;                       // complex elements per tile
   constexpr uint32_t TILE_BYTES = TILE * sizeof(T);
   constexpr bool AUX = has_aux(VAR);
@@ -1016,21 +1018,23 @@ inline CUtensorMap orbital_map(const void *base, const Basis &b, int S, int cwor
   return m;
 }
 
-template <typename R, typename CR, int N, int VAR>
+template <typename R, typename CR, int N, int VAR, int WIDE = 0>
 void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   using T = C2<R>;
   using TC = C2<CR>;
-  constexpr int W = tile_w<R, CR>();
+  constexpr int W = tile_w<R, CR, WIDE>();
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
   const int nbuf = has_aux(VAR) ? 2 : 1;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
-  constexpr int NT = block_threads_of<R, CR, N, VAR>();
+  constexpr int NT = block_threads_of<R, CR, N, VAR, WIDE>();
   const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + size_t(tw_entries<CR>(N) + N) * sizeof(TC) + 64 + 16 * 8;
   // shared memory per CTA: ~113 KB (two CTAs per SM) for the FP64 streaming passes; ~56 KB (four per SM)
   // for the wide-arithmetic, the kinetic and the producer-warp (single-precision) passes, whose
   // arithmetic needs more warps to hide latency (96^3 x 256 single: 3.81 ms per H against 3.89 with
   // four stages of 113 KB)
-  const size_t budget = (SPLIT || VAR == MID_KIN || ws_of<R, CR, N, VAR>()) ? 56 * 1024 : 113 * 1024;
+  size_t budget = (SPLIT || VAR == MID_KIN || ws_of<R, CR, N, VAR>()) ? 56 * 1024 : 113 * 1024;
+  // 512-byte-row streaming passes: three stages, one CTA per SM
+  if (WIDE) budget = 150 * 1024;
   int ns = int((budget - fixed) / (TILE_BYTES * nbuf));
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;
@@ -1039,7 +1043,7 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   gg.ntiles = (b.npoints / b.n[gg.axis]) * gg.nsb;
   const size_t smem = TILE_BYTES * nbuf * ns + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
-  auto kern = fft2_kernel<R, CR, N, VAR>;
+  auto kern = fft2_kernel<R, CR, N, VAR, WIDE>;
   // per instantiation: shared-memory attribute and occupancy, computed under a lock (several host
   // threads may drive contexts at once); the attribute only ever grows
   static std::mutex mtx;
@@ -1066,8 +1070,27 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   ctx.launches++;
 }
 
+// The plain streaming passes of single-precision sets of at least 64 states run with 512-byte rows
+// (64 states) in three stages, one CTA per SM (context option fft_wide, default 1).  Measured at
+// 96^3 x 256: 0.571 ms per pass against 0.633 ms with 256-byte rows at four CTAs per SM (6.35 against
+// 5.72 TB/s).  The same shape made the kinetic pass slower, and double-precision passes (32 states,
+// one CTA of 256 threads per SM) much slower (1.66 against 1.15 ms), so those keep 256-byte rows.
+inline bool wide_var(int var) { return var == FWD_STORE || var == INV_STORE || var == FWD_PERM || var == INV_PERM; }
+
 template <typename R, typename CR, int N>
-void launch_nc(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var) {
+void launch_nc(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var, bool wide = false) {
+  if constexpr (sizeof(R) == 4 && sizeof(CR) == 4) {
+    // 512-byte rows (64 single-precision states) for the plain streaming passes
+    if (wide) {
+      switch (var) {
+        case FWD_STORE: launch_kernel<R, CR, N, FWD_STORE, 1>(ctx, b, a, gg); return;
+        case INV_STORE: launch_kernel<R, CR, N, INV_STORE, 1>(ctx, b, a, gg); return;
+        case FWD_PERM: launch_kernel<R, CR, N, FWD_PERM, 1>(ctx, b, a, gg); return;
+        case INV_PERM: launch_kernel<R, CR, N, INV_PERM, 1>(ctx, b, a, gg); return;
+        default: break;
+      }
+    }
+  }
   switch (var) {
     case FWD_STORE: launch_kernel<R, CR, N, FWD_STORE>(ctx, b, a, gg); break;
     case INV_STORE: launch_kernel<R, CR, N, INV_STORE>(ctx, b, a, gg); break;
@@ -1102,7 +1125,8 @@ void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var)
     const bool single = mode == 0 || (mode >= 2 && bv == INV_FINAL) ||
                         (mode == 3 && a.axis == 2 && (bv == FWD_STORE || var == FWD_VPSI));
     if (single) {
-      launch_nc<R, float, N>(ctx, b, a, gg, var);
+      const bool wide = ctx.fft_wide && a.S >= 64 && wide_var(var);
+      launch_nc<R, float, N>(ctx, b, a, gg, var, wide);
       return;
     }
   }

@@ -75,6 +75,7 @@ struct Ctx {
   int mixed_compute = 0;     // butterfly arithmetic of single-precision orbitals (see inqb_ctx_set_option)
   int overlap_tc = 1;        // overlaps of single-precision sets on the tensor cores (split BF16)
   int nl_bulk = 0;           // nonlocal kernels: 0 automatic, 1 bulk-copy forms wherever they apply, -1 never
+  int fft_wide = 1;          // single-precision FFT passes without a second input: 512-byte rows (64 states)
   int stream_priority = 0;   // 0: the device's lowest stream priority, 1: its highest
   void *noalloc_partial = nullptr;  // device address of noalloc.cu's fixed partial-sum array on this device
 };

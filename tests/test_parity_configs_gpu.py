@@ -2,11 +2,12 @@
 
 The operator does not couple states, so a slice of a configuration's states is an exact check of
 the kernels the benchmark runs on it.  The slices keep every pass of H on the kernels the full
-configuration uses: 32 states give 512-byte (FP64) and 256-byte (FP32) rows, so the TMA FFT
-passes (96- and 120-point codelets, digit-reversed z order) and the bulk-copy nonlocal kernels run.
+configuration uses: 64 states give 1024-byte (FP64) and 512-byte (FP32) rows, so the TMA FFT
+passes (96- and 120-point codelets, digit-reversed z order, 512-byte-row streaming passes of the
+mixed form) and the bulk-copy nonlocal kernels run.
 
-* 96^3 grid, a = 20.52 bohr, 64 jittered atoms (2x2x2 diamond supercell), 32 states;
-* 120^3 grid, a = 25.6 bohr, 128 jittered atoms, 32 states (16 for the ETRS step).
+* 96^3 grid, a = 20.52 bohr, 64 jittered atoms (2x2x2 diamond supercell), 64 states;
+* 120^3 grid, a = 25.6 bohr, 128 jittered atoms, 64 states (16 for the ETRS step).
 
 Tolerances: plain FP64 form <= 1e-12 relative in H|psi> (ks_hamiltonian.hpp:137-156); mixed form
 <= 1e-6 relative in H|psi> and eigenvalues within 1e-6 Ha (energy.hpp:83-89) of the oracle; one
@@ -51,14 +52,14 @@ def _system(name, nst):
 
 @pytest.fixture(scope="module")
 def c2():
-    s = _system("c2", 32)
+    s = _system("c2", 64)
     yield s
     O.set_fft_workers(None)
 
 
 @pytest.fixture(scope="module")
 def c3():
-    s = _system("c3", 32)
+    s = _system("c3", 64)
     yield s
     O.set_fft_workers(None)
 
@@ -100,10 +101,14 @@ def test_c2_fp64_parity(c2, nl_bulk):
     _check_fp64(ib, c2, nl_bulk)
 
 
-@pytest.mark.parametrize("nl_bulk", [0, 1])
-def test_c2_mixed_parity(c2, nl_bulk):
+@pytest.mark.parametrize("nl_bulk,fft_wide", [(0, 1), (1, 1), (0, 0)])
+def test_c2_mixed_parity(c2, nl_bulk, fft_wide):
     import inq_b200 as ib
-    _check_mixed(ib, c2, nl_bulk)
+    c2["basis"].ctx.set_option("fft_wide", fft_wide)
+    try:
+        _check_mixed(ib, c2, nl_bulk)
+    finally:
+        c2["basis"].ctx.set_option("fft_wide", 1)
 
 
 def test_c2_fp64_eigenvalues(c2):
