@@ -113,13 +113,14 @@ void ensure_tables(Hamiltonian &h, const double kA[3]) {
   launch_nl_tables(*h.ctx, *h.basis, h, kA);
 }
 
-struct Accum {
-  void *acc1 = nullptr, *acc2 = nullptr;
-  double c1[2] = {0, 0}, c2[2] = {0, 0};
+// A Horner step of a Taylor exponential fused into the operator: out = base + c (H in) instead of H in.
+struct Horner {
+  const void *base = nullptr;
+  std::complex<double> c = 0.0;
 };
 
 template <typename R>
-void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &acc) {
+void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Horner &hz) {
   Ctx &ctx = *h.ctx;
   const Basis &b = *h.basis;
   const int S = in.nst;
@@ -187,15 +188,13 @@ void apply_real(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &
   a.nspin = h.nspin;
   a.spin = in.spin_index;
   a.vshift = R(0.5 * norm_cov(b, kA));
-  a.acc1 = static_cast<C2<R> *>(acc.acc1);
-  a.acc2 = static_cast<C2<R> *>(acc.acc2);
-  a.c1 = mk<C2<R>>(R(acc.c1[0]), R(acc.c1[1]));
-  a.c2 = mk<C2<R>>(R(acc.c2[0]), R(acc.c2[1]));
+  a.hbase = static_cast<const C2<R> *>(hz.base);
+  a.hc = mk<C2<R>>(R(hz.c.real()), R(hz.c.imag()));
   launch_fft_pass<R>(ctx, b, a, PRO_NONE, EPI_FINAL_REAL);
-  // nonlocal term added at the sphere points (and to the Taylor accumulators) by its own kernel: as a
-  // fully occupied kernel of its own it hides the latency of the hit-table and projection reads, which
-  // stall the FFT epilogue
-  if (h.proj.nproj > 0) launch_nl_apply<R>(ctx, h, projD, S, hpsi, a.acc1, a.c1, a.acc2, a.c2);
+  // nonlocal term (times the Horner coefficient in a Horner step) added at the sphere points by its own
+  // kernel: as a fully occupied kernel of its own it hides the latency of the hit-table and projection
+  // reads, which stall the FFT epilogue
+  if (h.proj.nproj > 0) launch_nl_apply<R>(ctx, h, projD, S, hpsi, hz.base != nullptr, a.hc);
 }
 
 template <typename R> void apply_fourier(Hamiltonian &h, const Orbitals &in, Orbitals &out) {
@@ -251,17 +250,18 @@ template <typename R> void apply_fourier(Hamiltonian &h, const Orbitals &in, Orb
   launch_fft_pass<R>(ctx, b, c, PRO_NONE, EPI_LAPL_ADD);
 }
 
-void apply_any(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Accum &acc = Accum()) {
+void apply_any(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Horner &hz = Horner()) {
   check_same_shape(in, out);
   INQB_REQUIRE(in.basis == h.basis, INQB_ERR_ARG, "orbitals and Hamiltonian live on different bases");
   INQB_REQUIRE(in.data != out.data, INQB_ERR_ARG, "H|psi> needs distinct input and output sets");
   INQB_REQUIRE(in.spin_index >= 0 && in.spin_index < h.nspin, INQB_ERR_ARG, "spin index out of range");
   if (in.space == INQB_REAL_SPACE) {
-    if (in.precision == INQB_F64) apply_real<double>(h, in, out, acc);
-    else apply_real<float>(h, in, out, acc);
+    INQB_REQUIRE(hz.base == nullptr || hz.base != out.data, INQB_ERR_ARG,
+                 "the base of a Horner step must be distinct from the operator's output");
+    if (in.precision == INQB_F64) apply_real<double>(h, in, out, hz);
+    else apply_real<float>(h, in, out, hz);
   } else {
-    INQB_REQUIRE(acc.acc1 == nullptr && acc.acc2 == nullptr, INQB_ERR_UNSUPPORTED,
-                 "Taylor accumulation is implemented for real-space sets");
+    INQB_REQUIRE(hz.base == nullptr, INQB_ERR_UNSUPPORTED, "Taylor exponentials are implemented for real-space sets");
     if (in.precision == INQB_F64) apply_fourier<double>(h, in, out);
     else apply_fourier<float>(h, in, out);
   }
@@ -288,33 +288,77 @@ void copy_set(const Orbitals &src, Orbitals &dst) {
   dst.space = src.space;
 }
 
-// exponential_2_for_1 / exponential_in_place (exponential.hpp:21-69) with every shift fused into the
-// epilogue of the H application that produces the term.
-void exponential(Hamiltonian &h, std::complex<double> f1, std::complex<double> f2, Orbitals &phi, Orbitals *exp1,
-                 int order) {
+// out = exp(f H) base to the given Taylor order (exponential.hpp:21-34), in Horner form: w_1 = base +
+// (f / order) H base, w_k = base + (f / (order - k + 1)) H w_{k-1}, out = w_order -- the same polynomial
+// in H as the reference's sum of f^n H^n base / n!, with each step fused into the epilogues of its H
+// application (the final FFT pass reads the base as a third tile, the nonlocal apply scales its term).
+// base must differ from out; one scratch set.
+void exponential_from(Hamiltonian &h, std::complex<double> f, const Orbitals &base, Orbitals &out, int order) {
   INQB_REQUIRE(order >= 1, INQB_ERR_ARG, "order must be >= 1");
-  INQB_REQUIRE(phi.space == INQB_REAL_SPACE, INQB_ERR_UNSUPPORTED, "exponential is implemented for real-space sets");
-  if (exp1) copy_set(phi, *exp1);
-  TempSet ta(phi), tb(phi);
-  std::complex<double> c1 = 1.0, c2 = 1.0;
-  const Orbitals *src = &phi;
-  Orbitals *bufs[2] = {&ta.o, &tb.o};
-  for (int it = 1; it <= order; it++) {
-    c1 *= f1 / double(it);
-    c2 *= f2 / double(it);
-    Accum acc;
-    if (exp1) {
-      acc.acc1 = exp1->data;
-      acc.c1[0] = c1.real();
-      acc.c1[1] = c1.imag();
-    }
-    acc.acc2 = phi.data;
-    acc.c2[0] = c2.real();
-    acc.c2[1] = c2.imag();
-    Orbitals *dst = bufs[(it - 1) % 2];
-    apply_any(h, *src, *dst, acc);
+  INQB_REQUIRE(base.space == INQB_REAL_SPACE, INQB_ERR_UNSUPPORTED, "exponential is implemented for real-space sets");
+  INQB_REQUIRE(base.data != out.data, INQB_ERR_ARG, "exponential_from needs distinct base and output sets");
+  check_same_shape(base, out);
+  std::unique_ptr<TempSet> t;
+  if (order > 1) t.reset(new TempSet(base));
+  const Orbitals *src = &base;
+  for (int k = 1; k <= order; k++) {
+    Orbitals *dst = ((order - k) % 2 == 0) ? &out : &t->o;  // the last step writes out
+    Horner hz;
+    hz.base = base.data;
+    hz.c = f / double(order - k + 1);
+    apply_any(h, *src, *dst, hz);
     src = dst;
   }
+  out.space = base.space;
+  for (int i = 0; i < 3; i++) out.kpoint[i] = base.kpoint[i];
+  out.spin_index = base.spin_index;
+}
+
+// exponential_in_place (exponential.hpp:21-34): phi <- exp(f H) phi
+void exponential_in_place(Hamiltonian &h, std::complex<double> f, Orbitals &phi, int order) {
+  TempSet base(phi);
+  copy_set(phi, base.o);
+  exponential_from(h, f, base.o, phi, order);
+}
+
+// exponential_2_for_1 (exponential.hpp:50-69): exp1 <- exp(f1 H) phi, phi <- exp(f2 H) phi from one set of
+// H^n phi.  The terms u_n = H^n phi are kept, and one element-wise pass forms both sums, adding the terms
+// in the reference's order; with the sums in the H epilogues instead, every term would cost two more
+// reads and writes of a set per accumulator.  Holds `order` scratch sets.
+void exponential_2_for_1(Hamiltonian &h, std::complex<double> f1, std::complex<double> f2, Orbitals &phi,
+                         Orbitals &exp1, int order) {
+  INQB_REQUIRE(order >= 1 && order <= 8, INQB_ERR_ARG, "order must be 1..8");
+  INQB_REQUIRE(phi.space == INQB_REAL_SPACE, INQB_ERR_UNSUPPORTED, "exponential is implemented for real-space sets");
+  check_same_shape(phi, exp1);
+  std::vector<std::unique_ptr<TempSet>> u;
+  const Orbitals *src = &phi;
+  double2 c1[8], c2[8];
+  std::complex<double> k1 = 1.0, k2 = 1.0;
+  for (int n = 1; n <= order; n++) {
+    u.emplace_back(new TempSet(phi));
+    apply_any(h, *src, u.back()->o);
+    src = &u.back()->o;
+    k1 *= f1 / double(n);
+    k2 *= f2 / double(n);
+    c1[n - 1] = make_double2(k1.real(), k1.imag());
+    c2[n - 1] = make_double2(k2.real(), k2.imag());
+  }
+  Ctx &ctx = *phi.ctx;
+  const long long n = phi.basis->npoints * phi.nst;
+  if (phi.precision == INQB_F64) {
+    const double2 *up[8];
+    for (int k = 0; k < order; k++) up[k] = static_cast<const double2 *>(u[k]->o.data);
+    launch_taylor_combine<double>(ctx, static_cast<const double2 *>(phi.data), up, order, c1, c2,
+                                  static_cast<double2 *>(exp1.data), static_cast<double2 *>(phi.data), n);
+  } else {
+    const float2 *up[8];
+    for (int k = 0; k < order; k++) up[k] = static_cast<const float2 *>(u[k]->o.data);
+    launch_taylor_combine<float>(ctx, static_cast<const float2 *>(phi.data), up, order, c1, c2,
+                                 static_cast<float2 *>(exp1.data), static_cast<float2 *>(phi.data), n);
+  }
+  exp1.space = phi.space;
+  for (int i = 0; i < 3; i++) exp1.kpoint[i] = phi.kpoint[i];
+  exp1.spin_index = phi.spin_index;
 }
 
 template <typename R> double *occ_to_device(Ctx &ctx, const double *occ, int S) {
@@ -1542,7 +1586,24 @@ int inqb_apply_host(const inqb_hamiltonian *hc, int nst, const double kpoint_cov
     const size_t npts = size_t(h->basis->npoints);
     int B = block_states > 0 ? block_states : int(512 / cs);  // 512-byte rows of a block by default
     if (B > nst) B = nst;
-    const int nblocks = (nst + B - 1) / B;
+    // block boundaries: with the default size, the first and the last block hold half a block (256-byte
+    // rows), which shortens the upload before the first operator and the download after the last one;
+    // in between both copy directions run at once (96^3 x 256 single: 48 GB/s each way with rows of 512
+    // bytes or more, 44 GB/s with 256-byte rows, 56 GB/s for one direction alone)
+    std::vector<int> starts;
+    {
+      int s0 = 0;
+      const bool halves = block_states == 0 && nst >= 2 * B && B % 2 == 0;
+      if (halves) starts.push_back(0), s0 = B / 2;
+      const int tail = halves ? B / 2 : 0;
+      while (s0 < nst - tail) starts.push_back(s0), s0 += B;
+      if (halves) {
+        if (s0 > nst - tail) s0 = nst - tail;  // the last full-size block may be shorter
+        starts.push_back(s0);
+      }
+      starts.push_back(nst);
+    }
+    const int nblocks = int(starts.size()) - 1;
     HostApplyRes r;
     r.ctx = &ctx;
     INQB_CUDA(cudaStreamCreateWithFlags(&r.up, cudaStreamNonBlocking));
@@ -1567,7 +1628,7 @@ int inqb_apply_host(const inqb_hamiltonian *hc, int nst, const double kpoint_cov
     const char *hin = static_cast<const char *>(host_in);
     char *hout = static_cast<char *>(host_out);
     for (int i = 0; i < nblocks; i++) {
-      const int slot = i & 1, s0 = i * B, nb = std::min(B, nst - s0);
+      const int slot = i & 1, s0 = starts[i], nb = starts[i + 1] - starts[i];
       // block i reuses the buffers of block i - 2: its upload waits for that block's operator, its
       // operator for that block's download
       if (i >= 2) INQB_CUDA(cudaStreamWaitEvent(r.up, r.ev_comp[slot], 0));
@@ -1894,7 +1955,7 @@ int inqb_exponential_in_place(const inqb_hamiltonian *hc, double re, double im, 
   return guarded(h ? h->ctx : nullptr, [&] {
     INQB_REQUIRE(h && phi, INQB_ERR_ARG, "null argument");
     set_device(*h->ctx);
-    exponential(*h, 0.0, std::complex<double>(re, im), *phi, nullptr, order);
+    exponential_in_place(*h, std::complex<double>(re, im), *phi, order);
   });
 }
 
@@ -1905,7 +1966,8 @@ int inqb_exponential_2_for_1(const inqb_hamiltonian *hc, double f1_re, double f1
     INQB_REQUIRE(h && phi && exp1, INQB_ERR_ARG, "null argument");
     check_same_shape(*phi, *exp1);
     set_device(*h->ctx);
-    exponential(*h, std::complex<double>(f1_re, f1_im), std::complex<double>(f2_re, f2_im), *phi, exp1, order);
+    exponential_2_for_1(*h, std::complex<double>(f1_re, f1_im), std::complex<double>(f2_re, f2_im), *phi, *exp1,
+                        order);
   });
 }
 
@@ -2044,7 +2106,8 @@ int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int n
     std::vector<std::unique_ptr<TempSet>> save;
     for (int k = 0; k < nsets; k++) {
       save.emplace_back(new TempSet(*phis[k]));
-      exponential(*h, std::complex<double>(0.0, -dt / 2.0), std::complex<double>(0.0, -dt), *phis[k], &save[k]->o, 4);
+      exponential_2_for_1(*h, std::complex<double>(0.0, -dt / 2.0), std::complex<double>(0.0, -dt), *phis[k],
+                          save[k]->o, 4);
     }
     double *dens = static_cast<double *>(dev_alloc(ctx, sizeof(double) * b.npoints));
     double *old = static_cast<double *>(dev_alloc(ctx, sizeof(double) * b.npoints));
@@ -2056,8 +2119,8 @@ int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int n
     int it = 0;
     for (int iscf = 0; iscf < nscf_max; iscf++) {
       for (int k = 0; k < nsets; k++) {
-        copy_set(save[k]->o, *phis[k]);  // restore (etrs.hpp:54-56) and phi = save (etrs.hpp:63)
-        exponential(*h, 0.0, std::complex<double>(0.0, -dt / 2.0), *phis[k], nullptr, 4);
+        // phi = exp(-i H dt / 2) save (etrs.hpp:54-64), straight from the saved half step: no restore copy
+        exponential_from(*h, std::complex<double>(0.0, -dt / 2.0), save[k]->o, *phis[k], 4);
       }
       std::swap(old, dens);
       density_dev(ctx, phis, nsets, occ, dens);

@@ -15,7 +15,7 @@
 //   * EPI_FINAL_REAL: out = scale*fft + (V + shift)*psi + nonlocal(psi) with the
 //     nonlocal term taken from the per-grid-point hit lists (owner computes, no
 //     atomics; projector_all.hpp:276-288) and the 1/N of to_real (transform.hpp:175-181);
-//     optional Taylor accumulators acc += c*out (shift.hpp:33-43, exponential.hpp:21-69);
+//     optionally a Horner step of a Taylor exponential, out = base + c*out (exponential.hpp:21-34);
 //   * PRO_VPSI: the tile is loaded as (V + shift)*psi + nonlocal (Fourier-form operator,
 //     ks_hamiltonian.hpp:166-172);
 //   * EPI_LAPL_ADD: out = fft + lapl(G)*psi_fourier (laplacian_add, laplacian.hpp:24-38).
@@ -93,9 +93,8 @@ __global__ void __launch_bounds__(256) fft_pass_kernel(PassArgs<R> a, Geom g, Ra
       R f = R(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc));
       v = cadd(v, cscale(a.psi[e], f));
     }
+    if (a.hbase) v = cadd(a.hbase[e], cmul(a.hc, v));
     a.out[e] = v;
-    if (a.acc1) a.acc1[e] = cadd(a.acc1[e], cmul(a.c1, v));
-    if (a.acc2) a.acc2[e] = cadd(a.acc2[e], cmul(a.c2, v));
   }
 }
 

@@ -743,7 +743,8 @@ template <typename R, typename CR, int N, int VAR, int WIDE = 0> constexpr int m
 template <typename R, typename CR, int N, int VAR, int WIDE>
 __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_ctas_of<R, CR, N, VAR, WIDE>()) fft2_kernel(const __grid_constant__ CUtensorMap map_in,
                                                    const __grid_constant__ CUtensorMap map_out,
-                                                   const __grid_constant__ CUtensorMap map_aux, PassArgs<R> a, Geom2 gg,
+                                                   const __grid_constant__ CUtensorMap map_aux,
+                                                   const __grid_constant__ CUtensorMap map_base, PassArgs<R> a, Geom2 gg,
                                                    const C2<CR> *__restrict__ twg, int *err) {
   using T = C2<R>;
   using TC = C2<CR>;
@@ -756,11 +757,14 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
   constexpr uint32_t TILE_BYTES = TILE * sizeof(T);
   constexpr bool AUX = has_aux(VAR);
   const int NS = gg.stages;
+  // a Horner step (final pass of the real-space operator): a third tile per stage holds the base
+  const bool horner = AUX && a.hbase != nullptr;
 
   extern __shared__ __align__(1024) unsigned char smem[];
   T *stage_in = reinterpret_cast<T *>(smem);                         // NS tiles
   T *stage_aux = stage_in + size_t(NS) * TILE;                       // NS tiles when AUX
-  TC *exch = reinterpret_cast<TC *>(stage_aux + (AUX ? size_t(NS) * TILE : 0));  // one tile when SPLIT
+  T *stage_base = stage_aux + (AUX ? size_t(NS) * TILE : 0);         // NS tiles for a Horner step
+  TC *exch = reinterpret_cast<TC *>(stage_base + (horner ? size_t(NS) * TILE : 0));  // one tile when SPLIT
   constexpr int TWN = tw_entries<CR>(N);
   TC *tw = exch + (SPLIT ? TILE : 0);                                // twiddles (high, then low parts)
   CR *linev = reinterpret_cast<CR *>(tw + TWN);                      // N per-point factors of the current line
@@ -792,9 +796,12 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
   auto issue = [&](int st, long long t) {
     int c0, c1, c2, c3;
     coords(t, c0, c1, c2, c3);
-    mbar_expect_tx(&bar[st], AUX ? 2 * TILE_BYTES : TILE_BYTES);
+    mbar_expect_tx(&bar[st], (AUX ? (horner ? 3 : 2) : 1) * TILE_BYTES);
     tma_load_4d(stage_in + size_t(st) * TILE, &map_in, &bar[st], c0, c1, c2, c3);
-    if constexpr (AUX) tma_load_4d(stage_aux + size_t(st) * TILE, &map_aux, &bar[st], c0, c1, c2, c3);
+    if constexpr (AUX) {
+      tma_load_4d(stage_aux + size_t(st) * TILE, &map_aux, &bar[st], c0, c1, c2, c3);
+      if (horner) tma_load_4d(stage_base + size_t(st) * TILE, &map_base, &bar[st], c0, c1, c2, c3);
+    }
   };
 
   // bounded wait on an mbarrier phase; false (and the error flag raised) on expiry or abort
@@ -850,7 +857,6 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
   }
 
   const bool scaled = a.scale != 1.0;
-  const bool accum = (a.acc1 != nullptr) || (a.acc2 != nullptr);
   int i = 0;
   for (long long t = blockIdx.x; t < gg.ntiles; t += gridDim.x, i++) {
     const int st = i % NS;
@@ -861,6 +867,7 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
 
     T *buf = stage_in + size_t(st) * TILE;
     const T *aux = stage_aux + size_t(st) * TILE;
+    const T *base = stage_base + size_t(st) * TILE;
     const long long L = t / gg.nsb;
     const int s0 = int(t % gg.nsb) * W;
     const int la = int(L / g.nb), lb = int(L % g.nb);
@@ -896,18 +903,15 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
       }
     }
 
-    // final value of one output element: scaling, epilogue term, Taylor accumulators
+    // final value of one output element: scaling, epilogue term, Horner step (base + c * value, the
+    // value rounded to the storage type first, as the operator's output would be)
     auto epi_out = [&](int m, int w, TC v) -> T {
-      const int s = s0 + w;
       if (scaled) v = kscale(v, a.scale);
       if constexpr (base_var(VAR) == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
-      const T o = conv<T>(v);
-      if (accum && s < a.S) {
-        const long long ge = (pbase + m * g.sp) * a.S + s;
-        if (a.acc1) a.acc1[ge] = cadd(a.acc1[ge], cmul(a.c1, o));
-        if (a.acc2) a.acc2[ge] = cadd(a.acc2[ge], cmul(a.c2, o));
+      if constexpr (AUX) {
+        if (horner) return cadd(base[m * W + w], cmul(a.hc, conv<T>(v)));
       }
-      return o;
+      return conv<T>(v);
     };
     auto put_out = [&](int m, int w, TC v) { buf[m * W + w] = epi_out(m, w, v); };
     const CR *pre = (VAR == FWD_VPSI && !a.nl_offs) ? linev : nullptr;
@@ -930,7 +934,7 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
         }
       }
       // plain passes (no scaling, no accumulators) store the transform's values as they are
-      const bool plain = !AUX && !scaled && !accum;
+      const bool plain = !AUX && !scaled;
       if constexpr (VAR == MID_KIN) {
         if (plain) tile_kin_inplace<N, W, NT, T>(buf, twt, linev, Identity());
         else tile_kin_inplace<N, W, NT, T>(buf, twt, linev, epi_out);
@@ -1024,7 +1028,7 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   using TC = C2<CR>;
   constexpr int W = tile_w<R, CR, WIDE>();
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
-  const int nbuf = has_aux(VAR) ? 2 : 1;
+  const int nbuf = has_aux(VAR) ? (a.hbase ? 3 : 2) : 1;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
   constexpr int NT = block_threads_of<R, CR, N, VAR, WIDE>();
   const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + size_t(tw_entries<CR>(N) + N) * sizeof(TC) + 64 + 16 * 8;
@@ -1064,8 +1068,9 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   CUtensorMap mi = orbital_map(a.in, b, a.S, cwords, gg.axis, W);
   CUtensorMap mo = orbital_map(a.out, b, a.S, cwords, gg.axis, W);
   CUtensorMap mx = has_aux(VAR) ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W) : mi;
+  CUtensorMap mb = (has_aux(VAR) && a.hbase) ? orbital_map(a.hbase, b, a.S, cwords, gg.axis, W) : mi;
   const TC *tw = reinterpret_cast<const TC *>(sizeof(CR) == 8 ? b.tw64[gg.axis] : b.tw32[gg.axis]);
-  kern<<<unsigned(grid), NT, smem, ctx.stream>>>(mi, mo, mx, a, gg, tw, ctx.d_err);
+  kern<<<unsigned(grid), NT, smem, ctx.stream>>>(mi, mo, mx, mb, a, gg, tw, ctx.d_err);
   INQB_CUDA(cudaGetLastError());
   ctx.launches++;
 }

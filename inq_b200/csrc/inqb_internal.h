@@ -206,9 +206,10 @@ template <typename R> struct PassArgs {
   const int *nl_hitp = nullptr;     // projector index of each hit
   const C2<R> *nl_hcoef = nullptr;
   const C2<R> *projD = nullptr;
-  // Taylor accumulators: acc1 += c1 * out, acc2 += c2 * out
-  C2<R> *acc1 = nullptr, *acc2 = nullptr;
-  C2<R> c1, c2;
+  // Horner step of a Taylor exponential (real-space final pass): out = hbase + hc * (H v), where v is
+  // the pass's orbital input; hbase may not alias `out` (the operator's intermediates live there)
+  const C2<R> *hbase = nullptr;
+  C2<R> hc;
 };
 
 template <typename R>
@@ -225,9 +226,14 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
 void launch_nl_tables(Ctx &ctx, const Basis &b, Hamiltonian &h, const double kA[3]);
 template <typename R>
 void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out);
+// out += term (scaled: out += scale * term) at the sphere points
 template <typename R>
-void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out, C2<R> *acc1, C2<R> c1,
-                     C2<R> *acc2, C2<R> c2);
+void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out, bool scaled, C2<R> scale);
+// Taylor terms combined: e1 = x + sum_n c1[n] u[n], e2 = x + sum_n c2[n] u[n] (n < nterms <= 8, summed in
+// order n = 0, 1, ...); e1 may be null, e2 may equal x
+template <typename R>
+void launch_taylor_combine(Ctx &ctx, const C2<R> *x, const C2<R> *const *u, int nterms, const double2 *c1,
+                           const double2 *c2, C2<R> *e1, C2<R> *e2, long long n);
 
 template <typename R> void launch_fill(Ctx &ctx, C2<R> *p, long long n, double re, double im);
 template <typename R>

@@ -465,8 +465,8 @@ void launch_nl_scatter(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
 }
 
 // out[pt][s] += nonlocal term at the grid points that lie in a sphere (ks_hamiltonian.hpp:153,
-// projector_all.hpp:276-288), hits of a point summed in projector order, no atomics; optional Taylor
-// accumulators acc += c * term (linear in the term).
+// projector_all.hpp:276-288), hits of a point summed in projector order, no atomics; optionally scaled,
+// out += scale * term (a Horner step of a Taylor exponential).
 // Owner computes: one warp per (grid point with sphere hits, chunk of 32 * U states), lanes over states.
 // The point's record gives its first hit and projector in one load, so the coefficient, projection and
 // output reads are all issued together (a two-level dependency instead of point -> CSR -> hit ->
@@ -476,8 +476,7 @@ __global__ void __launch_bounds__(128) nl_apply_kernel(long long nitems, int nch
                                                           const int4 *__restrict__ hrec, const int *__restrict__ hitp,
                                                           const C2<R> *__restrict__ hcoef,
                                                           const C2<R> *__restrict__ projD, C2<R> *__restrict__ out,
-                                                          C2<R> *__restrict__ acc1, C2<R> c1,
-                                                          C2<R> *__restrict__ acc2, C2<R> c2) {
+                                                          bool scaled, C2<R> scale) {
   using T = C2<R>;
   constexpr int U = 16 / sizeof(R);  // states per lane: 4 single, 2 double
   const int lane = threadIdx.x & 31;
@@ -518,9 +517,7 @@ __global__ void __launch_bounds__(128) nl_apply_kernel(long long nitems, int nch
           accv = cadd(accv, cmul(hcoef[(long long)h * 4 + l], projD[((long long)p * 4 + l) * S + s]));
       }
       const long long e = pt * S + s;
-      out[e] = cadd(o[u], accv);
-      if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, accv));
-      if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, accv));
+      out[e] = cadd(o[u], scaled ? cmul(scale, accv) : accv);
     }
   }
 }
@@ -541,8 +538,7 @@ __global__ void __launch_bounds__(NLA_NT + 32, sizeof(R) == 4 ? 6 : 3) nl_apply_
                                                                      const int *__restrict__ hitp,
                                                                      const C2<R> *__restrict__ hcoef,
                                                                      const C2<R> *__restrict__ projD, C2<R> *out,
-                                                                     C2<R> *acc1, C2<R> c1, C2<R> *acc2, C2<R> c2,
-                                                                     int *err) {
+                                                                     bool scaled, C2<R> scale, int *err) {
   using T = C2<R>;
   using namespace ptx;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -654,10 +650,7 @@ __global__ void __launch_bounds__(NLA_NT + 32, sizeof(R) == 4 ? 6 : 3) nl_apply_
             accv = cadd(accv, cmul(hcoef[(long long)h * 4 + l], projD[((long long)p * 4 + l) * S + s]));
         }
         T *o = rw + (size_t)q * S + s;
-        *o = cadd(*o, accv);
-        const long long e = (long long)rec.x * S + s;
-        if (acc1) acc1[e] = cadd(acc1[e], cmul(c1, accv));
-        if (acc2) acc2[e] = cadd(acc2[e], cmul(c2, accv));
+        *o = cadd(*o, scaled ? cmul(scale, accv) : accv);
       }
     }
     fence_proxy_async();
@@ -666,8 +659,7 @@ __global__ void __launch_bounds__(NLA_NT + 32, sizeof(R) == 4 ? 6 : 3) nl_apply_
 }
 
 template <typename R>
-void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out, C2<R> *acc1, C2<R> c1,
-                     C2<R> *acc2, C2<R> c2) {
+void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, C2<R> *out, bool scaled, C2<R> scale) {
   const Projectors &P = h.proj;
   if (P.nhitpts == 0) return;
   const C2<R> *hc;
@@ -704,8 +696,8 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
       const long long nbatch = (P.nhitpts + KB - 1) / KB;
       long long grid = (long long)(per_sm < 1 ? 1 : per_sm) * ctx.num_sms;
       if (grid > nbatch) grid = nbatch;
-      kern<<<unsigned(grid), NLA_NT + 32, smem, ctx.stream>>>(P.nhitpts, KB, S, P.d_hrec, P.d_hitp, hc, projD, out, acc1,
-                                                             c1, acc2, c2, ctx.d_err);
+      kern<<<unsigned(grid), NLA_NT + 32, smem, ctx.stream>>>(P.nhitpts, KB, S, P.d_hrec, P.d_hitp, hc, projD, out,
+                                                             scaled, scale, ctx.d_err);
       LAUNCHED(ctx);
       return;
     }
@@ -716,7 +708,7 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
   long long blocks = (nitems + 3) / 4;
   if (blocks > 148LL * 48) blocks = 148LL * 48;
   nl_apply_kernel<R><<<unsigned(blocks), 128, 0, ctx.stream>>>(nitems, nchunks, S, P.d_hrec, P.d_hitp, hc, projD, out,
-                                                               acc1, c1, acc2, c2);
+                                                               scaled, scale);
   LAUNCHED(ctx);
 }
 
@@ -1542,12 +1534,59 @@ void launch_ks_potential(Ctx &ctx, const double *n, const double *vion, const do
 }
 
 // ------------------------------------------------------------------ instantiations
+// ------------------------------------------------------------------ Taylor terms combined
+
+struct TaylorCoefs {
+  double2 c1[8], c2[8];
+};
+struct TaylorTerms {
+  const void *u[8];
+};
+
+// e1 = x + sum_n c1[n] u[n], e2 = x + sum_n c2[n] u[n], element-wise, terms added in order n = 0, 1, ...
+// (the order in which exponential.hpp:56-69 adds them); complex products in double
+template <typename R>
+__global__ void taylor_combine_kernel(const C2<R> *__restrict__ x, TaylorTerms u, int nterms, TaylorCoefs c,
+                                      C2<R> *e1, C2<R> *e2, long long n) {
+  using T = C2<R>;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const T xv = x[i];
+    double2 a1 = make_double2(double(xv.x), double(xv.y)), a2 = a1;
+    for (int k = 0; k < nterms; k++) {
+      const T t = static_cast<const T *>(u.u[k])[i];
+      const double2 tv = make_double2(double(t.x), double(t.y));
+      if (e1) a1 = cadd(a1, cmul(c.c1[k], tv));
+      a2 = cadd(a2, cmul(c.c2[k], tv));
+    }
+    if (e1) e1[i] = mk<T>(R(a1.x), R(a1.y));
+    e2[i] = mk<T>(R(a2.x), R(a2.y));
+  }
+}
+
+template <typename R>
+void launch_taylor_combine(Ctx &ctx, const C2<R> *x, const C2<R> *const *u, int nterms, const double2 *c1,
+                           const double2 *c2, C2<R> *e1, C2<R> *e2, long long n) {
+  INQB_REQUIRE(nterms >= 1 && nterms <= 8, INQB_ERR_UNSUPPORTED, "Taylor order must be 1..8");
+  TaylorTerms t{};
+  TaylorCoefs c{};
+  for (int k = 0; k < nterms; k++) {
+    t.u[k] = u[k];
+    c.c1[k] = c1 ? c1[k] : make_double2(0.0, 0.0);
+    c.c2[k] = c2[k];
+  }
+  long long blocks = (n + 255) / 256;
+  if (blocks > 16LL * ctx.num_sms) blocks = 16LL * ctx.num_sms;
+  taylor_combine_kernel<R><<<unsigned(blocks), 256, 0, ctx.stream>>>(x, t, nterms, c, e1, e2, n);
+  LAUNCHED(ctx);
+}
+
 #define INST(R)                                                                                                   \
   template void launch_nl_project<R>(Ctx &, const Basis &, const Hamiltonian &, const C2<R> *, int, C2<R> *,       \
                                      C2<R> *);                                                                    \
   template void launch_nl_scatter<R>(Ctx &, const Basis &, const Hamiltonian &, const C2<R> *, int, C2<R> *);     \
-  template void launch_nl_apply<R>(Ctx &, const Hamiltonian &, const C2<R> *, int, C2<R> *, C2<R> *, C2<R>,       \
-                                   C2<R> *, C2<R>);                                                              \
+  template void launch_nl_apply<R>(Ctx &, const Hamiltonian &, const C2<R> *, int, C2<R> *, bool, C2<R>);        \
+  template void launch_taylor_combine<R>(Ctx &, const C2<R> *, const C2<R> *const *, int, const double2 *,         \
+                                         const double2 *, C2<R> *, C2<R> *, long long);                           \
   template void launch_fill<R>(Ctx &, C2<R> *, long long, double, double);                                         \
   template void launch_axpy<R>(Ctx &, C2<R> *, const C2<R> *, long long, double, double);                          \
   template void launch_shift_vec<R>(Ctx &, C2<R> *, const C2<R> *, int, long long, const double *, double);        \

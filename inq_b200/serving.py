@@ -72,7 +72,8 @@ class Request:
         n = self.payload.system.npoints
         s = self.payload.system.nst
         cb = 16 if precision == F64 else 8
-        sets = 2 if self.kind == "apply" else 5   # in/out; ETRS: phi, saved half step, two H^n buffers, spare
+        # in/out; ETRS: phi, saved half step, the four kept Taylor terms H^n phi of the first exponential
+        sets = 2 if self.kind == "apply" else 6
         tables = n * 8 * 4 + self.payload.system.natoms * 4000 * 64   # potential, CSR, projector tables
         return sets * n * s * cb + tables + (64 << 20)
 

@@ -35,6 +35,24 @@ def test_apply_host_matches_device_call(c1, precision_name, tol, block):
     assert err < tol, err
 
 
+@pytest.mark.parametrize("precision_name,tol", [("F64", 1e-12), ("F32", 2e-6)])
+def test_apply_host_default_blocks_with_half_blocks_at_the_ends(precision_name, tol):
+    """136 states with the default blocks: half-size first and last blocks around full ones, and a
+    shortened full-size block before the last (single: 32, 64, 40; double: 16, 32, 32, 32, 8, 16)."""
+    import inq_b200 as ib
+    from inq_b200 import synthetic
+    sysm = synthetic.config("c1", nst=136)
+    basis, ham, phi64 = synthetic.build(sysm)
+    prec = getattr(ib, precision_name)
+    phi = phi64 if prec == ib.F64 else phi64.converted(prec)
+    ref = ham(phi).matrix()
+    host_in = np.ascontiguousarray(phi.matrix())
+    host_out = np.zeros_like(host_in)
+    ham.apply_host(host_in, host_out)
+    err = np.linalg.norm(host_out - ref) / np.linalg.norm(ref)
+    assert err < tol, err
+
+
 def test_apply_host_pinned_buffers_and_repeat(c1):
     import torch
     ib, basis, ham, phi64 = c1
