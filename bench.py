@@ -371,9 +371,12 @@ def overlap_leg(ctx, phi32, phi64, time_loop, reps=5):
                          "flop_per_call": flop}}
 
 
-def etrs_leg(ctx, steps=10, dt=0.005):
-    """C3: ETRS propagation at 120^3 / 256 states / 128 atoms after a 0.01 a.u. kick along x (phase
-    exp(i 0.01 x)), FP64 density every step; plain FP64 and mixed dipole series.
+def etrs_leg(ctx, steps=200, dt=0.005):
+    """C3: real-time propagation at 120^3 / 256 states / 128 atoms after a 0.01 a.u. kick along x (phase
+    exp(i 0.01 x)), through the real-time driver (real_time::propagate, propagate.hpp:87-119): every step
+    is one ETRS step (etrs.hpp:22-79, FP64 density each step) plus the energy of the step
+    (energy.calculate, propagate.hpp:99: one more H application and its reductions) and the dipole;
+    plain FP64 and mixed series side by side.
 
     The time step: the order-4 Taylor exponential (exponential.hpp:21-69) is stable only for
     dt * E_max < 2 sqrt(2), and the grid's kinetic energy reaches E_max = 3/2 (pi n / a)^2 = 325 Ha at
@@ -382,7 +385,7 @@ def etrs_leg(ctx, steps=10, dt=0.005):
     import numpy as np
     import torch
     import inq_b200 as ib
-    from inq_b200 import synthetic
+    from inq_b200 import real_time, synthetic
     sysm = synthetic.config("c3")
     basis, ham, phi64 = synthetic.build(sysm, ctx=ctx)
     ib.apply_phase_kick(phi64, [0.01, 0.0, 0.0])
@@ -391,36 +394,39 @@ def etrs_leg(ctx, steps=10, dt=0.005):
     emax = 1.5 * (np.pi * sysm.sizes[0] / sysm.lattice[0][0]) ** 2
     out = {}
     stream = torch.cuda.ExternalStream(ctx.stream())
+    series = {}
     for name, phi in (("fp64", phi64), ("mixed", phi32)):
-        dips = []
-        iters = []
         # one untimed step on a copy: the step's work buffers come from the stream-ordered pool, whose
         # first growth to this size (tens of GB at 120^3 FP64) would otherwise land in the timed steps
         warm = phi.copy()
-        ib.etrs(ham, [warm], [occ], dt)
+        real_time.propagate(ham, [warm], [occ], dt, 1)
         del warm
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ctx.synchronize()
         e0.record(stream)
-        for _ in range(steps):
-            _, dip, it = ib.etrs(ham, [phi], [occ], dt)
-            dips.append(dip.tolist())
-            iters.append(it)
+        res = real_time.propagate(ham, [phi], [occ], dt, steps)
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
         norm = ib.overlap_diagonal(phi).real
+        dip = np.array(res.dipole)
+        ene = np.array(res.total_energy)
+        series[name] = (dip, ene)
         out[name] = {"steps_per_s": steps / (ms / 1000.0), "ms_per_step": ms / steps,
-                     "scf_iterations": iters, "max_norm_drift": float(np.max(np.abs(norm - 1.0))),
-                     "dipole_series": dips}
-    d64 = np.array(out["fp64"]["dipole_series"])
-    d32 = np.array(out["mixed"]["dipole_series"])
+                     "max_norm_drift": float(np.max(np.abs(norm - 1.0))),
+                     "energy_first_last_ha": [float(ene[0]), float(ene[-1])],
+                     "max_energy_drift_ha": float(np.max(np.abs(ene - ene[0]))),
+                     "dipole_every_50_steps": dip[::50].tolist()}
+    d64, e64 = series["fp64"]
+    d32, e32 = series["mixed"]
     out["max_dipole_diff_mixed_vs_fp64"] = float(np.max(np.abs(d64 - d32)))
-    out["max_rel_dipole_change_fp64"] = float(np.max(np.abs(d64 - d64[0])))
+    out["max_energy_diff_mixed_vs_fp64_ha"] = float(np.max(np.abs(e64 - e32)))
+    out["max_dipole_change_fp64"] = float(np.max(np.abs(d64 - d64[0])))
     out["dt"] = dt
+    out["steps"] = steps
     out["dt_stability_bound"] = float(2 * np.sqrt(2) / emax)
     # interacting: the potential rebuilt from every density (Hartree + LDA on the device), FP64
-    isteps = max(1, steps // 2)
+    isteps = 5
     ham.set_interaction(sysm.local_potential())
     p = phi64.copy()
     ham.update_hamiltonian(ib.density([p], [occ]).reshape(-1))
@@ -444,7 +450,8 @@ def etrs_leg(ctx, steps=10, dt=0.005):
                                "scf_iterations": its, "dipole_series": dips,
                                "update": "V = V_ion + V_H (Poisson) + V_xc (LDA) from every density of the step"}
     out["workload"] = (f"c3: 120^3, {sysm.nst} states, {sysm.natoms} atoms, kick 0.01 x, dt {dt} "
-                       f"(0.05 exceeds the Taylor-4 stability bound {2 * np.sqrt(2) / emax:.4f}), {steps} steps")
+                       f"(0.05 exceeds the Taylor-4 stability bound {2 * np.sqrt(2) / emax:.4f}), {steps} steps "
+                       f"of ETRS + energy + dipole (real_time.propagate)")
     return out
 
 
@@ -687,7 +694,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-legs", action="store_true", help="skip the batched-systems, serving and ETRS legs")
-    ap.add_argument("--etrs-steps", type=int, default=10, help="ETRS steps of the 120^3 real-time leg (0: skip)")
+    ap.add_argument("--etrs-steps", type=int, default=200, help="ETRS steps of the 120^3 real-time leg (0: skip)")
     ap.add_argument("--etrs-dt", type=float, default=0.005, help="time step of the 120^3 real-time leg (a.u.)")
     ap.add_argument("--profile-case", action="store_true", help="small workload for ncu captures")
     ap.add_argument("--profile-states", type=int, default=32, help="orbitals of the --profile-case workload")

@@ -694,6 +694,7 @@ struct Geom2 {
   long long ntiles;
   int stages;
   int cwords;       // 32-bit words per complex element
+  int aux_single;   // second input tiles single-buffered (1) or one set per ring stage (0)
 };
 
 template <int VAR> constexpr int dir_first() { return (base_var(VAR) == INV_STORE || base_var(VAR) == INV_FINAL) ? -1 : +1; }
@@ -760,17 +761,25 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
   // a Horner step (final pass of the real-space operator): a third tile per stage holds the base
   const bool horner = AUX && a.hbase != nullptr;
 
+  // The second input tile (psi of V psi or of the Laplacian term) and the Horner base are needed only in
+  // the last step of a tile's transform.  Either every ring stage holds them beside its tile (loaded with
+  // it), or, when that would leave one CTA per SM (gg.aux_single), they are single-buffered: loaded for
+  // the CTA's next tile as soon as its current one is computed, so that they land during the next tile's
+  // first steps, while the ring stages hold one tile each.
+  const int naux = AUX ? (horner ? 2 : 1) : 0;
+  const bool aux1 = AUX && gg.aux_single;
+
   extern __shared__ __align__(1024) unsigned char smem[];
   T *stage_in = reinterpret_cast<T *>(smem);                         // NS tiles
-  T *stage_aux = stage_in + size_t(NS) * TILE;                       // NS tiles when AUX
-  T *stage_base = stage_aux + (AUX ? size_t(NS) * TILE : 0);         // NS tiles for a Horner step
-  TC *exch = reinterpret_cast<TC *>(stage_base + (horner ? size_t(NS) * TILE : 0));  // one tile when SPLIT
+  T *aux_ring = stage_in + size_t(NS) * TILE;                        // naux tiles, or NS x naux
+  TC *exch = reinterpret_cast<TC *>(aux_ring + size_t(aux1 ? 1 : NS) * naux * TILE);  // one tile when SPLIT
   constexpr int TWN = tw_entries<CR>(N);
   TC *tw = exch + (SPLIT ? TILE : 0);                                // twiddles (high, then low parts)
   CR *linev = reinterpret_cast<CR *>(tw + TWN);                      // N per-point factors of the current line
   uint64_t *bar = reinterpret_cast<uint64_t *>(tw + TWN + N);        // NS "tile loaded" barriers (8-byte aligned)
   uint64_t *done = bar + NS;                                         // NS "tile computed" barriers (producer warp)
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(done + NS);
+  uint64_t *abar = done + NS;                                        // "second input tiles loaded"
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(abar + 1);
 
   const Geom &g = gg.g;
   for (int i = threadIdx.x; i < TWN; i += NTT) tw[i] = twg[i];
@@ -780,6 +789,7 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
       mbar_init(&bar[s], 1);
       if constexpr (WS) mbar_init(&done[s], NT);
     }
+    mbar_init(abar, 1);
     mbar_init_fence();
   }
   __syncthreads();
@@ -796,12 +806,22 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
   auto issue = [&](int st, long long t) {
     int c0, c1, c2, c3;
     coords(t, c0, c1, c2, c3);
-    mbar_expect_tx(&bar[st], (AUX ? (horner ? 3 : 2) : 1) * TILE_BYTES);
+    mbar_expect_tx(&bar[st], uint32_t(aux1 ? 1 : 1 + naux) * TILE_BYTES);
     tma_load_4d(stage_in + size_t(st) * TILE, &map_in, &bar[st], c0, c1, c2, c3);
-    if constexpr (AUX) {
-      tma_load_4d(stage_aux + size_t(st) * TILE, &map_aux, &bar[st], c0, c1, c2, c3);
-      if (horner) tma_load_4d(stage_base + size_t(st) * TILE, &map_base, &bar[st], c0, c1, c2, c3);
+    if (AUX && !aux1) {
+      T *ax = aux_ring + size_t(st) * naux * TILE;
+      tma_load_4d(ax, &map_aux, &bar[st], c0, c1, c2, c3);
+      if (horner) tma_load_4d(ax + TILE, &map_base, &bar[st], c0, c1, c2, c3);
     }
+  };
+  // single-buffered: the second input tile (and the Horner base) of tile t; the k-th such load completes
+  // phase k of abar
+  auto issue_aux = [&](long long t) {
+    int c0, c1, c2, c3;
+    coords(t, c0, c1, c2, c3);
+    mbar_expect_tx(abar, uint32_t(naux) * TILE_BYTES);
+    tma_load_4d(aux_ring, &map_aux, abar, c0, c1, c2, c3);
+    if (horner) tma_load_4d(aux_ring + TILE, &map_base, abar, c0, c1, c2, c3);
   };
 
   // bounded wait on an mbarrier phase; false (and the error flag raised) on expiry or abort
@@ -821,16 +841,18 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
   // tiles whose loads the issuing thread has started (the i-th goes to stage i % NS, phase i / NS);
   // before the CTA ends, that thread waits (bounded) for the last NS of them, so that after an aborted
   // wait no load still lands in shared memory (on the normal path those phases are complete already)
-  int nissued = 0;
+  int nissued = 0, naux_issued = 0;
   auto drain = [&]() {
     for (int i = nissued - NS < 0 ? 0 : nissued - NS; i < nissued; i++)
       ptx::mbar_wait_bounded(&bar[i % NS], uint32_t(i / NS) & 1u, 2000000000ull);
+    if (naux_issued > 0) ptx::mbar_wait_bounded(abar, uint32_t(naux_issued - 1) & 1u, 2000000000ull);
   };
   if (threadIdx.x == (WS ? NT : 0)) {
     for (int s = 0; s < NS; s++) {
       const long long t = blockIdx.x + (long long)s * gridDim.x;
       if (t < gg.ntiles) issue(s, t), nissued++;
     }
+    if (aux1 && blockIdx.x < gg.ntiles) issue_aux(blockIdx.x), naux_issued++;
   }
   if constexpr (WS) {
     if (threadIdx.x >= NT) {
@@ -845,6 +867,8 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
           coords(t, c0, c1, c2, c3);
           tma_store_4d(&map_out, stage_in + size_t(st) * TILE, c0, c1, c2, c3);
           bulk_commit();
+          // the second input tiles were read by the finished tile's epilogue: load the next tile's
+          if (aux1 && t + gridDim.x < gg.ntiles) issue_aux(t + gridDim.x), naux_issued++;
           bulk_wait_read0();
           const long long tn = t + (long long)NS * gridDim.x;
           if (tn < gg.ntiles) issue(st, tn), nissued++;
@@ -866,8 +890,9 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
     if (csync_or<NT>(!ok || *abort_flag)) break;
 
     T *buf = stage_in + size_t(st) * TILE;
-    const T *aux = stage_aux + size_t(st) * TILE;
-    const T *base = stage_base + size_t(st) * TILE;
+    const T *aux = aux_ring + (aux1 ? 0 : size_t(st) * naux * TILE);
+    const T *base = aux + TILE;
+    bool aux_ready = !aux1;  // this thread has waited for the tile's second input (phase i of abar)
     const long long L = t / gg.nsb;
     const int s0 = int(t % gg.nsb) * W;
     const int la = int(L / g.nb), lb = int(L % g.nb);
@@ -906,6 +931,12 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
     // final value of one output element: scaling, epilogue term, Horner step (base + c * value, the
     // value rounded to the storage type first, as the operator's output would be)
     auto epi_out = [&](int m, int w, TC v) -> T {
+      if constexpr (AUX) {
+        if (!aux_ready) {
+          wait_bar(abar, uint32_t(i) & 1u);  // on expiry the error flag is raised and the tile loop ends
+          aux_ready = true;
+        }
+      }
       if (scaled) v = kscale(v, a.scale);
       if constexpr (base_var(VAR) == INV_FINAL || VAR == FWD_LAPLADD) v = cadd(v, cscale(conv<TC>(aux[m * W + w]), linev[m]));
       if constexpr (AUX) {
@@ -969,6 +1000,7 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
         coords(t, c0, c1, c2, c3);
         tma_store_4d(&map_out, buf, c0, c1, c2, c3);
         bulk_commit();
+        if (aux1 && t + gridDim.x < gg.ntiles) issue_aux(t + gridDim.x), naux_issued++;
         bulk_wait_read0();  // the stage may be refilled once the store has read it
         const long long tn = t + (long long)NS * gridDim.x;
         if (tn < gg.ntiles) issue(st, tn), nissued++;
@@ -1028,7 +1060,7 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   using TC = C2<CR>;
   constexpr int W = tile_w<R, CR, WIDE>();
   constexpr size_t TILE_BYTES = size_t(N) * W * sizeof(T);
-  const int nbuf = has_aux(VAR) ? (a.hbase ? 3 : 2) : 1;
+  const int naux = has_aux(VAR) ? (a.hbase ? 2 : 1) : 0;
   constexpr bool SPLIT = sizeof(CR) > sizeof(R);
   constexpr int NT = block_threads_of<R, CR, N, VAR, WIDE>();
   const size_t fixed = (SPLIT ? size_t(N) * W * sizeof(TC) : 0) + size_t(tw_entries<CR>(N) + N) * sizeof(TC) + 64 + 16 * 8;
@@ -1039,13 +1071,19 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   size_t budget = (SPLIT || VAR == MID_KIN || ws_of<R, CR, N, VAR>()) ? 56 * 1024 : 113 * 1024;
   // 512-byte-row streaming passes: three stages, one CTA per SM
   if (WIDE) budget = 150 * 1024;
-  int ns = int((budget - fixed) / (TILE_BYTES * nbuf));
+  // second input tiles beside every ring stage when two stages of them leave room for two CTAs per SM,
+  // else single-buffered (96^3 x 256: 0.80 against 0.92 ms for the single-precision final pass beside
+  // every stage; 120^3 x 256 double: 3.1 against 5.35 ms single-buffered, at two CTAs per SM against one)
+  gg.aux_single = naux > 0 && size_t(2) * (1 + naux) * TILE_BYTES + fixed > 113 * 1024;
+  const size_t per_stage = TILE_BYTES * (gg.aux_single ? 1 : 1 + naux);
+  const size_t fixed_aux = gg.aux_single ? naux * TILE_BYTES : 0;
+  int ns = budget > fixed + fixed_aux ? int((budget - fixed - fixed_aux) / per_stage) : 0;
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;
   gg.stages = ns;
   gg.nsb = (a.S + W - 1) / W;
   gg.ntiles = (b.npoints / b.n[gg.axis]) * gg.nsb;
-  const size_t smem = TILE_BYTES * nbuf * ns + fixed;
+  const size_t smem = per_stage * ns + fixed_aux + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
   auto kern = fft2_kernel<R, CR, N, VAR, WIDE>;
   // per instantiation: shared-memory attribute and occupancy, computed under a lock (several host
