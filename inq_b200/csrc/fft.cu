@@ -154,7 +154,9 @@ int fft2_perm_n2(const Ctx &ctx, const Basis &b, int S, int elem_bytes, int axis
   if (ctx.fft_impl == 1) return 0;
   const int n = b.n[axis];
   if (n != 24 && n != 32 && n != 40 && n != 48 && n != 64 && n != 72 && n != 96 && n != 120 && n != 128) return 0;
-  if ((size_t(S) * elem_bytes) % 16 != 0) return 0;
+  // rows that are not 16-byte multiples: single-precision orbitals only (the producer-warp kernels copy
+  // them); the caller keeps natural order when the arithmetic is not single precision
+  if ((size_t(S) * elem_bytes) % 16 != 0 && elem_bytes != 8) return 0;
   if (S < 256 / elem_bytes) return 0;
   return n / 8;
 }

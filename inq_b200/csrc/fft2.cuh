@@ -695,6 +695,8 @@ struct Geom2 {
   int stages;
   int cwords;       // 32-bit words per complex element
   int aux_single;   // second input tiles single-buffered (1) or one set per ring stage (0)
+  int cpa;          // rows that are not 16-byte multiples: the compute threads move tiles with 8-byte
+                    // cp.async loads and plain stores instead of TMA (two stages, second tiles per stage)
 };
 
 template <int VAR> constexpr int dir_first() { return (base_var(VAR) == INV_STORE || base_var(VAR) == INV_FINAL) ? -1 : +1; }
@@ -847,7 +849,7 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
       ptx::mbar_wait_bounded(&bar[i % NS], uint32_t(i / NS) & 1u, 2000000000ull);
     if (naux_issued > 0) ptx::mbar_wait_bounded(abar, uint32_t(naux_issued - 1) & 1u, 2000000000ull);
   };
-  if (threadIdx.x == (WS ? NT : 0)) {
+  if (threadIdx.x == (WS ? NT : 0) && !gg.cpa) {
     for (int s = 0; s < NS; s++) {
       const long long t = blockIdx.x + (long long)s * gridDim.x;
       if (t < gg.ntiles) issue(s, t), nissued++;
@@ -855,6 +857,8 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
     if (aux1 && blockIdx.x < gg.ntiles) issue_aux(blockIdx.x), naux_issued++;
   }
   if constexpr (WS) {
+    // rows that TMA cannot move: the compute threads copy them (below); the producer warp has no work
+    if (threadIdx.x >= NT && gg.cpa) return;
     if (threadIdx.x >= NT) {
       // producer warp: lane 0 stores every computed tile, waits for the store to read the stage and
       // refills it with the tile NS steps ahead
@@ -881,13 +885,49 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
   }
 
   const bool scaled = a.scale != 1.0;
+  // 8-byte copies by the compute threads (rows that are not 16-byte multiples, gg.cpa): tile t's rows of
+  // `src` into dst, consecutive threads on consecutive states; with the second input tiles of the stage
+  auto cpa_rows = [&](long long t, long long &pbase, int &s0, int &ws) {
+    const long long L = t / gg.nsb;
+    s0 = int(t % gg.nsb) * W;
+    ws = a.S - s0 < W ? a.S - s0 : W;
+    pbase = (L / g.nb) * g.sa + (L % g.nb) * g.sb;
+  };
+  auto cpa_load = [&](T *dst, const T *src, long long t) {
+    long long pbase;
+    int s0, ws;
+    cpa_rows(t, pbase, s0, ws);
+    for (int e = threadIdx.x; e < TILE; e += NT) {
+      const int r = e / W, c = e % W;
+      if (c < ws) ptx::cp_async8(dst + e, src + (pbase + r * g.sp) * a.S + s0 + c);
+    }
+  };
+  auto cpa_load_stage = [&](int st, long long t) {
+    cpa_load(stage_in + size_t(st) * TILE, a.in, t);
+    if constexpr (AUX) {
+      cpa_load(aux_ring + size_t(st) * naux * TILE, a.psi, t);
+      if (horner) cpa_load(aux_ring + size_t(st) * naux * TILE + TILE, a.hbase, t);
+    }
+  };
+  if (gg.cpa) {
+    if (blockIdx.x < gg.ntiles) cpa_load_stage(0, blockIdx.x);
+    ptx::cp_async_commit();
+  }
   int i = 0;
   for (long long t = blockIdx.x; t < gg.ntiles; t += gridDim.x, i++) {
     const int st = i % NS;
     const uint32_t par = uint32_t(i / NS) & 1u;
-    // bounded wait for this stage's TMA load; every compute thread takes the same decision
-    const bool ok = wait_bar(&bar[st], par);
-    if (csync_or<NT>(!ok || *abort_flag)) break;
+    if (gg.cpa) {
+      // two stages: the next tile's copies are issued before this tile's are awaited
+      if (t + gridDim.x < gg.ntiles) cpa_load_stage((i + 1) % NS, t + gridDim.x);
+      ptx::cp_async_commit();
+      ptx::cp_async_wait<1>();
+      csync<NT>();
+    } else {
+      // bounded wait for this stage's TMA load; every compute thread takes the same decision
+      const bool ok = wait_bar(&bar[st], par);
+      if (csync_or<NT>(!ok || *abort_flag)) break;
+    }
 
     T *buf = stage_in + size_t(st) * TILE;
     const T *aux = aux_ring + (aux1 ? 0 : size_t(st) * naux * TILE);
@@ -990,6 +1030,20 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
       }
     }
 
+    if (gg.cpa) {
+      // plain stores of the computed tile; the barrier after them frees the stage for the copies of the
+      // tile two steps ahead
+      csync<NT>();
+      long long pbase;
+      int s0, ws;
+      cpa_rows(t, pbase, s0, ws);
+      for (int e = threadIdx.x; e < TILE; e += NT) {
+        const int r = e / W, c = e % W;
+        if (c < ws) a.out[(pbase + r * g.sp) * a.S + s0 + c] = buf[e];
+      }
+      csync<NT>();
+      continue;
+    }
     fence_proxy_async();
     if constexpr (WS) {
       mbar_arrive(&done[st]);  // the producer warp stores the tile and refills the stage
@@ -1007,6 +1061,7 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
       }
     }
   }
+  if (gg.cpa) ptx::cp_async_wait_all();
   if (!WS && threadIdx.x == 0) {
     drain();
     bulk_wait0();
@@ -1074,12 +1129,14 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   // second input tiles beside every ring stage when two stages of them leave room for two CTAs per SM,
   // else single-buffered (96^3 x 256: 0.80 against 0.92 ms for the single-precision final pass beside
   // every stage; 120^3 x 256 double: 3.1 against 5.35 ms single-buffered, at two CTAs per SM against one)
-  gg.aux_single = naux > 0 && size_t(2) * (1 + naux) * TILE_BYTES + fixed > 113 * 1024;
+  gg.cpa = (size_t(a.S) * sizeof(T)) % 16 != 0;
+  gg.aux_single = !gg.cpa && naux > 0 && size_t(2) * (1 + naux) * TILE_BYTES + fixed > 113 * 1024;
   const size_t per_stage = TILE_BYTES * (gg.aux_single ? 1 : 1 + naux);
   const size_t fixed_aux = gg.aux_single ? naux * TILE_BYTES : 0;
   int ns = budget > fixed + fixed_aux ? int((budget - fixed - fixed_aux) / per_stage) : 0;
   ns = ns < 2 ? 2 : (ns > 6 ? 6 : ns);
   if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;
+  if (gg.cpa) ns = 2;
   gg.stages = ns;
   gg.nsb = (a.S + W - 1) / W;
   gg.ntiles = (b.npoints / b.n[gg.axis]) * gg.nsb;
@@ -1103,10 +1160,17 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   long long grid = (long long)(per_sm < 1 ? 1 : per_sm) * ctx.num_sms;
   if (grid > gg.ntiles) grid = gg.ntiles;
   const int cwords = int(sizeof(T) / 4);
-  CUtensorMap mi = orbital_map(a.in, b, a.S, cwords, gg.axis, W);
-  CUtensorMap mo = orbital_map(a.out, b, a.S, cwords, gg.axis, W);
-  CUtensorMap mx = has_aux(VAR) ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W) : mi;
-  CUtensorMap mb = (has_aux(VAR) && a.hbase) ? orbital_map(a.hbase, b, a.S, cwords, gg.axis, W) : mi;
+  // rows that are not 16-byte multiples have no tensor map; the compute threads copy them (gg.cpa)
+  constexpr bool has_producer = ws_of<R, CR, N, VAR>();
+  INQB_REQUIRE(!gg.cpa || has_producer, INQB_ERR_UNSUPPORTED,
+               "FFT pass rows that are not 16-byte multiples need the producer-warp kernel");
+  CUtensorMap mi{}, mo{}, mx{}, mb{};
+  if (!gg.cpa) {
+    mi = orbital_map(a.in, b, a.S, cwords, gg.axis, W);
+    mo = orbital_map(a.out, b, a.S, cwords, gg.axis, W);
+    mx = has_aux(VAR) ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W) : mi;
+    mb = (has_aux(VAR) && a.hbase) ? orbital_map(a.hbase, b, a.S, cwords, gg.axis, W) : mi;
+  }
   const TC *tw = reinterpret_cast<const TC *>(sizeof(CR) == 8 ? b.tw64[gg.axis] : b.tw32[gg.axis]);
   kern<<<unsigned(grid), NT, smem, ctx.stream>>>(mi, mo, mx, mb, a, gg, tw, ctx.d_err);
   INQB_CUDA(cudaGetLastError());
@@ -1160,13 +1224,17 @@ void launch_nc(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var
 //   0 single precision everywhere; 1 double precision everywhere;
 //   2 double except the final (inverse, epilogue) pass of the real-space operator;
 //   3 as 2 and the first forward pass (z) of every transform also single.
+// whether a pass over single-precision orbitals runs single-precision arithmetic (context option mixed_compute)
+template <typename R> bool single_arith(const Ctx &ctx, const PassArgs<R> &a, int var) {
+  const int mode = ctx.mixed_compute;
+  const int bv = base_var(var);
+  return mode == 0 || (mode >= 2 && bv == INV_FINAL) || (mode == 3 && a.axis == 2 && (bv == FWD_STORE || var == FWD_VPSI));
+}
+
 template <typename R, int N>
 void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var) {
   if constexpr (sizeof(R) == 4) {
-    const int mode = ctx.mixed_compute;
-    const int bv = base_var(var);
-    const bool single = mode == 0 || (mode >= 2 && bv == INV_FINAL) ||
-                        (mode == 3 && a.axis == 2 && (bv == FWD_STORE || var == FWD_VPSI));
+    const bool single = single_arith(ctx, a, var);
     if (single) {
       const bool wide = ctx.fft_wide && a.S >= 64 && wide_var(var);
       launch_nc<R, float, N>(ctx, b, a, gg, var, wide);
@@ -1182,7 +1250,6 @@ template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a
   if (ctx.fft_impl == 1) return false;
   const int n = b.n[a.axis];
   if (n != 24 && n != 32 && n != 40 && n != 48 && n != 64 && n != 72 && n != 96 && n != 120 && n != 128) return false;
-  if ((size_t(a.S) * sizeof(T)) % 16 != 0) return false;
   if (a.S < 256 / int(sizeof(T))) return false;  // fewer states than one 256-byte row: generic kernel
   int var;
   if (a.mid_kinetic) var = MID_KIN;
@@ -1191,6 +1258,9 @@ template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a
   else if (epilogue == EPI_LAPL_ADD) var = FWD_LAPLADD;
   else var = a.dir > 0 ? FWD_STORE : INV_STORE;
   if ((var == INV_FINAL && a.dir > 0) || ((var == FWD_VPSI || var == FWD_LAPLADD) && a.dir < 0)) return false;
+  // rows that are not 16-byte multiples (an odd number of single-precision states): only the kernels with
+  // a producer warp (single-precision arithmetic) move them, with 8-byte copies; otherwise the generic kernel
+  if ((size_t(a.S) * sizeof(T)) % 16 != 0 && !(sizeof(R) == 4 && single_arith(ctx, a, var))) return false;
   if (a.perm) {
     INQB_REQUIRE(var == FWD_STORE || var == INV_STORE || var == INV_FINAL, INQB_ERR_UNSUPPORTED,
                  "digit-reversed frequency order is only kept by the plain forward and inverse passes");

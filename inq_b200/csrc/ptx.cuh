@@ -69,6 +69,17 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 // the issuing thread's copy groups except the newest N have completed
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// global -> shared copy of 8 bytes (both addresses 8-byte aligned), tracked by cp.async groups
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+// arrive on `bar` once every cp.async this thread issued so far has completed; the arrival counts
+// toward the barrier's expected count (.noinc)
+__device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Waits for phase `parity` of `bar` for at most `limit_ns`; false on expiry.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
   const uint64_t t0 = global_ns();

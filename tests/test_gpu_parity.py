@@ -63,10 +63,12 @@ def test_fft_roundtrip_and_parity(ib, rng, sizes, nst, impl):
 @pytest.mark.parametrize("mixed_compute", [1, 0])
 @pytest.mark.parametrize("impl", [0, 1])
 @pytest.mark.parametrize("sizes,nst", [((48, 40, 36), 64), ((96, 96, 96), 32), ((24, 32, 72), 40),
-                                       ((96, 96, 96), 64), ((40, 48, 120), 72)])
+                                       ((96, 96, 96), 64), ((40, 48, 120), 72), ((96, 96, 96), 33),
+                                       ((72, 64, 48), 65), ((24, 120, 40), 127)])
 def test_fft_mixed_precision_kernels(ib, rng, sizes, nst, impl, mixed_compute):
     """FP32 transforms through both kernels: relative error <= 2e-6 against the FP64 oracle (64 and 72
-    states: the 512-byte-row streaming passes, the second tile of 72 states partly outside the set)."""
+    states: the 512-byte-row streaming passes, the second tile of 72 states partly outside the set; an
+    odd number of states: rows that are not 16-byte multiples, copied by the producer warp)."""
     rs = ib.RealSpace(ib.Cell.cubic(10.0), sizes=sizes)
     rs.ctx.set_option("fft_impl", impl)
     rs.ctx.set_option("mixed_compute", mixed_compute)
@@ -242,6 +244,34 @@ def test_hamiltonian_kernels_both_paths(ib, c1big, impl):
         basis.ctx.synchronize()
     finally:
         basis.ctx.set_option("fft_impl", 0)
+
+
+@pytest.mark.parametrize("nst", [33, 65, 97])
+def test_hamiltonian_odd_state_count_single(ib, nst):
+    """Mixed-form H|psi> of an odd number of states (rows of 8 mod 16 bytes, which TMA cannot move: the
+    producer warp copies them with 8-byte cp.async) against the oracle, 2e-6 relative, with k and A, and
+    within 1e-6 of the same states inside an even-sized set (whose 16-byte rows take the bulk-copy
+    nonlocal apply, which fuses its complex multiply-adds)."""
+    from inq_b200 import synthetic
+    sysm = synthetic.config("c1", nst=nst + 1)
+    basis, ham, phi = synthetic.build(sysm)
+    oh, ors = _oracle_system(sysm, A=(0.03, 0.0, -0.01))
+    ham.uniform_vector_potential = np.array([0.03, 0.0, -0.01])
+    try:
+        x = phi.hypercubic()[..., :nst]
+        kp = (0.1, -0.2, 0.05)
+        h = ham(ib.OrbitalSet.from_array(basis, x, kpoint=kp, precision=ib.F32)).hypercubic()
+        assert rel(h, oh.apply_real(x, kp)) < TOL32
+        h_even = ham(ib.OrbitalSet.from_array(basis, phi.hypercubic(), kpoint=kp, precision=ib.F32)).hypercubic()
+        assert rel(h, h_even[..., :nst]) < 1e-6
+        # a real-time step runs through the same passes (Horner steps and the kept Taylor terms)
+        p = ib.OrbitalSet.from_array(basis, x, kpoint=kp, precision=ib.F32)
+        occ = np.full(nst, 2.0)
+        dens, dip, iters = ib.etrs(ham, [p], [occ], 0.01, want_density=True)
+        ref, rdens, riters = O.etrs_step(oh, [x], [occ], 0.01, kpoints=[kp])
+        assert rel(p.hypercubic(), ref[0]) < 1e-5
+    finally:
+        ham.uniform_vector_potential = np.zeros(3)
 
 
 def test_hamiltonian_deterministic(ib, c1):
