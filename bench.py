@@ -304,6 +304,15 @@ def serving_leg(ctx, rates=(10.0, 50.0, 200.0, 1000.0, 2000.0), nreq=120, slots=
         out[f"{int(rate)}_req_s"] = {k: st[k] for k in ("completed", "rejected", "throughput_req_s",
                                                         "state_applications_per_s", "p50_ms", "p99_ms", "max_ms",
                                                         "by_size", "mean_phase_ms", "slowest_5pct_phase_ms")}
+    # sustained capacity: the same mix with every request present at the start (the server is never idle),
+    # then the latency at half and at 80 % of that rate, where the queue stays bounded
+    st = srv.run(serving.poisson_requests(pool, nreq, 1e9, seed=1, large=large))
+    cap = st["throughput_req_s"]
+    out["capacity"] = {"throughput_req_s": cap, "state_applications_per_s": st["state_applications_per_s"]}
+    for frac in (0.5, 0.8):
+        st = srv.run(serving.poisson_requests(pool, nreq, frac * cap, seed=2, large=large))
+        out["capacity"][f"at_{int(frac * 100)}pct"] = {"rate_req_s": frac * cap, "p50_ms": st["p50_ms"],
+                                                        "p99_ms": st["p99_ms"], "completed": st["completed"]}
     srv.close()
     return out
 
@@ -643,6 +652,7 @@ def run_ours(args):
         if "serving" in legs:
             line["serving_p50_ms"] = legs["serving"]["50_req_s"]["p50_ms"]
             line["serving_p99_ms"] = legs["serving"]["50_req_s"]["p99_ms"]
+            line["serving_capacity_req_s"] = legs["serving"]["capacity"]["throughput_req_s"]
         if cpu is not None:
             line["cpu_baseline"] = cpu
         # the figures the headline comparison rests on come last, so that a reader of the end of the line

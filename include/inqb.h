@@ -351,9 +351,10 @@ int inqb_density(inqb_orbitals *const *phis, int nsets, const double *const *occ
 int inqb_kick(inqb_orbitals *phi, const double efield_cart[3]);
 /* observables::dipole(density) (dipole.hpp:24-40) of a host density [npoint]: dV sum r n(r). */
 int inqb_dipole(const inqb_basis *basis, const double *density_host, double dipole[3]);
-/* One ETRS step (real_time/etrs.hpp:22-79) with a fixed Hamiltonian (no self-consistent
- * potential update): all sets advanced by dt; returns the density [npoint] (host, may be
- * NULL), the electronic dipole (may be NULL) and the number of SCF iterations taken. */
+/* One ETRS step (real_time/etrs.hpp:22-79): all sets advanced by dt; returns the density [npoint]
+ * (host or device memory of the context's device, may be NULL), the electronic dipole (may be NULL)
+ * and the number of SCF iterations taken.  A Hamiltonian with an interaction
+ * (inqb_hamiltonian_set_interaction) is rebuilt from every density the step forms. */
 int inqb_etrs_step(const inqb_hamiltonian *ham, inqb_orbitals *const *phis, int nsets,
                    const double *const *occupations, double dt, int nscf_max, double scf_threshold,
                    double *density_host, double dipole[3], int *iterations);

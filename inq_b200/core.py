@@ -25,7 +25,7 @@ from typing import Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import F32, F64, FOURIER_SPACE, REAL_SPACE, check, dptr
+from ._lib import DP, F32, F64, FOURIER_SPACE, REAL_SPACE, check, dptr
 
 # ---------------------------------------------------------------- context
 
@@ -771,15 +771,25 @@ def apply_phase_kick(phi: OrbitalSet, efield_cart):
 
 
 def etrs(ham: KSHamiltonian, phis: Sequence[OrbitalSet], occupations: Sequence, dt: float, nscf: int = 5,
-         scf_threshold: float = 5e-5, want_density: bool = False):
+         scf_threshold: float = 5e-5, want_density: bool = False, density_out=None):
     """One ETRS step (real_time/etrs.hpp:22-79); a Hamiltonian with an interaction
     (KSHamiltonian.set_interaction) is rebuilt from every density the step forms.
 
-    Returns (density or None, electronic dipole [3], number of SCF iterations)."""
+    Returns (density or None, electronic dipole [3], number of SCF iterations).  ``density_out``, a
+    float64 CUDA tensor of basis.size() elements, receives the density on the device instead (and is
+    returned in its place)."""
     hs, optrs, keep = _ptr_arrays(phis, occupations)
-    dens = np.zeros(phis[0].basis.size()) if want_density else None
     dip = np.zeros(3)
     iters = C.c_int()
+    if density_out is not None:
+        n = phis[0].basis.size()
+        if not (density_out.is_cuda and density_out.is_contiguous() and density_out.numel() == n
+                and str(density_out.dtype) == "torch.float64"):
+            raise ValueError("density_out must be a contiguous float64 CUDA tensor of basis.size() elements")
+        dens, dens_ptr = density_out, C.cast(C.c_void_p(density_out.data_ptr()), DP)
+    else:
+        dens = np.zeros(phis[0].basis.size()) if want_density else None
+        dens_ptr = dptr(dens) if dens is not None else None
     ham.ctx.check(ham.ctx.lib.inqb_etrs_step(ham.handle, hs, len(phis), optrs, float(dt), int(nscf), float(scf_threshold),
-                                             dptr(dens) if dens is not None else None, dptr(dip), C.byref(iters)))
+                                             dens_ptr, dptr(dip), C.byref(iters)))
     return dens, dip, iters.value

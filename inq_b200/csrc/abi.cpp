@@ -1979,7 +1979,8 @@ int inqb_density(inqb_orbitals *const *phis, int nsets, const double *const *occ
     const Basis &b = *phis[0]->basis;
     double *d = static_cast<double *>(dev_alloc(*ctx, sizeof(double) * b.npoints));
     density_dev(*ctx, phis, nsets, occ, d);
-    INQB_CUDA(cudaMemcpyAsync(density_host, d, sizeof(double) * b.npoints, cudaMemcpyDeviceToHost, ctx->stream));
+    // host or device output (cudaMemcpyDefault: the direction from the pointer)
+    INQB_CUDA(cudaMemcpyAsync(density_host, d, sizeof(double) * b.npoints, cudaMemcpyDefault, ctx->stream));
     dev_free(*ctx, d);
     INQB_CUDA(cudaStreamSynchronize(ctx->stream));
   });
@@ -2134,12 +2135,14 @@ int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int n
       if (delta < scf_threshold || iscf == nscf_max - 1) break;
     }
     if (iterations) *iterations = it;
-    if (density_host || dipole) {
+    // the density goes to a host or a device buffer (cudaMemcpyDefault: the direction from the pointer)
+    if (density_host)
+      INQB_CUDA(cudaMemcpyAsync(density_host, dens, sizeof(double) * b.npoints, cudaMemcpyDefault, ctx.stream));
+    if (dipole) {
       std::vector<double> hd(size_t(b.npoints));
       INQB_CUDA(cudaMemcpyAsync(hd.data(), dens, sizeof(double) * b.npoints, cudaMemcpyDeviceToHost, ctx.stream));
       INQB_CUDA(cudaStreamSynchronize(ctx.stream));
-      if (density_host) std::copy(hd.begin(), hd.end(), density_host);
-      if (dipole) dipole_host(b, hd.data(), dipole);
+      dipole_host(b, hd.data(), dipole);
     }
     dev_free(ctx, dens);
     dev_free(ctx, old);

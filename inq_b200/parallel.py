@@ -68,12 +68,27 @@ def sharded_density(local_density: np.ndarray, group=None, device=None) -> np.nd
 def sharded_etrs_step(ham, phi_local, occ_local, dt: float, basis, group=None, device=None):
     """One ETRS step on this rank's block of states, then the global density and dipole.
 
-    With the fixed Hamiltonian of the synthetic configurations the states evolve
-    independently, so the only exchange is the density sum."""
+    With the fixed Hamiltonian of the synthetic configurations the states evolve independently, so the
+    only exchanges are the density sum (density.hpp:99) and the sum of the dipoles, which are linear in
+    the density.  With NCCL the step writes its density into a device tensor and the all-reduce runs on
+    it in place: the density never leaves the device (returned as that tensor).  Other backends add
+    host arrays."""
+    import torch
+    import torch.distributed as dist
     from . import core
-    dens_local, _, iters = core.etrs(ham, [phi_local], [occ_local], dt, want_density=True)
+    nccl = dist.is_initialized() and dist.get_backend(group) == "nccl"
+    if nccl:
+        dev = torch.device("cuda", ham.ctx.device)
+        dens = torch.empty(basis.size(), dtype=torch.float64, device=dev)
+        _, dip, iters = core.etrs(ham, [phi_local], [occ_local], dt, density_out=dens)
+        dipt = torch.as_tensor(dip, dtype=torch.float64, device=dev)
+        # the step returned after its stream finished, so the tensors are complete for the collective
+        dist.all_reduce(dens, op=dist.ReduceOp.SUM, group=group)
+        dist.all_reduce(dipt, op=dist.ReduceOp.SUM, group=group)
+        return dens, dipt.cpu().numpy(), iters
+    dens_local, dip_local, iters = core.etrs(ham, [phi_local], [occ_local], dt, want_density=True)
     dens = sharded_density(dens_local, group, device)
-    return dens, core.dipole(basis, dens), iters
+    return dens, allreduce_sum(dip_local, group, device), iters
 
 
 class _DeviceWords:

@@ -1,6 +1,6 @@
-"""GPU tests of the state-parallel overlap, rotation, orthogonalisation and subspace diagonalisation
-(overlap.hpp:42-56, rotate.hpp:27-142, orthogonalize.hpp:25-31, subspace_diagonalization.hpp:21-29)
-through the device kernels.
+"""GPU tests of the state-parallel overlap, rotation, orthogonalisation, subspace diagonalisation and
+ETRS step (overlap.hpp:42-56, rotate.hpp:27-142, orthogonalize.hpp:25-31, subspace_diagonalization.hpp:21-29,
+density.hpp:99) through the device kernels.
 
 One GPU is available per run, so: the rectangular rotation kernel against numpy; the NCCL path (device
 buffers viewed in place, collectives ordered on the context's stream) with one rank; and two ranks as
@@ -76,6 +76,16 @@ def test_state_parallel_nccl_one_rank():
         w = parallel.sharded_subspace_diagonalization(ham, phi, part)
         assert np.max(np.abs(w - w_ref)) <= 1e-13 * np.max(np.abs(w_ref))
         assert np.max(np.abs(phi.matrix() - single.matrix())) <= 1e-12 * np.max(np.abs(single.matrix()))
+        # the state-sharded ETRS step: the density stays on the device and is all-reduced there
+        occ = np.full(10, 2.0)
+        a, b = phi.copy(), phi.copy()
+        dens, dip, it = parallel.sharded_etrs_step(ham, a, occ, 0.01, rs)
+        assert isinstance(dens, torch.Tensor) and dens.is_cuda
+        dref, dipref, itref = ib.etrs(ham, [b], [occ], 0.01, want_density=True)
+        assert it == itref
+        assert np.array_equal(dens.cpu().numpy(), dref)
+        assert np.max(np.abs(dip - dipref)) <= 1e-13 * np.max(np.abs(dipref))
+        assert np.array_equal(a.matrix(), b.matrix())
         torch.cuda.synchronize()
     finally:
         dist.destroy_process_group()
@@ -104,7 +114,11 @@ def _rank_main(rank, world, port, nst, out):
         parallel.sharded_orthogonalize(phi, part)
         orth = phi.hypercubic()
         w = parallel.sharded_subspace_diagonalization(_hamiltonian(rs), phi, part)
-        out[rank] = (part.start, part.end, S, orth, w, phi.hypercubic())
+        # the state-sharded ETRS step over gloo (host arrays): global density and dipole on every rank
+        occ = np.linspace(0.5, 2.0, nst)[part.start:part.end]
+        p2 = ib.OrbitalSet.from_array(rs, psi[..., part.start:part.end])
+        dens, dip, _ = parallel.sharded_etrs_step(_hamiltonian(rs), p2, occ, 0.01, rs)
+        out[rank] = (part.start, part.end, S, orth, w, phi.hypercubic(), dens, dip)
     finally:
         dist.destroy_process_group()
 
@@ -131,8 +145,12 @@ def test_state_parallel_two_ranks_one_gpu():
     w_ref = ham.subspace_diagonalization(phi)
     got = np.zeros_like(ref)
     sub = np.zeros_like(ref)
+    single = ib.OrbitalSet.from_array(rs, psi)
+    dref, dipref, _ = ib.etrs(ham, [single], [np.linspace(0.5, 2.0, nst)], 0.01, want_density=True)
     for r in range(world):
-        a, b, S, blk, w, sb = out[r]
+        a, b, S, blk, w, sb, dens, dip = out[r]
+        assert np.max(np.abs(dens - dref)) <= 1e-12 * np.max(np.abs(dref))
+        assert np.max(np.abs(dip - dipref)) <= 1e-11 * np.max(np.abs(dipref))
         assert np.max(np.abs(S - S_ref)) <= 1e-13 * np.max(np.abs(S_ref))
         assert np.max(np.abs(w - w_ref)) <= 1e-12 * np.max(np.abs(w_ref))
         got[..., a:b] = blk
