@@ -673,8 +673,8 @@ def run_ours(args):
 
 
 def run_profile_case(args):
-    """Small case for ncu captures: the C2 grid and atoms with ``--profile-states`` orbitals (32: 226 MB
-    per FP32 set, above L2; 128: 0.9 GB).
+    """Small case for ncu captures: the C2 (or, with ``--profile-config c3``, C3) grid and atoms with
+    ``--profile-states`` orbitals (C2, 32 states: 226 MB per FP32 set, above L2; 128: 0.9 GB).
 
     Sequence: FP64 build (3 FFT passes), then ``--steps`` mixed-form and ``--steps`` FP64 applications
     (each: 1 projection + 5 FFT passes + 1 nonlocal apply), then ``--steps`` tensor-core overlaps of the
@@ -682,7 +682,7 @@ def run_profile_case(args):
     import inq_b200 as ib
     from inq_b200 import synthetic
     S = args.profile_states
-    sysm = synthetic.config("c2", nst=S)
+    sysm = synthetic.config(args.profile_config, nst=S)
     basis, ham, phi64 = synthetic.build(sysm)
     phi32 = phi64.converted(ib.F32)
     out32, out64 = phi32.skeleton(), phi64.skeleton()
@@ -693,7 +693,7 @@ def run_profile_case(args):
     for _ in range(args.steps):
         ib.overlap(phi32)
     basis.ctx.synchronize()
-    print(json.dumps({"profile_case": f"c2 grid, {S} states", "launches": basis.ctx.launch_count()}))
+    print(json.dumps({"profile_case": f"{args.profile_config} grid, {S} states", "launches": basis.ctx.launch_count()}))
 
 
 def main():
@@ -708,6 +708,8 @@ def main():
     ap.add_argument("--etrs-dt", type=float, default=0.005, help="time step of the 120^3 real-time leg (a.u.)")
     ap.add_argument("--profile-case", action="store_true", help="small workload for ncu captures")
     ap.add_argument("--profile-states", type=int, default=32, help="orbitals of the --profile-case workload")
+    ap.add_argument("--profile-config", default="c2", choices=["c2", "c3"],
+                    help="grid and atoms of the --profile-case workload (96^3 / 64 atoms or 120^3 / 128 atoms)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
