@@ -75,7 +75,11 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * states through shared memory with bulk asynchronous copies), 1 (those forms wherever a row is a
  * multiple of 16 bytes) or -1 (never: register-held gathers); "fft_wide" = 1 (default: the plain streaming
  * FFT passes of single-precision sets of at least 64 states move 512-byte rows, 64 states, in three
- * stages at one CTA per SM) or 0 (256-byte rows, 32 states, as the other passes).  Changing the priority replaces
+ * stages at one CTA per SM, unless 64-state tiles would leave more than 8 more empty states in a line's
+ * last tile than 32-state tiles) or 0 (256-byte rows, 32 states, as the other passes);
+ * "nl_apply_points" = 0 (default: 8) or 1..32 hit points per batch of the bulk-copy nonlocal apply;
+ * "nl_project_points" = 0 (default: about 16 KB of rows) or 1..32 sphere points per stage of the
+ * bulk-copy projection.  Changing the priority replaces
  * the context's stream (after the work queued on it), so callers query inqb_ctx_stream again. */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Self-test of the bounded device-side waits: queues one kernel whose wait on an mbarrier phase that
@@ -151,6 +155,12 @@ int inqb_laplacian(const inqb_orbitals *in, inqb_orbitals *out, double factor, c
  * scalar potential zero, no projectors, exchange disabled. */
 int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, inqb_hamiltonian **out);
 int inqb_hamiltonian_destroy(inqb_hamiltonian *ham);
+/* Kernel-choice options of this Hamiltonian's applications: fft_impl, fft_stages, fft_wide, nl_bulk,
+ * nl_apply_points and nl_project_points (meanings as in inqb_ctx_set_option) take `value` while an
+ * operator application through this Hamiltonian is queued, whatever the context's setting; a negative
+ * value (other than nl_bulk's -1) removes the override.  Lets one batch (inqb_batch_apply) run every
+ * system with the options tuned for its shape.  No counterpart in the reference. */
+int inqb_hamiltonian_set_option(inqb_hamiltonian *ham, const char *key, long long value);
 /* ks_hamiltonian::scalar_potential() assignment; V is host [npoint][nspin] float64. */
 int inqb_potential_set(inqb_hamiltonian *ham, const double *V);
 /* ks_hamiltonian::uniform_vector_potential() assignment (covariant, ks_hamiltonian.hpp:259-264). */

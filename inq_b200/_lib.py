@@ -65,6 +65,7 @@ SIGNATURES = {
     "inqb_laplacian": (I, [P, P, D, DP]),
     "inqb_hamiltonian_create": (I, [P, P, I, C.POINTER(P)]),
     "inqb_hamiltonian_destroy": (I, [P]),
+    "inqb_hamiltonian_set_option": (I, [P, C.c_char_p, LL]),
     "inqb_potential_set": (I, [P, DP]),
     "inqb_vector_potential_set": (I, [P, DP]),
     "inqb_hamiltonian_set_interaction": (I, [P, DP, I, I]),

@@ -11,9 +11,10 @@ systems on one context:
   (``inqb_graph_capture_*``) which :meth:`Batch.launch` replays with a single
   launch per batch.
 
-:func:`autotune` picks, per system shape, the FFT kernel options (specialised TMA
-kernel or generic kernel, shared-memory ring depth) by timing them with CUDA events
-on the context's stream; :class:`Batch` groups systems by their tuned options.
+:func:`autotune` picks, per system shape, the kernel options (specialised TMA or generic
+FFT kernel, FFT row width and ring depth, nonlocal kernel form and batch sizes) by coordinate
+descent over CUDA-event timings on the context's stream, and sets them on each system's
+Hamiltonian, so one batched call runs every system with its own options.
 """
 
 from __future__ import annotations
@@ -24,12 +25,18 @@ from dataclasses import dataclass, field
 from . import _lib
 from .core import Context, KSHamiltonian, OrbitalSet
 
-DEFAULT_OPTIONS = {"fft_impl": 0, "fft_stages": 0}
+DEFAULT_OPTIONS = {"fft_impl": 0, "fft_wide": 1, "fft_stages": 0, "nl_bulk": 0, "nl_apply_points": 0,
+                   "nl_project_points": 0}
 
-
-def _apply_options(ctx: Context, opts: dict):
-    for k, v in opts.items():
-        ctx.set_option(k, v)
+# The knobs the autotuner searches, each with its candidate values (the first is the default):
+#   fft_impl           specialised persistent TMA kernels (0) or the generic kernel (1)
+#   fft_wide           512-byte (64-state) rows in the single-precision streaming passes (1) or 256-byte (0)
+#   fft_stages         ring depth of the TMA passes (0: from their shared-memory budget)
+#   nl_bulk            bulk-copy nonlocal kernels by size (0), wherever rows allow (1), never (-1)
+#   nl_apply_points    hit points per batch of the bulk-copy nonlocal apply (0: 8)
+#   nl_project_points  sphere points per stage of the bulk-copy projection (0: about 16 KB of rows)
+SEARCH_SPACE = (("fft_impl", (0, 1)), ("fft_wide", (1, 0)), ("fft_stages", (0, 2, 3, 4)), ("nl_bulk", (0, 1, -1)),
+                ("nl_apply_points", (0, 4, 16)), ("nl_project_points", (0, 4, 8, 16)))
 
 
 @dataclass
@@ -59,32 +66,46 @@ def _time_apply(ctx: Context, ham: KSHamiltonian, phi: OrbitalSet, out: OrbitalS
     return e0.elapsed_time(e1) / reps
 
 
-def autotune(systems, tuning: Tuning | None = None, reps: int = 3,
-             candidates=({"fft_impl": 0, "fft_stages": 0}, {"fft_impl": 0, "fft_stages": 2},
-                         {"fft_impl": 0, "fft_stages": 4}, {"fft_impl": 1, "fft_stages": 0})) -> Tuning:
-    """Time every candidate option set on one representative of each system shape.
+def _set_all(ham: KSHamiltonian, opts: dict):
+    for k, v in opts.items():
+        ham.set_option(k, v)
 
-    ``systems`` is a sequence of (ham, phi) pairs.  Candidates that a shape cannot use
-    (for example a ring too deep for shared memory) are skipped."""
+
+def autotune(systems, tuning: Tuning | None = None, reps: int = 3, search=SEARCH_SPACE,
+             min_gain: float = 0.02) -> Tuning:
+    """Per system shape, choose the kernel options by coordinate descent: each knob of ``search`` in turn
+    takes the candidate value that times fastest with the other knobs at their best so far (a candidate
+    must beat the current choice by ``min_gain`` relative).  Times are CUDA-event times of H applications
+    on the context's stream.
+
+    ``systems`` is a sequence of (ham, phi) pairs.  The result is stored in ``tuning`` and set on each
+    Hamiltonian as its option overrides (inqb_hamiltonian_set_option), so a batch runs every system with
+    its own options in one call.  Candidates a shape cannot use (a ring too deep for shared memory, for
+    example) are skipped."""
     tuning = tuning or Tuning()
     for ham, phi in systems:
         key = tuning.key(phi)
-        if key in tuning.table:
-            continue
-        ctx = ham.ctx
-        out = phi.skeleton()
-        best, best_ms = None, float("inf")
-        for cand in candidates:
-            try:
-                _apply_options(ctx, cand)
-                ms = _time_apply(ctx, ham, phi, out, reps)
-            except _lib.InqbError:
-                continue
-            finally:
-                _apply_options(ctx, DEFAULT_OPTIONS)
-            if ms < best_ms:
-                best, best_ms = dict(cand), ms
-        tuning.table[key] = best or dict(DEFAULT_OPTIONS)
+        if key not in tuning.table:
+            ctx = ham.ctx
+            out = phi.skeleton()
+            best = dict(DEFAULT_OPTIONS)
+            _set_all(ham, best)
+            best_ms = _time_apply(ctx, ham, phi, out, reps)
+            for knob, values in search:
+                for v in values:
+                    if v == best[knob]:
+                        continue
+                    cand = dict(best)
+                    cand[knob] = v
+                    try:
+                        _set_all(ham, cand)
+                        ms = _time_apply(ctx, ham, phi, out, reps)
+                    except _lib.InqbError:
+                        continue
+                    if ms < best_ms * (1.0 - min_gain):
+                        best, best_ms = cand, ms
+            tuning.table[key] = best
+        _set_all(ham, tuning.table[key])
     return tuning
 
 
@@ -96,24 +117,21 @@ class Batch:
         self.ctx = ctx
         self.nstreams = nstreams
         self.tuning = tuning
-        # group systems by their kernel options (options are per context, so each group is one call)
-        groups: dict = {}
-        for h, i, o in zip(hams, ins, outs):
-            opts = tuning.options(i) if tuning else dict(DEFAULT_OPTIONS)
-            groups.setdefault(tuple(sorted(opts.items())), []).append((h, i, o))
-        self.groups = [(dict(k), v) for k, v in groups.items()]
+        # every system runs with its own Hamiltonian's option overrides (set by autotune), so the whole
+        # batch is one fork/join call
+        if tuning is not None:
+            for h, i in zip(hams, ins):
+                _set_all(h, tuning.options(i))
+        self.members = list(zip(hams, ins, outs))
         self.graph = None
 
     def _call(self):
         lib = self.ctx.lib
-        for opts, members in self.groups:
-            _apply_options(self.ctx, opts)
-            n = len(members)
-            hs = (C.c_void_p * n)(*[m[0].handle.value for m in members])
-            ins = (C.c_void_p * n)(*[m[1].handle.value for m in members])
-            outs = (C.c_void_p * n)(*[m[2].handle.value for m in members])
-            self.ctx.check(lib.inqb_batch_apply(self.ctx.handle, n, hs, ins, outs, self.nstreams))
-        _apply_options(self.ctx, DEFAULT_OPTIONS)
+        n = len(self.members)
+        hs = (C.c_void_p * n)(*[m[0].handle.value for m in self.members])
+        ins = (C.c_void_p * n)(*[m[1].handle.value for m in self.members])
+        outs = (C.c_void_p * n)(*[m[2].handle.value for m in self.members])
+        self.ctx.check(lib.inqb_batch_apply(self.ctx.handle, n, hs, ins, outs, self.nstreams))
 
     def apply(self):
         """Eager batched application (asynchronous on the context's stream)."""

@@ -413,6 +413,11 @@ class KSHamiltonian:
         self.handle = h
         self._A = np.zeros(3)
 
+    def set_option(self, key: str, value: int):
+        """Kernel-option override for this Hamiltonian's applications (inqb_hamiltonian_set_option);
+        a negative value (other than nl_bulk's -1) removes it."""
+        self.ctx.check(self.ctx.lib.inqb_hamiltonian_set_option(self.handle, key.encode(), int(value)))
+
     # scalar_potential() (ks_hamiltonian.hpp:252-254): [npoint][nspin] float64
     def set_scalar_potential(self, V):
         v = np.ascontiguousarray(np.asarray(V, dtype=np.float64).reshape(self.basis.size(), self.nspin))

@@ -250,7 +250,46 @@ template <typename R> void apply_fourier(Hamiltonian &h, const Orbitals &in, Orb
   launch_fft_pass<R>(ctx, b, c, PRO_NONE, EPI_LAPL_ADD);
 }
 
+// The options that choose kernels and their shapes, settable on a context and overridable per
+// Hamiltonian (inqb_hamiltonian_set_option); nullptr for other keys.
+int *kernel_option(Ctx &ctx, const std::string &k) {
+  if (k == "fft_impl") return &ctx.fft_impl;
+  if (k == "fft_stages") return &ctx.fft_stages;
+  if (k == "fft_wide") return &ctx.fft_wide;
+  if (k == "nl_bulk") return &ctx.nl_bulk;
+  if (k == "nl_apply_points") return &ctx.nl_apply_points;
+  if (k == "nl_project_points") return &ctx.nl_project_points;
+  return nullptr;
+}
+void check_kernel_option(const std::string &k, long long value) {
+  if (k == "fft_impl") INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_impl is 0 (specialised) or 1 (generic)");
+  if (k == "fft_stages") INQB_REQUIRE(value >= 0 && value <= 8, INQB_ERR_ARG, "fft_stages is 0 (automatic) or 1..8");
+  if (k == "fft_wide") INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_wide is 0 (256-byte rows) or 1 (512-byte rows)");
+  if (k == "nl_bulk")
+    INQB_REQUIRE(value >= -1 && value <= 1, INQB_ERR_ARG, "nl_bulk is 0 (automatic), 1 (always) or -1 (never)");
+  if (k == "nl_apply_points" || k == "nl_project_points")
+    INQB_REQUIRE(value >= 0 && value <= 32, INQB_ERR_ARG, k + " is 0 (automatic) or 1..32");
+}
+
+// The Hamiltonian's kernel-option overrides (inqb_hamiltonian_set_option) in force on its context for
+// the lifetime of the scope: every launch of an operator application reads them.
+struct OptionScope {
+  Ctx &ctx;
+  std::vector<std::pair<int *, int>> saved;
+  explicit OptionScope(Hamiltonian &h) : ctx(*h.ctx) {
+    for (const auto &kv : h.opt_overrides) {
+      int *f = kernel_option(ctx, kv.first);
+      saved.emplace_back(f, *f);
+      *f = kv.second;
+    }
+  }
+  ~OptionScope() {
+    for (auto it = saved.rbegin(); it != saved.rend(); ++it) *it->first = it->second;
+  }
+};
+
 void apply_any(Hamiltonian &h, const Orbitals &in, Orbitals &out, const Horner &hz = Horner()) {
+  OptionScope scope(h);
   check_same_shape(in, out);
   INQB_REQUIRE(in.basis == h.basis, INQB_ERR_ARG, "orbitals and Hamiltonian live on different bases");
   INQB_REQUIRE(in.data != out.data, INQB_ERR_ARG, "H|psi> needs distinct input and output sets");
@@ -905,24 +944,15 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
   return guarded(ctx, [&] {
     INQB_REQUIRE(ctx && key, INQB_ERR_ARG, "null argument");
     const std::string k(key);
-    if (k == "fft_impl") {
-      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_impl is 0 (specialised) or 1 (generic)");
-      ctx->fft_impl = int(value);
-    } else if (k == "fft_stages") {
-      INQB_REQUIRE(value >= 0 && value <= 8, INQB_ERR_ARG, "fft_stages is 0 (automatic) or 1..8");
-      ctx->fft_stages = int(value);
+    if (int *field = kernel_option(*ctx, k)) {
+      check_kernel_option(k, value);
+      *field = int(value);
     } else if (k == "mixed_compute") {
       INQB_REQUIRE(value >= 0 && value <= 3, INQB_ERR_ARG, "mixed_compute is 0, 1, 2 or 3");
       ctx->mixed_compute = int(value);
     } else if (k == "overlap_tc") {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "overlap_tc is 0 (FP64 SIMT) or 1 (tensor cores)");
       ctx->overlap_tc = int(value);
-    } else if (k == "nl_bulk") {
-      INQB_REQUIRE(value >= -1 && value <= 1, INQB_ERR_ARG, "nl_bulk is 0 (automatic), 1 (always) or -1 (never)");
-      ctx->nl_bulk = int(value);
-    } else if (k == "fft_wide") {
-      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_wide is 0 (256-byte rows) or 1 (512-byte rows)");
-      ctx->fft_wide = int(value);
     } else if (k == "grid_sms") {
       INQB_REQUIRE(value >= 0 && value <= ctx->device_sms, INQB_ERR_ARG,
                    "grid_sms is 0 (every SM) or 1.." + std::to_string(ctx->device_sms));
@@ -949,6 +979,29 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     } else {
       throw Error(INQB_ERR_ARG, "unknown option " + k);
     }
+  });
+}
+
+int inqb_hamiltonian_set_option(inqb_hamiltonian *h, const char *key, long long value) {
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && key, INQB_ERR_ARG, "null argument");
+    const std::string k(key);
+    INQB_REQUIRE(kernel_option(*h->ctx, k) != nullptr, INQB_ERR_ARG,
+                 "a Hamiltonian overrides fft_impl, fft_stages, fft_wide, nl_bulk, nl_apply_points and "
+                 "nl_project_points only (got " + k + ")");
+    if (value < 0 && k != "nl_bulk") {
+      // a negative value removes the override (the context's value applies again)
+      for (size_t i = 0; i < h->opt_overrides.size(); i++)
+        if (h->opt_overrides[i].first == k) h->opt_overrides.erase(h->opt_overrides.begin() + long(i));
+      return;
+    }
+    check_kernel_option(k, value);
+    for (auto &kv : h->opt_overrides)
+      if (kv.first == k) {
+        kv.second = int(value);
+        return;
+      }
+    h->opt_overrides.emplace_back(k, int(value));
   });
 }
 

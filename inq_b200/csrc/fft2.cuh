@@ -1236,7 +1236,10 @@ void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var)
   if constexpr (sizeof(R) == 4) {
     const bool single = single_arith(ctx, a, var);
     if (single) {
-      const bool wide = ctx.fft_wide && a.S >= 64 && wide_var(var);
+      // 64-state tiles unless they would leave more of the last tile empty than 32-state tiles do
+      // (85 states: 43 empty slots against 11)
+      const int pad64 = (64 - a.S % 64) % 64, pad32 = (32 - a.S % 32) % 32;
+      const bool wide = ctx.fft_wide && a.S >= 64 && wide_var(var) && pad64 <= pad32 + 8;
       launch_nc<R, float, N>(ctx, b, a, gg, var, wide);
       return;
     }

@@ -76,6 +76,8 @@ struct Ctx {
   int overlap_tc = 1;        // overlaps of single-precision sets on the tensor cores (split BF16)
   int nl_bulk = 0;           // nonlocal kernels: 0 automatic, 1 bulk-copy forms wherever they apply, -1 never
   int fft_wide = 1;          // single-precision FFT passes without a second input: 512-byte rows (64 states)
+  int nl_apply_points = 0;   // hit points per batch of the bulk-copy nonlocal apply (0: 8)
+  int nl_project_points = 0; // sphere points per stage of the bulk-copy projection (0: about 16 KB of rows)
   int stream_priority = 0;   // 0: the device's lowest stream priority, 1: its highest
   void *noalloc_partial = nullptr;  // device address of noalloc.cu's fixed partial-sum array on this device
 };
@@ -173,6 +175,8 @@ struct Hamiltonian {
   // what the last device-side projector build was made of (for moving the atoms); natoms 0: none
   int dev_natoms = 0;
   DeviceProjectorSpec dev_spec;
+  // kernel-option overrides (key, value) applied to the context while this Hamiltonian is applied
+  std::vector<std::pair<std::string, int>> opt_overrides;
 };
 
 void free_projectors(Projectors &P, cudaStream_t st);

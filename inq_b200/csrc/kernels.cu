@@ -383,7 +383,7 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   if (bulk) {
     const int SCmax = std::min(NLA_NT * JB, S);
     const size_t srow = size_t(SCmax) * sizeof(C2<R>);
-    int KB = int(16384 / srow);  // about 16 KB of rows per stage
+    int KB = ctx.nl_project_points > 0 ? ctx.nl_project_points : int(16384 / srow);  // about 16 KB of rows per stage
     KB = KB < 1 ? 1 : (KB > 32 ? 32 : KB);
     const size_t abytes = dbl ? sizeof(double2) : sizeof(float2);
     const size_t smem = size_t(NLP_NS) * KB * srow + size_t(NLP_NS) * KB * 4 * abytes + 2 * NLP_NS * sizeof(uint64_t) + 16;
@@ -672,6 +672,7 @@ void launch_nl_apply(Ctx &ctx, const Hamiltonian &h, const C2<R> *projD, int S, 
     // 16 / 4 points and 466 / 562 with 32 / 16), fewer when a stage would pass 48 KB
     int KB = int(49152 / row_bytes);
     KB = KB < 1 ? 1 : (KB > 8 ? 8 : KB);
+    if (ctx.nl_apply_points > 0) KB = ctx.nl_apply_points;
     const size_t smem = size_t(NLA_NS) * KB * row_bytes + NLA_KMAX * 4 * sizeof(C2<R>) + NLA_NS * NLA_KMAX * sizeof(int4) +
                         2 * NLA_NS * sizeof(uint64_t) + 16;
     if (smem <= size_t(ctx.max_smem_optin)) {
