@@ -1639,23 +1639,12 @@ int inqb_apply_host(const inqb_hamiltonian *hc, int nst, const double kpoint_cov
     const size_t npts = size_t(h->basis->npoints);
     int B = block_states > 0 ? block_states : int(512 / cs);  // 512-byte rows of a block by default
     if (B > nst) B = nst;
-    // block boundaries: with the default size, the first and the last block hold half a block (256-byte
-    // rows), which shortens the upload before the first operator and the download after the last one;
-    // in between both copy directions run at once (96^3 x 256 single: 48 GB/s each way with rows of 512
-    // bytes or more, 44 GB/s with 256-byte rows, 56 GB/s for one direction alone)
+    // block boundaries: blocks of B states, the last one shorter.  Measured at 96^3 x 256 single (box to box
+    // 45-51 ms per call): neither a half-size first and last block nor quarter-size last blocks did better
+    // than equal 64-state blocks; rows of 128 bytes download at 22-35 GB/s against 48 GB/s for 512 bytes
     std::vector<int> starts;
-    {
-      int s0 = 0;
-      const bool halves = block_states == 0 && nst >= 2 * B && B % 2 == 0;
-      if (halves) starts.push_back(0), s0 = B / 2;
-      const int tail = halves ? B / 2 : 0;
-      while (s0 < nst - tail) starts.push_back(s0), s0 += B;
-      if (halves) {
-        if (s0 > nst - tail) s0 = nst - tail;  // the last full-size block may be shorter
-        starts.push_back(s0);
-      }
-      starts.push_back(nst);
-    }
+    for (int s0 = 0; s0 < nst; s0 += B) starts.push_back(s0);
+    starts.push_back(nst);
     const int nblocks = int(starts.size()) - 1;
     HostApplyRes r;
     r.ctx = &ctx;

@@ -36,9 +36,9 @@ def test_apply_host_matches_device_call(c1, precision_name, tol, block):
 
 
 @pytest.mark.parametrize("precision_name,tol", [("F64", 1e-12), ("F32", 2e-6)])
-def test_apply_host_default_blocks_with_half_blocks_at_the_ends(precision_name, tol):
-    """136 states with the default blocks: half-size first and last blocks around full ones, and a
-    shortened full-size block before the last (single: 32, 64, 40; double: 16, 32, 32, 32, 8, 16)."""
+def test_apply_host_default_blocks_ragged_end(precision_name, tol):
+    """136 states with the default blocks: full blocks and a short last one (single: 64, 64, 8;
+    double: 32, 32, 32, 32, 8)."""
     import inq_b200 as ib
     from inq_b200 import synthetic
     sysm = synthetic.config("c1", nst=136)
