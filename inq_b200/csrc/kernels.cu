@@ -386,7 +386,11 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
     int KB = ctx.nl_project_points > 0 ? ctx.nl_project_points : int(16384 / srow);  // about 16 KB of rows per stage
     KB = KB < 1 ? 1 : (KB > 32 ? 32 : KB);
     const size_t abytes = dbl ? sizeof(double2) : sizeof(float2);
-    const size_t smem = size_t(NLP_NS) * KB * srow + size_t(NLP_NS) * KB * 4 * abytes + 2 * NLP_NS * sizeof(uint64_t) + 16;
+    auto smem_of = [&](int kb) {
+      return size_t(NLP_NS) * kb * srow + size_t(NLP_NS) * kb * 4 * abytes + 2 * NLP_NS * sizeof(uint64_t) + 16;
+    };
+    while (KB > 1 && smem_of(KB) > size_t(ctx.max_smem_optin)) KB--;  // an option asking for more than fits
+    const size_t smem = smem_of(KB);
     const dim3 grid(P.nproj, NLP_RANGES, nchunks);
     if (dbl) {
       auto kern = nl_project_bulk_kernel<R, double, JB>;
