@@ -353,8 +353,9 @@ def setup_leg(ctx, reps=3):
 
 def overlap_leg(ctx, phi32, phi64, time_loop, reps=5):
     """Subspace overlap S = dV phi^H phi of the 96^3 / 256-state set: the mixed form's split-BF16
-    tensor-core kernel against the FP64 overlap of the FP64 set (tensor roofline: the executed
-    BF16 products, 4 x 8 N flop per computed element of S: the tiles on and above the diagonal)."""
+    tensor-core kernel against the FP64 overlap of the FP64 set, on the FP64 tensor cores and on SIMT
+    (tensor roofline: the executed BF16 products, 4 x 8 N flop per computed element of S: the tiles on
+    and above the diagonal)."""
     import numpy as np
     import inq_b200 as ib
     N = phi32.basis.size()
@@ -362,7 +363,15 @@ def overlap_leg(ctx, phi32, phi64, time_loop, reps=5):
     ref = ib.overlap(phi64)
     got = ib.overlap(phi32)
     ms_tc = time_loop(lambda: ib.overlap(phi32), reps) / reps
-    ms_64 = time_loop(lambda: ib.overlap(phi64), 1)
+    # FP64 overlap of the FP64 set: FP64 tensor cores (mma.sync m8n8k4, the default) and SIMT
+    ms_64 = time_loop(lambda: ib.overlap(phi64), 2) / 2
+    ctx.set_option("fp64_mma", 0)
+    ms_64_simt = time_loop(lambda: ib.overlap(phi64), 1)
+    ctx.set_option("fp64_mma", 1)
+    # executed FP64 products of the FP64 overlap: 8 N per computed element (64 x 64 tiles on and above
+    # the diagonal)
+    t64 = (S + 63) // 64
+    flop64 = 8.0 * N * min((t64 * (t64 + 1) // 2) * 64 * 64, S * S)
     # executed BF16 products: 4 x 8 N per computed result element; a set with itself is Hermitian, so
     # only the 128 x 128 tiles on and above the diagonal are computed
     t = (S + 127) // 128
@@ -372,7 +381,8 @@ def overlap_leg(ctx, phi32, phi64, time_loop, reps=5):
                                              "MEASURED_PEAKS.json")))["bf16_tflops"]) \
         if os.path.exists(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) else 1590.0
     return {"workload": f"overlap of the c2 set: {N} points, {S} x {S} states",
-            "ms_tensor_core_split_bf16": ms_tc, "ms_fp64_simt": ms_64,
+            "ms_tensor_core_split_bf16": ms_tc, "ms_fp64_tensor_core": ms_64, "ms_fp64_simt": ms_64_simt,
+            "fp64_tflops_executed": flop64 / (ms_64 / 1000.0) / 1e12,
             "rel_err_vs_fp64": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
             "max_abs_err_vs_fp64": float(np.max(np.abs(got - ref))),
             "roofline": {"bound": "tensor", "achieved": flop / (ms_tc / 1000.0) / 1e12, "peak": peak,

@@ -77,6 +77,8 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * FFT passes of single-precision sets of at least 64 states move 512-byte rows, 64 states, in three
  * stages at one CTA per SM, unless 64-state tiles would leave more than 8 more empty states in a line's
  * last tile than 32-state tiles) or 0 (256-byte rows, 32 states, as the other passes);
+ * "fp64_mma" = 1 (default: the FP64 products of overlaps of double-precision sets and of every rotation
+ * run on the FP64 tensor cores, mma.sync m8n8k4) or 0 (FP64 SIMT fused multiply-adds);
  * "nl_apply_points" = 0 (default: 8) or 1..32 hit points per batch of the bulk-copy nonlocal apply;
  * "nl_project_points" = 0 (default: about 16 KB of rows) or 1..32 sphere points per stage of the
  * bulk-copy projection.  Changing the priority replaces

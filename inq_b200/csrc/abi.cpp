@@ -950,6 +950,9 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     } else if (k == "mixed_compute") {
       INQB_REQUIRE(value >= 0 && value <= 3, INQB_ERR_ARG, "mixed_compute is 0, 1, 2 or 3");
       ctx->mixed_compute = int(value);
+    } else if (k == "fp64_mma") {
+      INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fp64_mma is 0 (SIMT) or 1 (FP64 tensor cores)");
+      ctx->fp64_mma = int(value);
     } else if (k == "overlap_tc") {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "overlap_tc is 0 (FP64 SIMT) or 1 (tensor cores)");
       ctx->overlap_tc = int(value);

@@ -1038,6 +1038,97 @@ __global__ void __launch_bounds__(256, 2) overlap64_kernel(const double2 *__rest
     }
 }
 
+// The same 64 x 64 tiles of a^H b on the FP64 tensor-core path: mma.sync m8n8k4 (DMMA), four per pair
+// of complex operand fragments (re.re + im.im into the real part, re.im - im.re into the imaginary).
+// 128 threads: each warp owns a 32 x 32 block of the tile, 4 x 4 fragments of 8 x 8, and steps through
+// the point chunk four points at a time; operand tiles double-buffered by cp.async as above, rows padded
+// to 66 complex numbers so that the fragment loads of a quarter-warp hit distinct banks.
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(128) overlap64_mma_kernel(const double2 *__restrict__ a, int Sa,
+                                                            const double2 *__restrict__ b, int Sb, long long npoints,
+                                                            long long chunk, int sym, double2 *partial) {
+  constexpr int TB = 64, KT = 16, LD = TB + 2;
+  extern __shared__ __align__(16) double2 osm[];  // [2 buffers][a, b][KT][LD]
+  int bi = blockIdx.x, bj = blockIdx.y;
+  if (sym) {
+    bj = 0;
+    while ((bj + 1) * (bj + 2) / 2 <= bi) bj++;
+    bi -= bj * (bj + 1) / 2;
+  }
+  const int ti = bi * TB, tj = bj * TB;
+  const long long p0 = blockIdx.z * chunk;
+  const long long p1 = min(npoints, p0 + chunk);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;  // the warp's block of the tile
+  auto tile = [&](int buf, int ab) { return osm + (size_t(buf) * 2 + ab) * KT * LD; };
+  auto issue = [&](int buf, long long k0) {
+    double2 *As = tile(buf, 0), *Bs = tile(buf, 1);
+    for (int e = threadIdx.x; e < KT * TB; e += 128) {
+      const int kk = e / TB, c = e % TB;
+      const long long p = k0 + kk;
+      const bool va = p < p1 && ti + c < Sa, vb = p < p1 && tj + c < Sb;
+      ptx::cp_async16(As + kk * LD + c, va ? a + p * Sa + ti + c : a, va ? 16u : 0u);
+      ptx::cp_async16(Bs + kk * LD + c, vb ? b + p * Sb + tj + c : b, vb ? 16u : 0u);
+    }
+    ptx::cp_async_commit();
+  };
+  double cre[4][4][2], cim[4][4][2];
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) cre[u][v][0] = cre[u][v][1] = cim[u][v][0] = cim[u][v][1] = 0.0;
+  if (p0 < p1) issue(0, p0);
+  int cur = 0;
+  // fragment coordinates: A (8 x 4, row-major) element (row lane / 4, col lane % 4), B (4 x 8,
+  // col-major) element (row lane % 4, col lane / 4); here the row of A and the col of B are states and
+  // the k index is the point
+  const int fk = lane & 3, fs = lane >> 2;
+  for (long long k0 = p0; k0 < p1; k0 += KT, cur ^= 1) {
+    if (k0 + KT < p1) {
+      issue(cur ^ 1, k0 + KT);
+      ptx::cp_async_wait<1>();
+    } else {
+      ptx::cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double2 *As = tile(cur, 0), *Bs = tile(cur, 1);
+#pragma unroll
+    for (int ks = 0; ks < KT; ks += 4) {
+      double2 af[4], bf[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) af[u] = As[(ks + fk) * LD + wm + 8 * u + fs];
+#pragma unroll
+      for (int v = 0; v < 4; v++) bf[v] = Bs[(ks + fk) * LD + wn + 8 * v + fs];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          dmma_8x8x4(cre[u][v], af[u].x, bf[v].x);
+          dmma_8x8x4(cre[u][v], af[u].y, bf[v].y);
+          dmma_8x8x4(cim[u][v], af[u].x, bf[v].y);
+          dmma_8x8x4(cim[u][v], -af[u].y, bf[v].x);
+        }
+    }
+    __syncthreads();
+  }
+  // accumulator fragment: element (row lane / 4, col 2 (lane % 4) + {0, 1}) of each 8 x 8 block
+  const long long base = (long long)blockIdx.z * Sa * Sb;
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int i = ti + wm + 8 * u + fs, j = tj + wn + 8 * v + 2 * fk + h;
+        if (i < Sa && j < Sb) partial[base + (long long)i * Sb + j] = make_double2(cre[u][v][h], cim[u][v][h]);
+      }
+}
+
 __global__ void sum_tiles_kernel(const double2 *partial, int nz, long long n, int S, int sym, double scale,
                                  double2 *out) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
@@ -1065,7 +1156,9 @@ void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, lo
   const int gi = (Sa + 63) / 64, gj = (Sb + 63) / 64;
   const int sym = (a == b && Sa == Sb) ? 1 : 0;
   const int tiles = sym ? gi * (gi + 1) / 2 : gi * gj;
-  int nz = int((2LL * ctx.device_sms + tiles - 1) / tiles);  // independent of grid_sms
+  // CTAs in flight: two per SM of the 256-thread SIMT kernel, four of the 128-thread tensor-core one
+  const int per_sm = (sizeof(R) == 8 && ctx.fp64_mma) ? 4 : 2;
+  int nz = int((long long)per_sm * ctx.device_sms + tiles - 1) / tiles;  // independent of grid_sms
   if (nz < 1) nz = 1;
   if (nz > 256) nz = 256;
   long long chunk = (npoints + nz - 1) / nz;
@@ -1074,9 +1167,15 @@ void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, lo
   double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * (size_t)nz * Sa * Sb));
   const dim3 grid = sym ? dim3(tiles, 1, nz) : dim3(gi, gj, nz);
   if constexpr (sizeof(R) == 8) {
-    const size_t smem = 2 * 2 * 16 * 64 * sizeof(double2);
-    ensure_smem_attr(reinterpret_cast<const void *>(overlap64_kernel), smem);
-    overlap64_kernel<<<grid, 256, smem, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, sym, partial);
+    if (ctx.fp64_mma) {
+      const size_t smem = 2 * 2 * 16 * 66 * sizeof(double2);
+      ensure_smem_attr(reinterpret_cast<const void *>(overlap64_mma_kernel), smem);
+      overlap64_mma_kernel<<<grid, 128, smem, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, sym, partial);
+    } else {
+      const size_t smem = 2 * 2 * 16 * 64 * sizeof(double2);
+      ensure_smem_attr(reinterpret_cast<const void *>(overlap64_kernel), smem);
+      overlap64_kernel<<<grid, 256, smem, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, sym, partial);
+    }
   } else {
     overlap_kernel<R><<<grid, 256, 0, ctx.stream>>>(a, Sa, b, Sb, npoints, chunk, sym, partial);
   }
@@ -1233,6 +1332,103 @@ __global__ void __launch_bounds__(256, 2) rotate_tiled_kernel(const C2<R> *__res
     }
 }
 
+// The tiled rotation on the FP64 tensor-core path (mma.sync m8n8k4, four per pair of complex fragments:
+// re.re - im.im into the real part, re.im + im.re into the imaginary): 64 points x 64 output states per
+// CTA of 128 threads, each warp a 32 x 32 block of 8 x 8 fragments; operand tiles double-buffered by
+// cp.async, rows padded (20 elements of in, 66 of R) so that the fragment loads hit distinct banks.
+template <typename R>
+__global__ void __launch_bounds__(128) rotate_mma_kernel(const C2<R> *__restrict__ in, int Sin, C2<R> *__restrict__ out,
+                                                         int Sout, long long npoints, const double2 *__restrict__ Rm,
+                                                         double2 alpha, double2 beta, int scaled, int use_beta) {
+  using T = C2<R>;
+  constexpr int TP = 64, TJ = 64, KT = 16, LDA = 20, LDB = TJ + 2;
+  constexpr int EPC = 16 / int(sizeof(T));  // elements of in per 16-byte copy
+  extern __shared__ __align__(16) unsigned char rsm[];
+  T *Abuf = reinterpret_cast<T *>(rsm);                                   // [2][TP][LDA]
+  double2 *Bbuf = reinterpret_cast<double2 *>(Abuf + 2 * TP * LDA);       // [2][KT][LDB]
+  const int njt = (Sout + TJ - 1) / TJ;
+  const int j0 = int(blockIdx.x % njt) * TJ;
+  const long long p0 = (long long)(blockIdx.x / njt) * TP;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int fk = lane & 3, fs = lane >> 2;
+  auto issue = [&](int buf, int k0) {
+    T *As = Abuf + buf * TP * LDA;
+    double2 *Bs = Bbuf + buf * KT * LDB;
+    for (int e = threadIdx.x; e < TP * KT / EPC; e += 128) {
+      const int r = e / (KT / EPC), kk = (e % (KT / EPC)) * EPC;
+      const long long p = p0 + r;
+      const bool v = p < npoints && k0 + kk < Sin;
+      ptx::cp_async16(As + r * LDA + kk, v ? in + p * Sin + k0 + kk : in, v ? 16u : 0u);
+    }
+    for (int e = threadIdx.x; e < KT * TJ; e += 128) {
+      const int kk = e / TJ, c = e % TJ;
+      const bool v = k0 + kk < Sin && j0 + c < Sout;
+      ptx::cp_async16(Bs + kk * LDB + c, v ? Rm + (long long)(k0 + kk) * Sout + j0 + c : Rm, v ? 16u : 0u);
+    }
+    ptx::cp_async_commit();
+  };
+  double cre[4][4][2], cim[4][4][2];
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) cre[u][v][0] = cre[u][v][1] = cim[u][v][0] = cim[u][v][1] = 0.0;
+  issue(0, 0);
+  int cur = 0;
+  for (int k0 = 0; k0 < Sin; k0 += KT, cur ^= 1) {
+    if (k0 + KT < Sin) {
+      issue(cur ^ 1, k0 + KT);
+      ptx::cp_async_wait<1>();
+    } else {
+      ptx::cp_async_wait<0>();
+    }
+    __syncthreads();
+    const T *As = Abuf + cur * TP * LDA;
+    const double2 *Bs = Bbuf + cur * KT * LDB;
+#pragma unroll
+    for (int ks = 0; ks < KT; ks += 4) {
+      double2 af[4], bf[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const T x = As[(wm + 8 * u + fs) * LDA + ks + fk];  // A (8 x 4, row-major): (point, input state)
+        af[u] = make_double2(double(x.x), double(x.y));
+      }
+#pragma unroll
+      for (int v = 0; v < 4; v++) bf[v] = Bs[(ks + fk) * LDB + wn + 8 * v + fs];  // B (4 x 8): (input, output)
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          dmma_8x8x4(cre[u][v], af[u].x, bf[v].x);
+          dmma_8x8x4(cre[u][v], -af[u].y, bf[v].y);
+          dmma_8x8x4(cim[u][v], af[u].x, bf[v].y);
+          dmma_8x8x4(cim[u][v], af[u].y, bf[v].x);
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const long long p = p0 + wm + 8 * u + fs;
+        const int j = j0 + wn + 8 * v + 2 * fk + h;
+        if (p < npoints && j < Sout) {
+          double2 w = make_double2(cre[u][v][h], cim[u][v][h]);
+          if (scaled) w = make_double2(alpha.x * w.x - alpha.y * w.y, alpha.x * w.y + alpha.y * w.x);
+          T *o = out + p * Sout + j;
+          if (use_beta) {
+            const double2 y = make_double2(double(o->x), double(o->y));
+            w.x += beta.x * y.x - beta.y * y.y;
+            w.y += beta.x * y.y + beta.y * y.x;
+          }
+          *o = mk<T>(R(w.x), R(w.y));
+        }
+      }
+}
+
 // out <- alpha (in Rm) + beta out, Rm [Sin][Sout]; in == out (Sin == Sout) rotates in place
 template <typename R>
 void launch_rotate_to(Ctx &ctx, const C2<R> *in, int Sin, C2<R> *out, int Sout, long long npoints, const double2 *Rdev,
@@ -1245,12 +1441,18 @@ void launch_rotate_to(Ctx &ctx, const C2<R> *in, int Sin, C2<R> *out, int Sout, 
     // tiled kernel, out of place; in place, chunks of 32768 points go through a scratch block and are
     // copied back (the kernel's CTAs for one tile of points read all of its states)
     const size_t tsmem = 2 * 64 * 16 * sizeof(C2<R>) + 2 * 16 * 64 * sizeof(double2);
-    ensure_smem_attr(reinterpret_cast<const void *>(rotate_tiled_kernel<R>), tsmem);
+    const size_t msmem = 2 * 64 * 20 * sizeof(C2<R>) + 2 * 16 * 66 * sizeof(double2);
+    if (ctx.fp64_mma) ensure_smem_attr(reinterpret_cast<const void *>(rotate_mma_kernel<R>), msmem);
+    else ensure_smem_attr(reinterpret_cast<const void *>(rotate_tiled_kernel<R>), tsmem);
     auto launch = [&](const C2<R> *src, C2<R> *dst, long long n) {
       const long long nblk = (long long)((Sout + 63) / 64) * ((n + 63) / 64);
       INQB_REQUIRE(nblk < (1LL << 31), INQB_ERR_UNSUPPORTED, "set too large for the rotation grid");
-      rotate_tiled_kernel<R><<<unsigned(nblk), 256, tsmem, ctx.stream>>>(src, Sin, dst, Sout, n, Rdev, alpha, beta,
-                                                                        scaled, use_beta);
+      if (ctx.fp64_mma)
+        rotate_mma_kernel<R><<<unsigned(nblk), 128, msmem, ctx.stream>>>(src, Sin, dst, Sout, n, Rdev, alpha, beta,
+                                                                         scaled, use_beta);
+      else
+        rotate_tiled_kernel<R><<<unsigned(nblk), 256, tsmem, ctx.stream>>>(src, Sin, dst, Sout, n, Rdev, alpha, beta,
+                                                                          scaled, use_beta);
       LAUNCHED(ctx);
     };
     if (in != out) {
