@@ -706,6 +706,87 @@ def run_profile_case(args):
     print(json.dumps({"profile_case": f"{args.profile_config} grid, {S} states", "launches": basis.ctx.launch_count()}))
 
 
+def _kernel_table(prof, label):
+    """Device time per kernel (summed over launches) of a torch.profiler capture, as a markdown table."""
+    import collections
+    tot = collections.defaultdict(lambda: [0, 0.0])
+    for e in prof.events():
+        if e.device_type.name == "CUDA":
+            k = e.name.split("(")[0].replace("void ", "").replace("inqb::", "").replace("v2::", "")[:70]
+            tot[k][0] += 1
+            tot[k][1] += e.device_time_total / 1000.0
+    total = sum(v[1] for v in tot.values())
+    lines = [f"== {label}: total device time {total:.2f} ms", "| kernel | launches | ms | share |",
+             "|---|---|---|---|"]
+    for k, (c, t) in sorted(tot.items(), key=lambda x: -x[1][1]):
+        lines.append(f"| `{k}` | {c} | {t:.2f} | {100 * t / total:.1f}% |")
+    print("\n".join(lines), flush=True)
+
+
+def run_breakdown(args):
+    """Per-kernel device times (torch.profiler, CUDA activity) of one piece of work, after one untimed
+    repetition of it:
+
+    * ``etrs``: one step of real_time.propagate at 120^3 / 128 atoms / 256 orbitals (ETRS, the band
+      energy, the dipole), FP64 and mixed form, starting from the kicked orbitals (the propagate call also
+      forms the step-0 density and energy);
+    * ``batch``: the 64 uneven systems of the batched workload applied one by one (mixed form), with the
+      time of each grid size's systems."""
+    import collections
+    import numpy as np
+    import torch
+    from torch.profiler import profile, ProfilerActivity
+    import inq_b200 as ib
+    from inq_b200 import synthetic, real_time
+    ctx = ib.Context(0)
+    if args.breakdown == "etrs":
+        sysm = synthetic.config("c3")
+        basis, ham, phi64 = synthetic.build(sysm, ctx=ctx)
+        ib.apply_phase_kick(phi64, [0.01, 0.0, 0.0])
+        phi32 = phi64.converted(ib.F32)
+        occ = np.full(sysm.nst, 2.0)
+        for name, phi in (("FP64", phi64), ("mixed", phi32)):
+            w = phi.copy()
+            real_time.propagate(ham, [w], [occ], args.etrs_dt, 1)
+            del w
+            p = phi.copy()
+            ctx.synchronize()
+            with profile(activities=[ProfilerActivity.CUDA]) as prof:
+                real_time.propagate(ham, [p], [occ], args.etrs_dt, 1)
+                ctx.synchronize()
+            _kernel_table(prof, f"one step of real_time.propagate at 120^3 x 256, {name}")
+            del p
+        return
+    sy = synthetic.batch_systems(64)
+    built = [synthetic.build(s, precision=ib.F32, ctx=ctx) for s in sy]
+    outs = [b[2].skeleton() for b in built]
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    groups = collections.defaultdict(list)
+    for i, s in enumerate(sy):
+        groups[s.sizes[0]].append(i)
+    for n in sorted(groups):
+        idx = groups[n]
+        for i in idx:
+            built[i][1].apply(built[i][2], outs[i])
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(5):
+            for i in idx:
+                built[i][1].apply(built[i][2], outs[i])
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        set_bytes = sum(sy[i].nst * n ** 3 * 8 for i in idx)
+        print(f"grid {n}^3: {len(idx)} systems, {sum(sy[i].nst for i in idx)} states, FP32 sets {set_bytes / 1e6:.1f} MB,"
+              f" {ms:.3f} ms one by one, {11 * set_bytes / ms / 1e9:.0f} GB/s for 11 transits of the set", flush=True)
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for b, o in zip(built, outs):
+            b[1].apply(b[2], o)
+        ctx.synchronize()
+    _kernel_table(prof, "the 64 uneven systems applied one by one, mixed form")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -720,10 +801,14 @@ def main():
     ap.add_argument("--profile-states", type=int, default=32, help="orbitals of the --profile-case workload")
     ap.add_argument("--profile-config", default="c2", choices=["c2", "c3"],
                     help="grid and atoms of the --profile-case workload (96^3 / 64 atoms or 120^3 / 128 atoms)")
+    ap.add_argument("--breakdown", choices=["etrs", "batch"],
+                    help="print per-kernel device times of one real-time step or of the batched systems")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.profile_case:
+    if args.breakdown:
+        run_breakdown(args)
+    elif args.profile_case:
         run_profile_case(args)
     elif args.impl == "reference":
         run_reference(args)

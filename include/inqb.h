@@ -158,10 +158,11 @@ int inqb_laplacian(const inqb_orbitals *in, inqb_orbitals *out, double factor, c
 int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, inqb_hamiltonian **out);
 int inqb_hamiltonian_destroy(inqb_hamiltonian *ham);
 /* Kernel-choice options of this Hamiltonian's applications: fft_impl, fft_stages, fft_wide, nl_bulk,
- * nl_apply_points and nl_project_points (meanings as in inqb_ctx_set_option) take `value` while an
- * operator application through this Hamiltonian is queued, whatever the context's setting; a negative
- * value (other than nl_bulk's -1) removes the override.  Lets one batch (inqb_batch_apply) run every
- * system with the options tuned for its shape.  No counterpart in the reference. */
+ * nl_apply_points, nl_project_points and grid_sms (meanings as in inqb_ctx_set_option) take `value`
+ * while an operator application through this Hamiltonian is queued, whatever the context's setting; a
+ * negative value (other than nl_bulk's -1) removes the override.  Lets one batch (inqb_batch_apply) run
+ * every system with the options tuned for its shape, and with grid_sms give small systems fewer SMs so
+ * that the systems on the batch's streams run side by side.  No counterpart in the reference. */
 int inqb_hamiltonian_set_option(inqb_hamiltonian *ham, const char *key, long long value);
 /* ks_hamiltonian::scalar_potential() assignment; V is host [npoint][nspin] float64. */
 int inqb_potential_set(inqb_hamiltonian *ham, const double *V);

@@ -259,9 +259,13 @@ int *kernel_option(Ctx &ctx, const std::string &k) {
   if (k == "nl_bulk") return &ctx.nl_bulk;
   if (k == "nl_apply_points") return &ctx.nl_apply_points;
   if (k == "nl_project_points") return &ctx.nl_project_points;
+  if (k == "grid_sms") return &ctx.num_sms;
   return nullptr;
 }
-void check_kernel_option(const std::string &k, long long value) {
+void check_kernel_option(const Ctx &ctx, const std::string &k, long long value) {
+  if (k == "grid_sms")
+    INQB_REQUIRE(value >= 0 && value <= ctx.device_sms, INQB_ERR_ARG,
+                 "grid_sms is 0 (every SM) or 1.." + std::to_string(ctx.device_sms));
   if (k == "fft_impl") INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_impl is 0 (specialised) or 1 (generic)");
   if (k == "fft_stages") INQB_REQUIRE(value >= 0 && value <= 8, INQB_ERR_ARG, "fft_stages is 0 (automatic) or 1..8");
   if (k == "fft_wide") INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_wide is 0 (256-byte rows) or 1 (512-byte rows)");
@@ -945,8 +949,9 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     INQB_REQUIRE(ctx && key, INQB_ERR_ARG, "null argument");
     const std::string k(key);
     if (int *field = kernel_option(*ctx, k)) {
-      check_kernel_option(k, value);
-      *field = int(value);
+      check_kernel_option(*ctx, k, value);
+      // grid_sms 0: every SM of the device
+      *field = (k == "grid_sms" && value == 0) ? ctx->device_sms : int(value);
     } else if (k == "mixed_compute") {
       INQB_REQUIRE(value >= 0 && value <= 3, INQB_ERR_ARG, "mixed_compute is 0, 1, 2 or 3");
       ctx->mixed_compute = int(value);
@@ -956,10 +961,6 @@ int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value) {
     } else if (k == "overlap_tc") {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "overlap_tc is 0 (FP64 SIMT) or 1 (tensor cores)");
       ctx->overlap_tc = int(value);
-    } else if (k == "grid_sms") {
-      INQB_REQUIRE(value >= 0 && value <= ctx->device_sms, INQB_ERR_ARG,
-                   "grid_sms is 0 (every SM) or 1.." + std::to_string(ctx->device_sms));
-      ctx->num_sms = value == 0 ? ctx->device_sms : int(value);
     } else if (k == "stream_priority") {
       INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "stream_priority is 0 (low) or 1 (high)");
       if (int(value) != ctx->stream_priority) {
@@ -990,21 +991,22 @@ int inqb_hamiltonian_set_option(inqb_hamiltonian *h, const char *key, long long 
     INQB_REQUIRE(h && key, INQB_ERR_ARG, "null argument");
     const std::string k(key);
     INQB_REQUIRE(kernel_option(*h->ctx, k) != nullptr, INQB_ERR_ARG,
-                 "a Hamiltonian overrides fft_impl, fft_stages, fft_wide, nl_bulk, nl_apply_points and "
-                 "nl_project_points only (got " + k + ")");
+                 "a Hamiltonian overrides fft_impl, fft_stages, fft_wide, nl_bulk, nl_apply_points, "
+                 "nl_project_points and grid_sms only (got " + k + ")");
     if (value < 0 && k != "nl_bulk") {
       // a negative value removes the override (the context's value applies again)
       for (size_t i = 0; i < h->opt_overrides.size(); i++)
         if (h->opt_overrides[i].first == k) h->opt_overrides.erase(h->opt_overrides.begin() + long(i));
       return;
     }
-    check_kernel_option(k, value);
+    check_kernel_option(*h->ctx, k, value);
+    const int v = (k == "grid_sms" && value == 0) ? h->ctx->device_sms : int(value);
     for (auto &kv : h->opt_overrides)
       if (kv.first == k) {
-        kv.second = int(value);
+        kv.second = v;
         return;
       }
-    h->opt_overrides.emplace_back(k, int(value));
+    h->opt_overrides.emplace_back(k, v);
   });
 }
 
@@ -1944,27 +1946,21 @@ int inqb_eigenvalues(const inqb_hamiltonian *hc, const inqb_orbitals *phi, doubl
     const int S = phi->nst;
     TempSet hp(*phi);
     apply_any(*h, *phi, hp.o);
+    // eigenvalues Re<phi|H phi>/<phi|phi> and, on request, |H phi - eig phi|^2 (energy.hpp:80-89): one pass over
+    // phi and H phi for both sums of the eigenvalues, one more for the residual norms (r is never formed)
     double2 *d = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * 2 * S));
-    ovdiag_dev(*phi, *phi, d);
-    ovdiag_dev(*phi, hp.o, d + S);
+    const double dv = set_volume_element(*phi);
+    double2 *res = normres ? d + S : nullptr;
+    if (phi->precision == INQB_F64)
+      launch_eigen_sums<double>(ctx, static_cast<const double2 *>(phi->data), static_cast<const double2 *>(hp.o.data), S,
+                                phi->basis->npoints, dv, d, res);
+    else
+      launch_eigen_sums<float>(ctx, static_cast<const float2 *>(phi->data), static_cast<const float2 *>(hp.o.data), S,
+                               phi->basis->npoints, dv, d, res);
     auto v = download<double2>(ctx, d, size_t(2) * S);
-    std::vector<double> e(S);
-    for (int s = 0; s < S; s++) e[s] = v[S + s].x / v[s].x;  // overlap_diagonal_normalized, real part
-    std::copy(e.begin(), e.end(), eig);
-    if (normres) {
-      double *de = static_cast<double *>(dev_alloc(ctx, sizeof(double) * S));
-      INQB_CUDA(cudaMemcpyAsync(de, e.data(), sizeof(double) * S, cudaMemcpyHostToDevice, ctx.stream));
-      if (phi->precision == INQB_F64)
-        launch_shift_vec<double>(ctx, static_cast<double2 *>(hp.o.data), static_cast<const double2 *>(phi->data), S,
-                                 phi->basis->npoints, de, -1.0);
-      else
-        launch_shift_vec<float>(ctx, static_cast<float2 *>(hp.o.data), static_cast<const float2 *>(phi->data), S,
-                                phi->basis->npoints, de, -1.0);
-      ovdiag_dev(hp.o, hp.o, d);
-      auto r = download<double2>(ctx, d, size_t(S));
-      for (int s = 0; s < S; s++) normres[s] = r[s].x;
-      dev_free(ctx, de);
-    }
+    for (int s = 0; s < S; s++) eig[s] = v[s].y / v[s].x;  // overlap_diagonal_normalized, real part
+    if (normres)
+      for (int s = 0; s < S; s++) normres[s] = v[S + s].x;
     dev_free(ctx, d);
   });
 }

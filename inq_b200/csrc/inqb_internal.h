@@ -252,6 +252,10 @@ void launch_overlap(Ctx &ctx, const C2<R> *a, int Sa, const C2<R> *b, int Sb, lo
 template <typename R>
 void launch_overlap_diag(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long long npoints, double dv,
                          double2 *out_dev /*[S]*/);
+// ne[s] = dv (<a|a>, Re<a|b>); res (optional) [s].x = dv sum_p |b - e_s a|^2, e_s = ne[s].y / ne[s].x
+template <typename R>
+void launch_eigen_sums(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long long npoints, double dv,
+                       double2 *ne_dev /*[S]*/, double2 *res_dev /*[S] or null*/);
 template <typename R>
 void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev);
 void launch_wait_timeout(Ctx &ctx, long long limit_ns);

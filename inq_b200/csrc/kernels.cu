@@ -825,29 +825,75 @@ void launch_laplacian(Ctx &ctx, const Basis &b, const C2<R> *in, C2<R> *out, int
 
 // ------------------------------------------------------------------ per-state reductions
 // Stage 1: block b handles a contiguous point range; thread t owns state s = t (blockDim >= S handled by loop)
-// and accumulates over its points in index order.  Stage 2 sums the block partials in order.
-constexpr int RED_BLOCKS = 296;
+// and accumulates over its points in a fixed order: U running sums over the points p = 0 .. U-1 mod U of the
+// range (U independent loads of each operand in flight per thread; U = 8 for single precision, whose 8-byte
+// elements need twice the loads in flight to cover the same bytes), added pairwise at the end.  Stage 2
+// sums the block partials in order.  592 blocks of 256 threads are resident at once (4 per SM).
+constexpr int RED_BLOCKS = 592;
+
+// MODE 0: conj(a) b; 1: conj(a) lapl a; 2: |b - e_s a|^2 (the residual norm of energy.hpp:86-89 without
+// forming the residual); 3: (|a|^2, Re conj(a) b), the two sums of one eigenvalue in one pass
+template <typename R, int MODE>
+__device__ __forceinline__ double2 state_term(const C2<R> *__restrict__ a, const C2<R> *__restrict__ b, int S,
+                                              long long p, int s, const Metric &m, double factor, const Vec3 &gc,
+                                              double k2, double es) {
+  const C2<R> x = a[p * S + s];
+  if (MODE == 0) {
+    const C2<R> y = b[p * S + s];
+    return make_double2(double(x.x) * double(y.x) + double(x.y) * double(y.y),
+                        double(x.x) * double(y.y) - double(x.y) * double(y.x));
+  } else if (MODE == 1) {
+    const double f = lapl_at(m, p, factor, gc.v, k2);
+    return make_double2(f * (double(x.x) * double(x.x) + double(x.y) * double(x.y)), 0.0);
+  } else if (MODE == 2) {
+    const C2<R> y = b[p * S + s];
+    const double rx = double(y.x) - es * double(x.x), ry = double(y.y) - es * double(x.y);
+    return make_double2(rx * rx + ry * ry, 0.0);
+  } else {
+    const C2<R> y = b[p * S + s];
+    return make_double2(double(x.x) * double(x.x) + double(x.y) * double(x.y),
+                        double(x.x) * double(y.x) + double(x.y) * double(y.y));
+  }
+}
 
 template <typename R, int MODE>
 __global__ void state_reduce_kernel(const C2<R> *__restrict__ a, const C2<R> *__restrict__ b, int S, long long npoints,
-                                    Metric m, double factor, Vec3 gc, double k2, double2 *partial) {
+                                    Metric m, double factor, Vec3 gc, double k2, const double2 *__restrict__ ne,
+                                    double2 *partial) {
   const long long chunk = (npoints + gridDim.x - 1) / gridDim.x;
   const long long p0 = blockIdx.x * chunk;
   const long long p1 = min(npoints, p0 + chunk);
+  constexpr int U = sizeof(R) == 4 ? 8 : 4;
   for (int s = threadIdx.x; s < S; s += blockDim.x) {
-    double re = 0.0, im = 0.0;
-    for (long long p = p0; p < p1; p++) {
-      C2<R> x = a[p * S + s];
-      if (MODE == 0) {  // conj(a) b
-        C2<R> y = b[p * S + s];
-        re += double(x.x) * double(y.x) + double(x.y) * double(y.y);
-        im += double(x.x) * double(y.y) - double(x.y) * double(y.x);
-      } else {          // conj(a) lapl a
-        double f = lapl_at(m, p, factor, gc.v, k2);
-        re += f * (double(x.x) * double(x.x) + double(x.y) * double(x.y));
+    // MODE 2: the eigenvalue Re<a|b>/<a|a> from the MODE 3 sums (the same division the host does)
+    const double es = MODE == 2 ? ne[s].y / ne[s].x : 0.0;
+    double2 acc[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) acc[u] = make_double2(0.0, 0.0);
+    long long p = p0;
+    for (; p + U - 1 < p1; p += U) {
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const double2 t = state_term<R, MODE>(a, b, S, p + u, s, m, factor, gc, k2, es);
+        acc[u].x += t.x;
+        acc[u].y += t.y;
       }
     }
-    partial[(long long)blockIdx.x * S + s] = make_double2(re, im);
+#pragma unroll
+    for (int u = 0; u < U - 1; u++)
+      if (p + u < p1) {
+        const double2 t = state_term<R, MODE>(a, b, S, p + u, s, m, factor, gc, k2, es);
+        acc[u].x += t.x;
+        acc[u].y += t.y;
+      }
+#pragma unroll
+    for (int w = U / 2; w >= 1; w /= 2)
+#pragma unroll
+      for (int u = 0; u < w; u++) {
+        acc[u].x += acc[u + w].x;
+        acc[u].y += acc[u + w].y;
+      }
+    partial[(long long)blockIdx.x * S + s] = acc[0];
   }
 }
 
@@ -867,10 +913,31 @@ void launch_overlap_diag(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long l
   double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * RED_BLOCKS * S));
   Metric m{};
   Vec3 g{{0, 0, 0}};
-  state_reduce_kernel<R, 0><<<RED_BLOCKS, 256, 0, ctx.stream>>>(a, b, S, npoints, m, 0.0, g, 0.0, partial);
+  state_reduce_kernel<R, 0><<<RED_BLOCKS, 256, 0, ctx.stream>>>(a, b, S, npoints, m, 0.0, g, 0.0, nullptr, partial);
   LAUNCHED(ctx);
   sum_partials_kernel<<<(S + 255) / 256, 256, 0, ctx.stream>>>(partial, RED_BLOCKS, S, dv, out);
   LAUNCHED(ctx);
+  dev_free(ctx, partial);
+}
+
+// Eigenvalues and residual norms of energy.hpp:80-89 in two passes over a and b = H a:
+// ne[s] = dv (<a|a>, Re<a|b>); when res is given, res[s].x = dv sum_p |b - e_s a|^2 with e_s = ne[s].y / ne[s].x
+template <typename R>
+void launch_eigen_sums(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long long npoints, double dv, double2 *ne,
+                       double2 *res) {
+  double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * RED_BLOCKS * S));
+  Metric m{};
+  Vec3 g{{0, 0, 0}};
+  state_reduce_kernel<R, 3><<<RED_BLOCKS, 256, 0, ctx.stream>>>(a, b, S, npoints, m, 0.0, g, 0.0, nullptr, partial);
+  LAUNCHED(ctx);
+  sum_partials_kernel<<<(S + 255) / 256, 256, 0, ctx.stream>>>(partial, RED_BLOCKS, S, dv, ne);
+  LAUNCHED(ctx);
+  if (res) {
+    state_reduce_kernel<R, 2><<<RED_BLOCKS, 256, 0, ctx.stream>>>(a, b, S, npoints, m, 0.0, g, 0.0, ne, partial);
+    LAUNCHED(ctx);
+    sum_partials_kernel<<<(S + 255) / 256, 256, 0, ctx.stream>>>(partial, RED_BLOCKS, S, dv, res);
+    LAUNCHED(ctx);
+  }
   dev_free(ctx, partial);
 }
 
@@ -879,7 +946,7 @@ void launch_kinetic_ev(Ctx &ctx, const Basis &b, const C2<R> *fphi, int S, doubl
                        double *out_dev) {
   double2 *partial = static_cast<double2 *>(dev_alloc(ctx, sizeof(double2) * (RED_BLOCKS * S + S)));
   Vec3 g{{gc[0], gc[1], gc[2]}};
-  state_reduce_kernel<R, 1><<<RED_BLOCKS, 256, 0, ctx.stream>>>(fphi, fphi, S, b.npoints, metric_of(b), factor, g, k2,
+  state_reduce_kernel<R, 1><<<RED_BLOCKS, 256, 0, ctx.stream>>>(fphi, fphi, S, b.npoints, metric_of(b), factor, g, k2, nullptr,
                                                                 partial);
   LAUNCHED(ctx);
   double2 *sums = partial + RED_BLOCKS * S;
@@ -1803,6 +1870,8 @@ void launch_taylor_combine(Ctx &ctx, const C2<R> *x, const C2<R> *const *u, int 
   template void launch_tpa_precondition<R>(Ctx &, const Basis &, C2<R> *, int, const double *);                    \
   template void launch_laplacian<R>(Ctx &, const Basis &, const C2<R> *, C2<R> *, int, double, const double *);    \
   template void launch_overlap_diag<R>(Ctx &, const C2<R> *, const C2<R> *, int, long long, double, double2 *);    \
+  template void launch_eigen_sums<R>(Ctx &, const C2<R> *, const C2<R> *, int, long long, double, double2 *,      \
+                                     double2 *);                                                                   \
   template void launch_kinetic_ev<R>(Ctx &, const Basis &, const C2<R> *, int, double, const double *, double,     \
                                      double *);                                                                   \
   template void launch_overlap<R>(Ctx &, const C2<R> *, int, const C2<R> *, int, long long, double, double2 *);   \

@@ -101,6 +101,14 @@ def test_hamiltonian_option_overrides(systems):
         ham.set_option("fft_impl", -1)
         ham.set_option("nl_bulk", 0)
     assert np.array_equal(ham(phi).matrix(), ref)
+    # fewer SMs for the persistent kernels: the same tiles, computed the same way
+    ham.set_option("grid_sms", 16)
+    try:
+        assert np.array_equal(ham(phi).matrix(), ref)
+    finally:
+        ham.set_option("grid_sms", -1)
+    with pytest.raises(ib.InqbError):
+        ham.set_option("grid_sms", 100000)
     n0 = ctx.launch_count()
     ham(phi)
     assert ctx.launch_count() - n0 == launches_default
