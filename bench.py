@@ -779,7 +779,17 @@ def run_breakdown(args):
         ms = e0.elapsed_time(e1) / 5
         set_bytes = sum(sy[i].nst * n ** 3 * 8 for i in idx)
         print(f"grid {n}^3: {len(idx)} systems, {sum(sy[i].nst for i in idx)} states, FP32 sets {set_bytes / 1e6:.1f} MB,"
-              f" {ms:.3f} ms one by one, {11 * set_bytes / ms / 1e9:.0f} GB/s for 11 transits of the set", flush=True)
+              f" {ms:.3f} ms one by one, {11 * set_bytes / ms / 1e6:.0f} GB/s for 11 transits of the set", flush=True)
+        per = []
+        for i in idx:
+            e0.record(stream)
+            for _ in range(5):
+                built[i][1].apply(built[i][2], outs[i])
+            e1.record(stream)
+            e1.synchronize()
+            ms_i = e0.elapsed_time(e1) / 5
+            per.append(f"{sy[i].nst}:{ms_i * 1e3:.0f}us/{11 * sy[i].nst * n ** 3 * 8 / ms_i / 1e6:.0f}")
+        print("    states:time/GB/s " + " ".join(per), flush=True)
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
         for b, o in zip(built, outs):
             b[1].apply(b[2], o)

@@ -77,6 +77,10 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * FFT passes of single-precision sets of at least 64 states move 512-byte rows, 64 states, in three
  * stages at one CTA per SM, unless 64-state tiles would leave more than 8 more empty states in a line's
  * last tile than 32-state tiles) or 0 (256-byte rows, 32 states, as the other passes);
+ * "fft_flat" = 1 (default: the y and x passes tile the flattened [nx][ny][nz*S] and [nx][ny*nz*S] views
+ * of a set, so every row holds a full tile width of (point, state) columns whatever the state count,
+ * odd counts included, when nz*S elements are a multiple of 16 bytes) or 0 (tiles of one grid line
+ * times a block of states, as the z passes);
  * "fp64_mma" = 1 (default: the FP64 products of overlaps of double-precision sets and of every rotation
  * run on the FP64 tensor cores, mma.sync m8n8k4) or 0 (FP64 SIMT fused multiply-adds);
  * "nl_apply_points" = 0 (default: 8) or 1..32 hit points per batch of the bulk-copy nonlocal apply;
@@ -157,7 +161,7 @@ int inqb_laplacian(const inqb_orbitals *in, inqb_orbitals *out, double factor, c
  * scalar potential zero, no projectors, exchange disabled. */
 int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, inqb_hamiltonian **out);
 int inqb_hamiltonian_destroy(inqb_hamiltonian *ham);
-/* Kernel-choice options of this Hamiltonian's applications: fft_impl, fft_stages, fft_wide, nl_bulk,
+/* Kernel-choice options of this Hamiltonian's applications: fft_impl, fft_stages, fft_wide, fft_flat, nl_bulk,
  * nl_apply_points, nl_project_points and grid_sms (meanings as in inqb_ctx_set_option) take `value`
  * while an operator application through this Hamiltonian is queued, whatever the context's setting; a
  * negative value (other than nl_bulk's -1) removes the override.  Lets one batch (inqb_batch_apply) run

@@ -256,6 +256,7 @@ int *kernel_option(Ctx &ctx, const std::string &k) {
   if (k == "fft_impl") return &ctx.fft_impl;
   if (k == "fft_stages") return &ctx.fft_stages;
   if (k == "fft_wide") return &ctx.fft_wide;
+  if (k == "fft_flat") return &ctx.fft_flat;
   if (k == "nl_bulk") return &ctx.nl_bulk;
   if (k == "nl_apply_points") return &ctx.nl_apply_points;
   if (k == "nl_project_points") return &ctx.nl_project_points;
@@ -269,6 +270,8 @@ void check_kernel_option(const Ctx &ctx, const std::string &k, long long value) 
   if (k == "fft_impl") INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_impl is 0 (specialised) or 1 (generic)");
   if (k == "fft_stages") INQB_REQUIRE(value >= 0 && value <= 8, INQB_ERR_ARG, "fft_stages is 0 (automatic) or 1..8");
   if (k == "fft_wide") INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_wide is 0 (256-byte rows) or 1 (512-byte rows)");
+  if (k == "fft_flat")
+    INQB_REQUIRE(value == 0 || value == 1, INQB_ERR_ARG, "fft_flat is 0 (line x state-block tiles) or 1 (flattened columns)");
   if (k == "nl_bulk")
     INQB_REQUIRE(value >= -1 && value <= 1, INQB_ERR_ARG, "nl_bulk is 0 (automatic), 1 (always) or -1 (never)");
   if (k == "nl_apply_points" || k == "nl_project_points")
@@ -991,7 +994,7 @@ int inqb_hamiltonian_set_option(inqb_hamiltonian *h, const char *key, long long 
     INQB_REQUIRE(h && key, INQB_ERR_ARG, "null argument");
     const std::string k(key);
     INQB_REQUIRE(kernel_option(*h->ctx, k) != nullptr, INQB_ERR_ARG,
-                 "a Hamiltonian overrides fft_impl, fft_stages, fft_wide, nl_bulk, nl_apply_points, "
+                 "a Hamiltonian overrides fft_impl, fft_stages, fft_wide, fft_flat, nl_bulk, nl_apply_points, "
                  "nl_project_points and grid_sms only (got " + k + ")");
     if (value < 0 && k != "nl_bulk") {
       // a negative value removes the override (the context's value applies again)

@@ -497,7 +497,7 @@ __device__ __forceinline__ void col_inverse_inplace(T *__restrict__ buf, const T
 //   inverse A: inverse N1-point DFTs down the columns j2, natural order
 template <int N, int W, int NT, typename T, typename Epi>
 __device__ __forceinline__ void tile_kin_inplace(T *__restrict__ buf, const T *__restrict__ tw,
-                                                 const decltype(T::x) *__restrict__ fac, Epi epi) {
+                                                 const decltype(T::x) *__restrict__ fac, int wsplit, Epi epi) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   constexpr int IB = N2 <= 12 ? (W * N1 + NT - 1) / NT : 1;
   col_forward_inplace<N, W, NT, T>(buf, tw);
@@ -518,9 +518,10 @@ __device__ __forceinline__ void tile_kin_inplace(T *__restrict__ buf, const T *_
       const int it = it0 + b * NT;
       if (it < W * N1) {
         const int w = it % W, k1 = it / W;
+        const auto *f = fac + (w >= wsplit ? N : 0);  // the column's line
         dft<N2, +1, N>(r[b], tw);
 #pragma unroll
-        for (int k2 = 0; k2 < N2; k2++) r[b][k2] = cscale(r[b][k2], fac[k1 + N1 * k2]);
+        for (int k2 = 0; k2 < N2; k2++) r[b][k2] = cscale(r[b][k2], f[k1 + N1 * k2]);
         dft<N2, -1, N>(r[b], tw);
         if (k1 > 0) {
 #pragma unroll
@@ -648,7 +649,7 @@ __device__ __forceinline__ void col_inverse(const TC *work, const TC *__restrict
 // `asrc` may be `work` itself.  No barrier follows the last step.
 template <int N, int W, int NT, typename TC, typename SA, typename Put>
 __device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC *__restrict__ tw,
-                                             const decltype(TC::x) *fac, Put put) {
+                                             const decltype(TC::x) *fac, int wsplit, Put put) {
   constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
   // rows of up to 12 points are batched (two transforms per row keep longer rows one at a time)
   constexpr int IB = N2 <= 12 ? (W * N1 + NT - 1) / NT : 1;
@@ -670,9 +671,10 @@ __device__ __forceinline__ void tile_dft_kin(const SA *asrc, TC *work, const TC 
       const int it = it0 + b * NT;
       if (it < W * N1) {
         const int w = it % W, k1 = it / W;
+        const auto *f = fac + (w >= wsplit ? N : 0);  // the column's line
         dft<N2, +1, N>(r[b], tw);
 #pragma unroll
-        for (int k2 = 0; k2 < N2; k2++) r[b][k2] = cscale(r[b][k2], fac[k1 + N1 * k2]);
+        for (int k2 = 0; k2 < N2; k2++) r[b][k2] = cscale(r[b][k2], f[k1 + N1 * k2]);
         dft<N2, -1, N>(r[b], tw);
         if (k1 > 0) {
 #pragma unroll
@@ -697,7 +699,18 @@ struct Geom2 {
   int aux_single;   // second input tiles single-buffered (1) or one set per ring stage (0)
   int cpa;          // rows that are not 16-byte multiples: the compute threads move tiles with 8-byte
                     // cp.async loads and plain stores instead of TMA (two stages, second tiles per stage)
+  int flat;         // y and x passes over flattened columns (below); nsb is then the column blocks per row
+  long long ncols;  // flat: columns per row, nz*S (y pass) or ny*nz*S (x pass)
 };
+
+// Flattened columns.  A y (x) transform acts on every column of the [nx][ny][nz*S] ([nx][ny*nz*S]) view
+// of the set alike, so a tile may take any W consecutive columns of that view: the (z, state) or
+// (y, z, state) pairs follow one another in memory.  Rows are then W full elements for every state count
+// (odd counts too, whose point rows are not 16-byte multiples, and counts that leave the last state block
+// of a line part-empty), and only the last tile of each row runs past its end (TMA fills the loads with
+// zeros and clips the stores).  With S a multiple of W the tiles, and their order, are those of the
+// (line, state block) decomposition.  The kinetic factor of a column depends on its (y, z) line; with
+// S >= W a tile's columns lie on at most two lines.
 
 template <int VAR> constexpr int dir_first() { return (base_var(VAR) == INV_STORE || base_var(VAR) == INV_FINAL) ? -1 : +1; }
 
@@ -797,6 +810,13 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
   __syncthreads();
 
   auto coords = [&](long long t, int &c0, int &c1, int &c2, int &c3) {
+    if (gg.flat) {
+      c0 = int((t % gg.nsb) * W) * gg.cwords;
+      c1 = 0;
+      c2 = gg.axis == 1 ? int(t / gg.nsb) : 0;
+      c3 = 0;
+      return;
+    }
     const long long L = t / gg.nsb;
     const int s0 = int(t % gg.nsb) * W;
     const int la = int(L / g.nb), lb = int(L % g.nb);
@@ -938,8 +958,23 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
     const int la = int(L / g.nb), lb = int(L % g.nb);
     const long long pbase = la * g.sa + lb * g.sb;
 
-    // per-point factors of this line (consumed after the first barrier of the transform)
+    // per-point factors of this line (consumed after the first barrier of the transform); flattened
+    // columns: of the tile's first line at linev[0, N) and, from column wsplit on, of the next at [N, 2N)
+    int wsplit = W;
     if constexpr (VAR == MID_KIN || VAR == FWD_LAPLADD) {
+      if (gg.flat) {
+        const long long col0 = (t % gg.nsb) * W, l0 = col0 / a.S, nlines = gg.ncols / a.S;
+        wsplit = (l0 + 1) * a.S - col0 < W ? int((l0 + 1) * a.S - col0) : W;
+        const int nl = (wsplit < W && l0 + 1 < nlines) ? 2 : 1;
+        for (int e = threadIdx.x; e < nl * N; e += NT) {
+          const long long l = l0 + e / N;  // x-line (y, z) = (l / nz, l % nz)
+          int ix, iy, iz;
+          line_coords(gg.axis, int(l / g.n[2]), int(l % g.n[2]), e % N, ix, iy, iz);
+          if (a.perm_n2[1]) iy = iy / a.perm_n2[1] + (g.n[1] / a.perm_n2[1]) * (iy % a.perm_n2[1]);
+          if (a.perm_n2[2]) iz = iz / a.perm_n2[2] + (g.n[2] / a.perm_n2[2]) * (iz % a.perm_n2[2]);
+          linev[e] = CR(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc));
+        }
+      } else
       for (int m = threadIdx.x; m < N; m += NT) {
         int ix, iy, iz;
         line_coords(gg.axis, la, lb, m, ix, iy, iz);
@@ -993,7 +1028,7 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
       static_assert(!is_perm(VAR), "digit-reversed passes run with equal storage and arithmetic types");
       if constexpr (VAR == MID_KIN) {
         // forward, multiply by the kinetic factor, backward
-        tile_dft_kin<N, W, NT, TC>(buf, exch, tw, linev, put_out);
+        tile_dft_kin<N, W, NT, TC>(buf, exch, tw, linev, wsplit, put_out);
       } else {
         tile_dft<N, D, W, NT, false, TC>(buf, exch, tw, pre, put_out);
       }
@@ -1007,8 +1042,8 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
       // plain passes (no scaling, no accumulators) store the transform's values as they are
       const bool plain = !AUX && !scaled;
       if constexpr (VAR == MID_KIN) {
-        if (plain) tile_kin_inplace<N, W, NT, T>(buf, twt, linev, Identity());
-        else tile_kin_inplace<N, W, NT, T>(buf, twt, linev, epi_out);
+        if (plain) tile_kin_inplace<N, W, NT, T>(buf, twt, linev, wsplit, Identity());
+        else tile_kin_inplace<N, W, NT, T>(buf, twt, linev, wsplit, epi_out);
       } else if constexpr (VAR == INV_FINAL_PERM) {
         tile_inv_perm_inplace<N, W, NT, T>(buf, twt, epi_out);
       } else if constexpr (VAR == FWD_PERM || VAR == INV_PERM) {
@@ -1109,6 +1144,23 @@ inline CUtensorMap orbital_map(const void *base, const Basis &b, int S, int cwor
   return m;
 }
 
+// 4-D map of the flattened-column view of a [nx][ny][nz][S] complex array as 32-bit words: y pass
+// [nx][ny][nz*S], x pass [nx][ny*nz*S]; box = W columns x N points along `axis`.
+inline CUtensorMap flat_map(const void *base, const Basis &b, long long ncols, int cwords, int axis, int W) {
+  CUtensorMap m;
+  const cuuint64_t roww = cuuint64_t(ncols) * cwords;
+  const cuuint64_t d1 = cuuint64_t(axis == 1 ? b.n[1] : b.n[0]), d2 = cuuint64_t(axis == 1 ? b.n[0] : 1);
+  cuuint64_t dims[4] = {roww, d1, d2, 1};
+  cuuint64_t strides[3] = {roww * 4, roww * 4 * d1, roww * 4 * d1 * d2};
+  cuuint32_t box[4] = {cuuint32_t(W * cwords), cuuint32_t(d1), 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, const_cast<void *>(base), dims, strides, box,
+                                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  INQB_REQUIRE(r == CUDA_SUCCESS, INQB_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+  return m;
+}
+
 template <typename R, typename CR, int N, int VAR, int WIDE = 0>
 void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   using T = C2<R>;
@@ -1129,7 +1181,7 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   // second input tiles beside every ring stage when two stages of them leave room for two CTAs per SM,
   // else single-buffered (96^3 x 256: 0.80 against 0.92 ms for the single-precision final pass beside
   // every stage; 120^3 x 256 double: 3.1 against 5.35 ms single-buffered, at two CTAs per SM against one)
-  gg.cpa = (size_t(a.S) * sizeof(T)) % 16 != 0;
+  gg.cpa = !gg.flat && (size_t(a.S) * sizeof(T)) % 16 != 0;
   gg.aux_single = !gg.cpa && naux > 0 && size_t(2) * (1 + naux) * TILE_BYTES + fixed > 113 * 1024;
   const size_t per_stage = TILE_BYTES * (gg.aux_single ? 1 : 1 + naux);
   const size_t fixed_aux = gg.aux_single ? naux * TILE_BYTES : 0;
@@ -1138,8 +1190,14 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   if (ctx.fft_stages > 0) ns = ctx.fft_stages < 2 ? 2 : ctx.fft_stages;
   if (gg.cpa) ns = 2;
   gg.stages = ns;
-  gg.nsb = (a.S + W - 1) / W;
-  gg.ntiles = (b.npoints / b.n[gg.axis]) * gg.nsb;
+  if (gg.flat) {
+    INQB_REQUIRE(VAR != MID_KIN || a.S >= W, INQB_ERR_UNSUPPORTED, "flattened kinetic tiles span more than two lines");
+    gg.nsb = (gg.ncols + W - 1) / W;
+    gg.ntiles = gg.axis == 1 ? (long long)b.n[0] * gg.nsb : gg.nsb;
+  } else {
+    gg.nsb = (a.S + W - 1) / W;
+    gg.ntiles = (b.npoints / b.n[gg.axis]) * gg.nsb;
+  }
   const size_t smem = per_stage * ns + fixed_aux + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
   auto kern = fft2_kernel<R, CR, N, VAR, WIDE>;
@@ -1165,7 +1223,11 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   INQB_REQUIRE(!gg.cpa || has_producer, INQB_ERR_UNSUPPORTED,
                "FFT pass rows that are not 16-byte multiples need the producer-warp kernel");
   CUtensorMap mi{}, mo{}, mx{}, mb{};
-  if (!gg.cpa) {
+  if (gg.flat) {
+    mi = flat_map(a.in, b, gg.ncols, cwords, gg.axis, W);
+    mo = flat_map(a.out, b, gg.ncols, cwords, gg.axis, W);
+    mx = mb = mi;
+  } else if (!gg.cpa) {
     mi = orbital_map(a.in, b, a.S, cwords, gg.axis, W);
     mo = orbital_map(a.out, b, a.S, cwords, gg.axis, W);
     mx = has_aux(VAR) ? orbital_map(a.psi, b, a.S, cwords, gg.axis, W) : mi;
@@ -1239,7 +1301,7 @@ void launch_n(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg, int var)
       // 64-state tiles unless they would leave more of the last tile empty than 32-state tiles do
       // (85 states: 43 empty slots against 11)
       const int pad64 = (64 - a.S % 64) % 64, pad32 = (32 - a.S % 32) % 32;
-      const bool wide = ctx.fft_wide && a.S >= 64 && wide_var(var) && pad64 <= pad32 + 8;
+      const bool wide = ctx.fft_wide && wide_var(var) && (gg.flat || (a.S >= 64 && pad64 <= pad32 + 8));
       launch_nc<R, float, N>(ctx, b, a, gg, var, wide);
       return;
     }
@@ -1261,9 +1323,13 @@ template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a
   else if (epilogue == EPI_LAPL_ADD) var = FWD_LAPLADD;
   else var = a.dir > 0 ? FWD_STORE : INV_STORE;
   if ((var == INV_FINAL && a.dir > 0) || ((var == FWD_VPSI || var == FWD_LAPLADD) && a.dir < 0)) return false;
+  // y and x passes without per-line data over flattened columns (context option fft_flat), when the
+  // rows of the flattened view are 16-byte multiples
+  const bool flat = ctx.fft_flat && a.axis != 2 && (var == FWD_STORE || var == INV_STORE || var == MID_KIN) &&
+                    (size_t(b.n[2]) * a.S * sizeof(T)) % 16 == 0;
   // rows that are not 16-byte multiples (an odd number of single-precision states): only the kernels with
   // a producer warp (single-precision arithmetic) move them, with 8-byte copies; otherwise the generic kernel
-  if ((size_t(a.S) * sizeof(T)) % 16 != 0 && !(sizeof(R) == 4 && single_arith(ctx, a, var))) return false;
+  if (!flat && (size_t(a.S) * sizeof(T)) % 16 != 0 && !(sizeof(R) == 4 && single_arith(ctx, a, var))) return false;
   if (a.perm) {
     INQB_REQUIRE(var == FWD_STORE || var == INV_STORE || var == INV_FINAL, INQB_ERR_UNSUPPORTED,
                  "digit-reversed frequency order is only kept by the plain forward and inverse passes");
@@ -1280,6 +1346,8 @@ template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a
   else if (a.axis == 1) { gg.g.nb = int(nz); gg.g.sa = ny * nz; gg.g.sb = 1; gg.g.sp = nz; }
   else { gg.g.nb = int(nz); gg.g.sa = nz; gg.g.sb = 1; gg.g.sp = ny * nz; }
   gg.axis = a.axis;
+  gg.flat = flat ? 1 : 0;
+  gg.ncols = a.axis == 1 ? nz * a.S : ny * nz * a.S;
   gg.nsb = (a.S + W - 1) / W;
   gg.ntiles = (b.npoints / n) * gg.nsb;
   gg.cwords = int(sizeof(T) / 4);

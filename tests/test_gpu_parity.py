@@ -274,6 +274,39 @@ def test_hamiltonian_odd_state_count_single(ib, nst):
         ham.uniform_vector_potential = np.zeros(3)
 
 
+@pytest.mark.parametrize("precision,mixed_compute,nst", [("F32", 0, 33), ("F32", 0, 40), ("F32", 0, 64),
+                                                          ("F32", 0, 100), ("F32", 1, 33), ("F32", 1, 72),
+                                                          ("F64", 0, 17), ("F64", 0, 40)])
+def test_flat_columns_match_line_tiles(ib, rng, precision, mixed_compute, nst):
+    """The y and x passes over flattened (point, state) columns (option fft_flat, the default) against
+    tiles of one line times a block of states: H|psi> (kinetic factors of two lines inside one tile
+    included) and to_fourier / to_real agree to rounding, and with the oracle, for odd, ragged and
+    whole-tile state counts."""
+    from inq_b200 import synthetic
+    sysm = synthetic.config("c1", nst=nst)
+    prec = getattr(ib, precision)
+    basis, ham, phi = synthetic.build(sysm, precision=prec)
+    ctx = basis.ctx
+    oh, ors = _oracle_system(sysm)
+    tol = TOL32 if prec == ib.F32 else TOL64
+    ctx.set_option("mixed_compute", mixed_compute)
+    try:
+        x = phi.hypercubic().astype(np.complex128)
+        h_flat = ham(phi).hypercubic()
+        f_flat = ib.to_fourier(phi).hypercubic()
+        ctx.set_option("fft_flat", 0)
+        h_line = ham(phi).hypercubic()
+        f_line = ib.to_fourier(phi).hypercubic()
+        ctx.set_option("fft_flat", 1)
+        assert rel(h_flat, h_line) < (1e-6 if prec == ib.F32 else 1e-14)
+        assert rel(f_flat, f_line) < (1e-6 if prec == ib.F32 else 1e-14)
+        assert rel(h_flat, oh.apply_real(x)) < tol
+        assert rel(f_flat, O.to_fourier(x)) < tol
+    finally:
+        ctx.set_option("fft_flat", 1)
+        ctx.set_option("mixed_compute", 0)
+
+
 def test_hamiltonian_deterministic(ib, c1):
     sysm, basis, ham, phi, oh, ors = c1
     a = ham(phi).matrix()
