@@ -12,7 +12,8 @@ The headline ``value`` is the mixed form (FP32 FFTs / potential / projector
 contraction, FP64 reductions); the plain FP64 form is timed beside it under
 ``fp64`` with the mixed form's error against it.  ``e2e`` is the same metric
 through the C ABI with host buffers: every step copies the orbitals in from
-pinned host memory and H|psi> back out.
+pinned host memory and H|psi> back out (the steps streamed through one
+inqb_apply_host_many call; one inqb_apply_host call per step beside it).
 
 ``--impl reference`` times the reference algorithm's CPU restatement (the FP64
 oracle: pocketFFT over all host threads + numpy/OpenBLAS) on a bounded sample
@@ -609,11 +610,20 @@ def run_ours(args):
         e2e_step()
     barrier()
     e2e_s = time.perf_counter() - t0
+    # the same steps streamed through one call (inqb_apply_host_many): every step still uploads its input
+    # set and downloads its result, and consecutive steps' copies overlap
+    ham.apply_host_many([hin_np] * 2, [hout_np] * 2)
+    barrier()
+    t0 = time.perf_counter()
+    ham.apply_host_many([hin_np] * e2e_steps, [hout_np] * e2e_steps)
+    barrier()
+    e2e_many_s = time.perf_counter() - t0
     if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
+        t = torch.tensor([e2e_s, e2e_many_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_v = world * S * e2e_steps / e2e_s
+        e2e_s, e2e_many_s = (float(x) for x in t.tolist())
+    e2e_single_v = world * S * e2e_steps / e2e_s
+    e2e_v = world * S * e2e_steps / e2e_many_s
 
     legs = {}
     if world == 1 and not args.skip_legs:
@@ -654,7 +664,10 @@ def run_ours(args):
                          "double_butterfly_pass": {"kernel": "fft2_kernel<float,double,96,FWD_STORE>",
                                                    "achieved": achieved_d, "frac": achieved_d / peak,
                                                    "launch_ms": pass_ms[1]}},
-            "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": N * S * 8, "d2h_bytes_per_step": N * S * 8},
+            "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": N * S * 8, "d2h_bytes_per_step": N * S * 8,
+                    "steps": e2e_steps, "how": "pinned host buffers; all steps streamed through one "
+                    "inqb_apply_host_many call (state blocks of 64, copies of consecutive steps overlapping)",
+                    "one_call_per_step": {"value": e2e_single_v, "how": "one inqb_apply_host call per step"}},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }

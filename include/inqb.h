@@ -252,6 +252,14 @@ int inqb_apply(const inqb_hamiltonian *ham, const inqb_orbitals *in, inqb_orbita
  * the same operator. */
 int inqb_apply_host(const inqb_hamiltonian *ham, int nst, const double kpoint_cov[3], int spin_index, int precision,
                     const void *host_in, void *host_out, int block_states);
+/* inqb_apply_host over nsets sets of one shape (host_in[k] -> host_out[k], every output buffer distinct
+ * from every input): the blocks of all sets go through one pipeline, so the upload of a set's first
+ * block overlaps the download of the previous set's last block, and the copy engines stay busy from
+ * the first upload to the last download.  For callers that apply one operator to many host-resident
+ * sets (successive requests, or states split into several arrays).  Returns when every host_out is
+ * complete.  No counterpart in the reference. */
+int inqb_apply_host_many(const inqb_hamiltonian *ham, int nsets, int nst, const double kpoint_cov[3], int spin_index,
+                         int precision, const void *const *host_in, void *const *host_out, int block_states);
 /* ks_hamiltonian::non_local (ks_hamiltonian.hpp:106-120). */
 int inqb_non_local(const inqb_hamiltonian *ham, const inqb_orbitals *in, inqb_orbitals *out);
 /* ks_hamiltonian::non_local_energy (ks_hamiltonian.hpp:124-133, projector_all.hpp:306-327);

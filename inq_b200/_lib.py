@@ -80,6 +80,7 @@ SIGNATURES = {
     "inqb_projectors_get": (I, [P, P, P, P, P]),
     "inqb_apply": (I, [P, P, P]),
     "inqb_apply_host": (I, [P, I, DP, I, I, P, P, I]),
+    "inqb_apply_host_many": (I, [P, I, I, DP, I, I, P, P, I]),
     "inqb_steepest_descent": (I, [P, P]),
     "inqb_orbitals_save": (I, [P, C.c_char_p]),
     "inqb_orbitals_load": (I, [P, C.c_char_p]),

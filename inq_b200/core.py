@@ -547,6 +547,33 @@ class KSHamiltonian:
                                                     int(block_states)))
         return host_out
 
+    def apply_host_many(self, host_ins, host_outs, kpoint=(0.0, 0.0, 0.0), spin_index: int = 0,
+                        block_states: int = 0):
+        """:meth:`apply_host` over several host sets of one shape in one call (inqb_apply_host_many): the
+        state blocks of all sets stream through one pipeline, so consecutive sets' copies overlap."""
+        host_ins, host_outs = list(host_ins), list(host_outs)
+        if not host_ins or len(host_ins) != len(host_outs):
+            raise ValueError("one output array per input array, at least one")
+        a0 = host_ins[0]
+        for a in host_ins + host_outs:
+            if a.dtype != a0.dtype or a.shape != a0.shape or a.ndim != 2 or not a.flags.c_contiguous:
+                raise ValueError("C-contiguous [npoint][nst] arrays of one complex type and shape expected")
+        if a0.dtype == np.complex128:
+            prec = F64
+        elif a0.dtype == np.complex64:
+            prec = F32
+        else:
+            raise ValueError("complex128 or complex64 arrays expected")
+        if a0.shape[0] != self.basis.size():
+            raise ValueError("host arrays must have one row per grid point")
+        n = len(host_ins)
+        ins = (C.c_void_p * n)(*[a.ctypes.data for a in host_ins])
+        outs = (C.c_void_p * n)(*[a.ctypes.data for a in host_outs])
+        kp = np.asarray(kpoint, dtype=np.float64).copy()
+        self.ctx.check(self.ctx.lib.inqb_apply_host_many(self.handle, n, int(a0.shape[1]), kp.ctypes.data_as(_lib.DP),
+                                                         int(spin_index), prec, ins, outs, int(block_states)))
+        return host_outs
+
     def non_local(self, phi: OrbitalSet) -> OrbitalSet:
         out = phi.skeleton()
         self.ctx.check(self.ctx.lib.inqb_non_local(self.handle, phi.handle, out.handle))

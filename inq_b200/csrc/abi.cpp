@@ -1632,87 +1632,113 @@ struct HostApplyRes {
   }
 };
 
+// H over nsets host sets of one shape, streamed through one pipeline of state blocks: the blocks of the
+// sets follow one another, so the upload of a set's first block overlaps the download of the previous
+// set's last one.
+void apply_host_sets(inqb_hamiltonian *h, int nsets, int nst, const double kpoint_cov[3], int spin_index,
+                     int precision, const void *const *host_in, void *const *host_out, int block_states) {
+  INQB_REQUIRE(h && host_in && host_out && nsets >= 1, INQB_ERR_ARG, "null argument");
+  INQB_REQUIRE(nst > 0 && block_states >= 0, INQB_ERR_ARG, "bad state count");
+  INQB_REQUIRE(precision == INQB_F64 || precision == INQB_F32, INQB_ERR_ARG, "bad precision tag");
+  INQB_REQUIRE(spin_index >= 0 && spin_index < h->nspin, INQB_ERR_ARG, "spin index out of range");
+  for (int k = 0; k < nsets; k++) {
+    INQB_REQUIRE(host_in[k] && host_out[k], INQB_ERR_ARG, "null argument");
+    for (int j = 0; j < nsets; j++)
+      INQB_REQUIRE(host_in[k] != host_out[j], INQB_ERR_ARG, "H|psi> needs distinct input and output buffers");
+  }
+  set_device(*h->ctx);
+  Ctx &ctx = *h->ctx;
+  const size_t cs = precision == INQB_F64 ? 16 : 8;
+  const size_t npts = size_t(h->basis->npoints);
+  int B = block_states > 0 ? block_states : int(512 / cs);  // 512-byte rows of a block by default
+  if (B > nst) B = nst;
+  // block boundaries: blocks of B states, the last one shorter.  Measured at 96^3 x 256 single (box to box
+  // 45-51 ms per call): neither a half-size first and last block nor quarter-size last blocks did better
+  // than equal 64-state blocks; rows of 128 bytes download at 22-35 GB/s against 48 GB/s for 512 bytes
+  std::vector<int> starts;
+  for (int s0 = 0; s0 < nst; s0 += B) starts.push_back(s0);
+  starts.push_back(nst);
+  const int nblocks = int(starts.size()) - 1;
+  const int total = nblocks * nsets;
+  HostApplyRes r;
+  r.ctx = &ctx;
+  INQB_CUDA(cudaStreamCreateWithFlags(&r.up, cudaStreamNonBlocking));
+  INQB_CUDA(cudaStreamCreateWithFlags(&r.down, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; i++) {
+    INQB_CUDA(cudaEventCreateWithFlags(&r.ev_in[i], cudaEventDisableTiming));
+    INQB_CUDA(cudaEventCreateWithFlags(&r.ev_comp[i], cudaEventDisableTiming));
+    INQB_CUDA(cudaEventCreateWithFlags(&r.ev_out[i], cudaEventDisableTiming));
+    for (void **p : {&r.bin[i], &r.bout[i]}) {
+      if (i == 1 && total == 1) continue;
+      cudaError_t e = counted_malloc_async(p, npts * B * cs, ctx.stream);
+      if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw Error(INQB_ERR_MEMORY, "device allocation of a state block failed: " + std::string(cudaGetErrorString(e)));
+      }
+    }
+  }
+  INQB_CUDA(cudaEventCreateWithFlags(&r.ev_join, cudaEventDisableTiming));
+  // the copies start after the work already queued on the context's stream
+  INQB_CUDA(cudaEventRecord(r.ev_join, ctx.stream));
+  INQB_CUDA(cudaStreamWaitEvent(r.up, r.ev_join, 0));
+  for (int i = 0; i < total; i++) {
+    const int set = i / nblocks, blk = i % nblocks;
+    const char *hin = static_cast<const char *>(host_in[set]);
+    char *hout = static_cast<char *>(host_out[set]);
+    const int slot = i & 1, s0 = starts[blk], nb = starts[blk + 1] - starts[blk];
+    // block i reuses the buffers of block i - 2: its upload waits for that block's operator, its
+    // operator for that block's download
+    if (i >= 2) INQB_CUDA(cudaStreamWaitEvent(r.up, r.ev_comp[slot], 0));
+    INQB_CUDA(cudaMemcpy2DAsync(r.bin[slot], nb * cs, hin + s0 * cs, nst * cs, nb * cs, npts, cudaMemcpyHostToDevice,
+                                r.up));
+    INQB_CUDA(cudaEventRecord(r.ev_in[slot], r.up));
+    INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_in[slot], 0));
+    if (i >= 2) INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_out[slot], 0));
+    Orbitals in, out;
+    in.ctx = out.ctx = &ctx;
+    in.basis = out.basis = h->basis;
+    in.nst = out.nst = nb;
+    for (int k = 0; k < 3; k++) in.kpoint[k] = out.kpoint[k] = kpoint_cov ? kpoint_cov[k] : 0.0;
+    in.spin_index = out.spin_index = spin_index;
+    in.space = out.space = INQB_REAL_SPACE;
+    in.precision = out.precision = precision;
+    in.data = r.bin[slot];
+    out.data = r.bout[slot];
+    apply_any(*h, in, out);
+    INQB_CUDA(cudaEventRecord(r.ev_comp[slot], ctx.stream));
+    INQB_CUDA(cudaStreamWaitEvent(r.down, r.ev_comp[slot], 0));
+    INQB_CUDA(cudaMemcpy2DAsync(hout + s0 * cs, nst * cs, r.bout[slot], nb * cs, nb * cs, npts,
+                                cudaMemcpyDeviceToHost, r.down));
+    INQB_CUDA(cudaEventRecord(r.ev_out[slot], r.down));
+  }
+  INQB_CUDA(cudaEventRecord(r.ev_join, r.down));
+  INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_join, 0));
+  INQB_CUDA(cudaStreamSynchronize(ctx.stream));
+  int flag = 0;
+  INQB_CUDA(cudaMemcpy(&flag, ctx.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    INQB_CUDA(cudaMemset(ctx.d_err, 0, sizeof(int)));
+    throw Error(INQB_ERR_TIMEOUT, "a device-side wait exceeded its time limit; host_out is invalid");
+  }
+}
+
 int inqb_apply_host(const inqb_hamiltonian *hc, int nst, const double kpoint_cov[3], int spin_index, int precision,
                     const void *host_in, void *host_out, int block_states) {
   auto *h = const_cast<inqb_hamiltonian *>(hc);
   return guarded(h ? h->ctx : nullptr, [&] {
     INQB_REQUIRE(h && host_in && host_out, INQB_ERR_ARG, "null argument");
-    INQB_REQUIRE(nst > 0 && block_states >= 0, INQB_ERR_ARG, "bad state count");
-    INQB_REQUIRE(precision == INQB_F64 || precision == INQB_F32, INQB_ERR_ARG, "bad precision tag");
-    INQB_REQUIRE(spin_index >= 0 && spin_index < h->nspin, INQB_ERR_ARG, "spin index out of range");
-    INQB_REQUIRE(host_in != host_out, INQB_ERR_ARG, "H|psi> needs distinct input and output buffers");
-    set_device(*h->ctx);
-    Ctx &ctx = *h->ctx;
-    const size_t cs = precision == INQB_F64 ? 16 : 8;
-    const size_t npts = size_t(h->basis->npoints);
-    int B = block_states > 0 ? block_states : int(512 / cs);  // 512-byte rows of a block by default
-    if (B > nst) B = nst;
-    // block boundaries: blocks of B states, the last one shorter.  Measured at 96^3 x 256 single (box to box
-    // 45-51 ms per call): neither a half-size first and last block nor quarter-size last blocks did better
-    // than equal 64-state blocks; rows of 128 bytes download at 22-35 GB/s against 48 GB/s for 512 bytes
-    std::vector<int> starts;
-    for (int s0 = 0; s0 < nst; s0 += B) starts.push_back(s0);
-    starts.push_back(nst);
-    const int nblocks = int(starts.size()) - 1;
-    HostApplyRes r;
-    r.ctx = &ctx;
-    INQB_CUDA(cudaStreamCreateWithFlags(&r.up, cudaStreamNonBlocking));
-    INQB_CUDA(cudaStreamCreateWithFlags(&r.down, cudaStreamNonBlocking));
-    for (int i = 0; i < 2; i++) {
-      INQB_CUDA(cudaEventCreateWithFlags(&r.ev_in[i], cudaEventDisableTiming));
-      INQB_CUDA(cudaEventCreateWithFlags(&r.ev_comp[i], cudaEventDisableTiming));
-      INQB_CUDA(cudaEventCreateWithFlags(&r.ev_out[i], cudaEventDisableTiming));
-      for (void **p : {&r.bin[i], &r.bout[i]}) {
-        if (i == 1 && nblocks == 1) continue;
-        cudaError_t e = counted_malloc_async(p, npts * B * cs, ctx.stream);
-        if (e != cudaSuccess) {
-          (void)cudaGetLastError();
-          throw Error(INQB_ERR_MEMORY, "device allocation of a state block failed: " + std::string(cudaGetErrorString(e)));
-        }
-      }
-    }
-    INQB_CUDA(cudaEventCreateWithFlags(&r.ev_join, cudaEventDisableTiming));
-    // the copies start after the work already queued on the context's stream
-    INQB_CUDA(cudaEventRecord(r.ev_join, ctx.stream));
-    INQB_CUDA(cudaStreamWaitEvent(r.up, r.ev_join, 0));
-    const char *hin = static_cast<const char *>(host_in);
-    char *hout = static_cast<char *>(host_out);
-    for (int i = 0; i < nblocks; i++) {
-      const int slot = i & 1, s0 = starts[i], nb = starts[i + 1] - starts[i];
-      // block i reuses the buffers of block i - 2: its upload waits for that block's operator, its
-      // operator for that block's download
-      if (i >= 2) INQB_CUDA(cudaStreamWaitEvent(r.up, r.ev_comp[slot], 0));
-      INQB_CUDA(cudaMemcpy2DAsync(r.bin[slot], nb * cs, hin + s0 * cs, nst * cs, nb * cs, npts, cudaMemcpyHostToDevice,
-                                  r.up));
-      INQB_CUDA(cudaEventRecord(r.ev_in[slot], r.up));
-      INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_in[slot], 0));
-      if (i >= 2) INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_out[slot], 0));
-      Orbitals in, out;
-      in.ctx = out.ctx = &ctx;
-      in.basis = out.basis = h->basis;
-      in.nst = out.nst = nb;
-      for (int k = 0; k < 3; k++) in.kpoint[k] = out.kpoint[k] = kpoint_cov ? kpoint_cov[k] : 0.0;
-      in.spin_index = out.spin_index = spin_index;
-      in.space = out.space = INQB_REAL_SPACE;
-      in.precision = out.precision = precision;
-      in.data = r.bin[slot];
-      out.data = r.bout[slot];
-      apply_any(*h, in, out);
-      INQB_CUDA(cudaEventRecord(r.ev_comp[slot], ctx.stream));
-      INQB_CUDA(cudaStreamWaitEvent(r.down, r.ev_comp[slot], 0));
-      INQB_CUDA(cudaMemcpy2DAsync(hout + s0 * cs, nst * cs, r.bout[slot], nb * cs, nb * cs, npts,
-                                  cudaMemcpyDeviceToHost, r.down));
-      INQB_CUDA(cudaEventRecord(r.ev_out[slot], r.down));
-    }
-    INQB_CUDA(cudaEventRecord(r.ev_join, r.down));
-    INQB_CUDA(cudaStreamWaitEvent(ctx.stream, r.ev_join, 0));
-    INQB_CUDA(cudaStreamSynchronize(ctx.stream));
-    int flag = 0;
-    INQB_CUDA(cudaMemcpy(&flag, ctx.d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) {
-      INQB_CUDA(cudaMemset(ctx.d_err, 0, sizeof(int)));
-      throw Error(INQB_ERR_TIMEOUT, "a device-side wait exceeded its time limit; host_out is invalid");
-    }
+    const void *ins[1] = {host_in};
+    void *outs[1] = {host_out};
+    apply_host_sets(h, 1, nst, kpoint_cov, spin_index, precision, ins, outs, block_states);
+  });
+}
+
+int inqb_apply_host_many(const inqb_hamiltonian *hc, int nsets, int nst, const double kpoint_cov[3], int spin_index,
+                         int precision, const void *const *host_in, void *const *host_out, int block_states) {
+  auto *h = const_cast<inqb_hamiltonian *>(hc);
+  return guarded(h ? h->ctx : nullptr, [&] {
+    INQB_REQUIRE(h && nsets >= 1, INQB_ERR_ARG, "null argument or no sets");
+    apply_host_sets(h, nsets, nst, kpoint_cov, spin_index, precision, host_in, host_out, block_states);
   });
 }
 
