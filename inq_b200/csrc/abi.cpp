@@ -2182,7 +2182,8 @@ int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int n
     }
     double *dens = static_cast<double *>(dev_alloc(ctx, sizeof(double) * b.npoints));
     double *old = static_cast<double *>(dev_alloc(ctx, sizeof(double) * b.npoints));
-    double *delta_dev = static_cast<double *>(dev_alloc(ctx, sizeof(double)));
+    double *delta_dev = static_cast<double *>(dev_alloc(ctx, sizeof(double) * 3));  // also the dipole's output
+    double *delta_dev3 = delta_dev;
     density_dev(ctx, phis, nsets, occ, dens);
     // etrs.hpp:51: H(t + dt) from the predicted density (nothing to update for a fixed Hamiltonian)
     const bool interacting = h->d_vion != nullptr;
@@ -2209,10 +2210,9 @@ int inqb_etrs_step(const inqb_hamiltonian *hc, inqb_orbitals *const *phis, int n
     if (density_host)
       INQB_CUDA(cudaMemcpyAsync(density_host, dens, sizeof(double) * b.npoints, cudaMemcpyDefault, ctx.stream));
     if (dipole) {
-      std::vector<double> hd(size_t(b.npoints));
-      INQB_CUDA(cudaMemcpyAsync(hd.data(), dens, sizeof(double) * b.npoints, cudaMemcpyDeviceToHost, ctx.stream));
-      INQB_CUDA(cudaStreamSynchronize(ctx.stream));
-      dipole_host(b, hd.data(), dipole);
+      // on the device: only the three components cross to the host
+      launch_dipole(ctx, b, dens, delta_dev3);
+      INQB_CUDA(cudaMemcpyAsync(dipole, delta_dev3, sizeof(double) * 3, cudaMemcpyDeviceToHost, ctx.stream));
     }
     dev_free(ctx, dens);
     dev_free(ctx, old);

@@ -260,6 +260,8 @@ void launch_eigen_sums(Ctx &ctx, const C2<R> *a, const C2<R> *b, int S, long lon
 template <typename R>
 void launch_rotate(Ctx &ctx, C2<R> *phi, int S, long long npoints, const double2 *Rdev);
 void launch_wait_timeout(Ctx &ctx, long long limit_ns);
+// dipole.hpp:24-60 of a device density [npoints]: out3_dev = dV sum_r n(r) r
+void launch_dipole(Ctx &ctx, const Basis &b, const double *dens, double *out3_dev);
 template <typename R>
 void launch_rotate_to(Ctx &ctx, const C2<R> *in, int Sin, C2<R> *out, int Sout, long long npoints, const double2 *Rdev,
                       double2 alpha, double2 beta);

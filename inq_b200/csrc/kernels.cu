@@ -1636,6 +1636,53 @@ void launch_absdiff_sum(Ctx &ctx, const double *a, const double *b, long long n,
   dev_free(ctx, partial);
 }
 
+// dipole = dV sum_r n(r) r (observables::dipole, dipole.hpp:24-60) of a device density: r from the
+// symmetric grid index of each point (cell-centred coordinates), contravariant -> cartesian.  Block b
+// sums a contiguous point range, threads strided, then a shared-memory tree; the partials are added in
+// block order.
+__global__ void dipole_kernel(const double *__restrict__ dens, int nx, int ny, int nz, long long n, Vec3 a0, Vec3 a1,
+                              Vec3 a2, double *partial) {
+  __shared__ double red[3][256];
+  const long long chunk = (n + gridDim.x - 1) / gridDim.x;
+  const long long p0 = blockIdx.x * chunk, p1 = min(n, p0 + chunk);
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (long long p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+    const int iz = int(p % nz), iy = int((p / nz) % ny), ix = int(p / ((long long)ny * nz));
+    const double c0 = (ix >= (nx + 1) / 2 ? ix - nx : ix) * (1.0 / nx);
+    const double c1 = (iy >= (ny + 1) / 2 ? iy - ny : iy) * (1.0 / ny);
+    const double c2 = (iz >= (nz + 1) / 2 ? iz - nz : iz) * (1.0 / nz);
+    const double d = dens[p];
+#pragma unroll
+    for (int j = 0; j < 3; j++) acc[j] += ((a0.v[j] * c0 + a1.v[j] * c1) + a2.v[j] * c2) * d;
+  }
+  for (int j = 0; j < 3; j++) red[j][threadIdx.x] = acc[j];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int j = 0; j < 3; j++) red[j][threadIdx.x] += red[j][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) partial[blockIdx.x * 3 + threadIdx.x] = red[threadIdx.x][0];
+}
+__global__ void dipole_final_kernel(const double *partial, int nb, double scale, double *out) {
+  if (blockIdx.x == 0 && threadIdx.x < 3) {
+    double s = 0.0;
+    for (int i = 0; i < nb; i++) s += partial[i * 3 + threadIdx.x];
+    out[threadIdx.x] = scale * s;
+  }
+}
+void launch_dipole(Ctx &ctx, const Basis &b, const double *dens, double *out3_dev) {
+  double *partial = static_cast<double *>(dev_alloc(ctx, sizeof(double) * 3 * RED_BLOCKS));
+  Vec3 a[3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) a[i].v[j] = b.lat[i][j];
+  dipole_kernel<<<RED_BLOCKS, 256, 0, ctx.stream>>>(dens, b.n[0], b.n[1], b.n[2], b.npoints, a[0], a[1], a[2], partial);
+  LAUNCHED(ctx);
+  dipole_final_kernel<<<1, 32, 0, ctx.stream>>>(partial, RED_BLOCKS, b.volume / double(b.npoints), out3_dev);
+  LAUNCHED(ctx);
+  dev_free(ctx, partial);
+}
+
 // ------------------------------------------------------------------ eigensolver pieces
 // y[pt][s] += scale * (coef[s] * x[pt][s]) with complex per-state factors (operations::shift, shift.hpp:19-31)
 template <typename R>
