@@ -85,7 +85,8 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * run on the FP64 tensor cores, mma.sync m8n8k4) or 0 (FP64 SIMT fused multiply-adds);
  * "nl_apply_points" = 0 (default: 8) or 1..32 hit points per batch of the bulk-copy nonlocal apply;
  * "nl_project_points" = 0 (default: about 16 KB of rows) or 1..32 sphere points per stage of the
- * bulk-copy projection.  Changing the priority replaces
+ * bulk-copy projection; "nl_project_ranges" = 0 (default: 16) or 1..64 ranges of each sphere's points,
+ * one CTA each, in the projection (the projection's summation order follows it).  Changing the priority replaces
  * the context's stream (after the work queued on it), so callers query inqb_ctx_stream again. */
 int inqb_ctx_set_option(inqb_ctx *ctx, const char *key, long long value);
 /* Self-test of the bounded device-side waits: queues one kernel whose wait on an mbarrier phase that
@@ -162,7 +163,7 @@ int inqb_laplacian(const inqb_orbitals *in, inqb_orbitals *out, double factor, c
 int inqb_hamiltonian_create(inqb_ctx *ctx, const inqb_basis *basis, int nspin, inqb_hamiltonian **out);
 int inqb_hamiltonian_destroy(inqb_hamiltonian *ham);
 /* Kernel-choice options of this Hamiltonian's applications: fft_impl, fft_stages, fft_wide, fft_flat, nl_bulk,
- * nl_apply_points, nl_project_points and grid_sms (meanings as in inqb_ctx_set_option) take `value`
+ * nl_apply_points, nl_project_points, nl_project_ranges and grid_sms (meanings as in inqb_ctx_set_option) take `value`
  * while an operator application through this Hamiltonian is queued, whatever the context's setting; a
  * negative value (other than nl_bulk's -1) removes the override.  Lets one batch (inqb_batch_apply) run
  * every system with the options tuned for its shape, and with grid_sms give small systems fewer SMs so

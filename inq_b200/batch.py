@@ -26,7 +26,7 @@ from . import _lib
 from .core import Context, KSHamiltonian, OrbitalSet
 
 DEFAULT_OPTIONS = {"fft_impl": 0, "fft_wide": 1, "fft_flat": 1, "fft_stages": 0, "nl_bulk": 0, "nl_apply_points": 0,
-                   "nl_project_points": 0}
+                   "nl_project_points": 0, "nl_project_ranges": 0}
 
 # The knobs the autotuner searches, each with its candidate values (the first is the default):
 #   fft_impl           specialised persistent TMA kernels (0) or the generic kernel (1)
@@ -36,9 +36,11 @@ DEFAULT_OPTIONS = {"fft_impl": 0, "fft_wide": 1, "fft_flat": 1, "fft_stages": 0,
 #   nl_bulk            bulk-copy nonlocal kernels by size (0), wherever rows allow (1), never (-1)
 #   nl_apply_points    hit points per batch of the bulk-copy nonlocal apply (0: 8)
 #   nl_project_points  sphere points per stage of the bulk-copy projection (0: about 16 KB of rows)
+#   nl_project_ranges  ranges of each sphere's points, one CTA each, in the projection (0: 16)
 SEARCH_SPACE = (("fft_impl", (0, 1)), ("fft_wide", (1, 0)), ("fft_flat", (1, 0)), ("fft_stages", (0, 2, 3, 4)),
                 ("nl_bulk", (0, 1, -1)),
-                ("nl_apply_points", (0, 4, 16)), ("nl_project_points", (0, 4, 8, 16)))
+                ("nl_apply_points", (0, 4, 16)), ("nl_project_points", (0, 4, 8, 16)),
+                ("nl_project_ranges", (0, 8, 24)))
 
 
 @dataclass

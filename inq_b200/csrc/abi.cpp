@@ -260,6 +260,7 @@ int *kernel_option(Ctx &ctx, const std::string &k) {
   if (k == "nl_bulk") return &ctx.nl_bulk;
   if (k == "nl_apply_points") return &ctx.nl_apply_points;
   if (k == "nl_project_points") return &ctx.nl_project_points;
+  if (k == "nl_project_ranges") return &ctx.nl_project_ranges;
   if (k == "grid_sms") return &ctx.num_sms;
   return nullptr;
 }
@@ -276,6 +277,8 @@ void check_kernel_option(const Ctx &ctx, const std::string &k, long long value) 
     INQB_REQUIRE(value >= -1 && value <= 1, INQB_ERR_ARG, "nl_bulk is 0 (automatic), 1 (always) or -1 (never)");
   if (k == "nl_apply_points" || k == "nl_project_points")
     INQB_REQUIRE(value >= 0 && value <= 32, INQB_ERR_ARG, k + " is 0 (automatic) or 1..32");
+  if (k == "nl_project_ranges")
+    INQB_REQUIRE(value >= 0 && value <= 64, INQB_ERR_ARG, "nl_project_ranges is 0 (16) or 1..64");
 }
 
 // The Hamiltonian's kernel-option overrides (inqb_hamiltonian_set_option) in force on its context for
@@ -995,7 +998,7 @@ int inqb_hamiltonian_set_option(inqb_hamiltonian *h, const char *key, long long 
     const std::string k(key);
     INQB_REQUIRE(kernel_option(*h->ctx, k) != nullptr, INQB_ERR_ARG,
                  "a Hamiltonian overrides fft_impl, fft_stages, fft_wide, fft_flat, nl_bulk, nl_apply_points, "
-                 "nl_project_points and grid_sms only (got " + k + ")");
+                 "nl_project_points, nl_project_ranges and grid_sms only (got " + k + ")");
     if (value < 0 && k != "nl_bulk") {
       // a negative value removes the override (the context's value applies again)
       for (size_t i = 0; i < h->opt_overrides.size(); i++)

@@ -77,6 +77,7 @@ struct Ctx {
   int nl_bulk = 0;           // nonlocal kernels: 0 automatic, 1 bulk-copy forms wherever they apply, -1 never
   int fft_wide = 1;          // single-precision FFT passes without a second input: 512-byte rows (64 states)
   int fft_flat = 1;          // y and x FFT passes over flattened (point, state) columns (option fft_flat)
+  int nl_project_ranges = 0; // ranges of each sphere's points in the projection (0: 16)
   int fp64_mma = 1;          // FP64 overlaps on the FP64 tensor-core path (mma.sync m8n8k4) or SIMT (0)
   int nl_apply_points = 0;   // hit points per batch of the bulk-copy nonlocal apply (0: 8)
   int nl_project_points = 0; // sphere points per stage of the bulk-copy projection (0: about 16 KB of rows)

@@ -153,7 +153,8 @@ __global__ void __launch_bounds__(NLP_WARPS * 32) nl_project_kernel(const C2<R> 
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const int sbase = blockIdx.z * 32 * K;
   const int np = npts[p];
-  const int rper = (np + NLP_RANGES - 1) / NLP_RANGES;
+  const int nr = int(gridDim.y);  // ranges of a sphere
+  const int rper = (np + nr - 1) / nr;
   const int r0 = rg * rper, r1 = min(np, r0 + rper);
   const int per = (max(r1 - r0, 0) + NLP_WARPS - 1) / NLP_WARPS;
   const int i0 = r0 + wp * per, i1 = min(r1, i0 + per);
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(NLP_WARPS * 32) nl_project_kernel(const C2<R> 
     const int s = sbase + sl;
     TA t = part[0][l][sl];
     for (int w = 1; w < NLP_WARPS; w++) t = cadd(t, part[w][l][sl]);
-    if (s < S) partial[(((long long)p * NLP_RANGES + rg) * 4 + l) * S + s] = t;
+    if (s < S) partial[(((long long)p * nr + rg) * 4 + l) * S + s] = t;
   }
 }
 
@@ -236,7 +237,8 @@ __global__ void __launch_bounds__(NLA_NT + 32) nl_project_bulk_kernel(const C2<R
   uint64_t *done = full + NLP_NS;                                            // stage consumed
   volatile int *abort_flag = reinterpret_cast<volatile int *>(done + NLP_NS);
   const int np = npts[p];
-  const int rper = (np + NLP_RANGES - 1) / NLP_RANGES;
+  const int nr = int(gridDim.y);  // ranges of a sphere
+  const int rper = (np + nr - 1) / nr;
   const int r0 = rg * rper, r1 = min(np, r0 + rper);
   const int n = max(r1 - r0, 0);
   const int nbatch = (n + KB - 1) / KB;
@@ -332,13 +334,13 @@ __global__ void __launch_bounds__(NLA_NT + 32) nl_project_bulk_kernel(const C2<R
     const int sl = tid + j * NLA_NT;
     if (sl < SC) {
 #pragma unroll
-      for (int l = 0; l < 4; l++) partial[(((long long)p * NLP_RANGES + rg) * 4 + l) * S + s0 + sl] = acc[j][l];
+      for (int l = 0; l < 4; l++) partial[(((long long)p * nr + rg) * 4 + l) * S + s0 + sl] = acc[j][l];
     }
   }
 }
 
 template <typename R, typename A>
-__global__ void nl_project_finish_kernel(const C2<A> *__restrict__ partial, int nproj, int S,
+__global__ void nl_project_finish_kernel(const C2<A> *__restrict__ partial, int nproj, int nr, int S,
                                          const A *__restrict__ coeff, C2<R> *projraw, C2<R> *projD) {
   using T = C2<R>;
   using TA = C2<A>;
@@ -348,8 +350,8 @@ __global__ void nl_project_finish_kernel(const C2<A> *__restrict__ partial, int 
     TA pr[4];
 #pragma unroll
     for (int l = 0; l < 4; l++) {
-      TA t = partial[(((long long)p * NLP_RANGES) * 4 + l) * S + s];
-      for (int rg = 1; rg < NLP_RANGES; rg++) t = cadd(t, partial[(((long long)p * NLP_RANGES + rg) * 4 + l) * S + s]);
+      TA t = partial[(((long long)p * nr) * 4 + l) * S + s];
+      for (int rg = 1; rg < nr; rg++) t = cadd(t, partial[(((long long)p * nr + rg) * 4 + l) * S + s]);
       pr[l] = t;
       projraw[((long long)p * 4 + l) * S + s] = mk<T>(R(t.x), R(t.y));
     }
@@ -369,7 +371,9 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   const Projectors &P = h.proj;
   if (P.nproj == 0) return;
   const bool dbl = sizeof(R) == 8 || ctx.mixed_compute != 0;  // double-precision coefficients and sums
-  const size_t pbytes = size_t(P.nproj) * NLP_RANGES * 4 * S * (dbl ? sizeof(double2) : sizeof(float2));
+  // ranges per sphere (option nl_project_ranges; the summation order follows it)
+  const int NR = ctx.nl_project_ranges > 0 ? ctx.nl_project_ranges : NLP_RANGES;
+  const size_t pbytes = size_t(P.nproj) * NR * 4 * S * (dbl ? sizeof(double2) : sizeof(float2));
   void *partial = dev_alloc(ctx, pbytes);
   const long long fin = (long long)P.nproj * S;
   // bulk form: rows of 16-byte multiples, and (automatic choice) enough CTAs to fill the device; the
@@ -379,7 +383,7 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   const int nchunks = (S + NLA_NT * JB - 1) / (NLA_NT * JB);
   const bool bulk_ok = row_bytes % 16 == 0 && reinterpret_cast<uintptr_t>(psi) % 16 == 0;
   const bool bulk = bulk_ok && (ctx.nl_bulk > 0 ||
-                                (ctx.nl_bulk == 0 && (long long)P.nproj * NLP_RANGES * nchunks >= 2LL * ctx.device_sms));
+                                (ctx.nl_bulk == 0 && (long long)P.nproj * NR * nchunks >= 2LL * ctx.device_sms));
   if (bulk) {
     const int SCmax = std::min(NLA_NT * JB, S);
     const size_t srow = size_t(SCmax) * sizeof(C2<R>);
@@ -391,7 +395,7 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
     };
     while (KB > 1 && smem_of(KB) > size_t(ctx.max_smem_optin)) KB--;  // an option asking for more than fits
     const size_t smem = smem_of(KB);
-    const dim3 grid(P.nproj, NLP_RANGES, nchunks);
+    const dim3 grid(P.nproj, NR, nchunks);
     if (dbl) {
       auto kern = nl_project_bulk_kernel<R, double, JB>;
       ensure_smem_attr(reinterpret_cast<const void *>(kern), smem);
@@ -399,7 +403,7 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
                                                     static_cast<double2 *>(partial), ctx.d_err);
       LAUNCHED(ctx);
       nl_project_finish_kernel<R, double><<<grid_for(fin, 256), 256, 0, ctx.stream>>>(
-          static_cast<const double2 *>(partial), P.nproj, S, P.d_coeff, projraw, projD);
+          static_cast<const double2 *>(partial), P.nproj, NR, S, P.d_coeff, projraw, projD);
     } else {
       auto kern = nl_project_bulk_kernel<R, float, JB>;
       ensure_smem_attr(reinterpret_cast<const void *>(kern), smem);
@@ -407,7 +411,7 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
                                                     static_cast<float2 *>(partial), ctx.d_err);
       LAUNCHED(ctx);
       nl_project_finish_kernel<R, float><<<grid_for(fin, 256), 256, 0, ctx.stream>>>(
-          static_cast<const float2 *>(partial), P.nproj, S, P.d_coeff32, projraw, projD);
+          static_cast<const float2 *>(partial), P.nproj, NR, S, P.d_coeff32, projraw, projD);
     }
     LAUNCHED(ctx);
     dev_free(ctx, partial);
@@ -415,22 +419,22 @@ void launch_nl_project(Ctx &ctx, const Basis &b, const Hamiltonian &h, const C2<
   }
   if (dbl) {
     constexpr int K = 2;
-    dim3 grid(P.nproj, NLP_RANGES, (S + 32 * K - 1) / (32 * K));
+    dim3 grid(P.nproj, NR, (S + 32 * K - 1) / (32 * K));
     nl_project_kernel<R, double, K><<<grid, NLP_WARPS * 32, 0, ctx.stream>>>(
         psi, S, P.d_pt, P.d_gcoef, P.d_npts, P.maxsph, static_cast<double2 *>(partial));
     LAUNCHED(ctx);
     nl_project_finish_kernel<R, double><<<grid_for(fin, 256), 256, 0, ctx.stream>>>(
-        static_cast<const double2 *>(partial), P.nproj, S, P.d_coeff, projraw, projD);
+        static_cast<const double2 *>(partial), P.nproj, NR, S, P.d_coeff, projraw, projD);
   } else {
     // two states per lane (64-state chunks) in single precision too: more CTAs with fewer registers
     // hide the gather latency better (measured 168 us against 202 us with four at 96^3 x 256)
     constexpr int K = 2;
-    dim3 grid(P.nproj, NLP_RANGES, (S + 32 * K - 1) / (32 * K));
+    dim3 grid(P.nproj, NR, (S + 32 * K - 1) / (32 * K));
     nl_project_kernel<R, float, K><<<grid, NLP_WARPS * 32, 0, ctx.stream>>>(
         psi, S, P.d_pt, P.d_gcoef32, P.d_npts, P.maxsph, static_cast<float2 *>(partial));
     LAUNCHED(ctx);
     nl_project_finish_kernel<R, float><<<grid_for(fin, 256), 256, 0, ctx.stream>>>(
-        static_cast<const float2 *>(partial), P.nproj, S, P.d_coeff32, projraw, projD);
+        static_cast<const float2 *>(partial), P.nproj, NR, S, P.d_coeff32, projraw, projD);
   }
   LAUNCHED(ctx);
   dev_free(ctx, partial);
