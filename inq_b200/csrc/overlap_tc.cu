@@ -60,10 +60,10 @@ constexpr uint64_t WAIT_NS = 2000000000ull;
 constexpr uint32_t COL_MAIN_RE = 0, COL_MAIN_IM = 128, COL_CORR_RE = 256, COL_CORR_IM = 384;
 
 __device__ __forceinline__ void split2(float x0, float x1, uint32_t &hi, uint32_t &lo) {
-  const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-  const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-  const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-  const __nv_bfloat162 h = __halves2bfloat162(h0, h1), l = __halves2bfloat162(l0, l1);
+  // packed conversions (two values per instruction), each value rounded to nearest as on its own
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
   hi = *reinterpret_cast<const uint32_t *>(&h);
   lo = *reinterpret_cast<const uint32_t *>(&l);
 }
