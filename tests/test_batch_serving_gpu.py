@@ -109,6 +109,14 @@ def test_hamiltonian_option_overrides(systems):
         ham.set_option("grid_sms", -1)
     with pytest.raises(ib.InqbError):
         ham.set_option("grid_sms", 100000)
+    # another number of projection ranges per sphere sums the projections in another order
+    ham.set_option("nl_project_ranges", 24)
+    try:
+        got = ham(phi).matrix()
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 2e-6
+    finally:
+        ham.set_option("nl_project_ranges", -1)
+    assert np.array_equal(ham(phi).matrix(), ref)
     n0 = ctx.launch_count()
     ham(phi)
     assert ctx.launch_count() - n0 == launches_default
