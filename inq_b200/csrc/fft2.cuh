@@ -963,13 +963,15 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
     int wsplit = W;
     if constexpr (VAR == MID_KIN || VAR == FWD_LAPLADD) {
       if (gg.flat) {
-        const long long col0 = (t % gg.nsb) * W, l0 = col0 / a.S, nlines = gg.ncols / a.S;
-        wsplit = (l0 + 1) * a.S - col0 < W ? int((l0 + 1) * a.S - col0) : W;
+        // 32-bit divisions: a view row has fewer than 2^31 words (the host checks it)
+        const int col0 = int(t % gg.nsb) * W, l0 = col0 / a.S, nlines = g.n[1] * g.n[2];
+        wsplit = (l0 + 1) * a.S - col0 < W ? (l0 + 1) * a.S - col0 : W;
         const int nl = (wsplit < W && l0 + 1 < nlines) ? 2 : 1;
         for (int e = threadIdx.x; e < nl * N; e += NT) {
-          const long long l = l0 + e / N;  // x-line (y, z) = (l / nz, l % nz)
+          const int l = l0 + e / N;  // x-line (y, z) = (l / nz, l % nz)
+          const int ly = l / g.n[2];
           int ix, iy, iz;
-          line_coords(gg.axis, int(l / g.n[2]), int(l % g.n[2]), e % N, ix, iy, iz);
+          line_coords(gg.axis, ly, l - ly * g.n[2], e % N, ix, iy, iz);
           if (a.perm_n2[1]) iy = iy / a.perm_n2[1] + (g.n[1] / a.perm_n2[1]) * (iy % a.perm_n2[1]);
           if (a.perm_n2[2]) iz = iz / a.perm_n2[2] + (g.n[2] / a.perm_n2[2]) * (iz % a.perm_n2[2]);
           linev[e] = CR(lapl_value(g, ix, iy, iz, a.lap_factor, a.gc));
