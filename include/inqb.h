@@ -79,8 +79,8 @@ int inqb_ctx_launch_count(inqb_ctx *ctx, long long *count);
  * last tile than 32-state tiles) or 0 (256-byte rows, 32 states, as the other passes);
  * "fft_flat" = 1 (default: the y and x passes tile the flattened [nx][ny][nz*S] and [nx][ny*nz*S] views
  * of a set, so every row holds a full tile width of (point, state) columns whatever the state count,
- * odd counts included, when nz*S elements are a multiple of 16 bytes) or 0 (tiles of one grid line
- * times a block of states, as the z passes);
+ * odd counts included, when nz*S elements are a multiple of 16 bytes and the state rows are not already
+ * whole 512-byte rows) or 0 (tiles of one grid line times a block of states, as the z passes);
  * "fp64_mma" = 1 (default: the FP64 products of overlaps of double-precision sets and of every rotation
  * run on the FP64 tensor cores, mma.sync m8n8k4) or 0 (FP64 SIMT fused multiply-adds);
  * "nl_apply_points" = 0 (default: 8) or 1..32 hit points per batch of the bulk-copy nonlocal apply;

@@ -1327,10 +1327,14 @@ template <typename R> bool launch(Ctx &ctx, const Basis &b, const PassArgs<R> &a
   if ((var == INV_FINAL && a.dir > 0) || ((var == FWD_VPSI || var == FWD_LAPLADD) && a.dir < 0)) return false;
   // y and x passes without per-line data over flattened columns (context option fft_flat), when the
   // rows of the flattened view are 16-byte multiples
-  // (and the 32-bit words of a view row stay below 2^31, the range of a TMA coordinate)
+  // (and the 32-bit words of a view row stay below 2^31, the range of a TMA coordinate).  When every tile
+  // width divides the state count (a multiple of 512-byte rows) the two decompositions give the same
+  // tiles, and the line tiles' per-tile index arithmetic is the cheaper (96^3 x 256 single: x pass 0.65
+  // against 0.69 ms), so they are kept there.
   const long long view_words = (a.axis == 1 ? (long long)b.n[2] : (long long)b.n[1] * b.n[2]) * a.S * (sizeof(T) / 4);
   const bool flat = ctx.fft_flat && a.axis != 2 && (var == FWD_STORE || var == INV_STORE || var == MID_KIN) &&
-                    (size_t(b.n[2]) * a.S * sizeof(T)) % 16 == 0 && view_words < (1LL << 31);
+                    (size_t(b.n[2]) * a.S * sizeof(T)) % 16 == 0 && view_words < (1LL << 31) &&
+                    (size_t(a.S) * sizeof(T)) % 512 != 0;
   // rows that are not 16-byte multiples (an odd number of single-precision states): only the kernels with
   // a producer warp (single-precision arithmetic) move them, with 8-byte copies; otherwise the generic kernel
   if (!flat && (size_t(a.S) * sizeof(T)) % 16 != 0 && !(sizeof(R) == 4 && single_arith(ctx, a, var))) return false;
