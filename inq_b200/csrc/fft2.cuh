@@ -953,9 +953,21 @@ __global__ void __launch_bounds__(block_threads_of<R, CR, N, VAR, WIDE>(), min_c
     const T *aux = aux_ring + (aux1 ? 0 : size_t(st) * naux * TILE);
     const T *base = aux + TILE;
     bool aux_ready = !aux1;  // this thread has waited for the tile's second input (phase i of abar)
-    const long long L = t / gg.nsb;
-    const int s0 = int(t % gg.nsb) * W;
-    const int la = int(L / g.nb), lb = int(L % g.nb);
+    long long L;
+    int s0, la, lb;
+    if constexpr (VAR == MID_KIN) {
+      // the issue-bound kinetic pass: 32-bit divisions (the host keeps the tile count below 2^31)
+      const int ti = int(t), Li = ti / gg.nsb;
+      L = Li;
+      s0 = (ti - Li * gg.nsb) * W;
+      la = Li / g.nb;
+      lb = Li - la * g.nb;
+    } else {
+      L = t / gg.nsb;
+      s0 = int(t % gg.nsb) * W;
+      la = int(L / g.nb);
+      lb = int(L % g.nb);
+    }
     const long long pbase = la * g.sa + lb * g.sb;
 
     // per-point factors of this line (consumed after the first barrier of the transform); flattened
@@ -1202,6 +1214,7 @@ void launch_kernel(Ctx &ctx, const Basis &b, const PassArgs<R> &a, Geom2 gg) {
   }
   const size_t smem = per_stage * ns + fixed_aux + fixed;
   INQB_REQUIRE(smem <= ctx.max_smem_optin, INQB_ERR_UNSUPPORTED, "FFT tile does not fit in shared memory");
+  INQB_REQUIRE(gg.ntiles < (1LL << 31), INQB_ERR_UNSUPPORTED, "FFT pass has more than 2^31 tiles");
   auto kern = fft2_kernel<R, CR, N, VAR, WIDE>;
   // per instantiation: shared-memory attribute and occupancy, computed under a lock (several host
   // threads may drive contexts at once); the attribute only ever grows
